@@ -1,0 +1,99 @@
+"""ctypes bindings of libb2c.so (the C ABI declared in include/b2c.h).
+
+The library is the product's only compute path: there is no CPU fallback.  Loading fails
+loudly if the library is missing and cannot be built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+c_int32 = ctypes.c_int32
+c_float = ctypes.c_float
+c_void_p = ctypes.c_void_p
+
+
+class Bodies(ctypes.Structure):
+    _fields_ = [("n", c_int32), ("xc", c_void_p), ("q", c_void_p), ("v", c_void_p), ("w", c_void_p),
+                ("pv", c_void_p), ("po", c_void_p), ("invM", c_void_p), ("IbInv", c_void_p), ("kin", c_void_p),
+                ("invIw", c_void_p)]
+
+
+class Beads(ctypes.Structure):
+    _fields_ = [("n", c_int32), ("rest", c_void_p), ("owner", c_void_p), ("world", c_void_p)]
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("dim_x", c_int32), ("dim_y", c_int32), ("dim_z", c_int32), ("cell", c_float),
+                ("bucket", c_void_p), ("start", c_void_p), ("cursor", c_void_p), ("sorted", c_void_p),
+                ("scan_tmp", c_void_p)]
+
+
+class Contacts(ctypes.Structure):
+    _fields_ = [("capacity", c_int32), ("bi", c_void_p), ("bj", c_void_p), ("pA", c_void_p), ("pB", c_void_p),
+                ("n", c_void_p), ("fa", c_void_p), ("fb", c_void_p), ("imp", c_void_p)]
+
+
+class JacobiParams(ctypes.Structure):
+    _fields_ = [("vit", c_int32), ("pit", c_int32), ("relax", c_float), ("mu", c_float)]
+
+
+HEADER_FIELDS = ("n_raw", "n_contacts", "n_kept", "n_pairs", "n_colors", "cache_hit", "error", "rounds")
+ERR_BITS = {1: "contact capacity overflow", 2: "a body pair carries more than 1024 contacts",
+            4: "a body pair carries more than 8 kept contacts", 8: "colour count exceeds the colour cap",
+            16: "colouring did not finish in its round budget", 32: "a bead has more than 64 neighbours within 2R",
+            64: "pair capacity overflow"}
+
+_P = ctypes.POINTER
+_SIGS = {
+    "b2c_version": ([], c_int32),
+    "b2c_last_error": ([], ctypes.c_char_p),
+    "b2c_scan_scratch_ints": ([c_int32], c_int32),
+    "b2c_exclusive_scan": ([c_void_p, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
+    "b2c_body_predict": ([_P(Bodies), c_float, c_void_p], c_int32),
+    "b2c_body_integrate": ([_P(Bodies), c_float, c_void_p], c_int32),
+    "b2c_bead_world": ([_P(Bodies), _P(Beads), _P(Grid), c_void_p], c_int32),
+    "b2c_grid_build": ([_P(Beads), _P(Grid), c_void_p], c_int32),
+    "b2c_bead_contacts": ([_P(Beads), _P(Grid), _P(Contacts), c_void_p, c_void_p], c_int32),
+    "b2c_jacobi_solve": ([_P(Bodies), _P(Contacts), c_void_p, c_void_p, _P(JacobiParams), c_float, c_void_p],
+                         c_int32),
+    "b2c_jacobi_substep": ([_P(Bodies), _P(Beads), _P(Grid), _P(Contacts), c_void_p, c_void_p, _P(JacobiParams),
+                            c_float, c_void_p, c_void_p], c_int32),
+}
+
+_LIB = None
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def load(build_if_missing: bool = True):
+    """Load libb2c.so (building it first when it is missing or older than its sources)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if build_if_missing:
+        try:
+            path = _build.build()
+        except RuntimeError:
+            if not os.path.exists(path):
+                raise
+    if not os.path.exists(path):
+        raise RuntimeError(f"b2c: CUDA library {path} is missing; build it with build.py (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    for name, (args, res) in _SIGS.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().b2c_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what} failed with status {rc}: {msg}")

@@ -1,0 +1,116 @@
+// Exclusive prefix sum over int32, three-phase (tile scan, scan of tile totals, add back),
+// recursive over the tile totals.  Used for bucket offsets of the hash grid, the emission
+// offsets of contact generation and the compaction of kept contacts.  The element count can
+// be read from the device (`dn`), so a scan inside a captured step needs no host read-back:
+// elements at or beyond *dn read as zero.
+#include "b2c_common.cuh"
+
+namespace b2c {
+
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int warp_incl_scan(int v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// block-wide exclusive scan of one int per thread; returns the exclusive prefix, *total the sum
+__device__ __forceinline__ int block_excl_scan(int v, int *total)
+{
+    __shared__ int warp_sums[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = warp_incl_scan(v);
+    if (lane == 31) warp_sums[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < kScanThreads / 32 ? warp_sums[lane] : 0;
+        int si = warp_incl_scan(s);
+        if (lane < kScanThreads / 32) warp_sums[lane] = si - s;
+    }
+    __syncthreads();
+    int excl = warp_sums[wid] + inc - v;
+    __shared__ int tot;
+    if (threadIdx.x == kScanThreads - 1) tot = excl + v;
+    __syncthreads();
+    *total = tot;
+    return excl;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int *__restrict__ in, int *__restrict__ out, int n,
+                                                              const int *__restrict__ dn, int *__restrict__ tile_sums)
+{
+    const int ne = dn ? min(*dn, n) : n;
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        long long i = base + k;
+        v[k] = (i < ne) ? in[i] : 0;
+        s += v[k];
+    }
+    int total;
+    int ex = block_excl_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        long long i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+    if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(int *__restrict__ out, int n, const int *__restrict__ tile_off)
+{
+    const long long i = (long long)blockIdx.x * kScanTile + threadIdx.x;
+    const int add = tile_off[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        long long j = i + (long long)k * kScanThreads;
+        if (j < n) out[j] += add;
+    }
+}
+
+int scan_scratch_ints(int n)
+{
+    if (n <= kScanTile) return 0;
+    int nt = (n + kScanTile - 1) / kScanTile;
+    return 2 * nt + scan_scratch_ints(nt);
+}
+
+int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, cudaStream_t s)
+{
+    if (n <= 0) return B2C_OK;
+    int nt = (n + kScanTile - 1) / kScanTile;
+    if (nt == 1) {
+        k_scan_tiles<<<1, kScanThreads, 0, s>>>(in, out, n, dn, nullptr);
+        return check_launch("scan");
+    }
+    int *sums = scratch, *offs = scratch + nt;
+    k_scan_tiles<<<nt, kScanThreads, 0, s>>>(in, out, n, dn, sums);
+    int rc = exclusive_scan(sums, offs, nt, nullptr, scratch + 2 * nt, s);
+    if (rc) return rc;
+    k_scan_add<<<nt, kScanThreads, 0, s>>>(out, n, offs);
+    return check_launch("scan_add");
+}
+
+}  // namespace b2c
+
+extern "C" int32_t b2c_scan_scratch_ints(int32_t n) { return b2c::scan_scratch_ints(n); }
+
+extern "C" int32_t b2c_exclusive_scan(const int32_t *in, int32_t *out, int32_t n, int32_t *scratch, b2c_stream s)
+{
+    if (!in || !out || n < 0 || (n > b2c::kScanTile && !scratch)) {
+        b2c::set_error("b2c_exclusive_scan: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::exclusive_scan(in, out, n, nullptr, scratch, b2c::stream_of(s));
+}

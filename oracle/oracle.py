@@ -1,0 +1,196 @@
+"""CPU oracle for the contact-solve hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may
+import this module.  It is the checker the CUDA product is compared against, never part of
+the product: the product package does not import it and fails loudly without its CUDA
+library.
+
+Python half of the oracle: the host-side body setup of the reference (numpy, float64 then
+cast to float32 exactly where the reference's ``wp.array(...)`` casts) and ctypes bindings to
+``liboracle.so`` (``oracle_contact.c``), which restates the reference's float32 kernels.
+
+Reference anchors:
+  * ``_voxbox``                        src/motion_engine/contact_engine_gpu.py:186-188
+  * ``RelaxedJacobiContactEngine._build`` src/motion_engine/contact_engine_gpu.py:209-239
+  * ``RelaxedJacobiContactEngine.step``  src/motion_engine/contact_engine_gpu.py:252-280
+  * ``_quat2R`` / ``get_state``          src/motion_engine/contact_engine_gpu.py:283-293
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+R = 0.05
+MAXC = 400000
+
+# variant indices of oracle_contact.c (g_fv[])
+FV_NAMES = ["DOT", "CROSS", "MATVEC", "MATMUL", "QROT", "QMUL", "QNORM", "VNORM", "SITE_GRAV", "SITE_VT",
+            "SITE_T1", "SITE_MAG", "SITE_JT", "SITE_APPLY", "SITE_INTX", "SITE_INTQ", "SITE_IMP"]
+FV = {n: i for i, n in enumerate(FV_NAMES)}
+
+# The contraction pattern that reproduces the reference's golden arrays bit for bit.
+PINNED_VARIANTS = {n: (1 if n.startswith("SITE_") else 0) for n in FV_NAMES}
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so beside this file (gcc, contraction off)."""
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "oracle_contact.c")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = build()
+        L = ctypes.CDLL(so)
+        P = ctypes.c_void_p
+        L.or_set_variant.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.or_get_variant.argtypes = [ctypes.c_int]
+        L.or_get_variant.restype = ctypes.c_int
+        L.or_jacobi_step.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P, P, P,
+                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_int, P, P]
+        L.or_jacobi_step.restype = ctypes.c_int
+        _LIB = L
+        set_variants(PINNED_VARIANTS)
+    return _LIB
+
+
+def set_variants(d: dict) -> None:
+    L = lib()
+    for k, v in d.items():
+        L.or_set_variant(FV[k], int(v))
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def voxbox(w, h, d, res=R * 2):
+    """Bead rest offsets of a box (contact_engine_gpu.py:186-188): per axis
+    arange(-L/2 + res/2, L/2, res), x fastest, then y, then z; float64."""
+    a = lambda L: np.arange(-L / 2 + res / 2, L / 2, res)
+    return np.array([[x, y, z] for z in a(d) for y in a(h) for x in a(w)], float)
+
+
+@dataclass
+class BodySetup:
+    """Device-ready body arrays, exactly as RelaxedJacobiContactEngine._build lays them out."""
+    rest: np.ndarray     # (P, 3) f32 per-bead rest offsets (uniform over bodies)
+    xc: np.ndarray       # (N, 3) f32
+    q: np.ndarray        # (N, 4) f32, (x, y, z, w)
+    v: np.ndarray
+    w: np.ndarray
+    invM: np.ndarray     # (N,) f32
+    IbInv: np.ndarray    # (N, 3, 3) f32
+    kin: np.ndarray      # (N,) int32
+    M: np.ndarray        # (N,) f64 (inf for bodies made kinematic after the build)
+
+
+def build_bodies(centers, dens, kin, dims) -> BodySetup:
+    """contact_engine_gpu.py:209-239 (also contact_engine_gpu_colored.py:836-850):
+    mass = density*vol, bead point-mass inertia Ib = sum mp (r.r I - r r^T), IbInv by
+    np.linalg.inv per body (identity for kinematic), identity quaternion."""
+    rest64 = voxbox(*dims)
+    P = len(rest64)
+    N = len(centers)
+    w_, h_, d_ = dims
+    vol = w_ * h_ * d_
+    mp = np.array(dens, float) * vol / P
+    M = mp * P
+    kinarr = np.array(kin, int)
+    invM = np.where(kinarr == 1, 0.0, 1.0 / M)
+    Ib = sum(mp[0] * ((r @ r) * np.eye(3) - np.outer(r, r)) for r in rest64)
+    IbInv = np.array([np.linalg.inv((mp[i] / mp[0]) * Ib) if kinarr[i] == 0 else np.eye(3) for i in range(N)])
+    if not np.all(np.isfinite(IbInv)):
+        raise ValueError("IbInv contains non-finite entries: degenerate body mass/inertia")
+    return BodySetup(rest=rest64.astype(np.float32),
+                     xc=np.array(np.array(centers, float), np.float32).reshape(N, 3),
+                     q=np.tile(np.array([0, 0, 0, 1.0], np.float32), (N, 1)),
+                     v=np.zeros((N, 3), np.float32), w=np.zeros((N, 3), np.float32),
+                     invM=invM.astype(np.float32), IbInv=IbInv.astype(np.float32).reshape(N, 3, 3),
+                     kin=kinarr.astype(np.int32), M=M.astype(np.float64))
+
+
+def quat_to_R(q: np.ndarray) -> np.ndarray:
+    """Host quaternion -> matrix of get_state (contact_engine_gpu.py:283-287), float32
+    arithmetic on float32 inputs as numpy does it there."""
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    one = np.float32(1); two = np.float32(2)
+    Rm = np.empty((len(q), 3, 3), np.float32)
+    Rm[:, 0, 0] = one - two * (y * y + z * z); Rm[:, 0, 1] = two * (x * y - z * w); Rm[:, 0, 2] = two * (x * z + y * w)
+    Rm[:, 1, 0] = two * (x * y + z * w); Rm[:, 1, 1] = one - two * (x * x + z * z); Rm[:, 1, 2] = two * (y * z - x * w)
+    Rm[:, 2, 0] = two * (x * z - y * w); Rm[:, 2, 1] = two * (y * z + x * w); Rm[:, 2, 2] = one - two * (x * x + y * y)
+    return Rm
+
+
+@dataclass
+class State:
+    xc: np.ndarray
+    Rm: np.ndarray
+    vc: np.ndarray
+    om: np.ndarray
+
+
+class JacobiOracle:
+    """CPU restatement of RelaxedJacobiContactEngine (contact_engine_gpu.py:191-299)."""
+    name = "relaxed_jacobi_oracle"
+
+    def __init__(self, dims=(0.3, 0.3, 0.2), relax=0.2, vit=40, pit=20, mu=0.5):
+        self.dims = dims; self.relax = relax; self.vit = vit; self.pit = pit; self.mu = mu
+        self._centers = []; self._dens = []; self._kin = []
+        self.b = None
+        self.n_contacts = 0
+
+    def add_body(self, center, density=700.0, kin=False):
+        self._centers.append(list(center)); self._dens.append(float(density)); self._kin.append(1 if kin else 0)
+        self.b = None
+        return len(self._centers) - 1
+
+    def _build(self):
+        self.b = build_bodies(self._centers, self._dens, self._kin, self.dims)
+        N = len(self._centers); P = len(self.b.rest)
+        self.N = N; self.P = P
+        self.rest_all = np.ascontiguousarray(np.tile(self.b.rest, (N, 1)))
+        self.owner = np.repeat(np.arange(N, dtype=np.int32), P)
+        self.force = np.zeros((N, 3))
+        self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
+
+    def set_kinematic(self, i, xc):
+        self._kin[i] = 1; self._centers[i] = list(xc)
+        if self.b is not None:
+            self.b.xc[i] = np.array(xc, np.float32); self.b.invM[i] = 0.0
+            self.b.v[i] = 0.0; self.b.w[i] = 0.0; self.b.kin[i] = 1; self.b.M[i] = np.inf
+
+    def step(self, dt, substeps=1):
+        if self.b is None:
+            self._build()
+        b = self.b
+        force = np.zeros((self.N, 3))
+        nc = np.zeros(substeps, np.int32)
+        rc = lib().or_jacobi_step(self.N, self.N * self.P, _p(self.rest_all), _p(self.owner), _p(b.xc), _p(b.q),
+                                  _p(b.v), _p(b.w), _p(self.pv), _p(self.po), _p(b.invM), _p(b.IbInv), _p(b.kin), _p(b.M), float(dt),
+                                  int(substeps), int(self.vit), int(self.pit), float(self.relax), float(self.mu),
+                                  MAXC, _p(force), _p(nc))
+        if rc != 0:
+            raise RuntimeError(f"oracle jacobi step failed with status {rc}")
+        self.force = force
+        self.n_contacts = int(nc[-1])
+
+    def get_state(self) -> State:
+        if self.b is None:
+            self._build()
+        return State(xc=self.b.xc.copy(), Rm=quat_to_R(self.b.q), vc=self.b.v.copy(), om=self.b.w.copy())
+
+    def contact_forces(self):
+        return self.force.copy()
