@@ -22,7 +22,41 @@ class Bodies(ctypes.Structure):
 
 
 class Beads(ctypes.Structure):
-    _fields_ = [("n", c_int32), ("rest", c_void_p), ("owner", c_void_p), ("world", c_void_p)]
+    _fields_ = [("n", c_int32), ("rest", c_void_p), ("owner", c_void_p), ("world", c_void_p),
+                ("bead_start", c_void_p)]
+
+
+class Manifold(ctypes.Structure):
+    _fields_ = [("capacity", c_int32), ("pair_capacity", c_int32), ("bead_count", c_void_p),
+                ("bead_offset", c_void_p), ("pair_local", c_void_p), ("pair_first", c_void_p), ("gorder", c_void_p),
+                ("body_npairs", c_void_p), ("pair_base", c_void_p), ("praw_start", c_void_p),
+                ("praw_count", c_void_p), ("jn_in", c_void_p), ("jn_red", c_void_p), ("jt_in", c_void_p),
+                ("keep", c_void_p), ("kidx", c_void_p), ("scan_tmp", c_void_p)]
+
+
+class Pairs(ctypes.Structure):
+    _fields_ = [("capacity", c_int32), ("max_colors", c_int32), ("pbi", c_void_p), ("pbj", c_void_p),
+                ("kcount", c_void_p), ("pstart", c_void_p), ("pidx", c_void_p), ("col", c_void_p),
+                ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
+                ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
+                ("cache_state", c_void_p), ("barrier", c_void_p)]
+
+
+class Warm(ctypes.Structure):
+    _fields_ = [("capacity", c_int32), ("keys", c_void_p), ("imp", c_void_p), ("n", c_void_p)]
+
+
+class ColorParams(ctypes.Structure):
+    _fields_ = [("vit", c_int32), ("pit", c_int32), ("max_points", c_int32), ("flags", c_int32), ("mu", c_float),
+                ("t2d", c_float), ("color_cap", c_int32), ("solve_blocks", c_int32),
+                ("barrier_timeout_ns", ctypes.c_int64)]
+
+
+COLOR_FIXED_FRAME = 1
+COLOR_APPLY_WARM = 2
+COLOR_CACHE = 4
+COLOR_WARM_START = 8
+COLOR_PER_CONTACT = 16
 
 
 class Grid(ctypes.Structure):
@@ -44,7 +78,7 @@ HEADER_FIELDS = ("n_raw", "n_contacts", "n_kept", "n_pairs", "n_colors", "cache_
 ERR_BITS = {1: "contact capacity overflow", 2: "a body pair carries more than 1024 contacts",
             4: "a body pair carries more than 8 kept contacts", 8: "colour count exceeds the colour cap",
             16: "colouring did not finish in its round budget", 32: "a bead has more than 64 neighbours within 2R",
-            64: "pair capacity overflow"}
+            64: "pair capacity overflow", 128: "a grid barrier of the persistent solve gave up waiting"}
 
 _P = ctypes.POINTER
 _SIGS = {
@@ -61,6 +95,15 @@ _SIGS = {
                          c_int32),
     "b2c_jacobi_substep": ([_P(Bodies), _P(Beads), _P(Grid), _P(Contacts), c_void_p, c_void_p, _P(JacobiParams),
                             c_float, c_void_p, c_void_p], c_int32),
+    "b2c_bead_contacts_sorted": ([_P(Beads), _P(Grid), _P(Contacts), _P(Manifold), c_void_p, c_void_p], c_int32),
+    "b2c_manifold_reduce": ([_P(Bodies), _P(Beads), _P(Contacts), _P(Manifold), _P(Contacts), c_void_p, _P(Pairs),
+                             _P(Warm), c_void_p, _P(ColorParams), c_void_p], c_int32),
+    "b2c_color_pairs": ([_P(Bodies), _P(Pairs), c_void_p, _P(ColorParams), c_void_p], c_int32),
+    "b2c_color_solve": ([_P(Bodies), _P(Contacts), _P(Pairs), c_void_p, _P(ColorParams), c_float, c_void_p],
+                        c_int32),
+    "b2c_warm_store": ([_P(Contacts), c_void_p, _P(Warm), c_void_p, c_void_p], c_int32),
+    "b2c_color_substep": ([_P(Bodies), _P(Beads), _P(Grid), _P(Contacts), _P(Manifold), _P(Contacts), c_void_p,
+                           _P(Pairs), _P(Warm), c_void_p, _P(ColorParams), c_float, c_void_p, c_void_p], c_int32),
 }
 
 _LIB = None

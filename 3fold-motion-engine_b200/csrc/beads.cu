@@ -1,25 +1,9 @@
 // Bead clouds: world positions, uniform hash grid, contact generation.
-#include "b2c_common.cuh"
+#include "b2c_grid.cuh"
 
 namespace b2c {
 
 int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, cudaStream_t s);
-
-struct GridView {
-    int dx, dy, dz;
-    float inv;  // 1 / cell
-};
-
-__device__ __forceinline__ int wrapi(int a, int m)
-{
-    int r = a % m;
-    return r < 0 ? r + m : r;
-}
-__device__ __forceinline__ int cellc(float x, float inv) { return (int)floorf(x * inv); }
-__device__ __forceinline__ int bucket_of(const GridView &g, int ix, int iy, int iz)
-{
-    return (wrapi(ix, g.dx) * g.dy + wrapi(iy, g.dy)) * g.dz + wrapi(iz, g.dz);
-}
 
 // k_worldp, contact_engine_gpu.py:55-59: allp = xc[b] + quat_rotate(q[b], rest)
 __global__ void k_bead_world(int nb, const float *__restrict__ xc, const float *__restrict__ q,
@@ -49,21 +33,6 @@ __global__ void k_grid_scatter(int nb, const int *__restrict__ bucket, const int
     sorted[start[b] + atomicAdd(cursor + b, 1)] = i;
 }
 
-// Query block of a point: every cell within 2R (plus a 1 % margin, so a neighbour at a cell
-// boundary is never missed by rounding; the exact distance test below decides).
-struct QueryRange {
-    int lo[3], hi[3];
-};
-__device__ __forceinline__ QueryRange query_range(f3 p, float r, float inv)
-{
-    const float m = r * 1.01f;
-    QueryRange q;
-    q.lo[0] = cellc(p.x - m, inv); q.hi[0] = cellc(p.x + m, inv);
-    q.lo[1] = cellc(p.y - m, inv); q.hi[1] = cellc(p.y + m, inv);
-    q.lo[2] = cellc(p.z - m, inv); q.hi[2] = cellc(p.z + m, inv);
-    return q;
-}
-
 __device__ __forceinline__ void append_contact(b2c_contacts c, int *n_raw, int bi, int bj, f3 pA, f3 pB, f3 nrm,
                                                float pen, int fa, int fb)
 {
@@ -91,24 +60,9 @@ __global__ void k_bead_contacts(int nb, const float *__restrict__ world, const i
     const int bi = owner[i];
     const float s = xi.z - B2C_R;
     if (s < 0.0f) append_contact(c, &hdr->n_raw, bi, -1, xi, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 1.0f}, -s, i, -1);
-    const QueryRange qr = query_range(xi, B2C_2R, g.inv);
-    for (int iz = qr.lo[2]; iz <= qr.hi[2]; ++iz)
-        for (int iy = qr.lo[1]; iy <= qr.hi[1]; ++iy)
-            for (int ix = qr.lo[0]; ix <= qr.hi[0]; ++ix) {
-                const int b = bucket_of(g, ix, iy, iz);
-                const int e = start[b + 1];
-                for (int t = start[b]; t < e; ++t) {
-                    const int j = sorted[t];
-                    if (j > i && owner[j] != bi) {
-                        const f3 xj = ld3(world, j);
-                        const f3 dvec = sub3(xi, xj);
-                        const float dist = len3(dvec);
-                        if (dist < B2C_2R && dist > 1e-9f)
-                            append_contact(c, &hdr->n_raw, bi, owner[j], xi, xj, div3(dvec, dist), B2C_2R - dist, i,
-                                           j);
-                    }
-                }
-            }
+    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int j, f3 xj, f3 dvec, float dist) {
+        append_contact(c, &hdr->n_raw, bi, owner[j], xi, xj, div3(dvec, dist), B2C_2R - dist, i, j);
+    });
 }
 
 __global__ void k_header_reset_contacts(b2c_header *hdr)
@@ -124,7 +78,6 @@ __global__ void k_header_finish_contacts(b2c_header *hdr, int cap)
     if (raw > cap) hdr->error |= B2C_ERR_CONTACT_OVERFLOW;
 }
 
-inline GridView view_of(const b2c_grid *g) { return GridView{g->dim_x, g->dim_y, g->dim_z, 1.0f / g->cell}; }
 
 int bead_world(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, cudaStream_t s)
 {

@@ -1,0 +1,1138 @@
+// Coloured Gauss-Seidel pair-chunk chain: GraphColoredContactEngine(manifold_reduce,
+// pair_chunks) and its ColorCache descendant (contact_engine_gpu_colored.py,
+// contact_engine_gpu_fixed_frame.py, _applied_warm.py, _deferred_force.py, _color_cache.py).
+//
+// B200 layout of a substep, with no host read-back anywhere:
+//   1. contacts in feature-key order by construction: per-bead counts, a scan, then every bead
+//      writes its ground contact and its neighbours sorted by bead id at its offset (replaces
+//      the atomic append + feature-key radix sort + gather of the reference);
+//   2. pair grouping: beads are body-major, so the contacts owned by a body A are contiguous and
+//      one warp per body groups them by partner (replaces the pair-key radix sort);
+//   3. warm start (binary search), float64 E-optimal selection per pair, compaction, kept pairs;
+//   4. Jones-Plassmann colouring of the pair graph in one CTA behind the device-side colour cache;
+//   5. the whole chunk solve (applied warm start, vit velocity and pit position sweeps over the
+//      colours) in ONE persistent kernel with a bounded grid barrier between colours;
+//   6. warm store.
+// Every float32 expression follows the reference kernels with the contraction pattern of
+// b2c_math.cuh; the selection is float64 without contraction, as the reference compiled it.
+#include "b2c_grid.cuh"
+
+namespace b2c {
+
+int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, cudaStream_t s);
+int body_predict(const b2c_bodies *b, float dt, cudaStream_t s);
+int body_integrate(const b2c_bodies *b, float dt, cudaStream_t s);
+int bead_world(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
+int grid_build(const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
+
+constexpr int kMaxNeighbors = 64;
+
+// ---------------------------------------------------------------------------------------------
+// 1. contact generation in feature order (k_gen_fid COL:102-122 + k_fkey/radix sort/k_gather)
+// ---------------------------------------------------------------------------------------------
+__global__ void k_bead_count(int nb, const float *__restrict__ world, const int *__restrict__ owner,
+                             const int *__restrict__ start, const int *__restrict__ sorted, GridView g,
+                             int *__restrict__ count, b2c_header *hdr)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) count[nb] = 0;
+    if (i >= nb) return;
+    const f3 xi = ld3(world, i);
+    const int bi = owner[i];
+    int nn = 0;
+    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int, f3, f3, float) { ++nn; });
+    if (nn > kMaxNeighbors) {
+        atomicOr(&hdr->error, B2C_ERR_NEIGHBOR_OVERFLOW);
+        nn = kMaxNeighbors;
+    }
+    count[i] = nn + ((xi.z - B2C_R) < 0.0f ? 1 : 0);
+}
+
+__device__ __forceinline__ void put_contact(b2c_contacts &c, int k, int bi, int bj, f3 pA, f3 pB, f3 nrm, float pen,
+                                            int fa, int fb)
+{
+    c.bi[k] = bi;
+    c.bj[k] = bj;
+    st4(c.pA, k, f4(pA, pen));
+    st4(c.pB, k, f4(pB, 0.0f));
+    st4(c.n, k, f4(nrm, 0.0f));
+    c.fa[k] = fa;
+    c.fb[k] = fb;
+}
+
+__global__ void k_bead_emit(int nb, const float *__restrict__ world, const int *__restrict__ owner,
+                            const int *__restrict__ start, const int *__restrict__ sorted, GridView g,
+                            const int *__restrict__ offset, b2c_contacts c, b2c_header *hdr)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        const int total = offset[nb];
+        hdr->n_raw = total;
+        hdr->n_contacts = total < c.capacity ? total : c.capacity;
+        if (total > c.capacity) atomicOr(&hdr->error, B2C_ERR_CONTACT_OVERFLOW);
+    }
+    if (i >= nb) return;
+    int k = offset[i];
+    if (k >= c.capacity) return;
+    const f3 xi = ld3(world, i);
+    const int bi = owner[i];
+    const float s = xi.z - B2C_R;
+    if (s < 0.0f) {
+        put_contact(c, k, bi, -1, xi, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 1.0f}, -s, i, -1);
+        if (++k >= c.capacity) return;
+    }
+    if (offset[i + 1] == k) return;  // no bead neighbours
+    int js[kMaxNeighbors];
+    int n = 0;
+    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int j, f3, f3, float) {
+        if (n < kMaxNeighbors) {  // insertion into ascending order of bead id
+            int t = n++;
+            while (t > 0 && js[t - 1] > j) {
+                js[t] = js[t - 1];
+                --t;
+            }
+            js[t] = j;
+        }
+    });
+    for (int t = 0; t < n && k < c.capacity; ++t, ++k) {
+        const int j = js[t];
+        const f3 xj = ld3(world, j);
+        const f3 dvec = sub3(xi, xj);
+        const float dist = len3(dvec);
+        put_contact(c, k, bi, owner[j], xi, xj, div3(dvec, dist), B2C_2R - dist, i, j);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2. pair grouping: stable pair-key order (COL:628-649) per body, one warp per body A
+// ---------------------------------------------------------------------------------------------
+__global__ void k_body_pairs(int nbodies, const int *__restrict__ bead_start, const int *__restrict__ offset, int cap,
+                             const int *__restrict__ cbj, int *__restrict__ pair_local, int2 *__restrict__ pair_first,
+                             int *__restrict__ gorder, int *__restrict__ body_npairs)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= nbodies) return;
+    const int lo = min(offset[bead_start[w]], cap), hi = min(offset[bead_start[w + 1]], cap);
+    const int L = hi - lo;
+    int firsts = 0;
+    for (int e = lane; e < L; e += 32) {
+        const int v = cbj[lo + e];
+        int less = 0, before = 0, same = 0;
+        for (int f = 0; f < L; ++f) {
+            const int u = cbj[lo + f];
+            less += (u < v);
+            same += (u == v);
+            before += (u == v && f < e);
+        }
+        gorder[lo + less + before] = lo + e;
+        pair_first[lo + e] = before == 0 ? make_int2(lo + less, same) : make_int2(-1, 0);
+        firsts += (before == 0);
+    }
+    __syncwarp();
+    for (int e = lane; e < L; e += 32) {
+        const int v = cbj[lo + e];
+        int dl = 0;
+        for (int f = 0; f < L; ++f) dl += (pair_first[lo + f].x >= 0 && cbj[lo + f] < v);
+        pair_local[lo + e] = dl;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) firsts += __shfl_xor_sync(0xffffffffu, firsts, o);
+    if (lane == 0) body_npairs[w] = firsts;
+    if (w == 0 && lane == 0) body_npairs[nbodies] = 0;
+}
+
+__global__ void k_pairs_write(const b2c_header *__restrict__ hdr_c, int nbodies, const int *__restrict__ cbi,
+                              const int *__restrict__ cbj, const int *__restrict__ pair_local,
+                              const int2 *__restrict__ pair_first, const int *__restrict__ pair_base, int pcap,
+                              int *__restrict__ pbi, int *__restrict__ pbj, int *__restrict__ praw_start,
+                              int *__restrict__ praw_count, b2c_header *hdr)
+{
+    const int C = hdr_c->n_contacts;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        const int P = pair_base[nbodies];
+        hdr->n_pairs = P < pcap ? P : pcap;
+        if (P > pcap) atomicOr(&hdr->error, B2C_ERR_PAIR_OVERFLOW);
+    }
+    for (int e = tid; e < C; e += gridDim.x * blockDim.x) {
+        const int2 pf = pair_first[e];
+        if (pf.x < 0) continue;
+        const int A = cbi[e];
+        const int p = pair_base[A] + pair_local[e];
+        if (p >= pcap) continue;
+        pbi[p] = A;
+        pbj[p] = cbj[e];
+        praw_start[p] = pf.x;
+        praw_count[p] = pf.y;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3. warm start, selection, compaction, kept pairs (COL:601-626, 651-751, 1158-1176)
+// ---------------------------------------------------------------------------------------------
+__global__ void k_warm(const b2c_header *__restrict__ hdr, const int *__restrict__ fa, const int *__restrict__ fb,
+                       long long stride, int use_warm, const long long *__restrict__ wkeys,
+                       const float *__restrict__ wimp, const int *__restrict__ wn_ptr, double *__restrict__ jn_in,
+                       float2 *__restrict__ jt_in)
+{
+    const int C = hdr->n_contacts;
+    const int wn = use_warm ? *wn_ptr : 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
+        double jn = 0.0;
+        float2 jt = make_float2(0.0f, 0.0f);
+        if (wn > 0) {
+            const long long k = (long long)fa[i] * stride + (long long)fb[i] + 1;
+            int lo = 0, hi = wn - 1, hit = -1;
+            while (lo <= hi) {
+                const int mid = (lo + hi) / 2;
+                const long long km = wkeys[mid];
+                if (km == k) {
+                    hit = mid;
+                    lo = hi + 1;
+                } else if (km < k) {
+                    lo = mid + 1;
+                } else {
+                    hi = mid - 1;
+                }
+            }
+            if (hit >= 0) {
+                const float4 w4 = ld4(wimp, hit);
+                jn = (double)w4.x;
+                jt = make_float2(w4.y, w4.z);
+            }
+        }
+        jn_in[i] = jn;
+        jt_in[i] = jt;
+    }
+}
+
+// _planar, COL:585-590: float32 difference promoted to float64
+__device__ __forceinline__ void planar(const float *__restrict__ cpA, int g, f3 ref, const double *u, const double *w,
+                                       double *r)
+{
+    const float4 p = ld4(cpA, g);
+    const float dx = p.x - ref.x, dy = p.y - ref.y, dz = p.z - ref.z;
+    const double ax = dx, ay = dy, az = dz;
+    r[0] = (ax * u[0] + ay * u[1]) + az * u[2];
+    r[1] = (ax * w[0] + ay * w[1]) + az * w[2];
+}
+
+// k_select, COL:651-728: one thread per body pair
+__global__ void k_select(const b2c_header *__restrict__ hdr, int mx, const int *__restrict__ praw_start,
+                         const int *__restrict__ praw_count, const int *__restrict__ gorder,
+                         const int *__restrict__ cbi, const float *__restrict__ cpA, const float *__restrict__ cn,
+                         const float *__restrict__ xc, const double *__restrict__ jn_in, int *__restrict__ keep,
+                         double *__restrict__ jn_out, int *__restrict__ kcount, b2c_header *hdr_w)
+{
+    const int P = hdr->n_pairs;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const int i = praw_start[p], L = praw_count[p];
+        if (L <= mx || L > 1024 || mx > 8) {
+            if (L > mx) atomicOr(&hdr_w->error, B2C_ERR_SEGMENT_OVERFLOW);
+            for (int t = 0; t < L; ++t) {
+                const int g = gorder[i + t];
+                keep[g] = 1;
+                jn_out[g] = jn_in[g];
+            }
+            kcount[p] = L;
+            continue;
+        }
+        int deep = 0;
+        float dbest = cpA[4 * gorder[i] + 3];
+        for (int t = 1; t < L; ++t) {
+            const float pn = cpA[4 * gorder[i + t] + 3];
+            if (pn > dbest) {
+                dbest = pn;
+                deep = t;
+            }
+        }
+        const int gd = gorder[i + deep];
+        const f3 nr = ld3(cn, gd);
+        double ax = 1.0, ay = 0.0, az = 0.0;
+        if (fabsf(nr.x) >= 0.9f) {
+            ax = 0.0;
+            ay = 1.0;
+            az = 0.0;
+        }
+        const double n0 = nr.x, n1 = nr.y, n2 = nr.z;
+        const double dn = (ax * n0 + ay * n1) + az * n2;
+        const double u0 = ax - dn * n0, u1 = ay - dn * n1, u2 = az - dn * n2;
+        const double ln = sqrt((u0 * u0 + u1 * u1) + u2 * u2);
+        const double u[3] = {u0 / ln, u1 / ln, u2 / ln};
+        const double w[3] = {n1 * u[2] - n2 * u[1], n2 * u[0] - n0 * u[2], n0 * u[1] - n1 * u[0]};
+        const f3 ref = ld3(xc, cbi[gd]);
+        double rd[2];
+        planar(cpA, gd, ref, u, w, rd);
+        double S00 = rd[0] * rd[0], S01 = rd[0] * rd[1], S10 = rd[1] * rd[0], S11 = rd[1] * rd[1];
+        int pick[8];
+        pick[0] = deep;
+        for (int k = 1; k < mx; ++k) {
+            double sbest = -1.0e300;
+            int tbest = -1;
+            double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+            for (int t = 0; t < L; ++t) {
+                bool taken = false;
+                for (int q = 0; q < k; ++q) taken |= (pick[q] == t);
+                if (taken) continue;
+                double rt[2];
+                planar(cpA, gorder[i + t], ref, u, w, rt);
+                const double a00 = S00 + rt[0] * rt[0], a01 = S01 + rt[0] * rt[1];
+                const double a10 = S10 + rt[1] * rt[0], a11 = S11 + rt[1] * rt[1];
+                const double tr = a00 + a11;
+                const double det = a00 * a11 - a01 * a10;
+                const double disc = fmax(tr * tr / 4.0 - det, 0.0);
+                const double lam = tr / 2.0 - sqrt(disc);
+                const double sc = fmin((double)(k + 1), lam);
+                if (sc > sbest) {
+                    sbest = sc;
+                    tbest = t;
+                    c00 = a00;
+                    c01 = a01;
+                    c10 = a10;
+                    c11 = a11;
+                }
+            }
+            if (tbest < 0) {  // only with non-finite scores: take the first free point, never index -1
+                for (int t = L - 1; t >= 0; --t) {
+                    bool taken = false;
+                    for (int q = 0; q < k; ++q) taken |= (pick[q] == t);
+                    if (!taken) tbest = t;
+                }
+            }
+            pick[k] = tbest;
+            S00 = c00;
+            S01 = c01;
+            S10 = c10;
+            S11 = c11;
+        }
+        for (int t = 0; t < L; ++t) keep[gorder[i + t]] = 0;
+        for (int k = 0; k < mx; ++k) {
+            const int g = gorder[i + pick[k]];
+            keep[g] = 1;
+            jn_out[g] = 0.0;
+        }
+        for (int t = 0; t < L; ++t) {
+            double rt[2];
+            planar(cpA, gorder[i + t], ref, u, w, rt);
+            double dbest2 = 1.0e300;
+            int kbest = 0;
+            for (int k = 0; k < mx; ++k) {
+                double rk[2];
+                planar(cpA, gorder[i + pick[k]], ref, u, w, rk);
+                const double e0 = rt[0] - rk[0], e1 = rt[1] - rk[1], d2 = e0 * e0 + e1 * e1;
+                if (d2 < dbest2) {
+                    dbest2 = d2;
+                    kbest = k;
+                }
+            }
+            const int gk = gorder[i + pick[kbest]];
+            jn_out[gk] = jn_out[gk] + jn_in[gorder[i + t]];
+        }
+        kcount[p] = mx;
+    }
+}
+
+__global__ void k_set_kept(b2c_header *hdr, const int *__restrict__ kidx) { hdr->n_kept = kidx[hdr->n_contacts]; }
+
+// plain coloured engine (COL:903-936, 1105-1137): every contact kept, one contact per chunk,
+// warm impulses uploaded as float32 (COL:931-936)
+__global__ void k_per_contact(b2c_header *hdr, long long stride, b2c_contacts c, const double *__restrict__ jn_in,
+                              const float2 *__restrict__ jt_in, b2c_contacts kept, long long *__restrict__ kept_keys,
+                              int pcap, int *__restrict__ pbi, int *__restrict__ pbj, int *__restrict__ kcount,
+                              int *__restrict__ pstart, int *__restrict__ pidx)
+{
+    const int C = hdr->n_contacts;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        hdr->n_kept = C;
+        hdr->n_pairs = C < pcap ? C : pcap;
+        if (C > pcap) atomicOr(&hdr->error, B2C_ERR_PAIR_OVERFLOW);
+    }
+    for (int i = tid; i < C && i < pcap; i += gridDim.x * blockDim.x) {
+        kept_keys[i] = (long long)c.fa[i] * stride + (long long)c.fb[i] + 1;
+        kept.bi[i] = c.bi[i];
+        kept.bj[i] = c.bj[i];
+        st4(kept.pA, i, ld4(c.pA, i));
+        st4(kept.pB, i, ld4(c.pB, i));
+        st4(kept.n, i, ld4(c.n, i));
+        kept.fa[i] = c.fa[i];
+        kept.fb[i] = c.fb[i];
+        const float2 jt = jt_in[i];
+        st4(kept.imp, i, make_float4((float)jn_in[i], jt.x, jt.y, 0.0f));
+        pbi[i] = c.bi[i];
+        pbj[i] = c.bj[i];
+        kcount[i] = 1;
+        pstart[i] = i;
+        pidx[i] = i;
+    }
+}
+
+// k_compact, COL:730-751: kept contacts in feature order, jn cast to float32
+__global__ void k_compact(const b2c_header *__restrict__ hdr, long long stride, b2c_contacts c,
+                          const int *__restrict__ keep, const int *__restrict__ kidx, const double *__restrict__ jn_red,
+                          const float2 *__restrict__ jt_in, b2c_contacts kept, long long *__restrict__ kept_keys)
+{
+    const int C = hdr->n_contacts;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
+        if (!keep[i]) continue;
+        const int d = kidx[i];
+        kept_keys[d] = (long long)c.fa[i] * stride + (long long)c.fb[i] + 1;
+        kept.bi[d] = c.bi[i];
+        kept.bj[d] = c.bj[i];
+        st4(kept.pA, d, ld4(c.pA, i));
+        st4(kept.pB, d, ld4(c.pB, i));
+        st4(kept.n, d, ld4(c.n, i));
+        kept.fa[d] = c.fa[i];
+        kept.fb[d] = c.fb[i];
+        const float2 jt = jt_in[i];
+        st4(kept.imp, d, make_float4((float)jn_red[i], jt.x, jt.y, 0.0f));
+    }
+}
+
+// pair-sorted kept list (k_pairkey + radix sort + k_pairbuild, COL:341-389, 1158-1176)
+__global__ void k_pair_kept(const b2c_header *__restrict__ hdr, const int *__restrict__ praw_start,
+                            const int *__restrict__ praw_count, const int *__restrict__ gorder,
+                            const int *__restrict__ keep, const int *__restrict__ kidx, const int *__restrict__ pstart,
+                            int *__restrict__ pidx, int *__restrict__ kcount, b2c_header *hdr_w)
+{
+    const int P = hdr->n_pairs;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const int i = praw_start[p], L = praw_count[p], base = pstart[p];
+        int r = 0;
+        for (int t = 0; t < L; ++t) {
+            const int e = gorder[i + t];
+            if (keep[e]) pidx[base + r++] = kidx[e];
+        }
+        if (r > 8) {  // _MAXCHUNK, COL:384-386
+            atomicOr(&hdr_w->error, B2C_ERR_CHUNK_OVERFLOW);
+            kcount[p] = 8;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 4. colouring behind the colour cache (COL:136-185, 1178-1208; color_cache.py:5-54), one CTA
+// ---------------------------------------------------------------------------------------------
+// Warp's rand_init / randi: the PCG-RXS-M-XS 32-bit output permutation used as a hash
+// (Jarzynski & Olano, "Hash Functions for GPU Rendering", JCGT 2020).
+__device__ __forceinline__ uint32_t pcg_hash(uint32_t state)
+{
+    const uint32_t b = state * 747796405u + 2891336453u;
+    const uint32_t c = ((b >> ((b >> 28u) + 4u)) ^ b) * 277803737u;
+    return (c >> 22u) ^ c;
+}
+// k_prio, COL:136-148: |int32(randi(rand_init(7919, p)))| << 32 | p
+__device__ __forceinline__ long long jp_priority(int p)
+{
+    const uint32_t st = pcg_hash(pcg_hash(7919u + pcg_hash((uint32_t)p)));
+    long long v = (long long)(int32_t)st;
+    if (v < 0) v = -v;
+    return v * 4294967296LL + (long long)p;
+}
+
+constexpr int kColorThreads = 1024;
+constexpr int kMaxColorsCap = 512;
+
+__global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, int nbodies,
+                                                                const float *__restrict__ invM, b2c_pairs pr,
+                                                                int use_cache, int color_cap, int max_rounds)
+{
+    __shared__ int s_flag;
+    __shared__ int s_left;
+    __shared__ int s_cnt[kMaxColorsCap];
+    __shared__ int s_cur[kMaxColorsCap];
+    const int P = hdr->n_pairs;
+    const int tid = threadIdx.x;
+    if (P == 0) {
+        if (tid == 0) {
+            hdr->n_colors = 0;
+            hdr->cache_hit = 0;
+        }
+        return;
+    }
+    // colour cache: reuse while the pair count, pbi, pbj and invM are unchanged
+    if (use_cache) {
+        if (tid == 0) s_flag = (pr.cache_state[2] == 1 && pr.cache_state[0] == P) ? 0 : 1;
+        __syncthreads();
+        if (s_flag == 0) {
+            int mism = 0;
+            for (int p = tid; p < P; p += kColorThreads) mism |= (pr.pbi[p] != pr.cached_a[p]) | (pr.pbj[p] != pr.cached_b[p]);
+            for (int i = tid; i < nbodies; i += kColorThreads) mism |= (invM[i] != pr.cached_mass[i]);
+            if (mism) atomicOr(&s_flag, 1);
+        }
+        __syncthreads();
+        if (s_flag == 0) {
+            if (tid == 0) {
+                hdr->n_colors = pr.cache_state[1];
+                pr.cache_state[3] += 1;
+                hdr->cache_hit = 1;
+            }
+            return;
+        }
+    }
+    for (int p = tid; p < P; p += kColorThreads) pr.col[p] = -1;
+    int r = 0;
+    bool done = false;
+    for (; r < max_rounds; ++r) {
+        for (int i = tid; i < nbodies; i += kColorThreads) pr.claim[i] = LLONG_MAX;
+        __syncthreads();  // also: every thread has read s_left of the previous round
+        if (tid == 0) s_left = 0;
+        for (int p = tid; p < P; p += kColorThreads) {
+            if (pr.col[p] >= 0) continue;
+            const long long k = jp_priority(p);
+            const int bi = pr.pbi[p], bj = pr.pbj[p];
+            if (invM[bi] > 0.0f) atomicMin(reinterpret_cast<long long *>(pr.claim) + bi, k);
+            if (bj >= 0 && invM[bj] > 0.0f) atomicMin(reinterpret_cast<long long *>(pr.claim) + bj, k);
+        }
+        __syncthreads();
+        for (int p = tid; p < P; p += kColorThreads) {
+            if (pr.col[p] >= 0) continue;
+            const long long k = jp_priority(p);
+            const int bi = pr.pbi[p], bj = pr.pbj[p];
+            bool ok = true;
+            if (invM[bi] > 0.0f && pr.claim[bi] != k) ok = false;
+            if (bj >= 0 && invM[bj] > 0.0f && pr.claim[bj] != k) ok = false;
+            if (ok) pr.col[p] = r;
+            else atomicAdd(&s_left, 1);
+        }
+        __syncthreads();
+        if (s_left == 0) {
+            done = true;
+            break;
+        }
+    }
+    const int ncol = done ? r + 1 : r;
+    if (!done || ncol > color_cap || ncol > pr.max_colors || ncol > kMaxColorsCap) {
+        if (tid == 0) {
+            atomicOr(&hdr->error, done ? B2C_ERR_COLOR_OVERFLOW : B2C_ERR_COLOR_TIMEOUT);
+            hdr->n_colors = 0;
+            hdr->cache_hit = 0;
+            hdr->rounds = r;
+            pr.cache_state[2] = 0;
+        }
+        return;
+    }
+    // group the pairs by colour (order inside a colour is free: its pairs share no dynamic body)
+    for (int c = tid; c < ncol; c += kColorThreads) s_cnt[c] = 0;
+    __syncthreads();
+    for (int p = tid; p < P; p += kColorThreads) atomicAdd(&s_cnt[pr.col[p]], 1);
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int c = 0; c < ncol; ++c) {
+            pr.cstart[c] = acc;
+            pr.ccount[c] = s_cnt[c];
+            s_cur[c] = acc;
+            acc += s_cnt[c];
+        }
+    }
+    __syncthreads();
+    for (int p = tid; p < P; p += kColorThreads) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
+    if (use_cache) {
+        for (int p = tid; p < P; p += kColorThreads) {
+            pr.cached_a[p] = pr.pbi[p];
+            pr.cached_b[p] = pr.pbj[p];
+        }
+        for (int i = tid; i < nbodies; i += kColorThreads) pr.cached_mass[i] = invM[i];
+    }
+    if (tid == 0) {
+        hdr->n_colors = ncol;
+        hdr->cache_hit = 0;
+        hdr->rounds = ncol;
+        pr.cache_state[0] = P;
+        pr.cache_state[1] = ncol;
+        pr.cache_state[2] = 1;
+        if (use_cache) pr.cache_state[4] += 1;  // cumulative misses ([3] counts hits)
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 5. the persistent chunk solve
+// ---------------------------------------------------------------------------------------------
+// body state is read and written through L2 (ld.cg / st.cg): CTAs on other SMs read it after a
+// grid barrier, and L1 is not coherent across SMs
+__device__ __forceinline__ float4 ldcg4(const float *p, int i) { return __ldcg(reinterpret_cast<const float4 *>(p) + i); }
+__device__ __forceinline__ void stcg4(float *p, int i, float4 v) { __stcg(reinterpret_cast<float4 *>(p) + i, v); }
+__device__ __forceinline__ f3 ldcg3(const float *p, int i) { return xyz(ldcg4(p, i)); }
+
+struct SolveArgs {
+    const b2c_header *hdr;
+    int *err;
+    // pairs
+    const int *porder, *cstart, *ccount, *pstart, *pcount, *pidx, *pbi, *pbj;
+    // kept contacts
+    const float *cpA, *cpB, *cn;
+    float *imp;
+    // bodies
+    const float *xc, *invIw, *invM;
+    float *v, *w, *pv, *po;
+    float mu, t2d, dt;
+    int vit, pit, fixed_frame, apply_warm;
+    unsigned int *bar_count, *bar_gen;
+    long long timeout_ns;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier with a wait limit.  Returns false (and sets B2C_ERR_BARRIER_TIMEOUT) when a
+// CTA waited longer than timeout_ns; every CTA then returns at its next barrier, so the kernel
+// always ends.
+template <bool kGrid>
+__device__ __forceinline__ bool solve_barrier(const SolveArgs &a)
+{
+    if (!kGrid) {
+        __syncthreads();
+        return true;
+    }
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned int *gen = a.bar_gen;
+        const unsigned int my_gen = *gen;
+        __threadfence();
+        const unsigned int prev = atomicAdd(a.bar_count, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(a.bar_count, 0u);
+            __threadfence();
+            atomicAdd(a.bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (*gen == my_gen) {
+                if (global_ns() - t0 > (unsigned long long)a.timeout_ns) {
+                    atomicOr(a.err, B2C_ERR_BARRIER_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        if (*(volatile int *)a.err & B2C_ERR_BARRIER_TIMEOUT) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// apply_warm, contact_engine_gpu_applied_warm.py:5-54
+__device__ void pair_apply_warm(const SolveArgs &a, int p)
+{
+    const int A = a.pbi[p], B = a.pbj[p];
+    const float iMA = a.invM[A], iMB = B >= 0 ? a.invM[B] : 0.0f;
+    f3 va = ldcg3(a.v, A), wa = ldcg3(a.w, A), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
+    if (B >= 0) {
+        vb = ldcg3(a.v, B);
+        wb = ldcg3(a.w, B);
+    }
+    const m3 IA = ldm(a.invIw, A);
+    m3 IB = IA;
+    if (B >= 0) IB = ldm(a.invIw, B);
+    const f3 xA = ld3(a.xc, A);
+    f3 xB{0.0f, 0.0f, 0.0f};
+    if (B >= 0) xB = ld3(a.xc, B);
+    const int st = a.pstart[p], n = a.pcount[p];
+    for (int k = 0; k < n; ++k) {
+        const int c = a.pidx[st + k];
+        const f3 nrm = ld3(a.cn, c);
+        f3 axis{1.0f, 0.0f, 0.0f};
+        if (fabsf(nrm.x) >= 0.9f) axis = f3{0.0f, 1.0f, 0.0f};
+        const float dd = dot3(axis, nrm);
+        const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, axis.x), fmaf(-dd, nrm.y, axis.y), fmaf(-dd, nrm.z, axis.z)});
+        const f3 t2 = cross3(nrm, t1);
+        const float4 im = ldcg4(a.imp, c);
+        const f3 J{fmaf(im.z, t2.x, fmaf(im.x, nrm.x, im.y * t1.x)), fmaf(im.z, t2.y, fmaf(im.x, nrm.y, im.y * t1.y)),
+                   fmaf(im.z, t2.z, fmaf(im.x, nrm.z, im.y * t1.z))};
+        if (iMA > 0.0f) {
+            va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
+            wa = add3(wa, matvec(IA, cross3(sub3(ld3(a.cpA, c), xA), J)));
+        }
+        if (B >= 0 && iMB > 0.0f) {
+            vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
+            wb = sub3(wb, matvec(IB, cross3(sub3(ld3(a.cpB, c), xB), J)));
+        }
+    }
+    if (iMA > 0.0f) {
+        stcg4(a.v, A, f4(va, 0.0f));
+        stcg4(a.w, A, f4(wa, 0.0f));
+    }
+    if (B >= 0 && iMB > 0.0f) {
+        stcg4(a.v, B, f4(vb, 0.0f));
+        stcg4(a.w, B, f4(wb, 0.0f));
+    }
+}
+
+// velocity chunk: k_fixed_frame (fixed_frame.py:7-77) or k_chunk_vel_r (COL:413-490)
+__device__ void pair_velocity(const SolveArgs &a, int p)
+{
+    const int bi = a.pbi[p], bj = a.pbj[p];
+    const float iMA = a.invM[bi];
+    const m3 IA = ldm(a.invIw, bi);
+    m3 IB = IA;
+    f3 vA = ldcg3(a.v, bi), wA = ldcg3(a.w, bi);
+    float iMB = 0.0f;
+    f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        iMB = a.invM[bj];
+        IB = ldm(a.invIw, bj);
+        vB = ldcg3(a.v, bj);
+        wB = ldcg3(a.w, bj);
+    }
+    const f3 xA = ld3(a.xc, bi);
+    f3 xB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) xB = ld3(a.xc, bj);
+    const int st = a.pstart[p], n = a.pcount[p];
+    for (int k = 0; k < n; ++k) {
+        const int c = a.pidx[st + k];
+        const f3 nrm = ld3(a.cn, c);
+        const f3 rA = sub3(ld3(a.cpA, c), xA);
+        f3 va = add3(vA, cross3(wA, rA));
+        f3 vb{0.0f, 0.0f, 0.0f}, rB{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) {
+            rB = sub3(ld3(a.cpB, c), xB);
+            vb = add3(vB, cross3(wB, rB));
+        }
+        f3 vrel = sub3(va, vb);
+        const float vn = dot3(vrel, nrm);
+        f3 t1;
+        bool axis_frame = a.fixed_frame;
+        if (!a.fixed_frame) {
+            const f3 vt{fmaf(-vn, nrm.x, vrel.x), fmaf(-vn, nrm.y, vrel.y), fmaf(-vn, nrm.z, vrel.z)};
+            const float mt = len3(vt);
+            t1 = div3(vt, mt);
+            axis_frame = mt <= 5e-3f;
+        }
+        if (axis_frame) {
+            f3 aa{1.0f, 0.0f, 0.0f};
+            if (fabsf(nrm.x) >= 0.9f) aa = f3{0.0f, 1.0f, 0.0f};
+            const float dd = dot3(aa, nrm);
+            t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
+        }
+        const f3 t2 = cross3(nrm, t1);
+        const f3 rnA = cross3(rA, nrm);
+        float meff = iMA + dot3(rnA, matvec(IA, rnA));
+        if (bj >= 0) {
+            const f3 rnB = cross3(rB, nrm);
+            meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
+        }
+        if (!(meff >= 1e-12f)) continue;
+        float4 im = ldcg4(a.imp, c);
+        float dj = -vn / meff;
+        const float nw = fmaxf(0.0f, im.x + dj);
+        dj = nw - im.x;
+        im.x = nw;
+        const f3 Jn = scale3(nrm, dj);
+        if (iMA > 0.0f) {
+            vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
+            wA = add3(wA, matvec(IA, cross3(rA, Jn)));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
+            wB = sub3(wB, matvec(IB, cross3(rB, Jn)));
+        }
+        va = add3(vA, cross3(wA, rA));
+        vb = f3{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+        vrel = sub3(va, vb);
+        const f3 rtA1 = cross3(rA, t1);
+        float meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
+        const f3 rtA2 = cross3(rA, t2);
+        float meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
+        if (bj >= 0) {
+            const f3 rtB1 = cross3(rB, t1);
+            meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
+            const f3 rtB2 = cross3(rB, t2);
+            meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
+        }
+        if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
+            const float o1 = im.y, o2 = im.z;
+            float a1 = o1 - dot3(vrel, t1) / meft1;
+            float a2 = o2 - dot3(vrel, t2) / meft2;
+            const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+            const float lim = a.mu * im.x;
+            if (mag > lim && mag > 1e-12f) {
+                a1 = a1 * lim / mag;
+                a2 = a2 * lim / mag;
+            }
+            im.y = a1;
+            im.z = a2;
+            const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+            const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+            if (iMA > 0.0f) {
+                vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
+                wA = add3(wA, matvec(IA, cross3(rA, Jt)));
+            }
+            if (bj >= 0 && iMB > 0.0f) {
+                vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
+                wB = sub3(wB, matvec(IB, cross3(rB, Jt)));
+            }
+        }
+        stcg4(a.imp, c, im);
+    }
+    if (iMA > 0.0f) {
+        stcg4(a.v, bi, f4(vA, 0.0f));
+        stcg4(a.w, bi, f4(wA, 0.0f));
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        stcg4(a.v, bj, f4(vB, 0.0f));
+        stcg4(a.w, bj, f4(wB, 0.0f));
+    }
+}
+
+// position chunk, k_chunk_pos_r (COL:510-554)
+__device__ void pair_position(const SolveArgs &a, int p)
+{
+    const int bi = a.pbi[p], bj = a.pbj[p];
+    const float iMA = a.invM[bi];
+    const m3 IA = ldm(a.invIw, bi);
+    m3 IB = IA;
+    f3 pvA = ldcg3(a.pv, bi), poA = ldcg3(a.po, bi);
+    float iMB = 0.0f;
+    f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        iMB = a.invM[bj];
+        IB = ldm(a.invIw, bj);
+        pvB = ldcg3(a.pv, bj);
+        poB = ldcg3(a.po, bj);
+    }
+    const f3 xA = ld3(a.xc, bi);
+    f3 xB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) xB = ld3(a.xc, bj);
+    const int st = a.pstart[p], n = a.pcount[p];
+    for (int k = 0; k < n; ++k) {
+        const int c = a.pidx[st + k];
+        const f3 nrm = ld3(a.cn, c);
+        const float4 pA4 = ld4(a.cpA, c);
+        const f3 rA = sub3(xyz(pA4), xA);
+        f3 rel = add3(pvA, cross3(poA, rA));
+        f3 rB{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) {
+            rB = sub3(ld3(a.cpB, c), xB);
+            rel = sub3(rel, add3(pvB, cross3(poB, rB)));
+        }
+        const f3 rnA = cross3(rA, nrm);
+        float meff = iMA + dot3(rnA, matvec(IA, rnA));
+        if (bj >= 0) {
+            const f3 rnB = cross3(rB, nrm);
+            meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
+        }
+        if (!(meff >= 1e-12f)) continue;
+        const float bias = B2C_BETA * fmaxf(pA4.w - B2C_SLOP, 0.0f) / a.dt;
+        float dj = (bias - dot3(rel, nrm)) / meff;
+        const float jp = __ldcg(a.imp + 4 * c + 3);
+        const float nw = fmaxf(0.0f, jp + dj);
+        dj = nw - jp;
+        __stcg(a.imp + 4 * c + 3, nw);
+        const f3 Jn = scale3(nrm, dj);
+        if (iMA > 0.0f) {
+            pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
+            poA = add3(poA, matvec(IA, cross3(rA, Jn)));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
+            poB = sub3(poB, matvec(IB, cross3(rB, Jn)));
+        }
+    }
+    if (iMA > 0.0f) {
+        stcg4(a.pv, bi, f4(pvA, 0.0f));
+        stcg4(a.po, bi, f4(poA, 0.0f));
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        stcg4(a.pv, bj, f4(pvB, 0.0f));
+        stcg4(a.po, bj, f4(poB, 0.0f));
+    }
+}
+
+template <bool kGrid>
+__global__ void __launch_bounds__(256) k_color_solve(SolveArgs a)
+{
+    const int nc = a.hdr->n_colors;
+    if (a.hdr->n_pairs == 0 || nc == 0) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (a.apply_warm) {
+        for (int ci = 0; ci < nc; ++ci) {
+            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            for (int t = tid; t < cnt; t += nth) pair_apply_warm(a, a.porder[s0 + t]);
+            if (!solve_barrier<kGrid>(a)) return;
+        }
+    }
+    for (int it = 0; it < a.vit; ++it)
+        for (int ci = 0; ci < nc; ++ci) {
+            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            for (int t = tid; t < cnt; t += nth) pair_velocity(a, a.porder[s0 + t]);
+            if (!solve_barrier<kGrid>(a)) return;
+        }
+    for (int it = 0; it < a.pit; ++it)
+        for (int ci = 0; ci < nc; ++ci) {
+            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            for (int t = tid; t < cnt; t += nth) pair_position(a, a.porder[s0 + t]);
+            if (!solve_barrier<kGrid>(a)) return;
+        }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 6. warm store (COL:1089-1093)
+// ---------------------------------------------------------------------------------------------
+__global__ void k_warm_store(const b2c_header *__restrict__ hdr, const long long *__restrict__ kept_keys,
+                             const float *__restrict__ imp, int use_warm, long long *__restrict__ wkeys,
+                             float *__restrict__ wimp, int *__restrict__ wn)
+{
+    const int Ck = hdr->n_contacts > 0 ? hdr->n_kept : 0;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) *wn = use_warm ? Ck : 0;
+    if (!use_warm) return;
+    for (int d = tid; d < Ck; d += gridDim.x * blockDim.x) {
+        wkeys[d] = kept_keys[d];
+        const float4 v = ld4(imp, d);
+        st4(wimp, d, make_float4(v.x, v.y, v.z, 0.0f));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------------------------
+int bead_contacts_sorted(const b2c_beads *beads, const b2c_grid *g, b2c_contacts *c, b2c_manifold *m,
+                         b2c_header *hdr, cudaStream_t s)
+{
+    const int nb = beads->n;
+    k_bead_count<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted,
+                                                         view_of(g), m->bead_count, hdr);
+    int rc = check_launch("bead_count");
+    if (rc) return rc;
+    rc = exclusive_scan(m->bead_count, m->bead_offset, nb + 1, nullptr, m->scan_tmp, s);
+    if (rc) return rc;
+    k_bead_emit<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted,
+                                                        view_of(g), m->bead_offset, *c, hdr);
+    return check_launch("bead_emit");
+}
+
+int manifold_reduce(const b2c_bodies *b, const b2c_beads *beads, const b2c_contacts *c, b2c_manifold *m,
+                    b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr, const b2c_warm *warm, b2c_header *hdr,
+                    const b2c_color_params *p, cudaStream_t s)
+{
+    const int N = b->n, cap = c->capacity, pcap = pr->capacity;
+    const long long stride = (long long)beads->n + 1;
+    const int cgrid = std::min(blocks_for(cap), kSMs * 8);
+    const int pgrid = std::min(blocks_for(pcap), kSMs * 8);
+    int rc;
+    if (p->flags & B2C_COLOR_PER_CONTACT) {
+        k_warm<<<cgrid, kThreads, 0, s>>>(hdr, c->fa, c->fb, stride, (p->flags & B2C_COLOR_WARM_START) ? 1 : 0,
+                                          reinterpret_cast<const long long *>(warm->keys), warm->imp, warm->n,
+                                          m->jn_in, reinterpret_cast<float2 *>(m->jt_in));
+        k_per_contact<<<cgrid, kThreads, 0, s>>>(hdr, stride, *c, m->jn_in, reinterpret_cast<const float2 *>(m->jt_in),
+                                                 *kept, reinterpret_cast<long long *>(kept_keys), pcap, pr->pbi,
+                                                 pr->pbj, pr->kcount, pr->pstart, pr->pidx);
+        return check_launch("per_contact");
+    }
+    k_body_pairs<<<blocks_for((long long)N * 32, 256), 256, 0, s>>>(
+        N, beads->bead_start, m->bead_offset, cap, c->bj, m->pair_local, reinterpret_cast<int2 *>(m->pair_first),
+        m->gorder, m->body_npairs);
+    rc = check_launch("body_pairs");
+    if (rc) return rc;
+    if ((rc = exclusive_scan(m->body_npairs, m->pair_base, N + 1, nullptr, m->scan_tmp, s))) return rc;
+    k_pairs_write<<<cgrid, kThreads, 0, s>>>(hdr, N, c->bi, c->bj, m->pair_local,
+                                             reinterpret_cast<const int2 *>(m->pair_first), m->pair_base, pcap, pr->pbi,
+                                             pr->pbj, m->praw_start, m->praw_count, hdr);
+    k_warm<<<cgrid, kThreads, 0, s>>>(hdr, c->fa, c->fb, stride, (p->flags & B2C_COLOR_WARM_START) ? 1 : 0,
+                                      reinterpret_cast<const long long *>(warm->keys), warm->imp, warm->n, m->jn_in,
+                                      reinterpret_cast<float2 *>(m->jt_in));
+    k_select<<<pgrid, 128, 0, s>>>(hdr, p->max_points, m->praw_start, m->praw_count, m->gorder, c->bi, c->pA, c->n,
+                                   b->xc, m->jn_in, m->keep, m->jn_red, pr->kcount, hdr);
+    if ((rc = check_launch("select"))) return rc;
+    if ((rc = exclusive_scan(m->keep, m->kidx, cap + 1, &hdr->n_contacts, m->scan_tmp, s))) return rc;
+    k_set_kept<<<1, 1, 0, s>>>(hdr, m->kidx);
+    k_compact<<<cgrid, kThreads, 0, s>>>(hdr, stride, *c, m->keep, m->kidx, m->jn_red,
+                                         reinterpret_cast<const float2 *>(m->jt_in), *kept,
+                                         reinterpret_cast<long long *>(kept_keys));
+    if ((rc = exclusive_scan(pr->kcount, pr->pstart, pcap + 1, &hdr->n_pairs, m->scan_tmp, s))) return rc;
+    k_pair_kept<<<pgrid, kThreads, 0, s>>>(hdr, m->praw_start, m->praw_count, m->gorder, m->keep, m->kidx,
+                                           pr->pstart, pr->pidx, pr->kcount, hdr);
+    return check_launch("manifold_reduce");
+}
+
+int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p, cudaStream_t s)
+{
+    const int cap = std::min(p->color_cap, std::min(pr->max_colors, kMaxColorsCap));
+    k_color_pairs<<<1, kColorThreads, 0, s>>>(hdr, b->n, b->invM, *pr, (p->flags & B2C_COLOR_CACHE) ? 1 : 0, cap,
+                                              kMaxColorsCap + 1);
+    return check_launch("color_pairs");
+}
+
+static int max_coresident_blocks()
+{
+    static int cached = -1;
+    if (cached < 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve<true>, 256, 0);
+        cached = std::max(1, sms * std::max(per, 1));
+    }
+    return cached;
+}
+
+int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
+                float dt, cudaStream_t s)
+{
+    SolveArgs a;
+    a.hdr = hdr;
+    a.err = &hdr->error;
+    a.porder = pr->porder;
+    a.cstart = pr->cstart;
+    a.ccount = pr->ccount;
+    a.pstart = pr->pstart;
+    a.pcount = pr->kcount;
+    a.pidx = pr->pidx;
+    a.pbi = pr->pbi;
+    a.pbj = pr->pbj;
+    a.cpA = kept->pA;
+    a.cpB = kept->pB;
+    a.cn = kept->n;
+    a.imp = kept->imp;
+    a.xc = b->xc;
+    a.invIw = b->invIw;
+    a.invM = b->invM;
+    a.v = b->v;
+    a.w = b->w;
+    a.pv = b->pv;
+    a.po = b->po;
+    a.mu = p->mu;
+    a.t2d = p->t2d;
+    a.dt = dt;
+    a.vit = p->vit;
+    a.pit = p->pit;
+    a.fixed_frame = (p->flags & B2C_COLOR_FIXED_FRAME) ? 1 : 0;
+    a.apply_warm = (p->flags & B2C_COLOR_APPLY_WARM) ? 1 : 0;
+    a.bar_count = pr->barrier;
+    a.bar_gen = pr->barrier + 1;
+    a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
+    int nblocks = p->solve_blocks > 0 ? p->solve_blocks : (b->n + 255) / 256;
+    nblocks = std::max(1, std::min(nblocks, max_coresident_blocks()));
+    if (nblocks == 1) {
+        k_color_solve<false><<<1, 256, 0, s>>>(a);
+        return check_launch("color_solve");
+    }
+    cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve<true>, a);
+    if (e != cudaSuccess) {
+        set_error("color_solve: cooperative launch of %d blocks: %s", nblocks, cudaGetErrorString(e));
+        return B2C_ECUDA;
+    }
+    return check_launch("color_solve");
+}
+
+int warm_store(const b2c_contacts *kept, const int64_t *kept_keys, b2c_warm *warm, const b2c_header *hdr, int use,
+               cudaStream_t s)
+{
+    k_warm_store<<<std::min(blocks_for(kept->capacity), kSMs * 8), kThreads, 0, s>>>(
+        hdr, reinterpret_cast<const long long *>(kept_keys), kept->imp, use, reinterpret_cast<long long *>(warm->keys),
+        warm->imp, warm->n);
+    return check_launch("warm_store");
+}
+
+}  // namespace b2c
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+static bool color_params_ok(const b2c_color_params *p)
+{
+    return p && p->vit >= 0 && p->pit >= 0 && p->max_points >= 1 && p->max_points <= 8 && p->color_cap >= 1;
+}
+
+extern "C" int32_t b2c_bead_contacts_sorted(const b2c_beads *beads, const b2c_grid *g, b2c_contacts *c,
+                                            b2c_manifold *m, b2c_header *hdr, b2c_stream s)
+{
+    if (!beads || !g || !c || !m || !hdr || !m->bead_count || !m->bead_offset) {
+        b2c::set_error("b2c_bead_contacts_sorted: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::bead_contacts_sorted(beads, g, c, m, hdr, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_manifold_reduce(const b2c_bodies *b, const b2c_beads *beads, const b2c_contacts *c,
+                                       b2c_manifold *m, b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr,
+                                       const b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, b2c_stream s)
+{
+    if (!b || !beads || !beads->bead_start || !c || !m || !kept || !kept_keys || !pr || !warm || !hdr ||
+        !color_params_ok(p) || kept->capacity < c->capacity) {
+        b2c::set_error("b2c_manifold_reduce: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::manifold_reduce(b, beads, c, m, kept, kept_keys, pr, warm, hdr, p, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
+                                   b2c_stream s)
+{
+    if (!b || !pr || !hdr || !color_params_ok(p) || pr->max_colors < 1) {
+        b2c::set_error("b2c_color_pairs: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::color_pairs(b, pr, hdr, p, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr,
+                                   const b2c_color_params *p, float dt, b2c_stream s)
+{
+    if (!b || !kept || !pr || !hdr || !color_params_ok(p) || !(dt > 0.0f) || !pr->barrier) {
+        b2c::set_error("b2c_color_solve: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::color_solve(b, kept, pr, hdr, p, dt, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_warm_store(const b2c_contacts *kept, const int64_t *kept_keys, b2c_warm *warm,
+                                  const b2c_header *hdr, b2c_stream s)
+{
+    if (!kept || !kept_keys || !warm || !hdr || warm->capacity < kept->capacity) {
+        b2c::set_error("b2c_warm_store: bad argument");
+        return B2C_EARG;
+    }
+    return b2c::warm_store(kept, kept_keys, warm, hdr, 1, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, b2c_contacts *c,
+                                     b2c_manifold *m, b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr,
+                                     b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, float dt,
+                                     float *vgrav, b2c_stream s)
+{
+    if (!b || !beads || !beads->bead_start || !g || !c || !m || !kept || !kept_keys || !pr || !warm || !hdr ||
+        !color_params_ok(p) || !vgrav || !(dt > 0.0f) || kept->capacity < c->capacity ||
+        warm->capacity < kept->capacity) {
+        b2c::set_error("b2c_color_substep: bad argument");
+        return B2C_EARG;
+    }
+    cudaStream_t st = b2c::stream_of(s);
+    int rc;
+    if ((rc = b2c::body_predict(b, dt, st))) return rc;
+    if (b->n > 0) {
+        cudaMemcpyAsync(vgrav, b->v, sizeof(float) * 4 * (size_t)b->n, cudaMemcpyDeviceToDevice, st);
+        // pv / po start every substep at zero (deferred_force.py:37-38, 54-55)
+        cudaMemsetAsync(b->pv, 0, sizeof(float) * 4 * (size_t)b->n, st);
+        cudaMemsetAsync(b->po, 0, sizeof(float) * 4 * (size_t)b->n, st);
+    }
+    if ((rc = b2c::bead_world(b, beads, g, st))) return rc;
+    if ((rc = b2c::grid_build(beads, g, st))) return rc;
+    if ((rc = b2c::bead_contacts_sorted(beads, g, c, m, hdr, st))) return rc;
+    if ((rc = b2c::manifold_reduce(b, beads, c, m, kept, kept_keys, pr, warm, hdr, p, st))) return rc;
+    if ((rc = b2c::color_pairs(b, pr, hdr, p, st))) return rc;
+    if ((rc = b2c::color_solve(b, kept, pr, hdr, p, dt, st))) return rc;
+    if ((rc = b2c::warm_store(kept, kept_keys, warm, hdr, (p->flags & B2C_COLOR_WARM_START) ? 1 : 0, st))) return rc;
+    return b2c::body_integrate(b, dt, st);
+}

@@ -167,6 +167,7 @@ class _BeadEngineBase:
         self.NB = NB
         self.rest = f32(_pad4(np.tile(self.rest_np.astype(np.float32), (N, 1))))
         self.owner = torch.from_numpy(np.repeat(np.arange(N, dtype=np.int32), self.P)).to(dev)
+        self.bead_start = torch.from_numpy((np.arange(N + 1) * self.P).astype(np.int32)).to(dev)
         self.world = torch.zeros((NB, 4), dtype=torch.float32, device=dev)
         self.header = torch.zeros(8, dtype=torch.int32, device=dev)
         self._hdr_host = torch.zeros(8, dtype=torch.int32, pin_memory=True)
@@ -194,7 +195,8 @@ class _BeadEngineBase:
         self.c_bodies = _lib.Bodies(self.N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
                                     _ptr(self.po), _ptr(self.invM), _ptr(self.IbInv), _ptr(self.kin),
                                     _ptr(self.invIw))
-        self.c_beads = _lib.Beads(self.NB, _ptr(self.rest), _ptr(self.owner), _ptr(self.world))
+        self.c_beads = _lib.Beads(self.NB, _ptr(self.rest), _ptr(self.owner), _ptr(self.world),
+                                  _ptr(self.bead_start))
 
     def _stream(self):
         return torch.cuda.current_stream(self.dev)

@@ -79,6 +79,7 @@ typedef struct b2c_beads {
     const float *rest;      /* (n,4) bead offset in its body's frame */
     const int32_t *owner;   /* (n) body of each bead; beads of a body are contiguous */
     float *world;           /* (n,4) world position, written each substep */
+    const int32_t *bead_start; /* (bodies+1) first bead of each body */
 } b2c_beads;
 
 /* Uniform hash grid over the beads (the reference uses wp.HashGrid, built at
@@ -123,6 +124,76 @@ typedef struct b2c_jacobi_params {
     float relax, mu;
 } b2c_jacobi_params;
 
+#define B2C_ERR_BARRIER_TIMEOUT 128  /* a grid barrier of the persistent solve gave up waiting */
+
+/* Scratch of the coloured chain's ordering and manifold stage (one slot per raw contact
+ * unless noted).  Replaces the radix-sort buffers, segment flags and selection arrays of
+ * _device_manifold (contact_engine_gpu_colored.py:1050-1087). */
+typedef struct b2c_manifold {
+    int32_t capacity;        /* raw contacts */
+    int32_t pair_capacity;   /* body pairs */
+    int32_t *bead_count;     /* (beads+1) contacts emitted per bead */
+    int32_t *bead_offset;    /* (beads+1) exclusive scan of bead_count: feature-order offsets */
+    int32_t *pair_local;     /* rank of the contact's pair among its body's pairs */
+    int32_t *pair_first;     /* first-occurrence start / count of a pair (packed 2 ints per slot) */
+    int32_t *gorder;         /* pair-sorted position -> feature index */
+    int32_t *body_npairs;    /* (bodies+1) pairs per body */
+    int32_t *pair_base;      /* (bodies+1) exclusive scan of body_npairs */
+    int32_t *praw_start;     /* (pair_capacity) first pair-sorted position of each pair */
+    int32_t *praw_count;     /* (pair_capacity) raw contacts of each pair */
+    double *jn_in;           /* warm-started normal impulse (float64, as COL:604) */
+    double *jn_red;          /* normal impulse after redistribution onto the kept points */
+    float *jt_in;            /* (cap,2) warm-started friction impulses */
+    int32_t *keep;           /* 1 = kept by the selection */
+    int32_t *kidx;           /* exclusive scan of keep: kept index */
+    int32_t *scan_tmp;       /* b2c_scan_scratch_ints(max(beads+1, capacity+1, pairs+1)) */
+} b2c_manifold;
+
+/* Kept contacts and their body pairs, the colouring, the colour cache and the warm store. */
+typedef struct b2c_pairs {
+    int32_t capacity;        /* pairs */
+    int32_t max_colors;      /* capacity of the per-colour arrays (the reference's _NCOLMAX = 512) */
+    int32_t *pbi, *pbj;      /* bodies of each pair, sorted by (pbi, pbj) */
+    int32_t *kcount;         /* kept contacts of each pair */
+    int32_t *pstart;         /* exclusive scan of kcount */
+    int32_t *pidx;           /* (kept cap) kept-contact index, pair-sorted, feature order inside a pair */
+    int32_t *col;            /* colour of each pair */
+    int32_t *porder;         /* pairs grouped by colour */
+    int32_t *cstart, *ccount;/* (max_colors) per-colour offset and count into porder */
+    int64_t *claim;          /* (bodies) Jones-Plassmann claims */
+    int32_t *cached_a, *cached_b; /* colour cache: pbi / pbj of the cached colouring */
+    float *cached_mass;      /* (bodies) invM of the cached colouring */
+    int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
+    uint32_t *barrier;       /* [count, generation] of the persistent solve's grid barrier */
+} b2c_pairs;
+
+/* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
+typedef struct b2c_warm {
+    int32_t capacity;
+    int64_t *keys;           /* (cap) */
+    float *imp;              /* (cap,4) jn, jt1, jt2, unused */
+    int32_t *n;              /* (1) entries stored */
+} b2c_warm;
+
+/* Flags of b2c_color_params.flags */
+#define B2C_COLOR_FIXED_FRAME 1  /* normal-derived tangent frame (contact_engine_gpu_fixed_frame.py) */
+#define B2C_COLOR_APPLY_WARM 2   /* apply the warm impulses once per colour before the sweeps */
+#define B2C_COLOR_CACHE 4        /* reuse the colouring while pairs and masses are unchanged */
+#define B2C_COLOR_WARM_START 8   /* warm start by feature key */
+#define B2C_COLOR_PER_CONTACT 16 /* no manifold reduction; every contact is its own chunk and is
+                                    coloured on the contact graph (the plain coloured engine) */
+
+typedef struct b2c_color_params {
+    int32_t vit, pit;        /* velocity / position sweeps */
+    int32_t max_points;      /* manifold points kept per pair (<= 8) */
+    int32_t flags;           /* B2C_COLOR_* */
+    float mu;                /* friction */
+    float t2d;               /* cross-slip damping of the chunk sweep (1 = full) */
+    int32_t color_cap;       /* error when the pair graph needs more colours (<= max_colors) */
+    int32_t solve_blocks;    /* CTAs of the persistent solve (0 = pick from the body count) */
+    int64_t barrier_timeout_ns; /* grid-barrier wait limit */
+} b2c_color_params;
+
 /* ---- version / errors ---- */
 B2C_API int32_t b2c_version(void);
 B2C_API const char *b2c_last_error(void);
@@ -162,6 +233,39 @@ B2C_API int32_t b2c_jacobi_solve(const b2c_bodies *b, b2c_contacts *c, const b2c
 B2C_API int32_t b2c_jacobi_substep(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, b2c_contacts *c,
                            b2c_header *hdr, int64_t *acc, const b2c_jacobi_params *p, float dt, float *vgrav,
                            b2c_stream s);
+
+/* ---- coloured Gauss-Seidel chain (contact_engine_gpu_colored.py, ColorCache descendants) ---- */
+/* k_gen_fid (COL:102-122) + the feature-key radix sort and gather (COL:1057-1061), done as one
+ * deterministic pass: per-bead counts, a scan, then each bead writes its ground contact and its
+ * neighbours in ascending bead order at its offset.  The output is in feature-key order. */
+B2C_API int32_t b2c_bead_contacts_sorted(const b2c_beads *beads, const b2c_grid *g, b2c_contacts *c,
+                                         b2c_manifold *m, b2c_header *hdr, b2c_stream s);
+/* Pair-key grouping (COL:1062-1064), warm start (k_warm COL:601-626), E-optimal selection
+ * (k_select COL:651-728), compaction (k_compact COL:730-751) and the kept-contact pair build
+ * (COL:1158-1176).  `kept` receives the kept contacts in feature order with their impulses. */
+B2C_API int32_t b2c_manifold_reduce(const b2c_bodies *b, const b2c_beads *beads, const b2c_contacts *c,
+                                    b2c_manifold *m, b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr,
+                                    const b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, b2c_stream s);
+/* Jones-Plassmann colouring of the pair graph (COL:1178-1208) behind the colour cache
+ * (contact_engine_gpu_color_cache.py:37-54), entirely on the device. */
+B2C_API int32_t b2c_color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
+                                b2c_stream s);
+/* The pair-chunk solve of one substep as one persistent kernel: applied warm start per colour
+ * (applied_warm.py:68-75), vit velocity sweeps (fixed frame, fixed_frame.py:7-77, or slip basis,
+ * COL:413-490) and pit position sweeps (COL:510-554) over the colours, a bounded grid barrier
+ * between colours. */
+B2C_API int32_t b2c_color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr,
+                                const b2c_color_params *p, float dt, b2c_stream s);
+/* _store_warm_device (COL:1089-1093). */
+B2C_API int32_t b2c_warm_store(const b2c_contacts *kept, const int64_t *kept_keys, b2c_warm *warm,
+                               const b2c_header *hdr, b2c_stream s);
+/* One whole ColorCache / pair-chunk substep: predict, beads, grid, sorted contacts, manifold,
+ * pairs, colouring (cached), solve, warm store, integrate.  vgrav receives the velocity after
+ * gravity (the deferred-force reference point, deferred_force.py:33). */
+B2C_API int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, b2c_contacts *c,
+                                  b2c_manifold *m, b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr,
+                                  b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, float dt,
+                                  float *vgrav, b2c_stream s);
 
 #ifdef __cplusplus
 }

@@ -32,11 +32,13 @@ MAXC = 400000
 
 # variant indices of oracle_contact.c (g_fv[])
 FV_NAMES = ["DOT", "CROSS", "MATVEC", "MATMUL", "QROT", "QMUL", "QNORM", "VNORM", "SITE_GRAV", "SITE_VT",
-            "SITE_T1", "SITE_MAG", "SITE_JT", "SITE_APPLY", "SITE_INTX", "SITE_INTQ", "SITE_IMP"]
+            "SITE_T1", "SITE_MAG", "SITE_JT", "SITE_APPLY", "SITE_INTX", "SITE_INTQ", "SITE_IMP", "QDOT",
+            "SITE_VUPD", "SITE_WUPD", "SITE_BIAS"]
 FV = {n: i for i, n in enumerate(FV_NAMES)}
 
 # The contraction pattern that reproduces the reference's golden arrays bit for bit.
 PINNED_VARIANTS = {n: (1 if n.startswith("SITE_") else 0) for n in FV_NAMES}
+PINNED_VARIANTS.update(SITE_WUPD=0, SITE_BIAS=0)
 
 
 def build(force: bool = False) -> str:
@@ -194,3 +196,109 @@ class JacobiOracle:
 
     def contact_forces(self):
         return self.force.copy()
+
+
+def _col_sigs(L):
+    P = ctypes.c_void_p
+    L.or_col_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                ctypes.c_int, ctypes.c_int]
+    L.or_col_create.restype = P
+    L.or_col_destroy.argtypes = [P]
+    L.or_col_stats.argtypes = [P, P]
+    L.or_col_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P, P, ctypes.c_double,
+                              ctypes.c_int, P]
+    L.or_col_step.restype = ctypes.c_int
+
+
+class ColoredOracle:
+    """CPU restatement of the coloured pair-chunk engines.
+
+    mode="pair_chunks": GraphColoredContactEngine(manifold_reduce=True, graph_capture=True,
+        pair_chunks=True) -- contact_engine_gpu_colored.py:793-1410, slip-basis chunk sweep.
+    mode="plain": GraphColoredContactEngine() -- per-contact colouring, no manifold reduction
+        (contact_engine_gpu_colored.py:903-936, 1105-1137, 188-320).
+    mode="color_cache": ColorCacheContactEngine -- contact_engine_gpu_color_cache.py:21-54 on top of
+        DeferredForce / AppliedWarm / FixedFrame (fixed tangent frame, warm impulses applied once per
+        colour before the sweeps, colouring reused while the pair graph and masses are unchanged).
+    """
+
+    def __init__(self, mode="color_cache", dims=(0.3, 0.3, 0.2), vit=40, pit=20, mu=0.5, max_points=4,
+                 t2_damp=1.0, cap=MAXC):
+        assert mode in ("pair_chunks", "color_cache", "plain")
+        self.mode = mode
+        self.name = f"{mode}_oracle"
+        self.dims = dims; self.vit = vit; self.pit = pit; self.mu = mu; self.mx = max_points; self.t2d = t2_damp
+        self.cap = cap
+        self._centers = []; self._dens = []; self._kin = []
+        self.b = None
+        self._h = None
+        self._force_dt = None
+
+    def add_body(self, center, density=700.0, kin=False):
+        self._centers.append(list(center)); self._dens.append(float(density)); self._kin.append(1 if kin else 0)
+        self.b = None
+        return len(self._centers) - 1
+
+    def _build(self):
+        L = lib()
+        if not hasattr(L, "_col_ready"):
+            _col_sigs(L); L._col_ready = True
+        self.b = build_bodies(self._centers, self._dens, self._kin, self.dims)
+        N = len(self._centers); P = len(self.b.rest)
+        self.N = N; self.P = P
+        self.rest_all = np.ascontiguousarray(np.tile(self.b.rest, (N, 1)))
+        self.owner = np.repeat(np.arange(N, dtype=np.int32), P)
+        self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
+        self.vgrav = np.zeros((N, 3), np.float32)
+        if self._h:
+            L.or_col_destroy(self._h)
+        self._h = L.or_col_create({"pair_chunks": 0, "color_cache": 1, "plain": 2}[self.mode], self.vit, self.pit,
+                                  self.mx, self.mu,
+                                  self.t2d, self.cap, N)
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().or_col_destroy(self._h)
+        except Exception:
+            pass
+
+    def set_kinematic(self, i, xc):
+        self._kin[i] = 1; self._centers[i] = list(xc)
+        if self.b is not None:
+            self.b.xc[i] = np.array(xc, np.float32); self.b.invM[i] = 0.0
+            self.b.v[i] = 0.0; self.b.w[i] = 0.0; self.b.kin[i] = 1; self.b.M[i] = np.inf
+
+    def step(self, dt, substeps=1):
+        if self.b is None:
+            self._build()
+        b = self.b
+        rc = lib().or_col_step(self._h, self.N, self.N * self.P, _p(self.rest_all), _p(self.owner), _p(b.xc), _p(b.q),
+                               _p(b.v), _p(b.w), _p(self.pv), _p(self.po), _p(b.invM), _p(b.IbInv), _p(b.kin),
+                               float(dt), int(substeps), _p(self.vgrav))
+        if rc != 0:
+            raise RuntimeError(f"oracle coloured step failed with status {rc}")
+        self._force_dt = dt / substeps
+
+    def stats(self):
+        out = np.zeros(7, np.int32)
+        lib().or_col_stats(self._h, _p(out))
+        return dict(zip(("n_contacts", "n_kept", "n_pairs", "n_colors", "hits", "misses", "seg_overflow"),
+                        out.tolist()))
+
+    @property
+    def n_contacts(self):
+        return self.stats()["n_contacts"]
+
+    def get_state(self) -> State:
+        if self.b is None:
+            self._build()
+        return State(xc=self.b.xc.copy(), Rm=quat_to_R(self.b.q), vc=self.b.v.copy(), om=self.b.w.copy())
+
+    def contact_forces(self):
+        f = np.zeros((len(self._centers), 3))
+        if self.b is None or self._force_dt is None:
+            return f
+        nk = self.b.kin == 0
+        f[nk] = self.b.M[nk, None] * (self.b.v[nk] - self.vgrav[nk]) / self._force_dt
+        return f

@@ -49,11 +49,20 @@ enum {
     FV_SITE_INTX,   /* xc + (v+pv)*dt                    CEG:178          */
     FV_SITE_INTQ,   /* q + 0.5*wq*q*dt                   CEG:179          */
     FV_SITE_IMP,    /* jn*n + jt1*t1 + jt2*t2            applied_warm:38  */
+    FV_QDOT,        /* dot(quat, quat) inside wp.normalize(quat)            */
+    FV_SITE_VUPD,   /* v + J*iM in the chunk sweeps      COL:460,546      */
+    FV_SITE_WUPD,   /* w + I*cross(r,J) in the chunk sweeps                 */
+    FV_SITE_BIAS,   /* beta*max(pen-slop,0)/dt form                         */
     FV_COUNT
 };
 /* pinned: builtins in their first-product-fused form (variant 0), every user-level
  * multiply-add site contracted (1) -- reproduces the golden arrays bit for bit */
-static int g_fv[32] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+static int g_fv[32] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1, 0, 0};
+/* variant table used inside the position chunk only (search aid; equal to g_fv when pinned) */
+static int g_fv_pos[32] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1, 0, 0};
+static int g_pos_override = 0;
+OR_API void or_set_pos_variant(int idx, int val) { if (idx >= 0 && idx < 32) { g_fv_pos[idx] = val; g_pos_override = 1; } }
+OR_API void or_clear_pos_variants(void) { g_pos_override = 0; }
 
 OR_API void or_set_variant(int idx, int val) { if (idx >= 0 && idx < 32) g_fv[idx] = val; }
 OR_API int or_get_variant(int idx) { return (idx >= 0 && idx < 32) ? g_fv[idx] : -1; }
@@ -173,10 +182,13 @@ static qt qmul(qt a, qt b)
 }
 static float qdot(qt a, qt b)
 {
-    switch (g_fv[FV_DOT]) {
+    switch (g_fv[FV_QDOT]) {
     case 0: return fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.x, b.x, a.y * b.y)));
     case 1: return fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.y, b.y, fmaf(a.x, b.x, 0.0f))));
     case 2: return fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)));
+    case 3: return fmaf(a.w, b.w, fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)));
+    case 4: return fmaf(a.x, b.x, fmaf(a.y, b.y, fmaf(a.z, b.z, a.w * b.w)));
+    case 5: return fmaf(a.w, b.w, fmaf(a.x, b.x, a.y * b.y) + a.z * b.z);
     default: return ((a.x * b.x + a.y * b.y) + a.z * b.z) + a.w * b.w;
     }
 }
@@ -572,4 +584,603 @@ OR_API int or_jacobi_step(int N, int nbead, const float *rest, const int *owner,
     free(jn); free(jt1); free(jt2); free(jp);
     for (int k = 0; k < 6; ++k) free(A.a[k]);
     return c.overflow ? 2 : 0;
+}
+
+/* ================================================================== */
+/* Coloured Gauss-Seidel chain: GraphColoredContactEngine with         */
+/* manifold_reduce + pair_chunks (COL), and the ColorCache descendant  */
+/* (fixed frame, applied warm start, colour cache, deferred forces).   */
+/* ================================================================== */
+
+typedef struct { int64_t key; int idx; } kv_t;
+static int cmp_kv(const void *a, const void *b)
+{
+    const kv_t *x = a, *y = b;
+    if (x->key < y->key) return -1;
+    if (x->key > y->key) return 1;
+    return x->idx - y->idx;           /* stable */
+}
+/* stable argsort of int64 keys */
+static void argsort_stable(const int64_t *keys, int n, int *perm)
+{
+    kv_t *t = malloc(sizeof(kv_t) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) { t[i].key = keys[i]; t[i].idx = i; }
+    qsort(t, n, sizeof(kv_t), cmp_kv);
+    for (int i = 0; i < n; ++i) perm[i] = t[i].idx;
+    free(t);
+}
+
+/* Warp's PCG hash (rand_init / randi), the published PCG-RXS-M-XS 32-bit output
+ * permutation used as a hash (Jarzynski & Olano, "Hash Functions for GPU Rendering", 2020). */
+static inline uint32_t pcg_hash(uint32_t state)
+{
+    uint32_t b = state * 747796405u + 2891336453u;
+    uint32_t c = ((b >> ((b >> 28u) + 4u)) ^ b) * 277803737u;
+    return (c >> 22u) ^ c;
+}
+/* k_prio, COL:136-148: key = |int32(randi(rand_init(7919, c)))| << 32 | c */
+static inline int64_t jp_priority(int c)
+{
+    uint32_t st = pcg_hash((uint32_t)7919 + pcg_hash((uint32_t)c));
+    st = pcg_hash(st);
+    int64_t p = (int64_t)(int32_t)st;
+    if (p < 0) p = -p;
+    return p * (int64_t)4294967296LL + (int64_t)c;
+}
+
+typedef struct {
+    int mode;            /* 0 = pair chunks (slip basis), 1 = ColorCache (fixed frame + applied warm + cache) */
+    int vit, pit, mx;
+    float mu, t2d;
+    int cap;
+    /* warm store (COL:1089-1093) */
+    int ws_n;
+    int64_t *ws_keys;
+    float *ws_jn, *ws_jt1, *ws_jt2;
+    /* colour cache (contact_engine_gpu_color_cache.py:26-54) and the colour grouping it reuses */
+    int cached_pairs, cached_colors, has_colors;
+    int *cached_a, *cached_b;
+    float *cached_mass;
+    int cached_N;
+    int *porder, *cstart, *ccount;
+    int hits, misses;
+    /* diagnostics of the last substep */
+    int n_contacts, n_kept, n_pairs, n_colors, seg_overflow;
+} col_engine_t;
+
+OR_API void *or_col_create(int mode, int vit, int pit, int mx, float mu, float t2d, int cap, int N)
+{
+    col_engine_t *e = calloc(1, sizeof *e);
+    e->mode = mode; e->vit = vit; e->pit = pit; e->mx = mx; e->mu = mu; e->t2d = t2d; e->cap = cap;
+    e->ws_keys = malloc(sizeof(int64_t) * cap);
+    e->ws_jn = malloc(sizeof(float) * cap); e->ws_jt1 = malloc(sizeof(float) * cap); e->ws_jt2 = malloc(sizeof(float) * cap);
+    e->cached_a = malloc(sizeof(int) * cap); e->cached_b = malloc(sizeof(int) * cap);
+    e->cached_mass = malloc(sizeof(float) * (N > 0 ? N : 1)); e->cached_N = N;
+    e->porder = malloc(sizeof(int) * cap); e->cstart = calloc(512, sizeof(int)); e->ccount = calloc(512, sizeof(int));
+    e->cached_pairs = -1;
+    return e;
+}
+OR_API void or_col_destroy(void *h)
+{
+    col_engine_t *e = h;
+    if (!e) return;
+    free(e->ws_keys); free(e->ws_jn); free(e->ws_jt1); free(e->ws_jt2);
+    free(e->cached_a); free(e->cached_b); free(e->cached_mass); free(e->porder); free(e->cstart); free(e->ccount);
+    free(e);
+}
+OR_API void or_col_stats(void *h, int *out)
+{
+    col_engine_t *e = h;
+    out[0] = e->n_contacts; out[1] = e->n_kept; out[2] = e->n_pairs; out[3] = e->n_colors;
+    out[4] = e->hits; out[5] = e->misses; out[6] = e->seg_overflow;
+}
+
+/* _planar, COL:585-590: float32 difference promoted to float64, contraction off */
+static inline void planar(v3 p, v3 ref, const double *u, const double *w, double *r)
+{
+    float dx = p.x - ref.x, dy = p.y - ref.y, dz = p.z - ref.z;
+    double ax = dx, ay = dy, az = dz;
+    r[0] = (ax * u[0] + ay * u[1]) + az * u[2];
+    r[1] = (ax * w[0] + ay * w[1]) + az * w[2];
+}
+
+/* k_select, COL:651-728: one body-pair segment of L contacts (pair-sorted positions i..i+L-1,
+ * feature indices gorder[]).  Keeps <= mx points, E-optimal, deepest first; moves every dropped
+ * normal impulse onto the nearest kept point in the contact plane. */
+static void select_segment(int i, int L, int mx, const int *gorder, const int *cbi, const float *cpA,
+                           const float *cn, const float *cpen, const float *xc, const double *jn_in, int *keep,
+                           double *jn_out, int *overflow)
+{
+    if (L <= mx) {
+        for (int t = 0; t < L; ++t) { int g = gorder[i + t]; keep[g] = 1; jn_out[g] = jn_in[g]; }
+        return;
+    }
+    if (L > 1024 || mx > 8) {
+        (*overflow)++;
+        for (int t = 0; t < L; ++t) { int g = gorder[i + t]; keep[g] = 1; jn_out[g] = jn_in[g]; }
+        return;
+    }
+    int deep = 0;
+    float dbest = cpen[gorder[i]];
+    for (int t = 1; t < L; ++t) {
+        float p = cpen[gorder[i + t]];
+        if (p > dbest) { dbest = p; deep = t; }
+    }
+    int gd = gorder[i + deep];
+    v3 nr = ld3(cn, gd);
+    double ax = 1.0, ay = 0.0, az = 0.0;
+    if (fabsf(nr.x) >= 0.9f) { ax = 0.0; ay = 1.0; az = 0.0; }
+    double n0 = nr.x, n1 = nr.y, n2 = nr.z;
+    double dn = (ax * n0 + ay * n1) + az * n2;
+    double u0 = ax - dn * n0, u1 = ay - dn * n1, u2 = az - dn * n2;
+    double ln = sqrt((u0 * u0 + u1 * u1) + u2 * u2);
+    double u[3] = {u0 / ln, u1 / ln, u2 / ln};
+    double w[3] = {n1 * u[2] - n2 * u[1], n2 * u[0] - n0 * u[2], n0 * u[1] - n1 * u[0]};
+    v3 ref = ld3(xc, cbi[gd]);
+    double rd[2];
+    planar(ld3(cpA, gd), ref, u, w, rd);
+    double S00 = rd[0] * rd[0], S01 = rd[0] * rd[1], S10 = rd[1] * rd[0], S11 = rd[1] * rd[1];
+    int pick[8];
+    pick[0] = deep;
+    for (int k = 1; k < mx; ++k) {
+        double sbest = -1.0e300;
+        int tbest = -1;
+        double c00 = 0, c01 = 0, c10 = 0, c11 = 0;
+        for (int t = 0; t < L; ++t) {
+            int taken = 0;
+            for (int q = 0; q < k; ++q) if (pick[q] == t) taken = 1;
+            if (taken) continue;
+            double rt[2];
+            planar(ld3(cpA, gorder[i + t]), ref, u, w, rt);
+            double a00 = S00 + rt[0] * rt[0], a01 = S01 + rt[0] * rt[1];
+            double a10 = S10 + rt[1] * rt[0], a11 = S11 + rt[1] * rt[1];
+            double tr = a00 + a11;
+            double det = a00 * a11 - a01 * a10;
+            double disc = fmax(tr * tr / 4.0 - det, 0.0);
+            double lam = tr / 2.0 - sqrt(disc);
+            double sc = fmin((double)(k + 1), lam);
+            if (sc > sbest) { sbest = sc; tbest = t; c00 = a00; c01 = a01; c10 = a10; c11 = a11; }
+        }
+        if (tbest < 0)  /* only with non-finite scores: first free point */
+            for (int t = L - 1; t >= 0; --t) {
+                int taken = 0;
+                for (int q = 0; q < k; ++q) if (pick[q] == t) taken = 1;
+                if (!taken) tbest = t;
+            }
+        pick[k] = tbest;
+        S00 = c00; S01 = c01; S10 = c10; S11 = c11;
+    }
+    for (int k = 0; k < mx; ++k) { int g = gorder[i + pick[k]]; keep[g] = 1; jn_out[g] = 0.0; }
+    for (int t = 0; t < L; ++t) {
+        double rt[2];
+        planar(ld3(cpA, gorder[i + t]), ref, u, w, rt);
+        double dbest2 = 1.0e300;
+        int kbest = 0;
+        for (int k = 0; k < mx; ++k) {
+            double rk[2];
+            planar(ld3(cpA, gorder[i + pick[k]]), ref, u, w, rk);
+            double e0 = rt[0] - rk[0], e1 = rt[1] - rk[1], d2 = e0 * e0 + e1 * e1;
+            if (d2 < dbest2) { dbest2 = d2; kbest = k; }
+        }
+        int gk = gorder[i + pick[kbest]];
+        jn_out[gk] = jn_out[gk] + jn_in[gorder[i + t]];
+    }
+}
+
+/* JP colouring of the pair graph, COL:1178-1208 (k_prio, k_clear_claim, k_claim, k_win) plus the
+ * stable grouping by colour.  Returns the colour count. */
+static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int *pbj, const float *invM)
+{
+    int *col = malloc(sizeof(int) * (P > 0 ? P : 1));
+    int64_t *key = malloc(sizeof(int64_t) * (P > 0 ? P : 1));
+    int64_t *claim = malloc(sizeof(int64_t) * (N > 0 ? N : 1));
+    for (int p = 0; p < P; ++p) { col[p] = -1; key[p] = jp_priority(p); }
+    int cur = 0;
+    for (;;) {
+        for (int i = 0; i < N; ++i) claim[i] = INT64_MAX;
+        for (int p = 0; p < P; ++p) {
+            if (col[p] >= 0) continue;
+            int bi = pbi[p], bj = pbj[p];
+            if (invM[bi] > 0.0f && key[p] < claim[bi]) claim[bi] = key[p];
+            if (bj >= 0 && invM[bj] > 0.0f && key[p] < claim[bj]) claim[bj] = key[p];
+        }
+        int left = 0;
+        /* every win test reads the claims of this round only (the claim kernel finished first) */
+        int *won = malloc(sizeof(int) * (P > 0 ? P : 1));
+        for (int p = 0; p < P; ++p) {
+            won[p] = 0;
+            if (col[p] >= 0) continue;
+            int bi = pbi[p], bj = pbj[p], ok = 1;
+            if (invM[bi] > 0.0f && claim[bi] != key[p]) ok = 0;
+            if (bj >= 0 && invM[bj] > 0.0f && claim[bj] != key[p]) ok = 0;
+            if (ok) won[p] = 1; else left++;
+        }
+        for (int p = 0; p < P; ++p) if (won[p]) col[p] = cur;
+        free(won);
+        cur++;
+        if (left == 0) break;
+        if (cur > P) break;
+    }
+    /* stable counting sort by colour -> porder, ccount, cstart (exclusive scan) */
+    for (int c = 0; c < 512; ++c) e->ccount[c] = 0;
+    for (int p = 0; p < P; ++p) if (col[p] < 512) e->ccount[col[p]]++;
+    int acc = 0;
+    for (int c = 0; c < cur && c < 512; ++c) { e->cstart[c] = acc; acc += e->ccount[c]; }
+    int *fill = calloc(512, sizeof(int));
+    for (int p = 0; p < P; ++p) if (col[p] < 512) e->porder[e->cstart[col[p]] + fill[col[p]]++] = p;
+    free(fill); free(col); free(key); free(claim);
+    return cur;
+}
+
+/* pair-chunk velocity sweep of one pair: COL:413-490 (slip basis) or
+ * contact_engine_gpu_fixed_frame.py:7-77 (normal-derived fixed frame) */
+static void chunk_velocity(int fixed_frame, int p, const int *pidx, const int *pstart, const int *pcount,
+                           const int *pbi, const int *pbj, const float *cpA, const float *cpB, const float *cn,
+                           float *jn, float *jt1, float *jt2, const float *xc, float *v, float *w,
+                           const float *invIw, const float *invM, float mu, float t2d)
+{
+    int fvt = g_fv[FV_SITE_VT], ft1 = g_fv[FV_SITE_T1], fmag = g_fv[FV_SITE_MAG], fjt = g_fv[FV_SITE_JT];
+    int st = pstart[p], n = pcount[p], bi = pbi[p], bj = pbj[p];
+    float iMA = invM[bi];
+    m33 IA = ldm(invIw, bi), IB = IA;
+    v3 vA = ld3(v, bi), wA = ld3(w, bi);
+    float iMB = 0.0f;
+    v3 vB = V(0, 0, 0), wB = V(0, 0, 0);
+    if (bj >= 0) { iMB = invM[bj]; IB = ldm(invIw, bj); vB = ld3(v, bj); wB = ld3(w, bj); }
+    for (int k = 0; k < n; ++k) {
+        int c = pidx[st + k];
+        v3 nrm = ld3(cn, c);
+        v3 rA = vsub(ld3(cpA, c), ld3(xc, bi));
+        v3 va = vadd(vA, cross3(wA, rA));
+        v3 vb = V(0, 0, 0), rB = V(0, 0, 0);
+        if (bj >= 0) { rB = vsub(ld3(cpB, c), ld3(xc, bj)); vb = vadd(vB, cross3(wB, rB)); }
+        v3 vrel = vsub(va, vb);
+        float vn = dot3(vrel, nrm);
+        v3 vt = V(msub(fvt, vrel.x, vn, nrm.x), msub(fvt, vrel.y, vn, nrm.y), msub(fvt, vrel.z, vn, nrm.z));
+        float mt = len3(vt);
+        v3 t1;
+        if (!fixed_frame) {
+            t1 = vdivs(vt, mt);
+        }
+        if (fixed_frame || mt <= 5e-3f) {
+            v3 aa = V(1.0f, 0.0f, 0.0f);
+            if (fabsf(nrm.x) >= 0.9f) aa = V(0.0f, 1.0f, 0.0f);
+            float dd = dot3(aa, nrm);
+            t1 = vnormalize(V(msub(ft1, aa.x, dd, nrm.x), msub(ft1, aa.y, dd, nrm.y), msub(ft1, aa.z, dd, nrm.z)));
+        }
+        v3 t2 = cross3(nrm, t1);
+        v3 rnA = cross3(rA, nrm);
+        float meff = iMA + dot3(rnA, matvec(&IA, rnA));
+        if (bj >= 0) {
+            v3 rnB = cross3(rB, nrm);
+            meff = (meff + iMB) + dot3(rnB, matvec(&IB, rnB));
+        }
+        if (!(meff >= 1e-12f)) continue;
+        float dj = -vn / meff;
+        float nw = fmaxf(0.0f, jn[c] + dj);
+        dj = nw - jn[c];
+        jn[c] = nw;
+        v3 Jn = vscale(nrm, dj);
+        if (iMA > 0.0f) {
+            vA = V(fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z));
+            wA = vadd(wA, matvec(&IA, cross3(rA, Jn)));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = V(fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z));
+            wB = vsub(wB, matvec(&IB, cross3(rB, Jn)));
+        }
+        va = vadd(vA, cross3(wA, rA));
+        vb = V(0, 0, 0);
+        if (bj >= 0) vb = vadd(vB, cross3(wB, rB));
+        vrel = vsub(va, vb);
+        v3 rtA1 = cross3(rA, t1);
+        float meft1 = iMA + dot3(rtA1, matvec(&IA, rtA1));
+        v3 rtA2 = cross3(rA, t2);
+        float meft2 = iMA + dot3(rtA2, matvec(&IA, rtA2));
+        if (bj >= 0) {
+            v3 rtB1 = cross3(rB, t1);
+            meft1 = (meft1 + iMB) + dot3(rtB1, matvec(&IB, rtB1));
+            v3 rtB2 = cross3(rB, t2);
+            meft2 = (meft2 + iMB) + dot3(rtB2, matvec(&IB, rtB2));
+        }
+        if (!(meft1 >= 1e-12f) || !(meft2 >= 1e-12f)) continue;
+        float o1 = jt1[c], o2 = jt2[c];
+        float a1 = o1 - dot3(vrel, t1) / meft1;
+        float a2 = o2 - dot3(vrel, t2) / meft2;
+        float mag = sqrtf(fmag ? fmaf(a1, a1, a2 * a2) : a1 * a1 + a2 * a2);
+        float lim = mu * jn[c];
+        if (mag > lim && mag > 1e-12f) { a1 = a1 * lim / mag; a2 = a2 * lim / mag; }
+        jt1[c] = a1;
+        jt2[c] = a2;
+        float e1 = a1 - o1, e2 = t2d * (a2 - o2);
+        v3 Jt;
+        if (fjt) Jt = V(fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z));
+        else Jt = vadd(vscale(t1, e1), vscale(t2, e2));
+        if (iMA > 0.0f) {
+            vA = V(fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z));
+            wA = vadd(wA, matvec(&IA, cross3(rA, Jt)));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = V(fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z));
+            wB = vsub(wB, matvec(&IB, cross3(rB, Jt)));
+        }
+    }
+    if (iMA > 0.0f) { st3(v, bi, vA); st3(w, bi, wA); }
+    if (bj >= 0 && iMB > 0.0f) { st3(v, bj, vB); st3(w, bj, wB); }
+}
+
+/* position chunk, COL:510-554 */
+static void chunk_position(int p, const int *pidx, const int *pstart, const int *pcount, const int *pbi,
+                           const int *pbj, const float *cpA, const float *cpB, const float *cn, const float *cpen,
+                           float *jp, const float *xc, float *pv, float *po, const float *invIw, const float *invM,
+                           float dt)
+{
+    int saved[32];
+    if (g_pos_override) { memcpy(saved, g_fv, sizeof saved); memcpy(g_fv, g_fv_pos, sizeof saved); }
+    int fvu = g_fv[FV_SITE_VUPD], fwu = g_fv[FV_SITE_WUPD], fb = g_fv[FV_SITE_BIAS];
+    int st = pstart[p], n = pcount[p], bi = pbi[p], bj = pbj[p];
+    float iMA = invM[bi];
+    m33 IA = ldm(invIw, bi), IB = IA;
+    v3 pvA = ld3(pv, bi), poA = ld3(po, bi);
+    float iMB = 0.0f;
+    v3 pvB = V(0, 0, 0), poB = V(0, 0, 0);
+    if (bj >= 0) { iMB = invM[bj]; IB = ldm(invIw, bj); pvB = ld3(pv, bj); poB = ld3(po, bj); }
+    for (int k = 0; k < n; ++k) {
+        int c = pidx[st + k];
+        v3 nrm = ld3(cn, c);
+        v3 rA = vsub(ld3(cpA, c), ld3(xc, bi));
+        v3 rel = vadd(pvA, cross3(poA, rA));
+        v3 rB = V(0, 0, 0);
+        if (bj >= 0) { rB = vsub(ld3(cpB, c), ld3(xc, bj)); rel = vsub(rel, vadd(pvB, cross3(poB, rB))); }
+        v3 rnA = cross3(rA, nrm);
+        float meff = iMA + dot3(rnA, matvec(&IA, rnA));
+        if (bj >= 0) {
+            v3 rnB = cross3(rB, nrm);
+            meff = (meff + iMB) + dot3(rnB, matvec(&IB, rnB));
+        }
+        if (!(meff >= 1e-12f)) continue;
+        float bias = fb == 0 ? K_BETA * fmaxf(cpen[c] - K_SLOP, 0.0f) / dt
+                   : fb == 1 ? K_BETA * (fmaxf(cpen[c] - K_SLOP, 0.0f) / dt)
+                             : (K_BETA / dt) * fmaxf(cpen[c] - K_SLOP, 0.0f);
+        float dj = (bias - dot3(rel, nrm)) / meff;
+        float nw = fmaxf(0.0f, jp[c] + dj);
+        dj = nw - jp[c];
+        jp[c] = nw;
+        v3 Jn = vscale(nrm, dj);
+        if (iMA > 0.0f) {
+            pvA = V(mad(fvu, Jn.x, iMA, pvA.x), mad(fvu, Jn.y, iMA, pvA.y), mad(fvu, Jn.z, iMA, pvA.z));
+            v3 d = matvec(&IA, cross3(rA, Jn));
+            poA = vadd(poA, d);
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            pvB = V(msub(fvu, pvB.x, Jn.x, iMB), msub(fvu, pvB.y, Jn.y, iMB), msub(fvu, pvB.z, Jn.z, iMB));
+            poB = vsub(poB, matvec(&IB, cross3(rB, Jn)));
+        }
+    }
+    (void)fwu;
+    if (iMA > 0.0f) { st3(pv, bi, pvA); st3(po, bi, poA); }
+    if (bj >= 0 && iMB > 0.0f) { st3(pv, bj, pvB); st3(po, bj, poB); }
+    if (g_pos_override) memcpy(g_fv, saved, sizeof saved);
+}
+
+/* apply_warm, contact_engine_gpu_applied_warm.py:5-54 */
+static void apply_warm_pair(int p, const int *pidx, const int *pstart, const int *pcount, const int *pbi,
+                            const int *pbj, const float *cpA, const float *cpB, const float *cn, const float *jn,
+                            const float *jt1, const float *jt2, const float *xc, float *v, float *w,
+                            const float *invIw, const float *invM)
+{
+    int fimp = g_fv[FV_SITE_IMP];
+    int a = pbi[p], b = pbj[p];
+    v3 va = ld3(v, a), wa = ld3(w, a), vb = V(0, 0, 0), wb = V(0, 0, 0);
+    if (b >= 0) { vb = ld3(v, b); wb = ld3(w, b); }
+    m33 Ia = ldm(invIw, a), Ib;
+    if (b >= 0) Ib = ldm(invIw, b);
+    for (int k = 0; k < pcount[p]; ++k) {
+        int c = pidx[pstart[p] + k];
+        v3 n = ld3(cn, c);
+        v3 axis = V(1.0f, 0.0f, 0.0f);
+        if (fabsf(n.x) >= 0.9f) axis = V(0.0f, 1.0f, 0.0f);
+        float dd = dot3(axis, n);
+        v3 t1 = vnormalize(V(fmaf(-dd, n.x, axis.x), fmaf(-dd, n.y, axis.y), fmaf(-dd, n.z, axis.z)));
+        v3 t2 = cross3(n, t1);
+        v3 imp;
+        if (fimp) imp = V(fmaf(jt2[c], t2.x, fmaf(jn[c], n.x, jt1[c] * t1.x)),
+                          fmaf(jt2[c], t2.y, fmaf(jn[c], n.y, jt1[c] * t1.y)),
+                          fmaf(jt2[c], t2.z, fmaf(jn[c], n.z, jt1[c] * t1.z)));
+        else imp = vadd(vadd(vscale(n, jn[c]), vscale(t1, jt1[c])), vscale(t2, jt2[c]));
+        if (invM[a] > 0.0f) {
+            va = V(fmaf(invM[a], imp.x, va.x), fmaf(invM[a], imp.y, va.y), fmaf(invM[a], imp.z, va.z));
+            wa = vadd(wa, matvec(&Ia, cross3(vsub(ld3(cpA, c), ld3(xc, a)), imp)));
+        }
+        if (b >= 0 && invM[b] > 0.0f) {
+            vb = V(fmaf(-invM[b], imp.x, vb.x), fmaf(-invM[b], imp.y, vb.y), fmaf(-invM[b], imp.z, vb.z));
+            wb = vsub(wb, matvec(&Ib, cross3(vsub(ld3(cpB, c), ld3(xc, b)), imp)));
+        }
+    }
+    if (invM[a] > 0.0f) { st3(v, a, va); st3(w, a, wa); }
+    if (b >= 0 && invM[b] > 0.0f) { st3(v, b, vb); st3(w, b, wb); }
+}
+
+/* One step of GraphColoredContactEngine(manifold_reduce, graph_capture, pair_chunks) (COL:1302-1375)
+ * or of ColorCacheContactEngine (contact_engine_gpu_deferred_force.py:13-64).  vgrav receives the
+ * velocity after gravity of the last substep (the contact-force reference of both engines). */
+OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *owner, float *xc, float *q, float *v,
+                       float *w, float *pv, float *po, const float *invM, const float *IbInv, const int *kin,
+                       double dt, int substeps, float *vgrav)
+{
+    col_engine_t *e = h;
+    int cap = e->cap;
+    float *invIw = malloc(sizeof(float) * 9 * (size_t)(N > 0 ? N : 1));
+    float *allp = malloc(sizeof(float) * 3 * (size_t)(nbead > 0 ? nbead : 1));
+    contacts_t c;
+    c.cap = cap;
+    c.bi = malloc(sizeof(int) * cap); c.bj = malloc(sizeof(int) * cap);
+    c.fa = malloc(sizeof(int) * cap); c.fb = malloc(sizeof(int) * cap);
+    c.pA = malloc(sizeof(float) * 3 * cap); c.pB = malloc(sizeof(float) * 3 * cap);
+    c.n = malloc(sizeof(float) * 3 * cap); c.pen = malloc(sizeof(float) * cap);
+    /* feature-ordered arrays */
+    int64_t *keys = malloc(sizeof(int64_t) * cap), *pk = malloc(sizeof(int64_t) * cap);
+    int *perm = malloc(sizeof(int) * cap), *gorder = malloc(sizeof(int) * cap);
+    int *tbi = malloc(sizeof(int) * cap), *tbj = malloc(sizeof(int) * cap);
+    float *tpA = malloc(sizeof(float) * 3 * cap), *tpB = malloc(sizeof(float) * 3 * cap);
+    float *tn = malloc(sizeof(float) * 3 * cap), *tpen = malloc(sizeof(float) * cap);
+    double *jn_in = malloc(sizeof(double) * cap), *jn_red = malloc(sizeof(double) * cap);
+    float *jt1_in = malloc(sizeof(float) * cap), *jt2_in = malloc(sizeof(float) * cap);
+    int *keep = malloc(sizeof(int) * cap);
+    /* kept arrays */
+    int64_t *okeys = malloc(sizeof(int64_t) * cap);
+    int *sbi = malloc(sizeof(int) * cap), *sbj = malloc(sizeof(int) * cap);
+    float *spA = malloc(sizeof(float) * 3 * cap), *spB = malloc(sizeof(float) * 3 * cap);
+    float *sn = malloc(sizeof(float) * 3 * cap), *spen = malloc(sizeof(float) * cap);
+    float *jn = malloc(sizeof(float) * cap), *jt1 = malloc(sizeof(float) * cap), *jt2 = malloc(sizeof(float) * cap);
+    float *jp = malloc(sizeof(float) * cap);
+    int *pidx = malloc(sizeof(int) * cap), *pstart = malloc(sizeof(int) * cap), *pcount = malloc(sizeof(int) * cap);
+    int *pbi = malloc(sizeof(int) * cap), *pbj = malloc(sizeof(int) * cap);
+    int rc = 0;
+    for (int s = 0; s < substeps; ++s) {
+        double sdt_d = dt / substeps;
+        float sdt = (float)sdt_d;
+        body_gravity(N, v, invM, sdt);
+        body_inv_inertia(N, q, IbInv, kin, invIw);
+        bead_world(nbead, xc, q, rest, owner, allp);
+        gen_contacts(nbead, allp, owner, &c);
+        if (c.overflow) rc = 2;
+        int C = c.C;
+        e->n_contacts = C;
+        memcpy(vgrav, v, sizeof(float) * 3 * N);
+        if (C > 0) {
+            /* C2: feature key = cfa * (N*P + 1) + cfb + 1, stable sort, gather (COL:592-599, 124-134) */
+            for (int i = 0; i < C; ++i) keys[i] = (int64_t)c.fa[i] * (int64_t)(nbead + 1) + (int64_t)c.fb[i] + 1;
+            argsort_stable(keys, C, perm);
+            int64_t *skey = pk;
+            for (int i = 0; i < C; ++i) {
+                int k = perm[i];
+                skey[i] = keys[k];
+                tbi[i] = c.bi[k]; tbj[i] = c.bj[k];
+                st3(tpA, i, ld3(c.pA, k)); st3(tpB, i, ld3(c.pB, k)); st3(tn, i, ld3(c.n, k)); tpen[i] = c.pen[k];
+            }
+            /* C3: pair key = bi*(N+1) + bj + 1 over the feature order, stable sort (COL:628-649) */
+            for (int i = 0; i < C; ++i) keys[i] = (int64_t)tbi[i] * (int64_t)(N + 1) + (int64_t)tbj[i] + 1;
+            argsort_stable(keys, C, gorder);
+            /* C4: warm start by binary search in the previous kept keys (COL:601-626) */
+            for (int i = 0; i < C; ++i) {
+                jn_in[i] = 0.0; jt1_in[i] = 0.0f; jt2_in[i] = 0.0f;
+                int wn = e->ws_n, lo = 0, hi = wn - 1, hit = -1;
+                if (wn == 0) continue;
+                int64_t k = skey[i];
+                while (lo <= hi) {
+                    int mid = (lo + hi) / 2;
+                    int64_t km = e->ws_keys[mid];
+                    if (km == k) { hit = mid; lo = hi + 1; }
+                    else if (km < k) lo = mid + 1;
+                    else hi = mid - 1;
+                }
+                if (hit >= 0) { jn_in[i] = (double)e->ws_jn[hit]; jt1_in[i] = e->ws_jt1[hit]; jt2_in[i] = e->ws_jt2[hit]; }
+            }
+            /* C5: E-optimal selection per pair segment (COL:651-728); the plain engine keeps all */
+            for (int i = 0; i < C; ++i) { keep[i] = (e->mode == 2); jn_red[i] = jn_in[i]; }
+            e->seg_overflow = 0;
+            for (int i = 0; i < C && e->mode != 2;) {
+                int L = 1;
+                while (i + L < C && keys[gorder[i + L]] == keys[gorder[i]]) L++;
+                select_segment(i, L, e->mx, gorder, tbi, tpA, tn, tpen, xc, jn_in, keep, jn_red, &e->seg_overflow);
+                i += L;
+            }
+            if (e->seg_overflow) rc = 2;
+            /* C6: compaction in feature order (COL:730-751) */
+            int Ck = 0;
+            for (int i = 0; i < C; ++i) {
+                if (!keep[i]) continue;
+                okeys[Ck] = skey[i]; sbi[Ck] = tbi[i]; sbj[Ck] = tbj[i];
+                st3(spA, Ck, ld3(tpA, i)); st3(spB, Ck, ld3(tpB, i)); st3(sn, Ck, ld3(tn, i)); spen[Ck] = tpen[i];
+                jn[Ck] = (float)jn_red[i]; jt1[Ck] = jt1_in[i]; jt2[Ck] = jt2_in[i]; jp[Ck] = 0.0f;
+                Ck++;
+            }
+            e->n_kept = Ck;
+            memset(pv, 0, sizeof(float) * 3 * N); memset(po, 0, sizeof(float) * 3 * N);
+            /* C7: pairs over the kept contacts (COL:1158-1176, 341-389); in the plain engine every
+             * contact is coloured on its own (COL:1105-1137), i.e. a one-contact chunk */
+            int P = 0;
+            if (e->mode == 2) {
+                for (int i = 0; i < Ck; ++i) { pidx[i] = i; pstart[i] = i; pcount[i] = 1; pbi[i] = sbi[i]; pbj[i] = sbj[i]; }
+                P = Ck;
+            } else {
+                for (int i = 0; i < Ck; ++i) keys[i] = (int64_t)sbi[i] * (int64_t)(N + 1) + (int64_t)sbj[i] + 1;
+                argsort_stable(keys, Ck, pidx);
+            }
+            for (int i = 0; i < Ck && e->mode != 2;) {
+                int L = 1;
+                while (i + L < Ck && keys[pidx[i + L]] == keys[pidx[i]]) L++;
+                if (L > 8) { rc = 2; L = 8; }
+                pstart[P] = i; pcount[P] = L; pbi[P] = sbi[pidx[i]]; pbj[P] = sbj[pidx[i]];
+                P++;
+                int LL = 1;
+                while (i + LL < Ck && keys[pidx[i + LL]] == keys[pidx[i]]) LL++;
+                i += LL;
+            }
+            e->n_pairs = P;
+            /* C8/C9: colouring of the pair graph, reused while (P, pbi, pbj, invM) are unchanged */
+            int ncol;
+            int hit = 0;
+            if (e->mode == 1 && P == e->cached_pairs && e->has_colors) {
+                hit = 1;
+                for (int p = 0; p < P && hit; ++p) if (pbi[p] != e->cached_a[p] || pbj[p] != e->cached_b[p]) hit = 0;
+                for (int i = 0; i < N && hit; ++i) if (invM[i] != e->cached_mass[i]) hit = 0;
+            }
+            if (hit) {
+                ncol = e->cached_colors;
+                e->hits++;
+            } else {
+                ncol = color_pairs(e, P, N, pbi, pbj, invM);
+                e->has_colors = 1;
+                if (e->mode == 1) {
+                    memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
+                    memcpy(e->cached_mass, invM, sizeof(float) * N);
+                    e->cached_pairs = P; e->cached_colors = ncol; e->misses++;
+                }
+            }
+            e->n_colors = ncol;
+            /* C10-C12: the captured chunk solve (applied_warm.py:68-75, COL:1210-1226) */
+            int fixed = (e->mode == 1);
+            if (fixed)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t)
+                        apply_warm_pair(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB, sn,
+                                        jn, jt1, jt2, xc, v, w, invIw, invM);
+            for (int it = 0; it < e->vit; ++it)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t)
+                        chunk_velocity(fixed, e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB,
+                                       sn, jn, jt1, jt2, xc, v, w, invIw, invM, e->mu, e->t2d);
+            for (int it = 0; it < e->pit; ++it)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t)
+                        chunk_position(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB, sn,
+                                       spen, jp, xc, pv, po, invIw, invM, sdt);
+            /* C14: warm store (COL:1089-1093) */
+            memcpy(e->ws_keys, okeys, sizeof(int64_t) * Ck);
+            memcpy(e->ws_jn, jn, sizeof(float) * Ck); memcpy(e->ws_jt1, jt1, sizeof(float) * Ck);
+            memcpy(e->ws_jt2, jt2, sizeof(float) * Ck);
+            e->ws_n = Ck;
+        } else {
+            e->n_kept = 0; e->n_pairs = 0; e->n_colors = 0;
+            memset(pv, 0, sizeof(float) * 3 * N); memset(po, 0, sizeof(float) * 3 * N);
+            e->ws_n = 0;
+        }
+        body_integrate(N, xc, q, v, w, pv, po, invM, sdt);
+    }
+    free(invIw); free(allp);
+    free(c.bi); free(c.bj); free(c.fa); free(c.fb); free(c.pA); free(c.pB); free(c.n); free(c.pen);
+    free(keys); free(pk); free(perm); free(gorder); free(tbi); free(tbj); free(tpA); free(tpB); free(tn); free(tpen);
+    free(jn_in); free(jn_red); free(jt1_in); free(jt2_in); free(keep); free(okeys); free(sbi); free(sbj);
+    free(spA); free(spB); free(sn); free(spen); free(jn); free(jt1); free(jt2); free(jp);
+    free(pidx); free(pstart); free(pcount); free(pbi); free(pbj);
+    return rc;
+}
+
+/* test hook: k_integ alone (orientation and position), for the variant search */
+OR_API void or_integrate(int N, float *xc, float *q, const float *v, const float *w, const float *pv, const float *po,
+                         const float *invM, float dt)
+{
+    body_integrate(N, xc, q, v, w, pv, po, invM, dt);
 }

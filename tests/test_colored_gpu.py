@@ -1,0 +1,184 @@
+"""Coloured Gauss-Seidel engines on the GPU: against the reference's golden arrays, bit-exact
+against the CPU oracle, bit-identical run to run, the reference's own contract checks
+(contact_engine_gpu_colored.py:1414-1515) and host-injected failures (colour cap, barrier wait
+limit, contact capacity)."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import DIMS, DT, SCENES, lattice, stack
+
+pytestmark = pytest.mark.gpu
+NAMES = ("xc", "Rm", "vc", "om", "force")
+EXACT = {("color_cache", "stack8"): 100, ("color_cache", "lattice1000"): 40,
+         ("pair_chunks", "stack8"): 71, ("pair_chunks", "lattice1000"): 40}
+XC_TOL = {"color_cache": 1e-8, "pair_chunks": 1e-6}
+
+
+def _digests(state, force):
+    arrs = (state.xc, state.Rm, state.vc, state.om, force)
+    return [hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest() for a in arrs]
+
+
+def _make(me, engine, **kw):
+    kw.setdefault("dims", DIMS)
+    kw.setdefault("mu", 0.5)
+    if engine == "color_cache":
+        return me.ColorCacheContactEngine(**kw)
+    if engine == "pair_chunks":
+        return me.GraphColoredContactEngine(manifold_reduce=True, graph_capture=True, pair_chunks=True, **kw)
+    return me.GraphColoredContactEngine(**kw)
+
+
+@pytest.mark.parametrize("engine", ["color_cache", "pair_chunks"])
+@pytest.mark.parametrize("scene", ["stack8", "lattice1000"])
+def test_colored_against_reference(engine, scene, golden, me):
+    make, steps = SCENES[scene]
+    e = _make(me, engine, vit=40, pit=10)
+    for c in make():
+        e.add_body(c)
+    dig = golden[f"{engine}__{scene}__digest"]
+    contacts = golden[f"{engine}__{scene}__contacts"]
+    sel = list(golden[f"{engine}__{scene}__steps"])
+    exact = EXACT[(engine, scene)]
+    for t in range(steps):
+        e.step(DT, 1)
+        st = e.get_state()
+        if t < exact:
+            assert e.n_contacts == contacts[t], f"step {t}: contact count {e.n_contacts} != {contacts[t]}"
+            got = _digests(st, e.contact_forces())
+            for k, n in enumerate(NAMES):
+                assert got[k] == dig[t, k].tobytes(), f"{engine} {scene} step {t}: {n} differs from the reference"
+        elif t in sel:
+            g = golden[f"{engine}__{scene}__xc"][sel.index(t)]
+            assert np.abs(st.xc.astype(np.float64) - g).max() < XC_TOL[engine], f"step {t}"
+
+
+def _random_scene(seed, n_cols=3):
+    rng = np.random.default_rng(seed)
+    centers, dens = [], []
+    for ix in range(n_cols):
+        for iy in range(n_cols):
+            base = np.array([ix * 0.33, iy * 0.33, 0.0]) + np.r_[rng.uniform(-0.02, 0.02, 2), 0]
+            for k in range(3):
+                centers.append(list(base + [rng.uniform(-0.03, 0.03), rng.uniform(-0.03, 0.03),
+                                            0.101 + 0.205 * k + rng.uniform(0, 0.01)]))
+                dens.append(float(rng.uniform(300, 1500)))
+    return centers, dens
+
+
+@pytest.mark.parametrize("engine", ["color_cache", "pair_chunks", "plain"])
+def test_colored_matches_oracle(engine, me, oracle_mod):
+    """Jittered columns with mixed densities and two substeps: bit-exact against the oracle."""
+    centers, dens = _random_scene(3)
+    vit, pit = (16, 10) if engine != "plain" else (12, 8)
+    e = _make(me, engine, vit=vit, pit=pit, mu=0.6)
+    o = oracle_mod.ColoredOracle(mode=engine, dims=DIMS, mu=0.6, vit=vit, pit=pit)
+    for c, d in zip(centers, dens):
+        e.add_body(c, density=d)
+        o.add_body(c, density=d)
+    for t in range(60):
+        e.step(DT, 2)
+        o.step(DT, 2)
+        se, so = e.get_state(), o.get_state()
+        for n in ("xc", "Rm", "vc", "om"):
+            a, b = getattr(se, n), getattr(so, n)
+            assert a.tobytes() == b.tobytes(), f"{engine} step {t} {n}: max |d| {np.abs(a - b).max():.3e}"
+        assert e.contact_forces().tobytes() == o.contact_forces().tobytes()
+    st = o.stats()
+    assert e.n_colors == st["n_colors"] and e.n_pairs == st["n_pairs"]
+    if engine == "color_cache":
+        assert (e.color_cache_hits, e.color_cache_misses) == (st["hits"], st["misses"])
+
+
+@pytest.mark.parametrize("blocks", [1, 4])
+def test_colored_runs_repeat_bit_identical(blocks, me):
+    runs = []
+    for _ in range(2):
+        e = _make(me, "color_cache", vit=16, pit=8, solve_blocks=blocks)
+        for c in lattice(300):
+            e.add_body(c)
+        for _ in range(30):
+            e.step(DT, 2)
+        runs.append(e.get_state())
+    for n in ("xc", "Rm", "vc", "om"):
+        assert getattr(runs[0], n).tobytes() == getattr(runs[1], n).tobytes(), n
+
+
+def test_single_cta_equals_grid_solve(me):
+    """The persistent solve on one CTA (block barriers) and on several CTAs (grid barrier) give
+    the same bits: within a colour the written bodies are disjoint."""
+    states = []
+    for blocks in (1, 3, 8):
+        e = _make(me, "color_cache", vit=16, pit=8, solve_blocks=blocks)
+        for c in lattice(400):
+            e.add_body(c)
+        for _ in range(25):
+            e.step(DT, 1)
+        states.append(e.get_state())
+    for s in states[1:]:
+        assert s.xc.tobytes() == states[0].xc.tobytes() and s.om.tobytes() == states[0].om.tobytes()
+
+
+def test_contract_checks(me):
+    """contact_engine_gpu_colored.py:1414-1515 on the engines built here."""
+    for engine in ("plain", "pair_chunks", "color_cache"):
+        e = _make(me, engine)
+        assert isinstance(e, me.ContactEngine)
+        for c in stack(8):
+            e.add_body(c)
+        for _ in range(400):
+            e.step(1 / 240)
+        st = e.get_state()
+        ke = float(np.sum(0.5 * e._M[:, None] * st.vc ** 2))
+        zs = sorted(st.xc[:, 2])
+        seps = [zs[i + 1] - zs[i] for i in range(7)]
+        assert ke < 0.5 and all(0.15 < s < 0.25 for s in seps), engine
+        if engine != "plain":
+            assert e.n_colors < 8
+        e2 = _make(me, engine)
+        e2.add_body([0, 0, 0.101])
+        for _ in range(200):
+            e2.step(1 / 240)
+        Fz = e2.contact_forces()[0, 2]
+        Mg = e2._M[0] * 9.81
+        assert abs(Fz - Mg) / Mg * 100 < (8 if engine == "plain" else 1), engine
+    e3 = _make(me, "color_cache")
+    e3.add_body([0, 0, 0.5])
+    e3.set_kinematic(0, [0, 0, 0.5])
+    for _ in range(120):
+        e3.step(1 / 240)
+    z_stay = e3.get_state().xc[0, 2]
+    e3.set_kinematic(0, [0.1, 0, 0.5])
+    e3.step(1 / 240)
+    assert abs(z_stay - 0.5) < 1e-6 and abs(e3.get_state().xc[0, 0] - 0.1) < 1e-6
+
+
+def test_color_cap_overflow_raises(me):
+    e = _make(me, "color_cache", color_cap=1)
+    for c in stack(4):
+        e.add_body(c)
+    for _ in range(12):
+        try:
+            e.step(DT)
+        except RuntimeError as err:
+            assert "colour" in str(err)
+            return
+    e.step(DT)
+    with pytest.raises(RuntimeError, match="colour"):
+        e.step(DT)
+
+
+def test_barrier_wait_limit_reports_timeout(me):
+    """A grid barrier that waits longer than its limit sets an error bit and the kernel returns;
+    the host raises and the context stays usable (a 1 ns limit makes every wait run out)."""
+    import torch
+    e = _make(me, "color_cache", vit=4, pit=2, solve_blocks=4, barrier_timeout_s=1e-9)
+    for c in lattice(200):
+        e.add_body(c)
+    with pytest.raises(RuntimeError, match="barrier"):
+        for _ in range(10):
+            e.step(DT)
+    x = torch.ones(4, device="cuda") * 2
+    assert float(x.sum()) == 8.0
