@@ -126,11 +126,11 @@ class GraphColoredContactEngine(_BeadEngineBase):
         self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(cap),
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
                            cached_a=i32(pcap), cached_b=i32(pcap), cached_mass=f32(N), cache_state=i32(8),
-                           barrier=torch.zeros(2, dtype=torch.int32, device=dev))
+                           barrier=torch.zeros(2, dtype=torch.int32, device=dev), prep=f32(16 * cap))
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
-            "cached_b", "cached_mass", "cache_state", "barrier")))
+            "cached_b", "cached_mass", "cache_state", "barrier", "prep")))
         # warm store
         self.w_keys, self.w_imp, self.w_n = i64(cap), torch.zeros((cap, 4), dtype=torch.float32, device=dev), i32(1)
         self.c_warm = _lib.Warm(cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
@@ -164,6 +164,84 @@ class GraphColoredContactEngine(_BeadEngineBase):
         self._graph_step(("colored", float(sdt), int(substeps)), lambda: self._launch_step(sdt, substeps))
         self._force_dt = sdt
         self._fetch_header()
+
+    # ---- staged substep with CUDA events between the stages (profiling; same launches as
+    #      b2c_color_substep, so it advances the state exactly like step(dt, 1)) ----
+    STAGES = ("predict", "beads", "grid", "contacts", "manifold", "colour", "solve", "warm_store", "integrate")
+
+    def profile_substep(self, dt):
+        """One substep launched stage by stage with CUDA events on the launching stream; returns
+        {stage: ms} once the substep has finished (the reference's _stage profile,
+        contact_engine_gpu_colored.py:1039-1048, without the device synchronisations)."""
+        if not self._built:
+            self._build()
+        self.check_errors()
+        L, b = self.L, ctypes.byref
+        stream = torch.cuda.current_stream(self.dev)
+        s = ctypes.c_void_p(stream.cuda_stream)
+        hdr = ctypes.c_void_p(_ptr(self.header))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(self.STAGES) + 1)]
+        sdt = ctypes.c_float(dt)
+        ev[0].record(stream)
+        _lib.check(L.b2c_body_predict(b(self.c_bodies), sdt, s), "predict")
+        self.vgrav.copy_(self.v)
+        self.pv.zero_()
+        self.po.zero_()
+        ev[1].record(stream)
+        _lib.check(L.b2c_bead_world(b(self.c_bodies), b(self.c_beads), b(self.c_grid), s), "beads")
+        ev[2].record(stream)
+        _lib.check(L.b2c_grid_build(b(self.c_beads), b(self.c_grid), s), "grid")
+        ev[3].record(stream)
+        _lib.check(L.b2c_bead_contacts_sorted(b(self.c_beads), b(self.c_grid), b(self.c_contacts),
+                                              b(self.c_manifold), hdr, s), "contacts")
+        ev[4].record(stream)
+        _lib.check(L.b2c_manifold_reduce(b(self.c_bodies), b(self.c_beads), b(self.c_contacts), b(self.c_manifold),
+                                         b(self.c_kept), ctypes.c_void_p(_ptr(self.k_keys)), b(self.c_pairs),
+                                         b(self.c_warm), hdr, b(self.c_params), s), "manifold")
+        ev[5].record(stream)
+        _lib.check(L.b2c_color_pairs(b(self.c_bodies), b(self.c_pairs), hdr, b(self.c_params), s), "colour")
+        ev[6].record(stream)
+        _lib.check(L.b2c_color_solve(b(self.c_bodies), b(self.c_kept), b(self.c_pairs), hdr, b(self.c_params), sdt,
+                                     s), "solve")
+        ev[7].record(stream)
+        _lib.check(L.b2c_warm_store(b(self.c_kept), ctypes.c_void_p(_ptr(self.k_keys)), b(self.c_warm), hdr, s),
+                   "warm_store")
+        ev[8].record(stream)
+        _lib.check(L.b2c_body_integrate(b(self.c_bodies), sdt, s), "integrate")
+        ev[9].record(stream)
+        self._force_dt = dt
+        self._fetch_header()
+        ev[9].synchronize()
+        return {name: ev[i].elapsed_time(ev[i + 1]) for i, name in enumerate(self.STAGES)}
+
+    def solve_bytes(self) -> dict:
+        """Algorithmic bytes of one persistent-solve launch (the last substep's counts): every SoA
+        element the sweeps read or write, counted once per sweep.  Per sweep over the colours:
+        pairs 20 B (porder, pstart, pcount, pbi, pbj), each dynamic pair endpoint 100 B (xc 12,
+        invM 4, invIw 36, v/w read 24 and write 24), each kept contact 64 B in a velocity sweep
+        (pidx 4, n 12, pA 12, pB 12, impulses read 12 and write 12) and 52 B in a position sweep
+        or the applied warm start."""
+        h = self.header_dict()
+        P, Ck = h["n_pairs"], h["n_kept"]
+        pbi = self.p_bufs["pbi"][:P].cpu().numpy()
+        pbj = self.p_bufs["pbj"][:P].cpu().numpy()
+        invM = self.invM.cpu().numpy()
+        E = int(np.sum(invM[pbi] > 0) + np.sum((pbj >= 0) & (invM[np.maximum(pbj, 0)] > 0)))
+        per_vel = 20 * P + 100 * E + 64 * Ck
+        per_pos = 20 * P + 100 * E + 52 * Ck
+        warm = per_pos if self._apply_warm else 0
+        return dict(pairs=P, kept=Ck, endpoints=E, colors=h["n_colors"],
+                    bytes=warm + self.vit * per_vel + self.pit * per_pos)
+
+    # ---- host state I/O (pinned staging) ----
+    def set_body_state(self, xc, q, v, w):
+        """Overwrite the body state from host arrays ((N,3), (N,4), (N,3), (N,3) float32; pinned
+        torch tensors are copied asynchronously on the engine's stream)."""
+        if not self._built:
+            self._build()
+        for dst, src, k in ((self.xc, xc, 3), (self.q, q, 4), (self.v, v, 3), (self.w, w, 3)):
+            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float32))
+            dst[:, :k].copy_(t, non_blocking=True)
 
     # ---- diagnostics ----
     @property

@@ -547,334 +547,8 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// 5. the persistent chunk solve
-// ---------------------------------------------------------------------------------------------
-// body state is read and written through L2 (ld.cg / st.cg): CTAs on other SMs read it after a
-// grid barrier, and L1 is not coherent across SMs
-__device__ __forceinline__ float4 ldcg4(const float *p, int i) { return __ldcg(reinterpret_cast<const float4 *>(p) + i); }
-__device__ __forceinline__ void stcg4(float *p, int i, float4 v) { __stcg(reinterpret_cast<float4 *>(p) + i, v); }
-__device__ __forceinline__ f3 ldcg3(const float *p, int i) { return xyz(ldcg4(p, i)); }
-
-struct SolveArgs {
-    const b2c_header *hdr;
-    int *err;
-    // pairs
-    const int *porder, *cstart, *ccount, *pstart, *pcount, *pidx, *pbi, *pbj;
-    // kept contacts
-    const float *cpA, *cpB, *cn;
-    float *imp;
-    // bodies
-    const float *xc, *invIw, *invM;
-    float *v, *w, *pv, *po;
-    float mu, t2d, dt;
-    int vit, pit, fixed_frame, apply_warm;
-    unsigned int *bar_count, *bar_gen;
-    long long timeout_ns;
-};
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Grid-wide barrier with a wait limit.  Returns false (and sets B2C_ERR_BARRIER_TIMEOUT) when a
-// CTA waited longer than timeout_ns; every CTA then returns at its next barrier, so the kernel
-// always ends.
-template <bool kGrid>
-__device__ __forceinline__ bool solve_barrier(const SolveArgs &a)
-{
-    if (!kGrid) {
-        __syncthreads();
-        return true;
-    }
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned int *gen = a.bar_gen;
-        const unsigned int my_gen = *gen;
-        __threadfence();
-        const unsigned int prev = atomicAdd(a.bar_count, 1u);
-        if (prev == gridDim.x - 1) {
-            atomicExch(a.bar_count, 0u);
-            __threadfence();
-            atomicAdd(a.bar_gen, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            while (*gen == my_gen) {
-                if (global_ns() - t0 > (unsigned long long)a.timeout_ns) {
-                    atomicOr(a.err, B2C_ERR_BARRIER_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*(volatile int *)a.err & B2C_ERR_BARRIER_TIMEOUT) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-// apply_warm, contact_engine_gpu_applied_warm.py:5-54
-__device__ void pair_apply_warm(const SolveArgs &a, int p)
-{
-    const int A = a.pbi[p], B = a.pbj[p];
-    const float iMA = a.invM[A], iMB = B >= 0 ? a.invM[B] : 0.0f;
-    f3 va = ldcg3(a.v, A), wa = ldcg3(a.w, A), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
-    if (B >= 0) {
-        vb = ldcg3(a.v, B);
-        wb = ldcg3(a.w, B);
-    }
-    const m3 IA = ldm(a.invIw, A);
-    m3 IB = IA;
-    if (B >= 0) IB = ldm(a.invIw, B);
-    const f3 xA = ld3(a.xc, A);
-    f3 xB{0.0f, 0.0f, 0.0f};
-    if (B >= 0) xB = ld3(a.xc, B);
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        f3 axis{1.0f, 0.0f, 0.0f};
-        if (fabsf(nrm.x) >= 0.9f) axis = f3{0.0f, 1.0f, 0.0f};
-        const float dd = dot3(axis, nrm);
-        const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, axis.x), fmaf(-dd, nrm.y, axis.y), fmaf(-dd, nrm.z, axis.z)});
-        const f3 t2 = cross3(nrm, t1);
-        const float4 im = ldcg4(a.imp, c);
-        const f3 J{fmaf(im.z, t2.x, fmaf(im.x, nrm.x, im.y * t1.x)), fmaf(im.z, t2.y, fmaf(im.x, nrm.y, im.y * t1.y)),
-                   fmaf(im.z, t2.z, fmaf(im.x, nrm.z, im.y * t1.z))};
-        if (iMA > 0.0f) {
-            va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
-            wa = add3(wa, matvec(IA, cross3(sub3(ld3(a.cpA, c), xA), J)));
-        }
-        if (B >= 0 && iMB > 0.0f) {
-            vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
-            wb = sub3(wb, matvec(IB, cross3(sub3(ld3(a.cpB, c), xB), J)));
-        }
-    }
-    if (iMA > 0.0f) {
-        stcg4(a.v, A, f4(va, 0.0f));
-        stcg4(a.w, A, f4(wa, 0.0f));
-    }
-    if (B >= 0 && iMB > 0.0f) {
-        stcg4(a.v, B, f4(vb, 0.0f));
-        stcg4(a.w, B, f4(wb, 0.0f));
-    }
-}
-
-// velocity chunk: k_fixed_frame (fixed_frame.py:7-77) or k_chunk_vel_r (COL:413-490)
-__device__ void pair_velocity(const SolveArgs &a, int p)
-{
-    const int bi = a.pbi[p], bj = a.pbj[p];
-    const float iMA = a.invM[bi];
-    const m3 IA = ldm(a.invIw, bi);
-    m3 IB = IA;
-    f3 vA = ldcg3(a.v, bi), wA = ldcg3(a.w, bi);
-    float iMB = 0.0f;
-    f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) {
-        iMB = a.invM[bj];
-        IB = ldm(a.invIw, bj);
-        vB = ldcg3(a.v, bj);
-        wB = ldcg3(a.w, bj);
-    }
-    const f3 xA = ld3(a.xc, bi);
-    f3 xB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) xB = ld3(a.xc, bj);
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        const f3 rA = sub3(ld3(a.cpA, c), xA);
-        f3 va = add3(vA, cross3(wA, rA));
-        f3 vb{0.0f, 0.0f, 0.0f}, rB{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) {
-            rB = sub3(ld3(a.cpB, c), xB);
-            vb = add3(vB, cross3(wB, rB));
-        }
-        f3 vrel = sub3(va, vb);
-        const float vn = dot3(vrel, nrm);
-        f3 t1;
-        bool axis_frame = a.fixed_frame;
-        if (!a.fixed_frame) {
-            const f3 vt{fmaf(-vn, nrm.x, vrel.x), fmaf(-vn, nrm.y, vrel.y), fmaf(-vn, nrm.z, vrel.z)};
-            const float mt = len3(vt);
-            t1 = div3(vt, mt);
-            axis_frame = mt <= 5e-3f;
-        }
-        if (axis_frame) {
-            f3 aa{1.0f, 0.0f, 0.0f};
-            if (fabsf(nrm.x) >= 0.9f) aa = f3{0.0f, 1.0f, 0.0f};
-            const float dd = dot3(aa, nrm);
-            t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
-        }
-        const f3 t2 = cross3(nrm, t1);
-        const f3 rnA = cross3(rA, nrm);
-        float meff = iMA + dot3(rnA, matvec(IA, rnA));
-        if (bj >= 0) {
-            const f3 rnB = cross3(rB, nrm);
-            meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
-        }
-        if (!(meff >= 1e-12f)) continue;
-        float4 im = ldcg4(a.imp, c);
-        float dj = -vn / meff;
-        const float nw = fmaxf(0.0f, im.x + dj);
-        dj = nw - im.x;
-        im.x = nw;
-        const f3 Jn = scale3(nrm, dj);
-        if (iMA > 0.0f) {
-            vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
-            wA = add3(wA, matvec(IA, cross3(rA, Jn)));
-        }
-        if (bj >= 0 && iMB > 0.0f) {
-            vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
-            wB = sub3(wB, matvec(IB, cross3(rB, Jn)));
-        }
-        va = add3(vA, cross3(wA, rA));
-        vb = f3{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-        vrel = sub3(va, vb);
-        const f3 rtA1 = cross3(rA, t1);
-        float meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
-        const f3 rtA2 = cross3(rA, t2);
-        float meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
-        if (bj >= 0) {
-            const f3 rtB1 = cross3(rB, t1);
-            meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
-            const f3 rtB2 = cross3(rB, t2);
-            meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
-        }
-        if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
-            const float o1 = im.y, o2 = im.z;
-            float a1 = o1 - dot3(vrel, t1) / meft1;
-            float a2 = o2 - dot3(vrel, t2) / meft2;
-            const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-            const float lim = a.mu * im.x;
-            if (mag > lim && mag > 1e-12f) {
-                a1 = a1 * lim / mag;
-                a2 = a2 * lim / mag;
-            }
-            im.y = a1;
-            im.z = a2;
-            const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
-            const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
-            if (iMA > 0.0f) {
-                vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
-                wA = add3(wA, matvec(IA, cross3(rA, Jt)));
-            }
-            if (bj >= 0 && iMB > 0.0f) {
-                vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
-                wB = sub3(wB, matvec(IB, cross3(rB, Jt)));
-            }
-        }
-        stcg4(a.imp, c, im);
-    }
-    if (iMA > 0.0f) {
-        stcg4(a.v, bi, f4(vA, 0.0f));
-        stcg4(a.w, bi, f4(wA, 0.0f));
-    }
-    if (bj >= 0 && iMB > 0.0f) {
-        stcg4(a.v, bj, f4(vB, 0.0f));
-        stcg4(a.w, bj, f4(wB, 0.0f));
-    }
-}
-
-// position chunk, k_chunk_pos_r (COL:510-554)
-__device__ void pair_position(const SolveArgs &a, int p)
-{
-    const int bi = a.pbi[p], bj = a.pbj[p];
-    const float iMA = a.invM[bi];
-    const m3 IA = ldm(a.invIw, bi);
-    m3 IB = IA;
-    f3 pvA = ldcg3(a.pv, bi), poA = ldcg3(a.po, bi);
-    float iMB = 0.0f;
-    f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) {
-        iMB = a.invM[bj];
-        IB = ldm(a.invIw, bj);
-        pvB = ldcg3(a.pv, bj);
-        poB = ldcg3(a.po, bj);
-    }
-    const f3 xA = ld3(a.xc, bi);
-    f3 xB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) xB = ld3(a.xc, bj);
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        const float4 pA4 = ld4(a.cpA, c);
-        const f3 rA = sub3(xyz(pA4), xA);
-        f3 rel = add3(pvA, cross3(poA, rA));
-        f3 rB{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) {
-            rB = sub3(ld3(a.cpB, c), xB);
-            rel = sub3(rel, add3(pvB, cross3(poB, rB)));
-        }
-        const f3 rnA = cross3(rA, nrm);
-        float meff = iMA + dot3(rnA, matvec(IA, rnA));
-        if (bj >= 0) {
-            const f3 rnB = cross3(rB, nrm);
-            meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
-        }
-        if (!(meff >= 1e-12f)) continue;
-        const float bias = B2C_BETA * fmaxf(pA4.w - B2C_SLOP, 0.0f) / a.dt;
-        float dj = (bias - dot3(rel, nrm)) / meff;
-        const float jp = __ldcg(a.imp + 4 * c + 3);
-        const float nw = fmaxf(0.0f, jp + dj);
-        dj = nw - jp;
-        __stcg(a.imp + 4 * c + 3, nw);
-        const f3 Jn = scale3(nrm, dj);
-        if (iMA > 0.0f) {
-            pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
-            poA = add3(poA, matvec(IA, cross3(rA, Jn)));
-        }
-        if (bj >= 0 && iMB > 0.0f) {
-            pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
-            poB = sub3(poB, matvec(IB, cross3(rB, Jn)));
-        }
-    }
-    if (iMA > 0.0f) {
-        stcg4(a.pv, bi, f4(pvA, 0.0f));
-        stcg4(a.po, bi, f4(poA, 0.0f));
-    }
-    if (bj >= 0 && iMB > 0.0f) {
-        stcg4(a.pv, bj, f4(pvB, 0.0f));
-        stcg4(a.po, bj, f4(poB, 0.0f));
-    }
-}
-
-template <bool kGrid>
-__global__ void __launch_bounds__(256) k_color_solve(SolveArgs a)
-{
-    const int nc = a.hdr->n_colors;
-    if (a.hdr->n_pairs == 0 || nc == 0) return;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    if (a.apply_warm) {
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_apply_warm(a, a.porder[s0 + t]);
-            if (!solve_barrier<kGrid>(a)) return;
-        }
-    }
-    for (int it = 0; it < a.vit; ++it)
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_velocity(a, a.porder[s0 + t]);
-            if (!solve_barrier<kGrid>(a)) return;
-        }
-    for (int it = 0; it < a.pit; ++it)
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_position(a, a.porder[s0 + t]);
-            if (!solve_barrier<kGrid>(a)) return;
-        }
-}
+int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
+                float dt, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------
 // 6. warm store (COL:1089-1093)
@@ -964,77 +638,6 @@ int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_c
     return check_launch("color_pairs");
 }
 
-static int max_coresident_blocks()
-{
-    static int cached = -1;
-    if (cached < 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve<true>, 256, 0);
-        cached = std::max(1, sms * std::max(per, 1));
-    }
-    return cached;
-}
-
-int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
-                float dt, cudaStream_t s)
-{
-    SolveArgs a;
-    a.hdr = hdr;
-    a.err = &hdr->error;
-    a.porder = pr->porder;
-    a.cstart = pr->cstart;
-    a.ccount = pr->ccount;
-    a.pstart = pr->pstart;
-    a.pcount = pr->kcount;
-    a.pidx = pr->pidx;
-    a.pbi = pr->pbi;
-    a.pbj = pr->pbj;
-    a.cpA = kept->pA;
-    a.cpB = kept->pB;
-    a.cn = kept->n;
-    a.imp = kept->imp;
-    a.xc = b->xc;
-    a.invIw = b->invIw;
-    a.invM = b->invM;
-    a.v = b->v;
-    a.w = b->w;
-    a.pv = b->pv;
-    a.po = b->po;
-    a.mu = p->mu;
-    a.t2d = p->t2d;
-    a.dt = dt;
-    a.vit = p->vit;
-    a.pit = p->pit;
-    a.fixed_frame = (p->flags & B2C_COLOR_FIXED_FRAME) ? 1 : 0;
-    a.apply_warm = (p->flags & B2C_COLOR_APPLY_WARM) ? 1 : 0;
-    a.bar_count = pr->barrier;
-    a.bar_gen = pr->barrier + 1;
-    a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
-    int nblocks = p->solve_blocks > 0 ? p->solve_blocks : (b->n + 255) / 256;
-    nblocks = std::max(1, std::min(nblocks, max_coresident_blocks()));
-    if (nblocks == 1) {
-        k_color_solve<false><<<1, 256, 0, s>>>(a);
-        return check_launch("color_solve");
-    }
-    cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nblocks);
-    cfg.blockDim = dim3(256);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve<true>, a);
-    if (e != cudaSuccess) {
-        set_error("color_solve: cooperative launch of %d blocks: %s", nblocks, cudaGetErrorString(e));
-        return B2C_ECUDA;
-    }
-    return check_launch("color_solve");
-}
 
 int warm_store(const b2c_contacts *kept, const int64_t *kept_keys, b2c_warm *warm, const b2c_header *hdr, int use,
                cudaStream_t s)
@@ -1090,7 +693,7 @@ extern "C" int32_t b2c_color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_heade
 extern "C" int32_t b2c_color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr,
                                    const b2c_color_params *p, float dt, b2c_stream s)
 {
-    if (!b || !kept || !pr || !hdr || !color_params_ok(p) || !(dt > 0.0f) || !pr->barrier) {
+    if (!b || !kept || !pr || !hdr || !color_params_ok(p) || !(dt > 0.0f) || !pr->barrier || !pr->prep) {
         b2c::set_error("b2c_color_solve: bad argument");
         return B2C_EARG;
     }
@@ -1114,7 +717,7 @@ extern "C" int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads
 {
     if (!b || !beads || !beads->bead_start || !g || !c || !m || !kept || !kept_keys || !pr || !warm || !hdr ||
         !color_params_ok(p) || !vgrav || !(dt > 0.0f) || kept->capacity < c->capacity ||
-        warm->capacity < kept->capacity) {
+        warm->capacity < kept->capacity || !pr->barrier || !pr->prep) {
         b2c::set_error("b2c_color_substep: bad argument");
         return B2C_EARG;
     }

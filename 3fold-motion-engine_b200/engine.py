@@ -132,6 +132,7 @@ class _BeadEngineBase:
         self._built = False
         self.n_graph_captures = 0
         self._graphs = {}
+        self.kernels_per_step = {}  # graph key -> kernel nodes of the captured step
         self._force_dt = None
 
     # ---- construction (data in) ----
@@ -258,12 +259,14 @@ class _BeadEngineBase:
             g.replay()
             return
         launch()
-        g = torch.cuda.CUDAGraph()
+        g = torch.cuda.CUDAGraph(keep_graph=True)
         cs = torch.cuda.Stream(self.dev)
         cs.wait_stream(torch.cuda.current_stream(self.dev))
         with torch.cuda.graph(g, stream=cs):
             launch()
         torch.cuda.current_stream(self.dev).wait_stream(cs)
+        self.kernels_per_step[key] = int(self.L.b2c_graph_kernel_nodes(ctypes.c_void_p(g.raw_cuda_graph())))
+        g.instantiate()
         if len(self._graphs) >= 8:
             self._graphs.clear()
         self._graphs[key] = g

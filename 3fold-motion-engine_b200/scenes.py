@@ -1,0 +1,74 @@
+"""Seeded synthetic scenes (the reference uses no dataset for this path).
+
+* stack / lattice -- the reference's own fixtures (scripts/colored_vs_jacobi.py:100-112): boxes
+  (0.3, 0.3, 0.2) resting-pitch apart in z, 0.35 m apart in x and y, dropped onto the ground.
+* unit_cube_stack -- 16 unit cubes with 1 mm seeded xy jitter on the ground (the plain
+  relaxed-Jacobi workload: 1 m cubes of 1 kg, i.e. density 1).
+* random_boxes -- N boxes with per-axis edges uniform in [lo, hi], dropped from seeded uniform
+  positions in an X x Y x Z volume without initial overlap, per-body friction uniform in a range
+  (the 10 000-box coloured Gauss-Seidel workload).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PITCH = 0.205
+
+
+def stack(K):
+    return [[0.0, 0.0, 0.101 + k * PITCH] for k in range(K)]
+
+
+def lattice(n_target, layers=2):
+    side = int(np.ceil(np.sqrt(n_target / layers)))
+    out = []
+    for lz in range(layers):
+        for iy in range(side):
+            for ix in range(side):
+                out.append([ix * 0.35, iy * 0.35, 0.101 + lz * PITCH])
+    return out[:n_target]
+
+
+def unit_cube_stack(K=16, seed=0):
+    rng = np.random.default_rng(seed)
+    j = rng.uniform(-1e-3, 1e-3, size=(K, 2))
+    return [[float(j[k, 0]), float(j[k, 1]), 0.501 + 1.001 * k] for k in range(K)]
+
+
+def random_boxes(n=10000, edge=(0.2, 0.6), box=(20.0, 20.0, 10.0), mu=(0.3, 0.8), density=1000.0,
+                 seed_size=1, seed_pos=2, seed_mu=3, max_tries=200):
+    """Returns dict(dims (n,3), centers (n,3), mu (n,), density (n,)).  Centres: x, y uniform in
+    [-X/2, X/2], z uniform in [h/2, Z] with h the box height, rejection-sampled against the
+    axis-aligned boxes already placed (a uniform grid of cell 2*max edge makes it O(n))."""
+    rs, rp, rm = (np.random.default_rng(s) for s in (seed_size, seed_pos, seed_mu))
+    dims = rs.uniform(edge[0], edge[1], size=(n, 3))
+    cell = 2.0 * edge[1]
+    grid = {}
+    centers = np.zeros((n, 3))
+    for i in range(n):
+        h = dims[i]
+        for _ in range(max_tries):
+            c = np.array([rp.uniform(-box[0] / 2, box[0] / 2), rp.uniform(-box[1] / 2, box[1] / 2),
+                          rp.uniform(h[2] / 2, box[2])])
+            key = tuple((c // cell).astype(int))
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                            if np.all(np.abs(centers[j] - c) < (dims[j] + h) / 2):
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                break
+        else:
+            raise RuntimeError("random_boxes: could not place a box without overlap; enlarge the volume")
+        centers[i] = c
+        grid.setdefault(key, []).append(i)
+    return dict(dims=dims, centers=centers, mu=rm.uniform(mu[0], mu[1], size=n), density=np.full(n, density))

@@ -1,0 +1,346 @@
+"""Throughput benchmark of the contact-solve hot path: body-steps/s on one B200 (or N replicas).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
+
+One "step" is one ContactEngine.step(dt, substeps) of the whole scene.  W warm-up steps run
+first (untimed; the scene settles into its contact-rich regime), then exactly K steps are timed
+with CUDA events on the engine's stream, bracketed by a barrier and a device synchronise, and
+the L2 is flushed (a 256 MiB write) between timed steps, outside the events.  With N > 1 every
+rank runs an independent replica (the single-scene solve does not shard: replicas only) and the
+time is the max over ranks.  Rank 0 prints one JSON line.
+
+`e2e` is the same metric through the public API with the body state in pinned host memory:
+every step uploads the state (set_body_state), steps, and downloads it again.
+
+`--impl reference` times the reference algorithm's CPU restatement (the oracle; Warp, which the
+reference's own CPU path needs, is not installed) on the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # the reference's ColorCache timing fixture (reports/innovation_stack_color_cache_l4.json):
+    # lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5, 40 velocity / 20 position sweeps,
+    # 1 substep, dt 1/240
+    "colorcache_lattice10k": dict(engine="color_cache", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5,
+                                  vit=40, pit=20, substeps=1, dt=1 / 240, warmup=20),
+    "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
+                              pit=20, substeps=1, dt=1 / 240, warmup=20),
+}
+DEFAULT_WORKLOAD = "colorcache_lattice10k"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def make_engine(me, wl, graph=True):
+    from importlib import import_module
+    scenes = import_module("motion_engine_b200.scenes")
+    if wl["engine"] == "color_cache":
+        e = me.ColorCacheContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    elif wl["engine"] == "jacobi":
+        e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"], graph=graph)
+    else:
+        raise ValueError(wl["engine"])
+    centers = scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])
+    for c in centers:
+        e.add_body(c)
+    return e
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out = ""
+            for ln in out.strip().splitlines():
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9:
+                    self.rows.append(parts)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline_sample(wl, max_seconds=20.0):
+    """The oracle (single-threaded C restatement) on the same workload from the same initial
+    state: steps until max_seconds of CPU work; returns body-steps/s and the sample taken."""
+    from oracle import oracle as O
+    from importlib import import_module
+    scenes = import_module("motion_engine_b200.scenes")
+    mode = {"color_cache": "color_cache", "jacobi": None}[wl["engine"]]
+    if mode is None:
+        o = O.JacobiOracle(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    else:
+        o = O.ColoredOracle(mode=mode, dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    centers = scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])
+    for c in centers:
+        o.add_body(c)
+    t0 = time.perf_counter()
+    for _ in range(wl.get("warmup", 20)):  # untimed: into the contact-rich regime, as the GPU run
+        o.step(wl["dt"], wl["substeps"])
+        if time.perf_counter() - t0 > 2 * max_seconds:
+            break
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(wl["dt"], wl["substeps"])
+        n += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or n >= 200:
+            break
+    return wl["n"] * n / el, n, el
+
+
+def run_reference(args, wl):
+    """--impl reference: the oracle port on every host core (one independent replica per
+    process, spawn start method), each timed over a bounded number of steps."""
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    procs = max(1, min(cores, 64))
+    ctx = mp.get_context("spawn")
+    per_step_budget = 60.0 / max(args.steps + args.warmup, 1)
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.starmap(_ref_worker, [(args.workload, args.steps, args.warmup, per_step_budget)] * procs)
+        wall = time.perf_counter() - t0
+    steps_done = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    value = wl["n"] * steps_done / busy
+    line = {"impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup",)}},
+            "dtype": "f32", "data": "synthetic",
+            "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": procs, "kind": "port",
+                             "sample": f"{procs} processes x {steps_done // procs} timed steps of independent "
+                                       f"replicas of the workload (after {args.warmup} untimed warm-up steps "
+                                       f"each, capped at ~60 s); the reference's Warp CPU path is not installed"},
+            "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def _ref_worker(workload, steps, warmup, per_step_budget):
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    from oracle import oracle as O
+    from importlib import import_module
+    ge.load_package()  # registers the package alias for the scene builders
+    scenes = import_module("motion_engine_b200.scenes")
+    wl = WORKLOADS[workload]
+    if wl["engine"] == "jacobi":
+        o = O.JacobiOracle(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    else:
+        o = O.ColoredOracle(mode="color_cache", dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    for c in (scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])):
+        o.add_body(c)
+    t_start = time.perf_counter()
+    for _ in range(warmup):
+        o.step(wl["dt"], wl["substeps"])
+        if time.perf_counter() - t_start > 30.0:
+            break
+    n = 0
+    t0 = time.perf_counter()
+    budget = per_step_budget * steps
+    while n < steps:
+        o.step(wl["dt"], wl["substeps"])
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return n, time.perf_counter() - t0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=None)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.warmup is None:
+        args.warmup = wl.get("warmup", 20)
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        import __graft_entry__ as ge
+        ge.load_package()
+        return run_reference(args, wl)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cpu_base = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import __graft_entry__ as ge
+        ge.load_package()
+        v, n, el = cpu_baseline_sample(wl)  # before the first GPU call
+        cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
+                    "sample": f"{n} steps of the same workload from the same initial state on one host core "
+                              f"({el:.1f} s; the oracle restatement, not the reference's Warp CPU path)"}
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import __graft_entry__ as ge
+    me = ge.load_package()
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    e = make_engine(me, wl)
+    dt, S = wl["dt"], wl["substeps"]
+    for _ in range(args.warmup):
+        e.step(dt, S)
+    torch.cuda.synchronize()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            e.step(dt, S)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    e.check_errors()
+    key = next(iter(e.kernels_per_step)) if e.kernels_per_step else None
+    launches_per_step = e.kernels_per_step.get(key, 0) if key else 0
+
+    # end to end through the public API with the state in pinned host memory
+    N = e.N
+    hx = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+    hq = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    hv = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+    hw = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+    hx.copy_(e.xc[:, :3]); hq.copy_(e.q); hv.copy_(e.v[:, :3]); hw.copy_(e.w[:, :3])
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    K2 = max(args.steps // 2, 3)
+    for k in range(K2):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.set_body_state(hx, hq, hv, hw)
+        e.step(dt, S)
+        hx.copy_(e.xc[:, :3], non_blocking=True); hq.copy_(e.q, non_blocking=True)
+        hv.copy_(e.v[:, :3], non_blocking=True); hw.copy_(e.w[:, :3], non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    bytes_io = N * (3 + 4 + 3 + 3) * 4
+
+    # the dominant kernel (the persistent chunk solve), timed live on its launching stream
+    solve_ms, solve_bytes, stage_ms = [], [], {}
+    if hasattr(e, "profile_substep"):
+        for _ in range(8):
+            st = e.profile_substep(dt / S)
+            for kk, vv in st.items():
+                stage_ms[kk] = stage_ms.get(kk, 0.0) + vv / 8
+            solve_ms.append(st["solve"])
+            solve_bytes.append(e.solve_bytes())
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = _peaks()
+    value = wl["n"] * world * args.steps / (ms / 1e3)
+    roof = None
+    if solve_ms:
+        avg_ms = float(np.mean(solve_ms))
+        avg_b = float(np.mean([b_["bytes"] for b_ in solve_bytes]))
+        achieved = avg_b / (avg_ms / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get(args.workload)
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_color_solve (persistent chunk solve, one launch per substep)",
+                "launch_ms": avg_ms, "algorithmic_bytes_per_launch": avg_b, "counts": solve_bytes[-1]}
+    h = e.header_dict()
+    line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene builders; the reference's own fixture)",
+            "config": {"workload": args.workload, "bodies": wl["n"], "substeps": S, "vit": wl["vit"],
+                       "pit": wl["pit"], "dt": dt, "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "clocks": clk.summary(),
+            "e2e": {"value": wl["n"] * world * K2 / (e2e_ms / 1e3), "unit": "body-steps/s",
+                    "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io, "steps": K2},
+            "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
+            "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -165,6 +165,8 @@ typedef struct b2c_pairs {
     float *cached_mass;      /* (bodies) invM of the cached colouring */
     int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
     uint32_t *barrier;       /* [count, generation] of the persistent solve's grid barrier */
+    float *prep;             /* (kept cap,16) per-contact terms that stay fixed during a solve:
+                                rA|meff, rB|meft1, t1|meft2, t2 (fixed tangent frame) */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -190,13 +192,18 @@ typedef struct b2c_color_params {
     float mu;                /* friction */
     float t2d;               /* cross-slip damping of the chunk sweep (1 = full) */
     int32_t color_cap;       /* error when the pair graph needs more colours (<= max_colors) */
-    int32_t solve_blocks;    /* CTAs of the persistent solve (0 = pick from the body count) */
+    int32_t solve_blocks;    /* persistent solve shape: 0 = pick from the body count; n > 0 = n CTAs
+                                with a grid barrier (1 = one CTA, block barriers); -n = a thread-block
+                                cluster of n CTAs with the hardware cluster barrier */
     int64_t barrier_timeout_ns; /* grid-barrier wait limit */
 } b2c_color_params;
 
 /* ---- version / errors ---- */
 B2C_API int32_t b2c_version(void);
 B2C_API const char *b2c_last_error(void);
+/* kernel nodes in a captured cudaGraph_t (child graphs included); -1 on error.  Used to report
+ * how many of this library's kernels one replayed step launches. */
+B2C_API int32_t b2c_graph_kernel_nodes(void *graph);
 /* ints of scratch that b2c_exclusive_scan needs for n elements */
 B2C_API int32_t b2c_scan_scratch_ints(int32_t n);
 /* exclusive prefix sum of n int32 (device pointers); out may alias nothing */

@@ -107,10 +107,11 @@ def test_colored_runs_repeat_bit_identical(blocks, me):
 
 
 def test_single_cta_equals_grid_solve(me):
-    """The persistent solve on one CTA (block barriers) and on several CTAs (grid barrier) give
+    """The persistent solve on one CTA (block barriers), several CTAs (grid barrier) and a
+    thread-block cluster (hardware cluster barrier) give
     the same bits: within a colour the written bodies are disjoint."""
     states = []
-    for blocks in (1, 3, 8):
+    for blocks in (1, 3, 8, -16, -4):
         e = _make(me, "color_cache", vit=16, pit=8, solve_blocks=blocks)
         for c in lattice(400):
             e.add_body(c)
