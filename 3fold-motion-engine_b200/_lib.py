@@ -39,7 +39,7 @@ class Pairs(ctypes.Structure):
                 ("kcount", c_void_p), ("pstart", c_void_p), ("pidx", c_void_p), ("col", c_void_p),
                 ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
                 ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
-                ("cache_state", c_void_p), ("barrier", c_void_p), ("prep", c_void_p)]
+                ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32)]
 
 
 class Warm(ctypes.Structure):
@@ -84,6 +84,7 @@ _P = ctypes.POINTER
 _SIGS = {
     "b2c_version": ([], c_int32),
     "b2c_graph_kernel_nodes": ([c_void_p], c_int32),
+    "b2c_pair_record_floats": ([c_int32, c_int32], ctypes.c_int64),
     "b2c_last_error": ([], ctypes.c_char_p),
     "b2c_scan_scratch_ints": ([c_int32], c_int32),
     "b2c_exclusive_scan": ([c_void_p, c_void_p, c_int32, c_void_p, c_void_p], c_int32),

@@ -103,7 +103,10 @@ class GraphColoredContactEngine(_BeadEngineBase):
         f32 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.float32, device=dev)
         f64 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.float64, device=dev)
         i64 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int64, device=dev)
-        pcap = cap
+        # body pairs: with the manifold reduction a pair keeps <= max_points contacts and the pair
+        # graph of boxes is sparse (a few partners per body); the plain engine colours contacts
+        pcap = min(cap, 8 * N + 4096) if self.manifold_reduce else cap
+        kslots = self.manifold_max_points if self.manifold_reduce else 1
         # kept contacts (feature order) and their keys
         self.k_bi, self.k_bj, self.k_fa, self.k_fb = i32(cap), i32(cap), i32(cap), i32(cap)
         self.k_pA, self.k_pB, self.k_n, self.k_imp = (torch.zeros((cap, 4), dtype=torch.float32, device=dev)
@@ -126,11 +129,12 @@ class GraphColoredContactEngine(_BeadEngineBase):
         self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(cap),
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
                            cached_a=i32(pcap), cached_b=i32(pcap), cached_mass=f32(N), cache_state=i32(8),
-                           barrier=torch.zeros(2, dtype=torch.int32, device=dev), prep=f32(16 * cap))
+                           barrier=torch.zeros(2, dtype=torch.int32, device=dev),
+                           rec=f32(self.L.b2c_pair_record_floats(pcap, kslots)))
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
-            "cached_b", "cached_mass", "cache_state", "barrier", "prep")))
+            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots)
         # warm store
         self.w_keys, self.w_imp, self.w_n = i64(cap), torch.zeros((cap, 4), dtype=torch.float32, device=dev), i32(1)
         self.c_warm = _lib.Warm(cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))

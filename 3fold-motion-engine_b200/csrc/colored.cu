@@ -528,7 +528,12 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         }
     }
     __syncthreads();
-    for (int p = tid; p < P; p += kColorThreads) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
+    // ground pairs first inside every colour, so a warp of the solve mostly runs one code path
+    for (int p = tid; p < P; p += kColorThreads)
+        if (pr.pbj[p] < 0) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
+    __syncthreads();
+    for (int p = tid; p < P; p += kColorThreads)
+        if (pr.pbj[p] >= 0) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
     if (use_cache) {
         for (int p = tid; p < P; p += kColorThreads) {
             pr.cached_a[p] = pr.pbi[p];
@@ -693,7 +698,7 @@ extern "C" int32_t b2c_color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_heade
 extern "C" int32_t b2c_color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr,
                                    const b2c_color_params *p, float dt, b2c_stream s)
 {
-    if (!b || !kept || !pr || !hdr || !color_params_ok(p) || !(dt > 0.0f) || !pr->barrier || !pr->prep) {
+    if (!b || !kept || !pr || !hdr || !color_params_ok(p) || !(dt > 0.0f) || !pr->barrier || !pr->rec || pr->kslots < 1) {
         b2c::set_error("b2c_color_solve: bad argument");
         return B2C_EARG;
     }
@@ -717,7 +722,7 @@ extern "C" int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads
 {
     if (!b || !beads || !beads->bead_start || !g || !c || !m || !kept || !kept_keys || !pr || !warm || !hdr ||
         !color_params_ok(p) || !vgrav || !(dt > 0.0f) || kept->capacity < c->capacity ||
-        warm->capacity < kept->capacity || !pr->barrier || !pr->prep) {
+        warm->capacity < kept->capacity || !pr->barrier || !pr->rec || pr->kslots < 1) {
         b2c::set_error("b2c_color_substep: bad argument");
         return B2C_EARG;
     }

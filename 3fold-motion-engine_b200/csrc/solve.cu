@@ -5,18 +5,26 @@
 //
 // The reference launches one kernel per colour per sweep ((1 + vit + pit) x ncol launches in a
 // graph).  Here the colours are separated by a barrier inside one kernel:
-//   * one CTA (small scenes): __syncthreads;
-//   * a thread-block cluster of up to 16 CTAs (up to ~32k bodies): the hardware cluster barrier
-//     (barrier.cluster arrive.release / wait.acquire) -- no spinning, a few hundred ns;
-//   * a cooperative grid (larger scenes): an atomic grid barrier whose wait is bounded by a
+//   * one CTA (tiny scenes): __syncthreads (~0.04 us measured on B200);
+//   * a thread-block cluster of up to 16 CTAs: the hardware cluster barrier
+//     (barrier.cluster arrive.release / wait.acquire; ~0.25 us measured);
+//   * a cooperative grid: an atomic grid barrier (~2.2 us measured) whose wait is bounded by a
 //     %globaltimer limit, after which it sets B2C_ERR_BARRIER_TIMEOUT and every CTA returns.
-// Body velocities are read and written through L2 (ld.cg / st.cg), since CTAs on other SMs read
-// them after a barrier and L1 is not coherent across SMs.
 //
-// Terms that do not change during a solve (lever arms rA, rB, the fixed tangent frame t1, t2 and
-// the effective masses meff, meft1, meft2) are computed once per substep by k_contact_prep with
-// exactly the reference's expressions, instead of in every sweep.  Same inputs, same operations:
-// the results are bit-identical to recomputing them.
+// Data layout.  The sweeps are bound by the latency of dependent loads, not by arithmetic or
+// bandwidth: following porder -> pair -> pidx -> contact -> body costs several L2 round trips
+// per pair and per phase.  So once per substep k_pair_gather writes every pair into a
+// colour-major record (slot s = position in porder): a header (bodies, contact count), both
+// bodies' inverse inertia rows and inverse masses, and per contact its normal|depth, the terms
+// that stay fixed during the solve (rA|meff, rB|meft1, t1|meft2 -- computed with exactly the
+// reference's expressions, so bit-identical to recomputing them every sweep) and its impulses.
+// A phase then needs one batch of independent 128-bit loads for the record and one for the two
+// bodies' velocities.  Records are structure-of-arrays by field, so consecutive threads read
+// consecutive 16-byte words.  After the solve k_imp_scatter returns the impulses to the kept
+// contacts (the warm store reads them there).
+//
+// Body velocities are read and written through L2 (ld.cg / st.cg): CTAs on other SMs read them
+// after a barrier, and L1 is not coherent across SMs.
 #include <cooperative_groups.h>
 
 #include "b2c_common.cuh"
@@ -29,14 +37,26 @@ __device__ __forceinline__ float4 ldcg4(const float *p, int i) { return __ldcg(r
 __device__ __forceinline__ void stcg4(float *p, int i, float4 v) { __stcg(reinterpret_cast<float4 *>(p) + i, v); }
 __device__ __forceinline__ f3 ldcg3(const float *p, int i) { return xyz(ldcg4(p, i)); }
 
+// record fields (float4 units)
+enum { kRecBody = 7, kRecContact = 5 };
+enum { kCN = 0, kCRA = 1, kCRB = 2, kCT1 = 3, kCImp = 4 };
+
+struct Records {
+    float4 *base;
+    int cap, K;
+    __device__ __forceinline__ int4 *hdr() const { return reinterpret_cast<int4 *>(base); }
+    __device__ __forceinline__ float4 *body(int f) const { return base + (size_t)(1 + f) * cap; }
+    __device__ __forceinline__ float4 *contact(int f, int j) const
+    {
+        return base + (size_t)(1 + kRecBody) * cap + ((size_t)f * K + j) * cap;
+    }
+};
+
 struct SolveArgs {
     const b2c_header *hdr;
     int *err;
-    const int *porder, *cstart, *ccount, *pstart, *pcount, *pidx, *pbi, *pbj;
-    const float *cpA, *cpB, *cn;
-    const float4 *prep;
-    float *imp;
-    const float *invIw, *invM;
+    const int *cstart, *ccount;
+    Records rec;
     float *v, *w, *pv, *po;
     float mu, t2d, dt;
     int vit, pit, fixed_frame, apply_warm;
@@ -45,55 +65,87 @@ struct SolveArgs {
 };
 
 // ---------------------------------------------------------------------------------------------
-// per-contact invariants of one solve
+// gather (once per substep) and scatter
 // ---------------------------------------------------------------------------------------------
-// rA = cpA - xc[bi], rB = cpB - xc[bj]; meff (normal); the axis-derived frame
-// t1 = normalize(a - (a.n) n), t2 = n x t1 with a = x (y when |n.x| >= 0.9) and its effective
-// masses meft1, meft2 -- the expressions of k_fixed_frame / apply_warm / k_chunk_pos_r.
-__global__ void k_contact_prep(const b2c_header *__restrict__ hdr, const int *__restrict__ kbi,
-                               const int *__restrict__ kbj, const float *__restrict__ cpA,
-                               const float *__restrict__ cpB, const float *__restrict__ cn,
-                               const float *__restrict__ xc, const float *__restrict__ invIw,
-                               const float *__restrict__ invM, float4 *__restrict__ prep)
+__global__ void k_pair_gather(const b2c_header *__restrict__ hdr, const int *__restrict__ porder,
+                              const int *__restrict__ pstart, const int *__restrict__ pcount,
+                              const int *__restrict__ pidx, const int *__restrict__ pbi, const int *__restrict__ pbj,
+                              b2c_contacts kept, const float *__restrict__ xc, const float *__restrict__ invIw,
+                              const float *__restrict__ invM, Records R, b2c_header *hdr_w)
 {
-    const int Ck = hdr->n_contacts > 0 ? hdr->n_kept : 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Ck; c += gridDim.x * blockDim.x) {
-        const int bi = kbi[c], bj = kbj[c];
-        const f3 nrm = ld3(cn, c);
-        const f3 rA = sub3(ld3(cpA, c), ld3(xc, bi));
+    const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
+        const int p = porder[s];
+        const int bi = pbi[p], bj = pbj[p];
+        int n = pcount[p];
+        if (n > R.K) {
+            atomicOr(&hdr_w->error, B2C_ERR_CHUNK_OVERFLOW);
+            n = R.K;
+        }
+        R.hdr()[s] = make_int4(bi, bj, n, p);
         const m3 IA = ldm(invIw, bi);
         const float iMA = invM[bi];
-        f3 rB{0.0f, 0.0f, 0.0f};
         m3 IB = IA;
         float iMB = 0.0f;
         if (bj >= 0) {
-            rB = sub3(ld3(cpB, c), ld3(xc, bj));
             IB = ldm(invIw, bj);
             iMB = invM[bj];
         }
-        f3 aa{1.0f, 0.0f, 0.0f};
-        if (fabsf(nrm.x) >= 0.9f) aa = f3{0.0f, 1.0f, 0.0f};
-        const float dd = dot3(aa, nrm);
-        const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
-        const f3 t2 = cross3(nrm, t1);
-        const f3 rnA = cross3(rA, nrm);
-        float meff = iMA + dot3(rnA, matvec(IA, rnA));
-        const f3 rtA1 = cross3(rA, t1);
-        float meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
-        const f3 rtA2 = cross3(rA, t2);
-        float meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
-        if (bj >= 0) {
-            const f3 rnB = cross3(rB, nrm);
-            meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
-            const f3 rtB1 = cross3(rB, t1);
-            meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
-            const f3 rtB2 = cross3(rB, t2);
-            meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
+        R.body(0)[s] = f4(IA.r0, 0.0f);
+        R.body(1)[s] = f4(IA.r1, 0.0f);
+        R.body(2)[s] = f4(IA.r2, 0.0f);
+        R.body(3)[s] = f4(IB.r0, 0.0f);
+        R.body(4)[s] = f4(IB.r1, 0.0f);
+        R.body(5)[s] = f4(IB.r2, 0.0f);
+        R.body(6)[s] = make_float4(iMA, iMB, 0.0f, 0.0f);
+        const f3 xA = ld3(xc, bi);
+        f3 xB{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) xB = ld3(xc, bj);
+        const int st = pstart[p];
+        for (int j = 0; j < n; ++j) {
+            const int c = pidx[st + j];
+            const float4 pA4 = ld4(kept.pA, c);
+            const f3 nrm = ld3(kept.n, c);
+            // the invariants of k_fixed_frame / apply_warm / k_chunk_pos_r, reference expressions
+            const f3 rA = sub3(xyz(pA4), xA);
+            f3 rB{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) rB = sub3(ld3(kept.pB, c), xB);
+            f3 aa{1.0f, 0.0f, 0.0f};
+            if (fabsf(nrm.x) >= 0.9f) aa = f3{0.0f, 1.0f, 0.0f};
+            const float dd = dot3(aa, nrm);
+            const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
+            const f3 t2 = cross3(nrm, t1);
+            const f3 rnA = cross3(rA, nrm);
+            float meff = iMA + dot3(rnA, matvec(IA, rnA));
+            const f3 rtA1 = cross3(rA, t1);
+            float meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
+            const f3 rtA2 = cross3(rA, t2);
+            float meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
+            if (bj >= 0) {
+                const f3 rnB = cross3(rB, nrm);
+                meff = (meff + iMB) + dot3(rnB, matvec(IB, rnB));
+                const f3 rtB1 = cross3(rB, t1);
+                meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
+                const f3 rtB2 = cross3(rB, t2);
+                meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
+            }
+            R.contact(kCN, j)[s] = f4(nrm, pA4.w);
+            R.contact(kCRA, j)[s] = f4(rA, meff);
+            R.contact(kCRB, j)[s] = f4(rB, meft1);
+            R.contact(kCT1, j)[s] = f4(t1, meft2);
+            R.contact(kCImp, j)[s] = ld4(kept.imp, c);
         }
-        prep[4 * c + 0] = f4(rA, meff);
-        prep[4 * c + 1] = f4(rB, meft1);
-        prep[4 * c + 2] = f4(t1, meft2);
-        prep[4 * c + 3] = f4(t2, 0.0f);
+    }
+}
+
+__global__ void k_imp_scatter(const b2c_header *__restrict__ hdr, const int *__restrict__ pstart,
+                              const int *__restrict__ pidx, Records R, float *__restrict__ imp)
+{
+    const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
+        const int4 h = R.hdr()[s];
+        const int st = pstart[h.w];
+        for (int j = 0; j < h.z; ++j) st4(imp, pidx[st + j], R.contact(kCImp, j)[s]);
     }
 }
 
@@ -152,248 +204,299 @@ __device__ __forceinline__ bool solve_barrier(const SolveArgs &a)
 }
 
 // ---------------------------------------------------------------------------------------------
-// one pair of a colour
+// one pair record of a colour.  The contact loop is software-pipelined: contact k+1's record is
+// loaded before contact k is computed, and contact 0's together with the pair's header, so a
+// phase pays about two dependent round trips (record, then the bodies' velocities) instead of
+// one per contact.
 // ---------------------------------------------------------------------------------------------
-// apply_warm, contact_engine_gpu_applied_warm.py:5-54
-__device__ void pair_apply_warm(const SolveArgs &a, int p)
-{
-    const int A = a.pbi[p], B = a.pbj[p];
-    const float iMA = a.invM[A], iMB = B >= 0 ? a.invM[B] : 0.0f;
-    f3 va = ldcg3(a.v, A), wa = ldcg3(a.w, A), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
-    const m3 IA = ldm(a.invIw, A);
-    m3 IB = IA;
-    if (B >= 0) {
-        vb = ldcg3(a.v, B);
-        wb = ldcg3(a.w, B);
-        IB = ldm(a.invIw, B);
+// Body state access through L2 (a policy class, so the pair physics is written once).
+struct GlobalBodies {
+    float *v, *w, *pv, *po;
+    __device__ __forceinline__ f3 get(int b, int k) const
+    {
+        const float *p = k == 0 ? v : k == 1 ? w : k == 2 ? pv : po;
+        return ldcg3(p, b);
     }
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        const float4 p0 = a.prep[4 * c + 0], p1 = a.prep[4 * c + 1], p2 = a.prep[4 * c + 2], p3 = a.prep[4 * c + 3];
-        const f3 t1 = xyz(p2), t2 = xyz(p3);
-        const float4 im = ldcg4(a.imp, c);
+    __device__ __forceinline__ void set(int b, int k, f3 x) const
+    {
+        float *p = k == 0 ? v : k == 1 ? w : k == 2 ? pv : po;
+        stcg4(p, b, f4(x, 0.0f));
+    }
+};
+struct PairBodies {
+    int bi, bj, n;
+    m3 IA, IB;
+    float iMA, iMB;
+};
+__device__ __forceinline__ PairBodies load_pair(const Records &R, int s)
+{
+    PairBodies q;
+    const int4 h = R.hdr()[s];
+    q.bi = h.x;
+    q.bj = h.y;
+    q.n = h.z;
+    const float4 i0 = R.body(0)[s], i1 = R.body(1)[s], i2 = R.body(2)[s];
+    const float4 j0 = R.body(3)[s], j1 = R.body(4)[s], j2 = R.body(5)[s], mm = R.body(6)[s];
+    q.IA = m3{xyz(i0), xyz(i1), xyz(i2)};
+    q.IB = m3{xyz(j0), xyz(j1), xyz(j2)};
+    q.iMA = mm.x;
+    q.iMB = mm.y;
+    return q;
+}
+struct CRec {
+    float4 n, ra, rb, t1, im;
+};
+__device__ __forceinline__ CRec load_contact(const Records &R, int s, int k)
+{
+    return CRec{R.contact(kCN, k)[s], R.contact(kCRA, k)[s], R.contact(kCRB, k)[s], R.contact(kCT1, k)[s],
+                R.contact(kCImp, k)[s]};
+}
+
+// apply_warm, contact_engine_gpu_applied_warm.py:5-54
+template <class BA>
+__device__ void pair_apply_warm(const SolveArgs &a, int s, const BA &BS)
+{
+    const PairBodies q = load_pair(a.rec, s);
+    CRec cur = load_contact(a.rec, s, 0);
+    const int A = q.bi, B = q.bj;
+    f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
+    if (B >= 0) {
+        vb = BS.get(B, 0);
+        wb = BS.get(B, 1);
+    }
+    for (int k = 0; k < q.n; ++k) {
+        CRec nxt;
+        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
+        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb), t1 = xyz(cur.t1);
+        const f3 t2 = cross3(nrm, t1);
+        const float4 im = cur.im;
         const f3 J{fmaf(im.z, t2.x, fmaf(im.x, nrm.x, im.y * t1.x)), fmaf(im.z, t2.y, fmaf(im.x, nrm.y, im.y * t1.y)),
                    fmaf(im.z, t2.z, fmaf(im.x, nrm.z, im.y * t1.z))};
-        if (iMA > 0.0f) {
-            va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
-            wa = add3(wa, matvec(IA, cross3(xyz(p0), J)));
+        if (q.iMA > 0.0f) {
+            va = f3{fmaf(q.iMA, J.x, va.x), fmaf(q.iMA, J.y, va.y), fmaf(q.iMA, J.z, va.z)};
+            wa = add3(wa, matvec(q.IA, cross3(rA, J)));
         }
-        if (B >= 0 && iMB > 0.0f) {
-            vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
-            wb = sub3(wb, matvec(IB, cross3(xyz(p1), J)));
+        if (B >= 0 && q.iMB > 0.0f) {
+            vb = f3{fmaf(-q.iMB, J.x, vb.x), fmaf(-q.iMB, J.y, vb.y), fmaf(-q.iMB, J.z, vb.z)};
+            wb = sub3(wb, matvec(q.IB, cross3(rB, J)));
         }
+        cur = nxt;
     }
-    if (iMA > 0.0f) {
-        stcg4(a.v, A, f4(va, 0.0f));
-        stcg4(a.w, A, f4(wa, 0.0f));
+    if (q.iMA > 0.0f) {
+        BS.set(A, 0, va);
+        BS.set(A, 1, wa);
     }
-    if (B >= 0 && iMB > 0.0f) {
-        stcg4(a.v, B, f4(vb, 0.0f));
-        stcg4(a.w, B, f4(wb, 0.0f));
+    if (B >= 0 && q.iMB > 0.0f) {
+        BS.set(B, 0, vb);
+        BS.set(B, 1, wb);
     }
 }
 
 // velocity chunk: k_fixed_frame (fixed_frame.py:7-77) or k_chunk_vel_r (COL:413-490)
-__device__ void pair_velocity(const SolveArgs &a, int p)
+template <class BA, bool kFixed>
+__device__ void pair_velocity(const SolveArgs &a, int s, const BA &B)
 {
-    const int bi = a.pbi[p], bj = a.pbj[p];
-    const float iMA = a.invM[bi];
-    const m3 IA = ldm(a.invIw, bi);
-    m3 IB = IA;
-    f3 vA = ldcg3(a.v, bi), wA = ldcg3(a.w, bi);
-    float iMB = 0.0f;
+    const PairBodies q = load_pair(a.rec, s);
+    CRec cur = load_contact(a.rec, s, 0);
+    const int bi = q.bi, bj = q.bj;
+    const float iMA = q.iMA, iMB = q.iMB;
+    f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
     f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
     if (bj >= 0) {
-        iMB = a.invM[bj];
-        IB = ldm(a.invIw, bj);
-        vB = ldcg3(a.v, bj);
-        wB = ldcg3(a.w, bj);
+        vB = B.get(bj, 0);
+        wB = B.get(bj, 1);
     }
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        const float4 p0 = a.prep[4 * c + 0], p1 = a.prep[4 * c + 1];
-        const f3 rA = xyz(p0), rB = xyz(p1);
-        const float meff = p0.w;
+    for (int k = 0; k < q.n; ++k) {
+        CRec nxt;
+        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
+        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
+        const float meff = cur.ra.w;
         f3 va = add3(vA, cross3(wA, rA));
         f3 vb{0.0f, 0.0f, 0.0f};
         if (bj >= 0) vb = add3(vB, cross3(wB, rB));
         f3 vrel = sub3(va, vb);
         const float vn = dot3(vrel, nrm);
-        f3 t1, t2;
-        float meft1, meft2;
-        bool axis_frame = a.fixed_frame;
-        if (!a.fixed_frame) {
+        f3 t1 = xyz(cur.t1);
+        f3 t2 = cross3(nrm, t1);
+        float meft1 = cur.rb.w, meft2 = cur.t1.w;
+        if (!kFixed) {
             const f3 vt{fmaf(-vn, nrm.x, vrel.x), fmaf(-vn, nrm.y, vrel.y), fmaf(-vn, nrm.z, vrel.z)};
             const float mt = len3(vt);
-            t1 = div3(vt, mt);
-            axis_frame = mt <= 5e-3f;
-        }
-        if (axis_frame) {
-            const float4 p2 = a.prep[4 * c + 2], p3 = a.prep[4 * c + 3];
-            t1 = xyz(p2);
-            t2 = xyz(p3);
-            meft1 = p1.w;
-            meft2 = p2.w;
-        } else {
-            t2 = cross3(nrm, t1);
-            const f3 rtA1 = cross3(rA, t1);
-            meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
-            const f3 rtA2 = cross3(rA, t2);
-            meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
-            if (bj >= 0) {
-                const f3 rtB1 = cross3(rB, t1);
-                meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
-                const f3 rtB2 = cross3(rB, t2);
-                meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
+            if (!(mt <= 5e-3f)) {  // slip basis t1 = vt / |vt|; otherwise the axis frame of the record
+                t1 = div3(vt, mt);
+                t2 = cross3(nrm, t1);
+                const f3 rtA1 = cross3(rA, t1);
+                meft1 = iMA + dot3(rtA1, matvec(q.IA, rtA1));
+                const f3 rtA2 = cross3(rA, t2);
+                meft2 = iMA + dot3(rtA2, matvec(q.IA, rtA2));
+                if (bj >= 0) {
+                    const f3 rtB1 = cross3(rB, t1);
+                    meft1 = (meft1 + iMB) + dot3(rtB1, matvec(q.IB, rtB1));
+                    const f3 rtB2 = cross3(rB, t2);
+                    meft2 = (meft2 + iMB) + dot3(rtB2, matvec(q.IB, rtB2));
+                }
             }
         }
-        if (!(meff >= 1e-12f)) continue;
-        float4 im = ldcg4(a.imp, c);
-        float dj = -vn / meff;
-        const float nw = fmaxf(0.0f, im.x + dj);
-        dj = nw - im.x;
-        im.x = nw;
-        const f3 Jn = scale3(nrm, dj);
-        if (iMA > 0.0f) {
-            vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
-            wA = add3(wA, matvec(IA, cross3(rA, Jn)));
-        }
-        if (bj >= 0 && iMB > 0.0f) {
-            vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
-            wB = sub3(wB, matvec(IB, cross3(rB, Jn)));
-        }
-        va = add3(vA, cross3(wA, rA));
-        vb = f3{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-        vrel = sub3(va, vb);
-        if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
-            const float o1 = im.y, o2 = im.z;
-            float a1 = o1 - dot3(vrel, t1) / meft1;
-            float a2 = o2 - dot3(vrel, t2) / meft2;
-            const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-            const float lim = a.mu * im.x;
-            if (mag > lim && mag > 1e-12f) {
-                a1 = a1 * lim / mag;
-                a2 = a2 * lim / mag;
-            }
-            im.y = a1;
-            im.z = a2;
-            const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
-            const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+        if (meff >= 1e-12f) {
+            float4 im = cur.im;
+            float dj = -vn / meff;
+            const float nw = fmaxf(0.0f, im.x + dj);
+            dj = nw - im.x;
+            im.x = nw;
+            const f3 Jn = scale3(nrm, dj);
             if (iMA > 0.0f) {
-                vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
-                wA = add3(wA, matvec(IA, cross3(rA, Jt)));
+                vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
+                wA = add3(wA, matvec(q.IA, cross3(rA, Jn)));
             }
             if (bj >= 0 && iMB > 0.0f) {
-                vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
-                wB = sub3(wB, matvec(IB, cross3(rB, Jt)));
+                vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
+                wB = sub3(wB, matvec(q.IB, cross3(rB, Jn)));
             }
+            va = add3(vA, cross3(wA, rA));
+            vb = f3{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+            vrel = sub3(va, vb);
+            if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
+                const float o1 = im.y, o2 = im.z;
+                float a1 = o1 - dot3(vrel, t1) / meft1;
+                float a2 = o2 - dot3(vrel, t2) / meft2;
+                const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+                const float lim = a.mu * im.x;
+                if (mag > lim && mag > 1e-12f) {
+                    a1 = a1 * lim / mag;
+                    a2 = a2 * lim / mag;
+                }
+                im.y = a1;
+                im.z = a2;
+                const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+                const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+                if (iMA > 0.0f) {
+                    vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
+                    wA = add3(wA, matvec(q.IA, cross3(rA, Jt)));
+                }
+                if (bj >= 0 && iMB > 0.0f) {
+                    vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
+                    wB = sub3(wB, matvec(q.IB, cross3(rB, Jt)));
+                }
+            }
+            a.rec.contact(kCImp, k)[s] = im;
         }
-        stcg4(a.imp, c, im);
+        cur = nxt;
     }
     if (iMA > 0.0f) {
-        stcg4(a.v, bi, f4(vA, 0.0f));
-        stcg4(a.w, bi, f4(wA, 0.0f));
+        B.set(bi, 0, vA);
+        B.set(bi, 1, wA);
     }
     if (bj >= 0 && iMB > 0.0f) {
-        stcg4(a.v, bj, f4(vB, 0.0f));
-        stcg4(a.w, bj, f4(wB, 0.0f));
+        B.set(bj, 0, vB);
+        B.set(bj, 1, wB);
     }
 }
 
 // position chunk, k_chunk_pos_r (COL:510-554)
-__device__ void pair_position(const SolveArgs &a, int p)
+template <class BA>
+__device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 {
-    const int bi = a.pbi[p], bj = a.pbj[p];
-    const float iMA = a.invM[bi];
-    const m3 IA = ldm(a.invIw, bi);
-    m3 IB = IA;
-    f3 pvA = ldcg3(a.pv, bi), poA = ldcg3(a.po, bi);
-    float iMB = 0.0f;
+    const PairBodies q = load_pair(a.rec, s);
+    CRec cur = load_contact(a.rec, s, 0);
+    const int bi = q.bi, bj = q.bj;
+    const float iMA = q.iMA, iMB = q.iMB;
+    f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
     f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
     if (bj >= 0) {
-        iMB = a.invM[bj];
-        IB = ldm(a.invIw, bj);
-        pvB = ldcg3(a.pv, bj);
-        poB = ldcg3(a.po, bj);
+        pvB = B.get(bj, 2);
+        poB = B.get(bj, 3);
     }
-    const int st = a.pstart[p], n = a.pcount[p];
-    for (int k = 0; k < n; ++k) {
-        const int c = a.pidx[st + k];
-        const f3 nrm = ld3(a.cn, c);
-        const float pen = a.cpA[4 * c + 3];
-        const float4 p0 = a.prep[4 * c + 0], p1 = a.prep[4 * c + 1];
-        const f3 rA = xyz(p0), rB = xyz(p1);
+    for (int k = 0; k < q.n; ++k) {
+        CRec nxt;
+        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
+        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
         f3 rel = add3(pvA, cross3(poA, rA));
         if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
-        const float meff = p0.w;
-        if (!(meff >= 1e-12f)) continue;
-        const float bias = B2C_BETA * fmaxf(pen - B2C_SLOP, 0.0f) / a.dt;
-        float dj = (bias - dot3(rel, nrm)) / meff;
-        const float jp = __ldcg(a.imp + 4 * c + 3);
-        const float nw = fmaxf(0.0f, jp + dj);
-        dj = nw - jp;
-        __stcg(a.imp + 4 * c + 3, nw);
-        const f3 Jn = scale3(nrm, dj);
-        if (iMA > 0.0f) {
-            pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
-            poA = add3(poA, matvec(IA, cross3(rA, Jn)));
+        const float meff = cur.ra.w;
+        if (meff >= 1e-12f) {
+            const float bias = B2C_BETA * fmaxf(cur.n.w - B2C_SLOP, 0.0f) / a.dt;
+            float dj = (bias - dot3(rel, nrm)) / meff;
+            float4 im = cur.im;
+            const float nw = fmaxf(0.0f, im.w + dj);
+            dj = nw - im.w;
+            im.w = nw;
+            a.rec.contact(kCImp, k)[s] = im;
+            const f3 Jn = scale3(nrm, dj);
+            if (iMA > 0.0f) {
+                pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
+                poA = add3(poA, matvec(q.IA, cross3(rA, Jn)));
+            }
+            if (bj >= 0 && iMB > 0.0f) {
+                pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
+                poB = sub3(poB, matvec(q.IB, cross3(rB, Jn)));
+            }
         }
-        if (bj >= 0 && iMB > 0.0f) {
-            pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
-            poB = sub3(poB, matvec(IB, cross3(rB, Jn)));
-        }
+        cur = nxt;
     }
     if (iMA > 0.0f) {
-        stcg4(a.pv, bi, f4(pvA, 0.0f));
-        stcg4(a.po, bi, f4(poA, 0.0f));
+        B.set(bi, 2, pvA);
+        B.set(bi, 3, poA);
     }
     if (bj >= 0 && iMB > 0.0f) {
-        stcg4(a.pv, bj, f4(pvB, 0.0f));
-        stcg4(a.po, bj, f4(poB, 0.0f));
+        B.set(bj, 2, pvB);
+        B.set(bj, 3, poB);
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// the persistent kernel
+// the persistent kernels: record slot cstart[ci] + t of colour ci on thread t mod (threads)
 // ---------------------------------------------------------------------------------------------
-template <int kKind>
-__device__ __forceinline__ void solve_body(const SolveArgs &a)
+template <int kKind, bool kFixed, class BA>
+__device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
-    if (a.hdr->n_pairs == 0 || nc == 0) return;
+    if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     if (a.apply_warm) {
         for (int ci = 0; ci < nc; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_apply_warm(a, a.porder[s0 + t]);
+            for (int t = tid; t < cnt; t += nth) pair_apply_warm(a, s0 + t, B);
             if (!solve_barrier<kKind>(a)) return;
         }
     }
     for (int it = 0; it < a.vit; ++it)
         for (int ci = 0; ci < nc; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_velocity(a, a.porder[s0 + t]);
+            for (int t = tid; t < cnt; t += nth) pair_velocity<BA, kFixed>(a, s0 + t, B);
             if (!solve_barrier<kKind>(a)) return;
         }
     for (int it = 0; it < a.pit; ++it)
         for (int ci = 0; ci < nc; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_position(a, a.porder[s0 + t]);
+            for (int t = tid; t < cnt; t += nth) pair_position(a, s0 + t, B);
             if (!solve_barrier<kKind>(a)) return;
         }
 }
 
-__global__ void __launch_bounds__(256) k_color_solve_block(SolveArgs a) { solve_body<kBlock>(a); }
-__global__ void __launch_bounds__(512) k_color_solve_cluster(SolveArgs a) { solve_body<kCluster>(a); }
-__global__ void __launch_bounds__(256) k_color_solve_grid(SolveArgs a) { solve_body<kGrid>(a); }
-
 constexpr int kClusterThreads = 512;
 constexpr int kClusterMax = 16;
+
+__global__ void __launch_bounds__(256) k_color_solve_block(SolveArgs a)
+{
+    const GlobalBodies B{a.v, a.w, a.pv, a.po};
+    if (a.fixed_frame) solve_body<kBlock, true>(a, B);
+    else solve_body<kBlock, false>(a, B);
+}
+__global__ void __launch_bounds__(256) k_color_solve_grid(SolveArgs a)
+{
+    const GlobalBodies B{a.v, a.w, a.pv, a.po};
+    if (a.fixed_frame) solve_body<kGrid, true>(a, B);
+    else solve_body<kGrid, false>(a, B);
+}
+// Cluster solve.  (Holding the body state in distributed shared memory instead measured slower
+// on B200 for this access pattern: 1.25 ms against 0.78 ms on the 10k-box lattice.)
+__global__ void __launch_bounds__(kClusterThreads) k_color_solve_cluster(SolveArgs a)
+{
+    const GlobalBodies B{a.v, a.w, a.pv, a.po};
+    if (a.fixed_frame) solve_body<kCluster, true>(a, B);
+    else solve_body<kCluster, false>(a, B);
+}
 
 static int max_coresident_grid_blocks()
 {
@@ -408,17 +511,32 @@ static int max_coresident_grid_blocks()
     return cached;
 }
 
-// largest cluster (<= 16) of k_color_solve_cluster CTAs the device can co-schedule; 0 if none.
-// A host-side occupancy query, done once (the first step of an engine runs eagerly, before any
-// graph capture).
-static int max_cluster_size()
+static int max_dyn_smem()
 {
     static int cached = -1;
     if (cached < 0) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
         cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cached = v;
+    }
+    return cached;
+}
+
+// largest power-of-two cluster (<= 16) of k_color_solve_cluster CTAs with `smem` bytes of
+// shared memory each that the device can co-schedule; a host-side occupancy query, cached per
+// size (an engine's first step runs eagerly, before any graph capture)
+static int max_cluster_size(int smem)
+{
+    static int cached_smem = -1, cached = 0;
+    if (smem != cached_smem) {
+        max_dyn_smem();
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kClusterMax);
         cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = smem;
         int cs = 0;
         if (cudaOccupancyMaxPotentialClusterSize(&cs, k_color_solve_cluster, &cfg) != cudaSuccess) {
             cudaGetLastError();
@@ -427,29 +545,9 @@ static int max_cluster_size()
         int p2 = 0;
         for (int c = 1; c <= std::min(cs, kClusterMax); c *= 2) p2 = c;
         cached = p2 >= 2 ? p2 : 0;
+        cached_smem = smem;
     }
     return cached;
-}
-
-static int launch_cluster(const SolveArgs &a, int csize, cudaStream_t s)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(csize);
-    cfg.blockDim = dim3(kClusterThreads);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = csize;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve_cluster, a);
-    if (e != cudaSuccess) {
-        set_error("color_solve: cluster launch of %d CTAs: %s", csize, cudaGetErrorString(e));
-        return B2C_ECUDA;
-    }
-    return check_launch("color_solve_cluster");
 }
 
 int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
@@ -458,21 +556,9 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     SolveArgs a;
     a.hdr = hdr;
     a.err = &hdr->error;
-    a.porder = pr->porder;
     a.cstart = pr->cstart;
     a.ccount = pr->ccount;
-    a.pstart = pr->pstart;
-    a.pcount = pr->kcount;
-    a.pidx = pr->pidx;
-    a.pbi = pr->pbi;
-    a.pbj = pr->pbj;
-    a.cpA = kept->pA;
-    a.cpB = kept->pB;
-    a.cn = kept->n;
-    a.prep = reinterpret_cast<const float4 *>(pr->prep);
-    a.imp = kept->imp;
-    a.invIw = b->invIw;
-    a.invM = b->invM;
+    a.rec = Records{reinterpret_cast<float4 *>(pr->rec), pr->capacity, pr->kslots};
     a.v = b->v;
     a.w = b->w;
     a.pv = b->pv;
@@ -488,43 +574,73 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     a.bar_gen = pr->barrier + 1;
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
-    k_contact_prep<<<std::min(blocks_for(kept->capacity), kSMs * 8), kThreads, 0, s>>>(
-        hdr, kept->bi, kept->bj, kept->pA, kept->pB, kept->n, b->xc, b->invIw, b->invM, reinterpret_cast<float4 *>(pr->prep));
-    int rc = check_launch("contact_prep");
+    const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
+    k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
+                                             *kept, b->xc, b->invIw, b->invM, a.rec, hdr);
+    int rc = check_launch("pair_gather");
     if (rc) return rc;
 
     int mode = p->solve_blocks;
-    if (mode == 0) {  // auto: one CTA for small scenes, a cluster up to ~32k bodies, else a grid
-        if (b->n <= 256) mode = 1;
-        else if (b->n <= 2 * kClusterMax * kClusterThreads * 2) mode = -kClusterMax;
-        else mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks());
+    if (mode == 0) {  // auto: one CTA for tiny scenes, else a cluster (colours wider than it loop)
+        if (b->n <= 64) mode = 1;
+        else mode = -kClusterMax;
     }
     if (mode < 0) {
-        const int cs = std::min(-mode, max_cluster_size());
-        if (cs >= 2) return launch_cluster(a, cs, s);
-        mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks());  // no cluster possible
+        const int cs = std::min(-mode, max_cluster_size(0));
+        if (cs >= 2) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cs);
+            cfg.blockDim = dim3(kClusterThreads);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cs;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve_cluster, a);
+            if (e != cudaSuccess) {
+                set_error("color_solve: cluster launch of %d CTAs: %s", cs, cudaGetErrorString(e));
+                return B2C_ECUDA;
+            }
+            if ((rc = check_launch("color_solve_cluster"))) return rc;
+        } else {
+            mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks());
+        }
     }
-    const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks()));
-    if (nblocks == 1) {
-        k_color_solve_block<<<1, 256, 0, s>>>(a);
-        return check_launch("color_solve_block");
+    if (mode > 0) {
+        const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks()));
+        if (nblocks == 1) {
+            k_color_solve_block<<<1, 256, 0, s>>>(a);
+            if ((rc = check_launch("color_solve_block"))) return rc;
+        } else {
+            cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (generation keeps counting)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nblocks);
+            cfg.blockDim = dim3(256);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve_grid, a);
+            if (e != cudaSuccess) {
+                set_error("color_solve: cooperative launch of %d blocks: %s", nblocks, cudaGetErrorString(e));
+                return B2C_ECUDA;
+            }
+            if ((rc = check_launch("color_solve_grid"))) return rc;
+        }
     }
-    cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nblocks);
-    cfg.blockDim = dim3(256);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve_grid, a);
-    if (e != cudaSuccess) {
-        set_error("color_solve: cooperative launch of %d blocks: %s", nblocks, cudaGetErrorString(e));
-        return B2C_ECUDA;
-    }
-    return check_launch("color_solve_grid");
+    k_imp_scatter<<<pgrid, kThreads, 0, s>>>(hdr, pr->pstart, pr->pidx, a.rec, kept->imp);
+    return check_launch("imp_scatter");
 }
 
 }  // namespace b2c
+
+extern "C" int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots)
+{
+    if (pair_capacity < 0 || kslots < 1) return -1;
+    return 4LL * (int64_t)pair_capacity * (1 + b2c::kRecBody + b2c::kRecContact * (int64_t)kslots);
+}

@@ -165,8 +165,11 @@ typedef struct b2c_pairs {
     float *cached_mass;      /* (bodies) invM of the cached colouring */
     int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
     uint32_t *barrier;       /* [count, generation] of the persistent solve's grid barrier */
-    float *prep;             /* (kept cap,16) per-contact terms that stay fixed during a solve:
-                                rA|meff, rB|meft1, t1|meft2, t2 (fixed tangent frame) */
+    float *rec;              /* colour-major pair records of the solve, b2c_pair_record_floats()
+                                floats: per slot a header, both bodies' inverse inertia and mass,
+                                and per contact its normal|depth, the terms that stay fixed
+                                during a solve (rA|meff, rB|meft1, t1|meft2, t2) and its impulses */
+    int32_t kslots;          /* contact slots per record (>= the most contacts one pair keeps) */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -204,6 +207,8 @@ B2C_API const char *b2c_last_error(void);
 /* kernel nodes in a captured cudaGraph_t (child graphs included); -1 on error.  Used to report
  * how many of this library's kernels one replayed step launches. */
 B2C_API int32_t b2c_graph_kernel_nodes(void *graph);
+/* floats of b2c_pairs.rec for `pair_capacity` pairs of up to `kslots` contacts each */
+B2C_API int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots);
 /* ints of scratch that b2c_exclusive_scan needs for n elements */
 B2C_API int32_t b2c_scan_scratch_ints(int32_t n);
 /* exclusive prefix sum of n int32 (device pointers); out may alias nothing */
