@@ -49,7 +49,17 @@ class Warm(ctypes.Structure):
 class ColorParams(ctypes.Structure):
     _fields_ = [("vit", c_int32), ("pit", c_int32), ("max_points", c_int32), ("flags", c_int32), ("mu", c_float),
                 ("t2d", c_float), ("color_cap", c_int32), ("solve_blocks", c_int32),
-                ("barrier_timeout_ns", ctypes.c_int64)]
+                ("barrier_timeout_ns", ctypes.c_int64), ("body_mu", c_void_p)]
+
+
+class Boxes(ctypes.Structure):
+    _fields_ = [("n", c_int32), ("half", c_void_p), ("mu", c_void_p), ("margin", c_float), ("cell", c_float),
+                ("dim_x", c_int32), ("dim_y", c_int32), ("dim_z", c_int32), ("cand_capacity", c_int32),
+                ("bucket", c_void_p), ("start", c_void_p), ("cursor", c_void_p), ("sorted", c_void_p),
+                ("cand_count", c_void_p), ("cand_offset", c_void_p), ("cand_a", c_void_p), ("cand_b", c_void_p),
+                ("cont_count", c_void_p), ("cont_offset", c_void_p), ("pair_flag", c_void_p),
+                ("pair_offset", c_void_p), ("slot_p", c_void_p), ("slot_n", c_void_p), ("slot_f", c_void_p),
+                ("scan_tmp", c_void_p)]
 
 
 COLOR_FIXED_FRAME = 1
@@ -106,6 +116,13 @@ _SIGS = {
     "b2c_warm_store": ([_P(Contacts), c_void_p, _P(Warm), c_void_p, c_void_p], c_int32),
     "b2c_color_substep": ([_P(Bodies), _P(Beads), _P(Grid), _P(Contacts), _P(Manifold), _P(Contacts), c_void_p,
                            _P(Pairs), _P(Warm), c_void_p, _P(ColorParams), c_float, c_void_p, c_void_p], c_int32),
+    "b2c_box_candidates": ([_P(Bodies), _P(Boxes), c_void_p, c_void_p], c_int32),
+    "b2c_box_contacts": ([_P(Bodies), _P(Boxes), _P(Contacts), c_void_p, _P(Pairs), _P(Warm), c_void_p,
+                          _P(ColorParams), c_void_p], c_int32),
+    "b2c_box_substep": ([_P(Bodies), _P(Boxes), _P(Contacts), c_void_p, _P(Pairs), _P(Warm), c_void_p,
+                         _P(ColorParams), c_float, c_void_p, c_void_p], c_int32),
+    "b2c_box_narrowphase_test": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
+                                  c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
 }
 
 _LIB = None

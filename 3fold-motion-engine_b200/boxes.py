@@ -1,0 +1,243 @@
+"""Box engine: box/plane + box/box narrowphase contacts solved by the coloured pair-chunk solve.
+
+The reference's box contact model is BoxWorld (src/motion_engine/ncp/ncp_gpu.py:1237-1405):
+solid boxes with per-body half extents, vertex-plane contacts against z = 0 and SAT box-box
+manifolds (<= 4 points per pair), generated on the host.  Here the same narrowphase (float64)
+runs on the device for every candidate pair of a body-AABB broadphase, and the contacts feed the
+coloured Gauss-Seidel pair solve of the ColorCache chain (fixed tangent frame, warm impulses
+applied once per colour, colouring cached while the pair graph and masses are unchanged).
+Per-body sizes and per-body friction (sqrt(mu_a mu_b) per pair, mu_a against the ground) are
+the superset the 10 000-random-box workload needs; with one size and a scalar mu it is the
+plain setting.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .colored import NCOLMAX
+from .engine import _BeadEngineBase, _pad4, _ptr
+
+MARGIN = 2e-3
+
+
+def box_body_arrays(centers, halves, dens, kin):
+    """Solid boxes (Box.Ib, ncp_gpu.py:1105-1109): mass = density * 8 hx hy hz,
+    Ib = m/12 diag(h_y^2 + h_z^2, ...) with full edges h = 2 half; float64, cast to float32."""
+    c = np.array(centers, float).reshape(-1, 3)
+    h = np.array(halves, float).reshape(-1, 3)
+    N = len(c)
+    M = np.array(dens, float) * 8.0 * h[:, 0] * h[:, 1] * h[:, 2]
+    kinarr = np.array(kin, int)
+    e = 2.0 * h
+    Ib = (M / 12.0)[:, None] * np.stack([e[:, 1] ** 2 + e[:, 2] ** 2, e[:, 0] ** 2 + e[:, 2] ** 2,
+                                         e[:, 0] ** 2 + e[:, 1] ** 2], axis=1)
+    IbInv = np.zeros((N, 3, 3))
+    for i in range(N):
+        IbInv[i] = np.eye(3) if kinarr[i] else np.linalg.inv(np.diag(Ib[i]))
+    if not np.all(np.isfinite(IbInv)) or np.any(M <= 0):
+        raise ValueError("box engine: degenerate box mass / inertia")
+    invM = np.where(kinarr == 1, 0.0, 1.0 / M)
+    return dict(xc=c.astype(np.float32), half=h.astype(np.float32), M=M, invM=invM.astype(np.float32),
+                IbInv=IbInv.astype(np.float32), kin=kinarr.astype(np.int32))
+
+
+class BoxContactEngine(_BeadEngineBase):
+    """ContactEngine over solid boxes (box/plane + box/box contacts) with the ColorCache solve."""
+    name = "box_color_cache_b200"
+
+    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, fixed_frame=True, apply_warm=True,
+                 color_cache=True, warm_start=True, margin=MARGIN, device="cuda", color_cap=NCOLMAX,
+                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16):
+        super().__init__(dims=dims, mu=mu, device=device, graph=True)
+        self.vit, self.pit = int(vit), int(pit)
+        self.fixed_frame, self.apply_warm = bool(fixed_frame), bool(apply_warm)
+        self.color_cache, self.warm_start = bool(color_cache), bool(warm_start)
+        self.margin = float(margin)
+        self.color_cap = int(color_cap)
+        self.solve_blocks = int(solve_blocks)
+        self.barrier_timeout_ns = int(barrier_timeout_s * 1e9)
+        self.cand_per_body = int(cand_per_body)
+        self._halves, self._mus = [], []
+        self._has_manifold = True
+
+    def add_body(self, center, density=700.0, kin=False):
+        return self.add_box(center, dims=self.dims, density=density, kin=kin)
+
+    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False):
+        d = self.dims if dims is None else tuple(float(x) for x in dims)
+        self._halves.append([0.5 * d[0], 0.5 * d[1], 0.5 * d[2]])
+        self._mus.append(self.mu if mu is None else float(mu))
+        return super().add_body(center, density=density, kin=kin)
+
+    def _build(self):
+        A = box_body_arrays(self._centers, self._halves, self._dens, self._kin)
+        N = len(self._centers)
+        self.N = N
+        self._M = A["M"]
+        self._kinarr = A["kin"].astype(int)
+        dev = self.dev
+        f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+        i32 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int32, device=dev)
+        self.xc = f32(_pad4(A["xc"]))
+        self.q = f32(np.tile(np.array([0, 0, 0, 1.0], np.float32), (N, 1)))
+        z4 = lambda: torch.zeros((N, 4), dtype=torch.float32, device=dev)
+        self.v, self.w, self.pv, self.po, self.vgrav = z4(), z4(), z4(), z4(), z4()
+        self.invM = f32(A["invM"])
+        Ib12 = np.zeros((N, 3, 4), np.float32)
+        Ib12[:, :, :3] = A["IbInv"]
+        self.IbInv = f32(Ib12.reshape(N, 12))
+        self.kin = torch.from_numpy(A["kin"]).to(dev)
+        self.invIw = torch.zeros((N, 12), dtype=torch.float32, device=dev)
+        self.half = f32(_pad4(A["half"]))
+        mus = np.array(self._mus, np.float32)
+        self.per_body_mu = bool(np.any(mus != np.float32(self.mu)))
+        self.body_mu = f32(mus)
+        self.header = torch.zeros(8, dtype=torch.int32, device=dev)
+        self._hdr_host = torch.zeros(8, dtype=torch.int32, pin_memory=True)
+        # broadphase grid over body centres
+        hmax = float(np.max(np.linalg.norm(A["half"], axis=1))) if N else 0.5
+        cell = 1.01 * (2.0 * hmax + self.margin)  # every sphere-test pair lies in adjacent cells
+        dims = (32, 32, 16) if N > 2000 else (16, 16, 8)
+        nbk = dims[0] * dims[1] * dims[2]
+        cand_cap = max(self.cand_per_body * N + N, 64)
+        kept_cap = 4 * cand_cap + 8 * N
+        self.bx_bufs = dict(bucket=i32(N), start=i32(nbk + 1), cursor=i32(nbk + 1), sorted=i32(N), cand_count=i32(N + 1),
+                            cand_offset=i32(N + 1), cand_a=i32(cand_cap), cand_b=i32(cand_cap),
+                            cont_count=i32(cand_cap + 1), cont_offset=i32(cand_cap + 1), pair_flag=i32(cand_cap + 1),
+                            pair_offset=i32(cand_cap + 1),
+                            slot_p=torch.zeros((cand_cap * 8, 4), dtype=torch.float32, device=dev),
+                            slot_n=torch.zeros((cand_cap, 4), dtype=torch.float32, device=dev),
+                            slot_f=i32(cand_cap * 8),
+                            scan_tmp=i32(self.L.b2c_scan_scratch_ints(max(nbk, N, cand_cap) + 1)))
+        b = self.bx_bufs
+        self.c_boxes = _lib.Boxes(N, _ptr(self.half), _ptr(self.body_mu), self.margin, cell, dims[0], dims[1], dims[2],
+                                  cand_cap, *(_ptr(b[k]) for k in (
+                                      "bucket", "start", "cursor", "sorted", "cand_count", "cand_offset", "cand_a",
+                                      "cand_b", "cont_count", "cont_offset", "pair_flag", "pair_offset", "slot_p",
+                                      "slot_n", "slot_f", "scan_tmp")))
+        # kept contacts, pairs, colouring, records, warm store
+        i64 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int64, device=dev)
+        f4 = lambda n: torch.zeros((max(int(n), 1), 4), dtype=torch.float32, device=dev)
+        self.k_bi, self.k_bj, self.k_fa, self.k_fb = i32(kept_cap), i32(kept_cap), i32(kept_cap), i32(kept_cap)
+        self.k_pA, self.k_pB, self.k_n, self.k_imp = f4(kept_cap), f4(kept_cap), f4(kept_cap), f4(kept_cap)
+        self.k_keys = i64(kept_cap)
+        self.c_kept = _lib.Contacts(kept_cap, _ptr(self.k_bi), _ptr(self.k_bj), _ptr(self.k_pA), _ptr(self.k_pB),
+                                    _ptr(self.k_n), _ptr(self.k_fa), _ptr(self.k_fb), _ptr(self.k_imp))
+        pcap, kslots = cand_cap, 8
+        self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(kept_cap),
+                           col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
+                           cached_a=i32(pcap), cached_b=i32(pcap),
+                           cached_mass=torch.zeros(max(N, 1), dtype=torch.float32, device=dev), cache_state=i32(8),
+                           barrier=torch.zeros(2, dtype=torch.int32, device=dev),
+                           rec=torch.zeros(max(int(self.L.b2c_pair_record_floats(pcap, kslots)), 1),
+                                           dtype=torch.float32, device=dev))
+        pb = self.p_bufs
+        self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
+            "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
+            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots)
+        self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
+        self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
+        self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
+                                    _ptr(self.po), _ptr(self.invM), _ptr(self.IbInv), _ptr(self.kin), _ptr(self.invIw))
+        flags = ((_lib.COLOR_FIXED_FRAME if self.fixed_frame else 0) | (_lib.COLOR_APPLY_WARM if self.apply_warm else 0)
+                 | (_lib.COLOR_CACHE if self.color_cache else 0) | (_lib.COLOR_WARM_START if self.warm_start else 0))
+        self.c_params = _lib.ColorParams(self.vit, self.pit, 8, flags, self.mu, 1.0, min(self.color_cap, NCOLMAX),
+                                         self.solve_blocks, self.barrier_timeout_ns,
+                                         _ptr(self.body_mu) if self.per_body_mu else None)
+        self._graphs = {}
+        self._built = True
+
+    def _launch_step(self, sdt, substeps):
+        s = torch.cuda.current_stream(self.dev).cuda_stream
+        for _ in range(substeps):
+            rc = self.L.b2c_box_substep(ctypes.byref(self.c_bodies), ctypes.byref(self.c_boxes),
+                                        ctypes.byref(self.c_kept), ctypes.c_void_p(_ptr(self.k_keys)),
+                                        ctypes.byref(self.c_pairs), ctypes.byref(self.c_warm),
+                                        ctypes.c_void_p(_ptr(self.header)), ctypes.byref(self.c_params),
+                                        ctypes.c_float(sdt), ctypes.c_void_p(_ptr(self.vgrav)), ctypes.c_void_p(s))
+            _lib.check(rc, "b2c_box_substep")
+
+    def step(self, dt, substeps=1):
+        if not self._built:
+            self._build()
+        self.check_errors()
+        sdt = dt / substeps
+        self._graph_step(("box", float(sdt), int(substeps)), lambda: self._launch_step(sdt, substeps))
+        self._force_dt = sdt
+        self._fetch_header()
+
+    def set_kinematic(self, i, xc):
+        super().set_kinematic(i, xc)
+
+    @property
+    def color_cache_hits(self):
+        return int(self.p_bufs["cache_state"][3].item()) if self._built else 0
+
+    @property
+    def color_cache_misses(self):
+        return int(self.p_bufs["cache_state"][4].item()) if self._built else 0
+
+    def set_body_state(self, xc, q, v, w):
+        if not self._built:
+            self._build()
+        for dst, src, k in ((self.xc, xc, 3), (self.q, q, 4), (self.v, v, 3), (self.w, w, 3)):
+            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float32))
+            dst[:, :k].copy_(t, non_blocking=True)
+
+    # staged substep with CUDA events (profiling); same launches as b2c_box_substep
+    STAGES = ("predict", "candidates", "narrowphase", "colour", "solve", "warm_store", "integrate")
+
+    def profile_substep(self, dt):
+        if not self._built:
+            self._build()
+        self.check_errors()
+        L, b = self.L, ctypes.byref
+        stream = torch.cuda.current_stream(self.dev)
+        s = ctypes.c_void_p(stream.cuda_stream)
+        hdr = ctypes.c_void_p(_ptr(self.header))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(self.STAGES) + 1)]
+        sdt = ctypes.c_float(dt)
+        ev[0].record(stream)
+        _lib.check(L.b2c_body_predict(b(self.c_bodies), sdt, s), "predict")
+        self.vgrav.copy_(self.v)
+        self.pv.zero_()
+        self.po.zero_()
+        ev[1].record(stream)
+        _lib.check(L.b2c_box_candidates(b(self.c_bodies), b(self.c_boxes), hdr, s), "candidates")
+        ev[2].record(stream)
+        _lib.check(L.b2c_box_contacts(b(self.c_bodies), b(self.c_boxes), b(self.c_kept),
+                                      ctypes.c_void_p(_ptr(self.k_keys)), b(self.c_pairs), b(self.c_warm), hdr,
+                                      b(self.c_params), s), "narrowphase")
+        ev[3].record(stream)
+        _lib.check(L.b2c_color_pairs(b(self.c_bodies), b(self.c_pairs), hdr, b(self.c_params), s), "colour")
+        ev[4].record(stream)
+        _lib.check(L.b2c_color_solve(b(self.c_bodies), b(self.c_kept), b(self.c_pairs), hdr, b(self.c_params), sdt, s),
+                   "solve")
+        ev[5].record(stream)
+        _lib.check(L.b2c_warm_store(b(self.c_kept), ctypes.c_void_p(_ptr(self.k_keys)), b(self.c_warm), hdr, s),
+                   "warm_store")
+        ev[6].record(stream)
+        _lib.check(L.b2c_body_integrate(b(self.c_bodies), sdt, s), "integrate")
+        ev[7].record(stream)
+        self._force_dt = dt
+        self._fetch_header()
+        ev[7].synchronize()
+        return {name: ev[i].elapsed_time(ev[i + 1]) for i, name in enumerate(self.STAGES)}
+
+    def solve_bytes(self) -> dict:
+        """Algorithmic bytes of one persistent-solve launch (see GraphColoredContactEngine.solve_bytes)."""
+        h = self.header_dict()
+        P, Ck = h["n_pairs"], h["n_kept"]
+        pbi = self.p_bufs["pbi"][:P].cpu().numpy()
+        pbj = self.p_bufs["pbj"][:P].cpu().numpy()
+        invM = self.invM.cpu().numpy()
+        E = int(np.sum(invM[pbi] > 0) + np.sum((pbj >= 0) & (invM[np.maximum(pbj, 0)] > 0)))
+        per_vel = 20 * P + 100 * E + 64 * Ck
+        per_pos = 20 * P + 100 * E + 52 * Ck
+        warm = per_pos if self.apply_warm else 0
+        return dict(pairs=P, kept=Ck, endpoints=E, colors=h["n_colors"],
+                    bytes=warm + self.vit * per_vel + self.pit * per_pos)

@@ -32,6 +32,7 @@ B2C_HD f3 sub3(f3 a, f3 b) { return f3{a.x - b.x, a.y - b.y, a.z - b.z}; }
 B2C_HD f3 scale3(f3 a, float s) { return f3{a.x * s, a.y * s, a.z * s}; }
 B2C_HD f3 div3(f3 a, float s) { return f3{a.x / s, a.y / s, a.z / s}; }  // wp.div(vec3, float)
 B2C_HD f3 xyz(float4 a) { return f3{a.x, a.y, a.z}; }
+B2C_HD qf qf4(float4 a) { return qf{a.x, a.y, a.z, a.w}; }
 B2C_HD float4 f4(f3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
 
 // wp.dot(vec3, vec3): a0*b0 + a1*b1 + a2*b2

@@ -71,7 +71,8 @@ __global__ void k_pair_gather(const b2c_header *__restrict__ hdr, const int *__r
                               const int *__restrict__ pstart, const int *__restrict__ pcount,
                               const int *__restrict__ pidx, const int *__restrict__ pbi, const int *__restrict__ pbj,
                               b2c_contacts kept, const float *__restrict__ xc, const float *__restrict__ invIw,
-                              const float *__restrict__ invM, Records R, b2c_header *hdr_w)
+                              const float *__restrict__ invM, const float *__restrict__ body_mu, float mu, Records R,
+                              b2c_header *hdr_w)
 {
     const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
@@ -97,7 +98,10 @@ __global__ void k_pair_gather(const b2c_header *__restrict__ hdr, const int *__r
         R.body(3)[s] = f4(IB.r0, 0.0f);
         R.body(4)[s] = f4(IB.r1, 0.0f);
         R.body(5)[s] = f4(IB.r2, 0.0f);
-        R.body(6)[s] = make_float4(iMA, iMB, 0.0f, 0.0f);
+        // friction of the pair: the scalar mu, or sqrt(mu_a mu_b) (ground pair: mu_a) per body
+        float mu_p = mu;
+        if (body_mu) mu_p = bj >= 0 ? sqrtf(body_mu[bi] * body_mu[bj]) : body_mu[bi];
+        R.body(6)[s] = make_float4(iMA, iMB, mu_p, 0.0f);
         const f3 xA = ld3(xc, bi);
         f3 xB{0.0f, 0.0f, 0.0f};
         if (bj >= 0) xB = ld3(xc, bj);
@@ -226,7 +230,7 @@ struct GlobalBodies {
 struct PairBodies {
     int bi, bj, n;
     m3 IA, IB;
-    float iMA, iMB;
+    float iMA, iMB, mu;
 };
 __device__ __forceinline__ PairBodies load_pair(const Records &R, int s)
 {
@@ -241,6 +245,7 @@ __device__ __forceinline__ PairBodies load_pair(const Records &R, int s)
     q.IB = m3{xyz(j0), xyz(j1), xyz(j2)};
     q.iMA = mm.x;
     q.iMB = mm.y;
+    q.mu = mm.z;
     return q;
 }
 struct CRec {
@@ -361,7 +366,7 @@ __device__ void pair_velocity(const SolveArgs &a, int s, const BA &B)
                 float a1 = o1 - dot3(vrel, t1) / meft1;
                 float a2 = o2 - dot3(vrel, t2) / meft2;
                 const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-                const float lim = a.mu * im.x;
+                const float lim = q.mu * im.x;
                 if (mag > lim && mag > 1e-12f) {
                     a1 = a1 * lim / mag;
                     a2 = a2 * lim / mag;
@@ -576,7 +581,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
     k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
-                                             *kept, b->xc, b->invIw, b->invM, a.rec, hdr);
+                                             *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, a.rec, hdr);
     int rc = check_launch("pair_gather");
     if (rc) return rc;
 

@@ -180,6 +180,33 @@ typedef struct b2c_warm {
     int32_t *n;              /* (1) entries stored */
 } b2c_warm;
 
+/* Boxes for the box/plane + box/box narrowphase (ncp/ncp_gpu.py:1097-1227): per-body half
+ * extents, a body-AABB hash grid, candidate pairs and per-candidate contact slots. */
+typedef struct b2c_boxes {
+    int32_t n;
+    const float *half;        /* (n,4) half extents */
+    const float *mu;          /* (n) friction per body (contact: sqrt(mu_a mu_b), ground: mu_a) or NULL */
+    float margin;             /* contact margin (the reference's 2e-3) */
+    float cell;               /* broadphase cell >= 2 x the largest AABB half extent + margin */
+    int32_t dim_x, dim_y, dim_z; /* broadphase hash-grid dims (>= 8 each) */
+    int32_t cand_capacity;    /* candidate pairs (ground + box-box) */
+    int32_t *bucket;          /* (n) */
+    int32_t *start;           /* (dims+1) */
+    int32_t *cursor;          /* (dims+1) */
+    int32_t *sorted;          /* (n) */
+    int32_t *cand_count;      /* (n+1) candidates owned by each body */
+    int32_t *cand_offset;     /* (n+1) */
+    int32_t *cand_a, *cand_b; /* (cand cap) candidate pair, b = -1 for the ground */
+    int32_t *cont_count;      /* (cand cap+1) contacts of each candidate */
+    int32_t *cont_offset;     /* (cand cap+1) */
+    int32_t *pair_flag;       /* (cand cap+1) 1 when the candidate has contacts */
+    int32_t *pair_offset;     /* (cand cap+1) */
+    float *slot_p;            /* (cand cap x 8, 4) contact point | gap */
+    float *slot_n;            /* (cand cap, 4) normal from b to a */
+    int32_t *slot_f;          /* (cand cap x 8) feature id */
+    int32_t *scan_tmp;        /* b2c_scan_scratch_ints(max(dims, n, cand cap) + 1) */
+} b2c_boxes;
+
 /* Flags of b2c_color_params.flags */
 #define B2C_COLOR_FIXED_FRAME 1  /* normal-derived tangent frame (contact_engine_gpu_fixed_frame.py) */
 #define B2C_COLOR_APPLY_WARM 2   /* apply the warm impulses once per colour before the sweeps */
@@ -199,6 +226,8 @@ typedef struct b2c_color_params {
                                 with a grid barrier (1 = one CTA, block barriers); -n = a thread-block
                                 cluster of n CTAs with the hardware cluster barrier */
     int64_t barrier_timeout_ns; /* grid-barrier wait limit */
+    const float *body_mu;    /* (bodies) per-body friction, or NULL for the scalar mu: a body pair's
+                                contacts use sqrt(mu_a mu_b), a ground pair mu_a */
 } b2c_color_params;
 
 /* ---- version / errors ---- */
@@ -278,6 +307,29 @@ B2C_API int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads, b
                                   b2c_manifold *m, b2c_contacts *kept, int64_t *kept_keys, b2c_pairs *pr,
                                   b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, float dt,
                                   float *vgrav, b2c_stream s);
+
+/* ---- box engine: body-AABB broadphase + box/plane and box/box narrowphase ---- */
+/* Candidate pairs from a uniform hash grid over the body centres: per body its ground
+ * candidate (when its AABB reaches z < margin) and every later body whose AABB overlaps, in
+ * ascending order (the reference tests all pairs, BoxWorld.contacts, ncp_gpu.py:1273-1280). */
+B2C_API int32_t b2c_box_candidates(const b2c_bodies *b, b2c_boxes *bx, b2c_header *hdr, b2c_stream s);
+/* float64 SAT per candidate (box_plane_contacts / box_box_contacts, ncp_gpu.py:1148-1227), then
+ * compaction into kept contacts (pair order, feature order inside a pair, point on both bodies,
+ * depth = -gap) with warm-started impulses, and the pair arrays of the coloured solve. */
+B2C_API int32_t b2c_box_contacts(const b2c_bodies *b, b2c_boxes *bx, b2c_contacts *kept, int64_t *kept_keys,
+                                 b2c_pairs *pr, const b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p,
+                                 b2c_stream s);
+/* One box-engine substep: predict, candidates, narrowphase, colouring (cached), the persistent
+ * chunk solve, warm store, integrate. */
+B2C_API int32_t b2c_box_substep(const b2c_bodies *b, b2c_boxes *bx, b2c_contacts *kept, int64_t *kept_keys,
+                                b2c_pairs *pr, b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p,
+                                float dt, float *vgrav, b2c_stream s);
+/* One box pair / one box and the ground through the device narrowphase (for parity checks):
+ * inputs (n,4) half, x, q for a and b; per pair up to 8 points (8,4 = point|gap), a normal
+ * (4), 8 feature ids and a count.  b_half == NULL means box a against the ground. */
+B2C_API int32_t b2c_box_narrowphase_test(int32_t n, const float *a_half, const float *a_x, const float *a_q,
+                                         const float *b_half, const float *b_x, const float *b_q, float margin,
+                                         double *pts, double *nrm, int32_t *fid, int32_t *count, b2c_stream s);
 
 #ifdef __cplusplus
 }

@@ -302,3 +302,108 @@ class ColoredOracle:
         nk = self.b.kin == 0
         f[nk] = self.b.M[nk, None] * (self.b.v[nk] - self.vgrav[nk]) / self._force_dt
         return f
+
+
+def _box_sigs(L):
+    P = ctypes.c_void_p
+    L.or_box_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_float, P, P, P, P, P, P, P, P, P,
+                              ctypes.c_double, ctypes.c_int, ctypes.c_double, P]
+    L.or_box_step.restype = ctypes.c_int
+    L.or_box_box.argtypes = [P, P, P, P, P, P, ctypes.c_double, P, P, P, P]
+    L.or_box_box.restype = ctypes.c_int
+    L.or_box_plane.argtypes = [P, P, P, ctypes.c_double, P, P, P]
+    L.or_box_plane.restype = ctypes.c_int
+
+
+def box_plane(half, x, q, margin=2e-3):
+    """Oracle box_plane_contacts (ncp_gpu.py:1148-1154): (points (m,3), gaps (m,), feature ids)."""
+    L = lib(); _box_sigs(L)
+    a = [np.ascontiguousarray(v, np.float64) for v in (half, x, q)]
+    po, go, fo = np.zeros(24), np.zeros(8), np.zeros(8, np.int32)
+    m = L.or_box_plane(*[_p(v) for v in a], float(margin), _p(po), _p(go), _p(fo))
+    return po[:3 * m].reshape(m, 3), go[:m], fo[:m]
+
+
+def box_box(ha, xa, qa, hb, xb, qb, margin=2e-3):
+    """Oracle box_box_contacts (ncp_gpu.py:1157-1227): (points (m,3), normal B->A, gaps, feature ids)."""
+    L = lib(); _box_sigs(L)
+    a = [np.ascontiguousarray(v, np.float64) for v in (ha, xa, qa, hb, xb, qb)]
+    po, no, go, fo = np.zeros(12), np.zeros(3), np.zeros(4), np.zeros(4, np.int32)
+    m = L.or_box_box(*[_p(v) for v in a], float(margin), _p(po), _p(no), _p(go), _p(fo))
+    return po[:3 * m].reshape(m, 3), no, go[:m], fo[:m]
+
+
+class BoxOracle:
+    """CPU restatement of the box engine: all-pairs box/plane + box/box narrowphase (BoxWorld.contacts,
+    ncp_gpu.py:1273-1280) with the ColorCache pair solve of the coloured chain, per-body friction."""
+    name = "box_color_cache_oracle"
+
+    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=15, margin=2e-3, cap=MAXC):
+        self.dims = dims; self.mu = mu; self.vit = vit; self.pit = pit; self.flags = flags; self.margin = margin
+        self.cap = cap
+        self._centers, self._halves, self._dens, self._mus, self._kin = [], [], [], [], []
+        self.b = None; self._h = None; self._force_dt = None
+
+    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False):
+        d = self.dims if dims is None else dims
+        self._centers.append(list(center)); self._halves.append([0.5 * d[0], 0.5 * d[1], 0.5 * d[2]])
+        self._dens.append(float(density)); self._mus.append(self.mu if mu is None else float(mu))
+        self._kin.append(1 if kin else 0)
+        self.b = None
+        return len(self._centers) - 1
+
+    def _build(self):
+        L = lib()
+        if not hasattr(L, "_col_ready"):
+            _col_sigs(L); L._col_ready = True
+        _box_sigs(L)
+        c = np.array(self._centers, float); h = np.array(self._halves, float); N = len(c)
+        M = np.array(self._dens) * 8.0 * h[:, 0] * h[:, 1] * h[:, 2]
+        e = 2.0 * h
+        Ib = (M / 12.0)[:, None] * np.stack([e[:, 1] ** 2 + e[:, 2] ** 2, e[:, 0] ** 2 + e[:, 2] ** 2,
+                                             e[:, 0] ** 2 + e[:, 1] ** 2], axis=1)
+        kin = np.array(self._kin, int)
+        IbInv = np.array([np.eye(3) if kin[i] else np.linalg.inv(np.diag(Ib[i])) for i in range(N)])
+        self.N = N
+        self.b = BodySetup(rest=np.zeros((0, 3), np.float32), xc=c.astype(np.float32),
+                           q=np.tile(np.array([0, 0, 0, 1.0], np.float32), (N, 1)),
+                           v=np.zeros((N, 3), np.float32), w=np.zeros((N, 3), np.float32),
+                           invM=np.where(kin == 1, 0.0, 1.0 / M).astype(np.float32),
+                           IbInv=IbInv.astype(np.float32), kin=kin.astype(np.int32), M=M)
+        self.half4 = np.zeros((N, 4), np.float32); self.half4[:, :3] = h
+        self.mus = np.array(self._mus, np.float32)
+        self.per_body = bool(np.any(self.mus != np.float32(self.mu)))
+        self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
+        self.vgrav = np.zeros((N, 3), np.float32)
+        self._h = L.or_col_create(1, self.vit, self.pit, 4, self.mu, 1.0, self.cap, N)
+
+    def step(self, dt, substeps=1):
+        if self.b is None:
+            self._build()
+        b = self.b
+        rc = lib().or_box_step(self._h, self.flags, self.N, _p(self.half4), _p(self.mus) if self.per_body else None,
+                               float(self.mu), _p(b.xc), _p(b.q), _p(b.v), _p(b.w), _p(self.pv), _p(self.po),
+                               _p(b.invM), _p(b.IbInv), _p(b.kin), float(dt), int(substeps),
+                               float(np.float32(self.margin)), _p(self.vgrav))
+        if rc != 0:
+            raise RuntimeError(f"oracle box step failed with status {rc}")
+        self._force_dt = dt / substeps
+
+    def stats(self):
+        out = np.zeros(7, np.int32)
+        lib().or_col_stats(self._h, _p(out))
+        return dict(zip(("n_contacts", "n_kept", "n_pairs", "n_colors", "hits", "misses", "seg_overflow"),
+                        out.tolist()))
+
+    def get_state(self) -> State:
+        if self.b is None:
+            self._build()
+        return State(xc=self.b.xc.copy(), Rm=quat_to_R(self.b.q), vc=self.b.v.copy(), om=self.b.w.copy())
+
+    def contact_forces(self):
+        f = np.zeros((len(self._centers), 3))
+        if self.b is None or self._force_dt is None:
+            return f
+        nk = self.b.kin == 0
+        f[nk] = self.b.M[nk, None] * (self.b.v[nk] - self.vgrav[nk]) / self._force_dt
+        return f

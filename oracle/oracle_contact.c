@@ -1184,3 +1184,429 @@ OR_API void or_integrate(int N, float *xc, float *q, const float *v, const float
 {
     body_integrate(N, xc, q, v, w, pv, po, invM, dt);
 }
+
+/* ================================================================== */
+/* Box/plane and box/box narrowphase, float64 (ncp/ncp_gpu.py:1112-1227) */
+/* ================================================================== */
+typedef struct { double x, y, z; } d3;
+static inline d3 D3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static inline d3 dadd(d3 a, d3 b) { return D3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline d3 dsub(d3 a, d3 b) { return D3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline d3 dscale(d3 a, double s) { return D3(a.x * s, a.y * s, a.z * s); }
+static inline double ddot(d3 a, d3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline d3 dcross(d3 a, d3 b) { return D3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline double dget(d3 a, int i) { return i == 0 ? a.x : i == 1 ? a.y : a.z; }
+
+typedef struct { d3 col[3]; } dR;          /* rotation as columns R[:, i] */
+
+/* _quat_to_R, ncp_gpu.py:1089-1093 (rows of the matrix, stored as columns here) */
+static dR dquat_R(const double *q)
+{
+    double x = q[0], y = q[1], z = q[2], w = q[3];
+    double r00 = 1 - 2 * (y * y + z * z), r01 = 2 * (x * y - z * w), r02 = 2 * (x * z + y * w);
+    double r10 = 2 * (x * y + z * w), r11 = 1 - 2 * (x * x + z * z), r12 = 2 * (y * z - x * w);
+    double r20 = 2 * (x * z - y * w), r21 = 2 * (y * z + x * w), r22 = 1 - 2 * (x * x + y * y);
+    dR R;
+    R.col[0] = D3(r00, r10, r20);
+    R.col[1] = D3(r01, r11, r21);
+    R.col[2] = D3(r02, r12, r22);
+    return R;
+}
+static inline d3 dR_apply(const dR *R, d3 a)  /* R @ a */
+{
+    return D3((R->col[0].x * a.x + R->col[1].x * a.y) + R->col[2].x * a.z,
+              (R->col[0].y * a.x + R->col[1].y * a.y) + R->col[2].y * a.z,
+              (R->col[0].z * a.x + R->col[1].z * a.y) + R->col[2].z * a.z);
+}
+static inline d3 dRT_apply(const dR *R, d3 a)  /* R^T @ a */
+{
+    return D3(ddot(R->col[0], a), ddot(R->col[1], a), ddot(R->col[2], a));
+}
+/* _corners, ncp_gpu.py:1112-1117: corner k = x + R (s * half), s = (+-1,+-1,+-1), k = 4 ix + 2 iy + iz */
+static void dcorners(d3 half, d3 x, const dR *R, d3 out[8])
+{
+    for (int k = 0; k < 8; ++k) {
+        d3 s = D3((k & 4) ? 1.0 : -1.0, (k & 2) ? 1.0 : -1.0, (k & 1) ? 1.0 : -1.0);
+        out[k] = dadd(x, dR_apply(R, D3(s.x * half.x, s.y * half.y, s.z * half.z)));
+    }
+}
+/* _face_corners, ncp_gpu.py:1120-1126 */
+static void dface(d3 half, d3 x, const dR *R, int axis, double sgn, d3 poly[4], d3 *n, d3 *c)
+{
+    int i = axis, j = (axis + 1) % 3, k = (axis + 2) % 3;
+    *n = dscale(R->col[i], sgn);
+    *c = dadd(x, dscale(*n, dget(half, i)));
+    d3 u = dscale(R->col[j], dget(half, j)), v = dscale(R->col[k], dget(half, k));
+    poly[0] = dadd(dadd(*c, u), v);
+    poly[1] = dadd(dsub(*c, u), v);
+    poly[2] = dsub(dsub(*c, u), v);
+    poly[3] = dsub(dadd(*c, u), v);
+}
+/* _clip, ncp_gpu.py:1129-1145: Sutherland-Hodgman against |(p-c).ax| <= ha; n <= 8 -> <= 8 */
+static int dclip(d3 *poly, int n, d3 c, d3 ax, double ha)
+{
+    d3 out[16];
+    for (int si = 0; si < 2; ++si) {
+        double s = si == 0 ? 1.0 : -1.0;
+        int m = 0;
+        for (int i = 0; i < n; ++i) {
+            d3 p = poly[i], q = poly[(i + 1) % n];
+            double dp = s * ddot(dsub(p, c), ax) - ha;
+            double dq = s * ddot(dsub(q, c), ax) - ha;
+            if (dp <= 0) out[m++] = p;
+            if (dp * dq < 0) out[m++] = dadd(p, dscale(dsub(q, p), dp / (dp - dq)));
+        }
+        for (int i = 0; i < m; ++i) poly[i] = out[i];
+        n = m;
+        if (n == 0) return 0;
+    }
+    return n;
+}
+
+/* box_plane_contacts, ncp_gpu.py:1148-1154 */
+OR_API int or_box_plane(const double *half, const double *x, const double *q, double margin, double *p_out,
+                        double *g_out, int *f_out)
+{
+    dR R = dquat_R(q);
+    d3 cs[8];
+    dcorners(D3(half[0], half[1], half[2]), D3(x[0], x[1], x[2]), &R, cs);
+    int m = 0;
+    for (int k = 0; k < 8; ++k)
+        if (cs[k].z < margin) {
+            p_out[3 * m] = cs[k].x; p_out[3 * m + 1] = cs[k].y; p_out[3 * m + 2] = cs[k].z;
+            g_out[m] = cs[k].z; f_out[m] = k; m++;
+        }
+    return m;
+}
+
+typedef struct { double sp; int kind; int idx; d3 ax; int set; } sat_best_t;
+
+/* sep_of, ncp_gpu.py:1166-1170 */
+static inline double dsep(d3 ax, d3 d, const dR *Ra, d3 ha, const dR *Rb, d3 hb, d3 *axo)
+{
+    d3 a = dRT_apply(Ra, ax), b = dRT_apply(Rb, ax);
+    double ra = (fabs(a.x) * ha.x + fabs(a.y) * ha.y) + fabs(a.z) * ha.z;
+    double rb = (fabs(b.x) * hb.x + fabs(b.y) * hb.y) + fabs(b.z) * hb.z;
+    double proj = ddot(d, ax);
+    *axo = proj >= 0 ? ax : dscale(ax, -1.0);
+    return fabs(proj) - (ra + rb);
+}
+
+/* box_box_contacts, ncp_gpu.py:1157-1227.  Normal points from B to A; <= 4 points. */
+OR_API int or_box_box(const double *ha_, const double *xa_, const double *qa, const double *hb_, const double *xb_,
+                      const double *qb, double margin, double *p_out, double *n_out, double *g_out, int *f_out)
+{
+    d3 ha = D3(ha_[0], ha_[1], ha_[2]), hb = D3(hb_[0], hb_[1], hb_[2]);
+    d3 xa = D3(xa_[0], xa_[1], xa_[2]), xb = D3(xb_[0], xb_[1], xb_[2]);
+    dR Ra = dquat_R(qa), Rb = dquat_R(qb);
+    d3 d = dsub(xb, xa);
+    sat_best_t F = {0}, E = {0};
+    for (int kind = 0; kind < 2; ++kind) {
+        const dR *R = kind == 0 ? &Ra : &Rb;
+        for (int i = 0; i < 3; ++i) {
+            d3 ax;
+            double sp = dsep(R->col[i], d, &Ra, ha, &Rb, hb, &ax);
+            if (sp > margin) return 0;
+            double better = (F.set && kind == 1 && F.kind == 0) ? 1e-4 : 1e-12;
+            if (!F.set || sp > F.sp + better) { F.sp = sp; F.kind = kind; F.idx = i; F.ax = ax; F.set = 1; }
+        }
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            d3 cr = dcross(Ra.col[i], Rb.col[j]);
+            double nn = sqrt(ddot(cr, cr));
+            if (nn <= 1e-6) continue;
+            d3 ax;
+            double sp = dsep(dscale(cr, 1.0 / nn), d, &Ra, ha, &Rb, hb, &ax);
+            if (sp > margin) return 0;
+            if (!E.set || sp > E.sp + 1e-12) { E.sp = sp; E.kind = 2; E.idx = 3 * i + j; E.ax = ax; E.set = 1; }
+        }
+    if (E.set && E.sp > F.sp + 1e-3) {
+        d3 ca[8], cb[8];
+        dcorners(ha, xa, &Ra, ca);
+        dcorners(hb, xb, &Rb, cb);
+        int ka = 0, kb = 0;
+        double best_a = ddot(ca[0], E.ax), best_b = ddot(cb[0], E.ax);
+        for (int k = 1; k < 8; ++k) {
+            double da = ddot(ca[k], E.ax), db = ddot(cb[k], E.ax);
+            if (da > best_a) { best_a = da; ka = k; }
+            if (db < best_b) { best_b = db; kb = k; }
+        }
+        d3 p = dscale(dadd(ca[ka], cb[kb]), 0.5);
+        p_out[0] = p.x; p_out[1] = p.y; p_out[2] = p.z;
+        n_out[0] = -E.ax.x; n_out[1] = -E.ax.y; n_out[2] = -E.ax.z;
+        g_out[0] = E.sp; f_out[0] = 100 + E.idx;
+        return 1;
+    }
+    d3 nAB = F.ax, nBA;
+    d3 rhalf, rx, ihalf, ix;
+    const dR *rR, *iR;
+    int raxis = F.idx;
+    double rsgn;
+    if (F.kind == 0) {
+        rhalf = ha; rx = xa; rR = &Ra; ihalf = hb; ix = xb; iR = &Rb;
+        rsgn = ddot(Ra.col[raxis], nAB) >= 0 ? 1.0 : -1.0;
+        nBA = dscale(nAB, -1.0);
+    } else {
+        rhalf = hb; rx = xb; rR = &Rb; ihalf = ha; ix = xa; iR = &Ra;
+        rsgn = ddot(Rb.col[raxis], dscale(nAB, -1.0)) >= 0 ? 1.0 : -1.0;
+        nBA = nAB;
+    }
+    d3 rpoly[4], rn, rc;
+    dface(rhalf, rx, rR, raxis, rsgn, rpoly, &rn, &rc);
+    int mmin = 0;
+    double dmin = 0;
+    for (int a = 0; a < 3; ++a)
+        for (int sg = 0; sg < 2; ++sg) {
+            double v = ddot(dscale(iR->col[a], sg == 0 ? 1.0 : -1.0), rn);
+            int k = 2 * a + sg;
+            if (k == 0 || v < dmin) { dmin = v; mmin = k; }
+        }
+    d3 poly[16], in_n, in_c;
+    dface(ihalf, ix, iR, mmin / 2, (mmin % 2 == 0) ? 1.0 : -1.0, poly, &in_n, &in_c);
+    int j = (raxis + 1) % 3, k = (raxis + 2) % 3;
+    int np_ = dclip(poly, 4, rc, rR->col[j], dget(rhalf, j));
+    if (!np_) return 0;
+    np_ = dclip(poly, np_, rc, rR->col[k], dget(rhalf, k));
+    if (!np_) return 0;
+    double gs[16];
+    d3 ps[16];
+    int m = 0;
+    for (int i = 0; i < np_; ++i) {
+        double g = ddot(dsub(poly[i], rc), rn);
+        if (g < margin) { gs[m] = g; ps[m] = poly[i]; m++; }
+    }
+    if (m == 0) return 0;
+    if (m > 4) {  /* stable sort by gap, keep the 4 deepest (sorted(...)[:4]) */
+        for (int a = 1; a < m; ++a) {
+            double gv = gs[a]; d3 pv = ps[a];
+            int b = a - 1;
+            while (b >= 0 && gs[b] > gv) { gs[b + 1] = gs[b]; ps[b + 1] = ps[b]; --b; }
+            gs[b + 1] = gv; ps[b + 1] = pv;
+        }
+        m = 4;
+    }
+    int base = (raxis * 2 + (rsgn > 0 ? 0 : 1)) * 8;
+    for (int i = 0; i < m; ++i) {
+        p_out[3 * i] = ps[i].x; p_out[3 * i + 1] = ps[i].y; p_out[3 * i + 2] = ps[i].z;
+        g_out[i] = gs[i]; f_out[i] = base + i;
+    }
+    n_out[0] = nBA.x; n_out[1] = nBA.y; n_out[2] = nBA.z;
+    return m;
+}
+
+/* ================================================================== */
+/* Box engine: all-pairs box/plane + box/box narrowphase (BoxWorld.     */
+/* contacts, ncp_gpu.py:1273-1280) feeding the ColorCache pair solve   */
+/* (fixed frame, applied warm start, colour cache), per-pair friction. */
+/* ================================================================== */
+static inline int64_t box_key(int a, int b, int f, int N) { return ((int64_t)a * (N + 1) + (int64_t)(b + 1)) * 256 + f; }
+
+/* flags: 1 fixed frame, 2 applied warm start, 4 colour cache, 8 warm start (as B2C_COLOR_*) */
+/* ---- box engine pair enumeration ------------------------------------------------------------
+ * The pair test of the box engine: bounding spheres at most the margin apart,
+ * |xb - xa|^2 <= (ra + rb + margin)^2 in float64 (the same expression, in the same order, as the
+ * CUDA broadphase).  Pairs come out with b ascending for each a.  A uniform grid of cell size
+ * >= 1.01 (2 r_max + margin) over the centres' bounding box makes every such pair lie in
+ * adjacent cells. */
+static double box_radius(const float *h)
+{
+    double x = h[0], y = h[1], z = h[2];
+    return sqrt((x * x + y * y) + z * z);
+}
+static int box_sphere_pair(const float *xa, double ra, const float *xb, double rb, double margin)
+{
+    double dx = (double)xb[0] - (double)xa[0], dy = (double)xb[1] - (double)xa[1], dz = (double)xb[2] - (double)xa[2];
+    double rr = (ra + rb) + margin;
+    return (dx * dx + dy * dy) + dz * dz <= rr * rr;
+}
+typedef struct {
+    int dim[3], ncell, cap_cells, cap_items;
+    double lo[3], cell;
+    int *start, *items;
+} box_cells_t;
+static int box_cell_axis(const box_cells_t *g, double x, int k)
+{
+    int c = (int)floor((x - g->lo[k]) / g->cell);
+    return c < 0 ? 0 : (c >= g->dim[k] ? g->dim[k] - 1 : c);
+}
+static int box_cell_of(const box_cells_t *g, const float *x)
+{
+    return (box_cell_axis(g, x[0], 0) * g->dim[1] + box_cell_axis(g, x[1], 1)) * g->dim[2] + box_cell_axis(g, x[2], 2);
+}
+static void box_cells_build(box_cells_t *g, int N, const float *xc, const double *rad, double margin)
+{
+    double rmax = 0.0, hi[3];
+    for (int i = 0; i < N; ++i) rmax = rad[i] > rmax ? rad[i] : rmax;
+    g->cell = 1.01 * (2.0 * rmax + margin);
+    for (int k = 0; k < 3; ++k) { g->lo[k] = N ? xc[k] : 0.0; hi[k] = g->lo[k]; }
+    for (int i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) {
+            double x = xc[3 * i + k];
+            if (x < g->lo[k]) g->lo[k] = x;
+            if (x > hi[k]) hi[k] = x;
+        }
+    for (int k = 0; k < 3; ++k) {
+        double span = (hi[k] - g->lo[k]) / g->cell;
+        g->dim[k] = span > 255.0 ? 256 : (int)span + 1;
+    }
+    g->ncell = g->dim[0] * g->dim[1] * g->dim[2];
+    if (g->ncell + 1 > g->cap_cells) { free(g->start); g->cap_cells = g->ncell + 1; g->start = malloc(sizeof(int) * g->cap_cells); }
+    if (N > g->cap_items) { free(g->items); g->cap_items = N; g->items = malloc(sizeof(int) * N); }
+    memset(g->start, 0, sizeof(int) * (g->ncell + 1));
+    for (int i = 0; i < N; ++i) g->start[box_cell_of(g, xc + 3 * i) + 1]++;
+    for (int c = 0; c < g->ncell; ++c) g->start[c + 1] += g->start[c];
+    int *fill = malloc(sizeof(int) * (g->ncell > 0 ? g->ncell : 1));
+    memcpy(fill, g->start, sizeof(int) * g->ncell);
+    for (int i = 0; i < N; ++i) g->items[fill[box_cell_of(g, xc + 3 * i)]++] = i;
+    free(fill);
+}
+static int box_int_cmp(const void *a, const void *b) { return *(const int *)a - *(const int *)b; }
+static int box_cells_partners(const box_cells_t *g, int a, const float *xc, const double *rad, double margin, int *out)
+{
+    int ca[3], n = 0;
+    for (int k = 0; k < 3; ++k) ca[k] = box_cell_axis(g, xc[3 * a + k], k);
+    for (int x = ca[0] - 1; x <= ca[0] + 1; ++x)
+        for (int y = ca[1] - 1; y <= ca[1] + 1; ++y)
+            for (int z = ca[2] - 1; z <= ca[2] + 1; ++z) {
+                if (x < 0 || y < 0 || z < 0 || x >= g->dim[0] || y >= g->dim[1] || z >= g->dim[2]) continue;
+                int c = (x * g->dim[1] + y) * g->dim[2] + z;
+                for (int t = g->start[c]; t < g->start[c + 1]; ++t) {
+                    int b = g->items[t];
+                    if (b > a && box_sphere_pair(xc + 3 * a, rad[a], xc + 3 * b, rad[b], margin)) out[n++] = b;
+                }
+            }
+    qsort(out, n, sizeof(int), box_int_cmp);
+    return n;
+}
+
+OR_API int or_box_step(void *h, int flags, int N, const float *half, const float *body_mu, float mu, float *xc,
+                       float *q, float *v, float *w, float *pv, float *po, const float *invM, const float *IbInv,
+                       const int *kin, double dt, int substeps, double margin, float *vgrav)
+{
+    col_engine_t *e = h;
+    int cap = e->cap;
+    float *invIw = malloc(sizeof(float) * 9 * (size_t)(N > 0 ? N : 1));
+    int64_t *keys = malloc(sizeof(int64_t) * cap);
+    int *sbi = malloc(sizeof(int) * cap), *sbj = malloc(sizeof(int) * cap);
+    float *spA = malloc(sizeof(float) * 3 * cap), *spB = malloc(sizeof(float) * 3 * cap);
+    float *sn = malloc(sizeof(float) * 3 * cap), *spen = malloc(sizeof(float) * cap);
+    float *jn = malloc(sizeof(float) * cap), *jt1 = malloc(sizeof(float) * cap), *jt2 = malloc(sizeof(float) * cap);
+    float *jp = malloc(sizeof(float) * cap), *pmu = malloc(sizeof(float) * cap);
+    int *pidx = malloc(sizeof(int) * cap), *pstart = malloc(sizeof(int) * cap), *pcount = malloc(sizeof(int) * cap);
+    int *pbi = malloc(sizeof(int) * cap), *pbj = malloc(sizeof(int) * cap);
+    int rc = 0;
+    double *rad = malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
+    int *partners = malloc(sizeof(int) * (size_t)(N > 0 ? N : 1));
+    for (int i = 0; i < N; ++i) rad[i] = box_radius(half + 4 * i);
+    box_cells_t bc = {0};
+    e->mode = (flags & 1) ? 1 : 0;
+    for (int s = 0; s < substeps; ++s) {
+        double sdt_d = dt / substeps;
+        float sdt = (float)sdt_d;
+        body_gravity(N, v, invM, sdt);
+        body_inv_inertia(N, q, IbInv, kin, invIw);
+        memcpy(vgrav, v, sizeof(float) * 3 * N);
+        memset(pv, 0, sizeof(float) * 3 * N);
+        memset(po, 0, sizeof(float) * 3 * N);
+        /* narrowphase over the sphere-test pairs in (a, b) order, the ground first */
+        box_cells_build(&bc, N, xc, rad, margin);
+        int C = 0, P = 0;
+        for (int a = 0; a < N; ++a) {
+            double ha[3] = {half[4 * a], half[4 * a + 1], half[4 * a + 2]};
+            double xa[3] = {xc[3 * a], xc[3 * a + 1], xc[3 * a + 2]};
+            double qa[4] = {q[4 * a], q[4 * a + 1], q[4 * a + 2], q[4 * a + 3]};
+            int nb = box_cells_partners(&bc, a, xc, rad, margin, partners);
+            for (int t = -1; t < nb; ++t) {
+                int b = t < 0 ? -1 : partners[t];
+                double pts[24], nrm[3] = {0.0, 0.0, 1.0}, gs[8];
+                int fs[8], m;
+                if (b < 0) {
+                    m = or_box_plane(ha, xa, qa, margin, pts, gs, fs);
+                } else {
+                    double hb[3] = {half[4 * b], half[4 * b + 1], half[4 * b + 2]};
+                    double xb[3] = {xc[3 * b], xc[3 * b + 1], xc[3 * b + 2]};
+                    double qb[4] = {q[4 * b], q[4 * b + 1], q[4 * b + 2], q[4 * b + 3]};
+                    m = or_box_box(ha, xa, qa, hb, xb, qb, margin, pts, nrm, gs, fs);
+                }
+                if (m == 0) continue;
+                if (C + m > cap || P >= cap) { rc = 2; continue; }
+                pbi[P] = a; pbj[P] = b; pstart[P] = C; pcount[P] = m;
+                pmu[P] = body_mu ? (b >= 0 ? sqrtf(body_mu[a] * body_mu[b]) : body_mu[a]) : mu;
+                for (int k = 0; k < m; ++k) {
+                    int d = C + k;
+                    v3 pf = V((float)pts[3 * k], (float)pts[3 * k + 1], (float)pts[3 * k + 2]);
+                    sbi[d] = a; sbj[d] = b; st3(spA, d, pf); st3(spB, d, pf);
+                    st3(sn, d, V((float)nrm[0], (float)nrm[1], (float)nrm[2]));
+                    spen[d] = -(float)gs[k];
+                    keys[d] = box_key(a, b, fs[k], N);
+                    pidx[d] = d;
+                    /* warm start by feature key */
+                    jn[d] = 0.0f; jt1[d] = 0.0f; jt2[d] = 0.0f; jp[d] = 0.0f;
+                    if ((flags & 8) && e->ws_n > 0) {
+                        int lo = 0, hi = e->ws_n - 1;
+                        while (lo <= hi) {
+                            int mid = (lo + hi) / 2;
+                            if (e->ws_keys[mid] == keys[d]) { jn[d] = e->ws_jn[mid]; jt1[d] = e->ws_jt1[mid]; jt2[d] = e->ws_jt2[mid]; break; }
+                            if (e->ws_keys[mid] < keys[d]) lo = mid + 1; else hi = mid - 1;
+                        }
+                    }
+                }
+                C += m; P++;
+            }
+        }
+        e->n_contacts = C; e->n_kept = C; e->n_pairs = P;
+        if (P > 0) {
+            int ncol, hit = 0;
+            if ((flags & 4) && P == e->cached_pairs && e->has_colors) {
+                hit = 1;
+                for (int p = 0; p < P && hit; ++p) if (pbi[p] != e->cached_a[p] || pbj[p] != e->cached_b[p]) hit = 0;
+                for (int i = 0; i < N && hit; ++i) if (invM[i] != e->cached_mass[i]) hit = 0;
+            }
+            if (hit) { ncol = e->cached_colors; e->hits++; }
+            else {
+                ncol = color_pairs(e, P, N, pbi, pbj, invM);
+                e->has_colors = 1;
+                if (flags & 4) {
+                    memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
+                    memcpy(e->cached_mass, invM, sizeof(float) * N);
+                    e->cached_pairs = P; e->cached_colors = ncol; e->misses++;
+                }
+            }
+            e->n_colors = ncol;
+            int fixed = flags & 1;
+            if (flags & 2)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t)
+                        apply_warm_pair(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB, sn, jn,
+                                        jt1, jt2, xc, v, w, invIw, invM);
+            for (int it = 0; it < e->vit; ++it)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t) {
+                        int p = e->porder[e->cstart[ci] + t];
+                        chunk_velocity(fixed, p, pidx, pstart, pcount, pbi, pbj, spA, spB, sn, jn, jt1, jt2, xc, v, w,
+                                       invIw, invM, pmu[p], e->t2d);
+                    }
+            for (int it = 0; it < e->pit; ++it)
+                for (int ci = 0; ci < ncol; ++ci)
+                    for (int t = 0; t < e->ccount[ci]; ++t)
+                        chunk_position(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB, sn,
+                                       spen, jp, xc, pv, po, invIw, invM, sdt);
+        } else {
+            e->n_colors = 0;
+        }
+        if (flags & 8) {
+            memcpy(e->ws_keys, keys, sizeof(int64_t) * C);
+            memcpy(e->ws_jn, jn, sizeof(float) * C); memcpy(e->ws_jt1, jt1, sizeof(float) * C);
+            memcpy(e->ws_jt2, jt2, sizeof(float) * C);
+            e->ws_n = C;
+        } else {
+            e->ws_n = 0;
+        }
+        body_integrate(N, xc, q, v, w, pv, po, invM, sdt);
+    }
+    free(invIw); free(keys); free(sbi); free(sbj); free(spA); free(spB); free(sn); free(spen);
+    free(jn); free(jt1); free(jt2); free(jp); free(pmu); free(pidx); free(pstart); free(pcount); free(pbi); free(pbj);
+    free(rad); free(partners); free(bc.start); free(bc.items);
+    return rc;
+}
