@@ -39,7 +39,8 @@ class Pairs(ctypes.Structure):
                 ("kcount", c_void_p), ("pstart", c_void_p), ("pidx", c_void_p), ("col", c_void_p),
                 ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
                 ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
-                ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32)]
+                ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
+                ("body_colors", c_void_p)]
 
 
 class Warm(ctypes.Structure):
@@ -67,6 +68,7 @@ COLOR_APPLY_WARM = 2
 COLOR_CACHE = 4
 COLOR_WARM_START = 8
 COLOR_PER_CONTACT = 16
+COLOR_FIRST_FIT = 32
 
 
 class Grid(ctypes.Structure):

@@ -51,7 +51,7 @@ class BoxContactEngine(_BeadEngineBase):
 
     def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, fixed_frame=True, apply_warm=True,
                  color_cache=True, warm_start=True, margin=MARGIN, device="cuda", color_cap=NCOLMAX,
-                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16):
+                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16, first_fit=True):
         super().__init__(dims=dims, mu=mu, device=device, graph=True)
         self.vit, self.pit = int(vit), int(pit)
         self.fixed_frame, self.apply_warm = bool(fixed_frame), bool(apply_warm)
@@ -61,6 +61,7 @@ class BoxContactEngine(_BeadEngineBase):
         self.solve_blocks = int(solve_blocks)
         self.barrier_timeout_ns = int(barrier_timeout_s * 1e9)
         self.cand_per_body = int(cand_per_body)
+        self.first_fit = bool(first_fit)
         self._halves, self._mus = [], []
         self._has_manifold = True
 
@@ -132,19 +133,21 @@ class BoxContactEngine(_BeadEngineBase):
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
                            cached_a=i32(pcap), cached_b=i32(pcap),
                            cached_mass=torch.zeros(max(N, 1), dtype=torch.float32, device=dev), cache_state=i32(8),
+                           body_colors=i64(N),
                            barrier=torch.zeros(2, dtype=torch.int32, device=dev),
                            rec=torch.zeros(max(int(self.L.b2c_pair_record_floats(pcap, kslots)), 1),
                                            dtype=torch.float32, device=dev))
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
-            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots)
+            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots, _ptr(pb["body_colors"]))
         self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
         self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
         self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
                                     _ptr(self.po), _ptr(self.invM), _ptr(self.IbInv), _ptr(self.kin), _ptr(self.invIw))
         flags = ((_lib.COLOR_FIXED_FRAME if self.fixed_frame else 0) | (_lib.COLOR_APPLY_WARM if self.apply_warm else 0)
-                 | (_lib.COLOR_CACHE if self.color_cache else 0) | (_lib.COLOR_WARM_START if self.warm_start else 0))
+                 | (_lib.COLOR_CACHE if self.color_cache else 0) | (_lib.COLOR_WARM_START if self.warm_start else 0)
+                 | (_lib.COLOR_FIRST_FIT if self.first_fit else 0))
         self.c_params = _lib.ColorParams(self.vit, self.pit, 8, flags, self.mu, 1.0, min(self.color_cap, NCOLMAX),
                                          self.solve_blocks, self.barrier_timeout_ns,
                                          _ptr(self.body_mu) if self.per_body_mu else None)

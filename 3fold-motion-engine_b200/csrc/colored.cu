@@ -436,10 +436,12 @@ constexpr int kMaxColorsCap = 512;
 
 __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, int nbodies,
                                                                 const float *__restrict__ invM, b2c_pairs pr,
-                                                                int use_cache, int color_cap, int max_rounds)
+                                                                int use_cache, int color_cap, int max_rounds,
+                                                                int first_fit)
 {
     __shared__ int s_flag;
     __shared__ int s_left;
+    __shared__ int s_ncol;
     __shared__ int s_cnt[kMaxColorsCap];
     __shared__ int s_cur[kMaxColorsCap];
     const int P = hdr->n_pairs;
@@ -472,6 +474,10 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         }
     }
     for (int p = tid; p < P; p += kColorThreads) pr.col[p] = -1;
+    unsigned long long *used = reinterpret_cast<unsigned long long *>(pr.body_colors);
+    if (first_fit)
+        for (int i = tid; i < nbodies; i += kColorThreads) used[i] = 0ull;
+    if (tid == 0) s_ncol = 0;
     int r = 0;
     bool done = false;
     for (; r < max_rounds; ++r) {
@@ -493,8 +499,22 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
             bool ok = true;
             if (invM[bi] > 0.0f && pr.claim[bi] != k) ok = false;
             if (bj >= 0 && invM[bj] > 0.0f && pr.claim[bj] != k) ok = false;
-            if (ok) pr.col[p] = r;
-            else atomicAdd(&s_left, 1);
+            if (!ok) {
+                atomicAdd(&s_left, 1);
+            } else if (!first_fit) {
+                pr.col[p] = r;
+            } else {
+                // the winners of a round share no dynamic body: their masks are theirs alone
+                const bool da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
+                const unsigned long long m = (da ? used[bi] : 0ull) | (db ? used[bj] : 0ull);
+                const int c = (~m == 0ull) ? 64 : __ffsll((long long)~m) - 1;
+                pr.col[p] = c;
+                if (c < 64) {
+                    if (da) used[bi] |= 1ull << c;
+                    if (db) used[bj] |= 1ull << c;
+                }
+                atomicMax(&s_ncol, c + 1);
+            }
         }
         __syncthreads();
         if (s_left == 0) {
@@ -502,7 +522,7 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
             break;
         }
     }
-    const int ncol = done ? r + 1 : r;
+    const int ncol = first_fit ? s_ncol : (done ? r + 1 : r);
     if (!done || ncol > color_cap || ncol > pr.max_colors || ncol > kMaxColorsCap) {
         if (tid == 0) {
             atomicOr(&hdr->error, done ? B2C_ERR_COLOR_OVERFLOW : B2C_ERR_COLOR_TIMEOUT);
@@ -638,8 +658,13 @@ int manifold_reduce(const b2c_bodies *b, const b2c_beads *beads, const b2c_conta
 int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p, cudaStream_t s)
 {
     const int cap = std::min(p->color_cap, std::min(pr->max_colors, kMaxColorsCap));
-    k_color_pairs<<<1, kColorThreads, 0, s>>>(hdr, b->n, b->invM, *pr, (p->flags & B2C_COLOR_CACHE) ? 1 : 0, cap,
-                                              kMaxColorsCap + 1);
+    const int first_fit = (p->flags & B2C_COLOR_FIRST_FIT) ? 1 : 0;
+    if (first_fit && !pr->body_colors) {
+        set_error("color_pairs: B2C_COLOR_FIRST_FIT needs pairs->body_colors");
+        return B2C_EARG;
+    }
+    k_color_pairs<<<1, kColorThreads, 0, s>>>(hdr, b->n, b->invM, *pr, (p->flags & B2C_COLOR_CACHE) ? 1 : 0,
+                                              first_fit ? std::min(cap, 64) : cap, kMaxColorsCap + 1, first_fit);
     return check_launch("color_pairs");
 }
 

@@ -2,18 +2,24 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl b200|reference]
 
-One "step" is one ContactEngine.step(dt, substeps) of the whole scene.  W warm-up steps run
-first (untimed; the scene settles into its contact-rich regime), then exactly K steps are timed
-with CUDA events on the engine's stream, bracketed by a barrier and a device synchronise, and
-the L2 is flushed (a 256 MiB write) between timed steps, outside the events.  With N > 1 every
-rank runs an independent replica (the single-scene solve does not shard: replicas only) and the
-time is the max over ranks.  Rank 0 prints one JSON line.
+One "step" is one ContactEngine.step(dt, substeps) of the whole scene.  The default workload is
+10 000 random boxes (edges U[0.2, 0.6] m, density 1000, per-body mu U[0.3, 0.8]) dropped into a
+20 x 20 x 10 m volume onto the ground; box/plane + box/box contacts, ColorCache pair solve with
+first-fit colours (15-17 on this pile: the largest pair count of one body, so at most 32
+allowed), 2 substeps x (16 velocity + 10 position sweeps), dt 1/240, 600 steps.  The
+first 300 steps are set-up (boxes land, the pile forms; untimed), W warm-up steps follow, then
+exactly K steps (default 300, the rest of the 600-step run) are timed with CUDA events on the
+engine's stream, bracketed by a barrier and a device synchronise; the L2 is flushed (a 256 MiB
+write) between timed steps, outside the events.  With N > 1 every rank runs an independent
+replica (a single scene does not shard: replicas only) and the time is the max over ranks.
+Rank 0 prints one JSON line.
 
 `e2e` is the same metric through the public API with the body state in pinned host memory:
 every step uploads the state (set_body_state), steps, and downloads it again.
 
-`--impl reference` times the reference algorithm's CPU restatement (the oracle; Warp, which the
-reference's own CPU path needs, is not installed) on the same workload on the host cores.
+`--impl reference` times the CPU restatement of the same algorithm (the oracle; the reference
+runs these engines through Warp, which is not installed) on the same workload, one replica per
+host core, rank 0 only.
 """
 from __future__ import annotations
 
@@ -23,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -31,15 +38,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    # 10 000 random boxes, SAT contacts, per-body friction, ColorCache pair solve
+    "boxes10k": dict(engine="box", scene="random_boxes", n=10000, edge=(0.2, 0.6), box=(20.0, 20.0, 10.0),
+                     mu_range=(0.3, 0.8), density=1000.0, vit=16, pit=10, substeps=2, dt=1 / 240, color_cap=32,
+                     preroll=300, steps=300, warmup=3),
     # the reference's ColorCache timing fixture (reports/innovation_stack_color_cache_l4.json):
     # lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5, 40 velocity / 20 position sweeps,
     # 1 substep, dt 1/240
     "colorcache_lattice10k": dict(engine="color_cache", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5,
-                                  vit=40, pit=20, substeps=1, dt=1 / 240, warmup=20),
+                                  vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20),
     "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
-                              pit=20, substeps=1, dt=1 / 240, warmup=20),
+                              pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20),
 }
-DEFAULT_WORKLOAD = "colorcache_lattice10k"
+DEFAULT_WORKLOAD = "boxes10k"
 
 
 def _peaks():
@@ -50,19 +61,50 @@ def _peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def make_engine(me, wl, graph=True):
+def _scenes():
     from importlib import import_module
-    scenes = import_module("motion_engine_b200.scenes")
+    return import_module("motion_engine_b200.scenes")
+
+
+def scene_of(wl):
+    sc = _scenes()
+    if wl["scene"] == "random_boxes":
+        return sc.random_boxes(n=wl["n"], edge=wl["edge"], box=wl["box"], mu=wl["mu_range"], density=wl["density"])
+    return {"centers": sc.lattice(wl["n"]) if wl["scene"] == "lattice" else sc.stack(wl["n"])}
+
+
+def make_engine(me, wl, scene):
+    if wl["engine"] == "box":
+        e = me.BoxContactEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
+                                color_cap=wl["color_cap"])
+        for c, d, m, de in zip(scene["centers"], scene["dims"], scene["mu"], scene["density"]):
+            e.add_box(c, dims=d, density=de, mu=m)
+        return e
     if wl["engine"] == "color_cache":
         e = me.ColorCacheContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
     elif wl["engine"] == "jacobi":
-        e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"], graph=graph)
+        e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
     else:
         raise ValueError(wl["engine"])
-    centers = scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])
-    for c in centers:
+    for c in scene["centers"]:
         e.add_body(c)
     return e
+
+
+def make_oracle(wl, scene):
+    from oracle import oracle as O
+    if wl["engine"] == "box":
+        o = O.BoxOracle(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"])
+        for c, d, m, de in zip(scene["centers"], scene["dims"], scene["mu"], scene["density"]):
+            o.add_box(c, dims=d, density=de, mu=m)
+        return o
+    if wl["engine"] == "jacobi":
+        o = O.JacobiOracle(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    else:
+        o = O.ColoredOracle(mode="color_cache", dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    for c in scene["centers"]:
+        o.add_body(c)
+    return o
 
 
 class ClockSampler:
@@ -109,125 +151,135 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline_sample(wl, max_seconds=20.0):
-    """The oracle (single-threaded C restatement) on the same workload from the same initial
-    state: steps until max_seconds of CPU work; returns body-steps/s and the sample taken."""
-    from oracle import oracle as O
-    from importlib import import_module
-    scenes = import_module("motion_engine_b200.scenes")
-    mode = {"color_cache": "color_cache", "jacobi": None}[wl["engine"]]
-    if mode is None:
-        o = O.JacobiOracle(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
-    else:
-        o = O.ColoredOracle(mode=mode, dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
-    centers = scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])
-    for c in centers:
-        o.add_body(c)
-    t0 = time.perf_counter()
-    for _ in range(wl.get("warmup", 20)):  # untimed: into the contact-rich regime, as the GPU run
-        o.step(wl["dt"], wl["substeps"])
-        if time.perf_counter() - t0 > 2 * max_seconds:
-            break
+def _time_oracle(o, wl, max_seconds, max_steps):
     n = 0
     t0 = time.perf_counter()
     while True:
         o.step(wl["dt"], wl["substeps"])
         n += 1
         el = time.perf_counter() - t0
-        if el > max_seconds or n >= 200:
-            break
+        if el > max_seconds or n >= max_steps:
+            return n, el
+
+
+def cpu_baseline_sample(wl, scene, state=None, max_seconds=20.0):
+    """The oracle (single-threaded C restatement) on the same workload: from the GPU's body state
+    at the start of the timed region when given (box workload), else from the initial state after
+    the same warm-up; steps until max_seconds of CPU work."""
+    o = make_oracle(wl, scene)
+    if state is not None:
+        o.set_body_state(*state)
+    else:
+        t0 = time.perf_counter()
+        for _ in range(wl["preroll"] + wl["warmup"]):
+            o.step(wl["dt"], wl["substeps"])
+            if time.perf_counter() - t0 > 2 * max_seconds:
+                break
+    n, el = _time_oracle(o, wl, max_seconds, 200)
     return wl["n"] * n / el, n, el
 
 
 def run_reference(args, wl):
     """--impl reference: the oracle port on every host core (one independent replica per
-    process, spawn start method), each timed over a bounded number of steps."""
+    process, spawn start method), each timed over a bounded number of steps from the workload's
+    state after its set-up steps (computed once here, by the oracle)."""
     import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
     procs = max(1, min(cores, 64))
-    ctx = mp.get_context("spawn")
-    per_step_budget = 60.0 / max(args.steps + args.warmup, 1)
-    with ctx.Pool(procs) as pool:
-        t0 = time.perf_counter()
-        res = pool.starmap(_ref_worker, [(args.workload, args.steps, args.warmup, per_step_budget)] * procs)
-        wall = time.perf_counter() - t0
+    scene = scene_of(wl)
+    t_pre = time.perf_counter()
+    o = make_oracle(wl, scene)
+    for _ in range(wl["preroll"]):
+        o.step(wl["dt"], wl["substeps"])
+    pre_s = time.perf_counter() - t_pre
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    try:
+        st = o.body_state() if hasattr(o, "body_state") else None
+        np.savez(path, **{k: np.asarray(v) for k, v in scene.items()},
+                 **({} if st is None else dict(s_xc=st[0], s_q=st[1], s_v=st[2], s_w=st[3])))
+        del o
+        ctx = mp.get_context("spawn")
+        budget = 60.0
+        with ctx.Pool(procs) as pool:
+            t0 = time.perf_counter()
+            res = pool.starmap(_ref_worker, [(args.workload, path, args.steps, args.warmup, budget)] * procs)
+            wall = time.perf_counter() - t0
+    finally:
+        os.unlink(path)
     steps_done = sum(r[0] for r in res)
     busy = max(r[1] for r in res)
     value = wl["n"] * steps_done / busy
     line = {"impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
             "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup",)}},
+            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup", "steps")}},
             "dtype": "f32", "data": "synthetic",
             "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": procs, "kind": "port",
-                             "sample": f"{procs} processes x {steps_done // procs} timed steps of independent "
-                                       f"replicas of the workload (after {args.warmup} untimed warm-up steps "
-                                       f"each, capped at ~60 s); the reference's Warp CPU path is not installed"},
+                             "sample": f"{procs} processes x {steps_done / procs:.1f} timed steps (<= {args.steps} "
+                                       f"each, capped at ~{budget:.0f} s) of independent replicas from the state "
+                                       f"after the workload's {wl['preroll']} set-up steps (oracle, {pre_s:.0f} s) and "
+                                       f"{args.warmup} warm-up steps; the reference's Warp CPU path is not installed"},
             "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
 
 
-def _ref_worker(workload, steps, warmup, per_step_budget):
+def _ref_worker(workload, path, steps, warmup, budget):
     sys.path.insert(0, ROOT)
     import __graft_entry__ as ge
-    from oracle import oracle as O
-    from importlib import import_module
     ge.load_package()  # registers the package alias for the scene builders
-    scenes = import_module("motion_engine_b200.scenes")
     wl = WORKLOADS[workload]
-    if wl["engine"] == "jacobi":
-        o = O.JacobiOracle(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    d = dict(np.load(path))
+    scene = {k: d[k] for k in d if not k.startswith("s_")}
+    o = make_oracle(wl, scene)
+    if "s_xc" in d:
+        o.set_body_state(d["s_xc"], d["s_q"], d["s_v"], d["s_w"])
     else:
-        o = O.ColoredOracle(mode="color_cache", dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
-    for c in (scenes.lattice(wl["n"]) if wl["scene"] == "lattice" else scenes.stack(wl["n"])):
-        o.add_body(c)
+        for _ in range(wl["preroll"]):
+            o.step(wl["dt"], wl["substeps"])
     t_start = time.perf_counter()
     for _ in range(warmup):
         o.step(wl["dt"], wl["substeps"])
         if time.perf_counter() - t_start > 30.0:
             break
-    n = 0
-    t0 = time.perf_counter()
-    budget = per_step_budget * steps
-    while n < steps:
-        o.step(wl["dt"], wl["substeps"])
-        n += 1
-        if time.perf_counter() - t0 > budget:
-            break
-    return n, time.perf_counter() - t0
+    return _time_oracle(o, wl, budget, steps)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.steps is None:
+        args.steps = wl["steps"]
     if args.warmup is None:
-        args.warmup = wl.get("warmup", 20)
+        args.warmup = wl["warmup"]
     args.warmup = max(args.warmup, 3)
+    import __graft_entry__ as ge
     if args.impl == "reference":
-        import __graft_entry__ as ge
         ge.load_package()
         return run_reference(args, wl)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    ge.load_package()
+    scene = scene_of(wl)
     cpu_base = None
-    if rank == 0 and not args.no_cpu_baseline:
-        import __graft_entry__ as ge
+    do_cpu = rank == 0 and not args.no_cpu_baseline
+    if do_cpu and wl["engine"] != "box":
         ge.load_package()
-        v, n, el = cpu_baseline_sample(wl)  # before the first GPU call
+        v, n, el = cpu_baseline_sample(wl, scene)  # before the first GPU call
         cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
-                    "sample": f"{n} steps of the same workload from the same initial state on one host core "
+                    "sample": f"{n} steps of the same workload after the same warm-up on one host core "
                               f"({el:.1f} s; the oracle restatement, not the reference's Warp CPU path)"}
     import torch
     import torch.distributed as dist
@@ -235,7 +287,6 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    import __graft_entry__ as ge
     me = ge.load_package()
     dev = torch.device("cuda", local)
 
@@ -243,14 +294,22 @@ def main():
         if world > 1:
             dist.barrier()
 
-    e = make_engine(me, wl)
+    e = make_engine(me, wl, scene)
     dt, S = wl["dt"], wl["substeps"]
+    for _ in range(wl["preroll"]):
+        e.step(dt, S)
     for _ in range(args.warmup):
         e.step(dt, S)
+    e.check_errors()
     torch.cuda.synchronize()
+    start_state = None
+    if do_cpu and wl["engine"] == "box":
+        start_state = (e.xc[:, :3].cpu().numpy(), e.q.cpu().numpy(), e.v[:, :3].cpu().numpy(),
+                       e.w[:, :3].cpu().numpy())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     stream = torch.cuda.current_stream()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    counts = []
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
@@ -262,9 +321,8 @@ def main():
         torch.cuda.synchronize()
         barrier()
     ms = sum(a.elapsed_time(b) for a, b in evs)
-    e.check_errors()
-    key = next(iter(e.kernels_per_step)) if e.kernels_per_step else None
-    launches_per_step = e.kernels_per_step.get(key, 0) if key else 0
+    h_end = e.check_errors()
+    launches_per_step = max(e.kernels_per_step.values()) if e.kernels_per_step else 0
 
     # end to end through the public API with the state in pinned host memory
     N = e.N
@@ -275,7 +333,8 @@ def main():
     hx.copy_(e.xc[:, :3]); hq.copy_(e.q); hv.copy_(e.v[:, :3]); hw.copy_(e.w[:, :3])
     torch.cuda.synchronize()
     e2e_ms = 0.0
-    K2 = max(args.steps // 2, 3)
+    K2 = max(min(args.steps, 100) // 2, 3)
+    colors = []
     for k in range(K2):
         flush.fill_(float(k))
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -287,6 +346,8 @@ def main():
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
+        colors.append(e.header_dict()["n_colors"])
+    e.check_errors()
     bytes_io = N * (3 + 4 + 3 + 3) * 4
 
     # the dominant kernel (the persistent chunk solve), timed live on its launching stream
@@ -298,6 +359,7 @@ def main():
                 stage_ms[kk] = stage_ms.get(kk, 0.0) + vv / 8
             solve_ms.append(st["solve"])
             solve_bytes.append(e.solve_bytes())
+        e.check_errors()
     t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -306,6 +368,12 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
+    if do_cpu and wl["engine"] == "box":
+        v, n, el = cpu_baseline_sample(wl, scene, state=start_state)
+        cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
+                    "sample": f"{n} steps of the same workload from the GPU's body state at the start of the timed "
+                              f"region, on one host core ({el:.1f} s; the oracle restatement, not the reference's "
+                              f"Warp CPU path)"}
     peaks, peak_kind = _peaks()
     value = wl["n"] * world * args.steps / (ms / 1e3)
     roof = None
@@ -324,19 +392,22 @@ def main():
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "k_color_solve (persistent chunk solve, one launch per substep)",
                 "launch_ms": avg_ms, "algorithmic_bytes_per_launch": avg_b, "counts": solve_bytes[-1]}
-    h = e.header_dict()
+    cfg = {"workload": args.workload, "bodies": wl["n"], "substeps": S, "vit": wl["vit"], "pit": wl["pit"], "dt": dt,
+           "setup_steps": wl["preroll"], "l2": "flushed between timed steps (256 MiB write)",
+           "parallelism": f"replicas x{world}"}
+    if wl["engine"] == "box":
+        cfg.update(edge=wl["edge"], volume=wl["box"], mu=wl["mu_range"], density=wl["density"],
+                   color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3")
     line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene builders; the reference's own fixture)",
-            "config": {"workload": args.workload, "bodies": wl["n"], "substeps": S, "vit": wl["vit"],
-                       "pit": wl["pit"], "dt": dt, "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"replicas x{world}"},
+            "data": "synthetic (seeded scene builders)", "config": cfg,
             "clocks": clk.summary(),
             "e2e": {"value": wl["n"] * world * K2 / (e2e_ms / 1e3), "unit": "body-steps/s",
                     "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io, "steps": K2},
             "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
-            "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h}
+            "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h_end,
+            "colors_e2e_steps": {"max": max(colors), "mean": float(np.mean(colors))}}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

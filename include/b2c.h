@@ -170,6 +170,8 @@ typedef struct b2c_pairs {
                                 and per contact its normal|depth, the terms that stay fixed
                                 during a solve (rA|meff, rB|meft1, t1|meft2, t2) and its impulses */
     int32_t kslots;          /* contact slots per record (>= the most contacts one pair keeps) */
+    uint64_t *body_colors;   /* (bodies) colours used around each body; needed with
+                                B2C_COLOR_FIRST_FIT only, else NULL */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -212,6 +214,12 @@ typedef struct b2c_boxes {
 #define B2C_COLOR_APPLY_WARM 2   /* apply the warm impulses once per colour before the sweeps */
 #define B2C_COLOR_CACHE 4        /* reuse the colouring while pairs and masses are unchanged */
 #define B2C_COLOR_WARM_START 8   /* warm start by feature key */
+#define B2C_COLOR_FIRST_FIT 32   /* Jones-Plassmann with first-fit colours: a pair that wins its
+                                     round takes the smallest colour not used around its bodies
+                                     (the greedy colouring in priority order: at least the largest
+                                     pair count D of one body, at most 2D - 1 colours, and <= 64)
+                                     instead of the round number.  Not in the reference; the box
+                                     engine's default, as it needs fewer colour phases. */
 #define B2C_COLOR_PER_CONTACT 16 /* no manifold reduction; every contact is its own chunk and is
                                     coloured on the contact graph (the plain coloured engine) */
 

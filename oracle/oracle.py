@@ -334,11 +334,13 @@ def box_box(ha, xa, qa, hb, xb, qb, margin=2e-3):
 
 
 class BoxOracle:
-    """CPU restatement of the box engine: all-pairs box/plane + box/box narrowphase (BoxWorld.contacts,
-    ncp_gpu.py:1273-1280) with the ColorCache pair solve of the coloured chain, per-body friction."""
+    """CPU restatement of the box engine: box/plane + box/box narrowphase (BoxWorld.contacts,
+    ncp_gpu.py:1273-1280) over the pairs whose bounding spheres are within the margin, with the
+    ColorCache pair solve of the coloured chain and per-body friction.  flags: 1 fixed frame,
+    2 applied warm, 4 colour cache, 8 warm start, 32 first-fit colours."""
     name = "box_color_cache_oracle"
 
-    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=15, margin=2e-3, cap=MAXC):
+    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=47, margin=2e-3, cap=MAXC):
         self.dims = dims; self.mu = mu; self.vit = vit; self.pit = pit; self.flags = flags; self.margin = margin
         self.cap = cap
         self._centers, self._halves, self._dens, self._mus, self._kin = [], [], [], [], []
@@ -394,6 +396,19 @@ class BoxOracle:
         lib().or_col_stats(self._h, _p(out))
         return dict(zip(("n_contacts", "n_kept", "n_pairs", "n_colors", "hits", "misses", "seg_overflow"),
                         out.tolist()))
+
+    def set_body_state(self, xc, q, v, w):
+        """Overwrite positions, quaternions (x, y, z, w) and velocities (the warm-start store is kept)."""
+        if self.b is None:
+            self._build()
+        for dst, src in ((self.b.xc, xc), (self.b.q, q), (self.b.v, v), (self.b.w, w)):
+            dst[...] = np.asarray(src, np.float32).reshape(dst.shape)
+
+    def body_state(self):
+        """(xc, q, v, w) float32 copies."""
+        if self.b is None:
+            self._build()
+        return self.b.xc.copy(), self.b.q.copy(), self.b.v.copy(), self.b.w.copy()
 
     def get_state(self) -> State:
         if self.b is None:

@@ -769,9 +769,12 @@ static void select_segment(int i, int L, int mx, const int *gorder, const int *c
 
 /* JP colouring of the pair graph, COL:1178-1208 (k_prio, k_clear_claim, k_claim, k_win) plus the
  * stable grouping by colour.  Returns the colour count. */
-static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int *pbj, const float *invM)
+static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int *pbj, const float *invM,
+                       int first_fit)
 {
     int *col = malloc(sizeof(int) * (P > 0 ? P : 1));
+    uint64_t *used = calloc((size_t)(N > 0 ? N : 1), sizeof(uint64_t));
+    int ncol_ff = 0;
     int64_t *key = malloc(sizeof(int64_t) * (P > 0 ? P : 1));
     int64_t *claim = malloc(sizeof(int64_t) * (N > 0 ? N : 1));
     for (int p = 0; p < P; ++p) { col[p] = -1; key[p] = jp_priority(p); }
@@ -795,12 +798,27 @@ static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int 
             if (bj >= 0 && invM[bj] > 0.0f && claim[bj] != key[p]) ok = 0;
             if (ok) won[p] = 1; else left++;
         }
-        for (int p = 0; p < P; ++p) if (won[p]) col[p] = cur;
+        for (int p = 0; p < P; ++p) {
+            if (!won[p]) continue;
+            if (!first_fit) { col[p] = cur; continue; }
+            /* first fit: the smallest colour not used around the pair's dynamic bodies (the
+             * round's winners share no dynamic body, so the order of this loop is free) */
+            int bi = pbi[p], bj = pbj[p];
+            int da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
+            uint64_t m = (da ? used[bi] : 0) | (db ? used[bj] : 0);
+            int c = 0;
+            while (c < 64 && ((m >> c) & 1)) c++;
+            col[p] = c;
+            if (c < 64) { if (da) used[bi] |= (uint64_t)1 << c; if (db) used[bj] |= (uint64_t)1 << c; }
+            if (c + 1 > ncol_ff) ncol_ff = c + 1;
+        }
         free(won);
         cur++;
         if (left == 0) break;
         if (cur > P) break;
     }
+    free(used);
+    if (first_fit) cur = ncol_ff;
     /* stable counting sort by colour -> porder, ccount, cstart (exclusive scan) */
     for (int c = 0; c < 512; ++c) e->ccount[c] = 0;
     for (int p = 0; p < P; ++p) if (col[p] < 512) e->ccount[col[p]]++;
@@ -1131,7 +1149,7 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
                 ncol = e->cached_colors;
                 e->hits++;
             } else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM);
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, 0);
                 e->has_colors = 1;
                 if (e->mode == 1) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
@@ -1565,7 +1583,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             }
             if (hit) { ncol = e->cached_colors; e->hits++; }
             else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM);
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, (flags & 32) ? 1 : 0);
                 e->has_colors = 1;
                 if (flags & 4) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
