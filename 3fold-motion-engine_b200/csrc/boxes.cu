@@ -324,27 +324,6 @@ __global__ void k_box_scatter(int n, const int *__restrict__ bucket, const int *
     sorted[start[b] + atomicAdd(cursor + b, 1)] = i;
 }
 
-template <class F>
-__device__ __forceinline__ void for_each_box_neighbor(int i, const float *__restrict__ xc, const float *__restrict__ half,
-                                                      const int *__restrict__ start, const int *__restrict__ sorted,
-                                                      const BoxGrid &g, float margin, F &&f)
-{
-    const f3 xi = ld3(xc, i);
-    const double ri = bound_radius(ld4(half, i));
-    const int cx = bcell(xi.x, g.inv), cy = bcell(xi.y, g.inv), cz = bcell(xi.z, g.inv);
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int b = bbucket(g, cx + dx, cy + dy, cz + dz);
-                const int e = start[b + 1];
-                for (int t = start[b]; t < e; ++t) {
-                    const int j = sorted[t];
-                    if (j <= i) continue;
-                    if (sphere_pair(xi, ri, ld3(xc, j), bound_radius(ld4(half, j)), margin)) f(j);
-                }
-            }
-}
-
 // a box can touch the ground only if its lowest bounding-sphere point is below the margin
 // (box_plane decides; this test only has to keep every box that has a corner below it)
 __device__ __forceinline__ bool ground_candidate(int i, const float *__restrict__ xc, const float *__restrict__ half,
@@ -353,57 +332,109 @@ __device__ __forceinline__ bool ground_candidate(int i, const float *__restrict_
     return (double)ld3(xc, i).z - bound_radius(ld4(half, i)) < (double)margin + 1e-9;
 }
 
-__global__ void k_box_cand_count(int n, const float *__restrict__ xc, const float *__restrict__ q,
-                                 const float *__restrict__ half, const int *__restrict__ start,
-                                 const int *__restrict__ sorted, BoxGrid g, float margin, int *__restrict__ count,
-                                 b2c_header *hdr)
+// One warp per body i: lane l < 27 holds the bucket range of neighbour cell l; the ranges are
+// flattened by a warp prefix sum, and the lanes walk the flat list 32 entries at a time, so the
+// dependent loads of one body's candidates overlap.  f(j, pass) is called by every lane of every
+// iteration (pass = j is a partner of i: j > i and the sphere test holds), uniformly per warp.
+template <class F>
+__device__ __forceinline__ void warp_box_neighbors(int i, const float *__restrict__ xc, const float *__restrict__ half,
+                                                   const int *__restrict__ start, const int *__restrict__ sorted,
+                                                   const BoxGrid &g, float margin, F &&f)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) count[n] = 0;
-    if (i >= n) return;
-    int c = 0;
-    for_each_box_neighbor(i, xc, half, start, sorted, g, margin, [&](int) { ++c; });
-    if (c > kMaxBoxCandidates) {
-        atomicOr(&hdr->error, B2C_ERR_NEIGHBOR_OVERFLOW);
-        c = kMaxBoxCandidates;
+    const int lane = threadIdx.x & 31;
+    const f3 xi = ld3(xc, i);
+    const double ri = bound_radius(ld4(half, i));
+    const int cx = bcell(xi.x, g.inv), cy = bcell(xi.y, g.inv), cz = bcell(xi.z, g.inv);
+    int lo = 0, cnt = 0;
+    if (lane < 27) {
+        const int b = bbucket(g, cx + lane % 3 - 1, cy + (lane / 3) % 3 - 1, cz + lane / 9 - 1);
+        lo = start[b];
+        cnt = start[b + 1] - lo;
     }
-    count[i] = c + (ground_candidate(i, xc, half, margin) ? 1 : 0);
+    int incl = cnt;  // inclusive prefix over lanes
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - cnt;
+    for (int base = 0; base < total; base += 32) {
+        const int k = base + lane;
+        // the cell of flat entry k: the last lane whose exclusive prefix is <= k
+        int cell = 0;
+        for (int l = 1; l < 27; ++l) cell = (__shfl_sync(0xffffffffu, excl, l) <= k) ? l : cell;
+        const int t = __shfl_sync(0xffffffffu, lo, cell) + (k - __shfl_sync(0xffffffffu, excl, cell));
+        bool pass = false;
+        int j = -1;
+        if (k < total) {
+            j = sorted[t];
+            pass = j > i && sphere_pair(xi, ri, ld3(xc, j), bound_radius(ld4(half, j)), margin);
+        }
+        f(j, pass);
+    }
 }
 
-__global__ void k_box_cand_emit(int n, const float *__restrict__ xc, const float *__restrict__ q,
-                                const float *__restrict__ half, const int *__restrict__ start,
-                                const int *__restrict__ sorted, BoxGrid g, float margin,
-                                const int *__restrict__ offset, int cap, int *__restrict__ ca, int *__restrict__ cb,
-                                b2c_header *hdr)
+constexpr int kBroadWarps = 4;  // warps (bodies) per CTA of the broadphase kernels
+
+__global__ void __launch_bounds__(32 * kBroadWarps)
+    k_box_cand_count(int n, const float *__restrict__ xc, const float *__restrict__ half,
+                     const int *__restrict__ start, const int *__restrict__ sorted, BoxGrid g, float margin,
+                     int *__restrict__ count, b2c_header *hdr)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && offset[n] > cap) atomicOr(&hdr->error, B2C_ERR_PAIR_OVERFLOW);
-    if (i >= n) return;
+    const int i = blockIdx.x * kBroadWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0) count[n] = 0;
+    if (i >= n) return;  // warp-uniform
+    int c = 0;
+    warp_box_neighbors(i, xc, half, start, sorted, g, margin,
+                       [&](int, bool pass) { c += __popc(__ballot_sync(0xffffffffu, pass)); });
+    if (lane == 0) {
+        if (c > kMaxBoxCandidates) {
+            atomicOr(&hdr->error, B2C_ERR_NEIGHBOR_OVERFLOW);
+            c = kMaxBoxCandidates;
+        }
+        count[i] = c + (ground_candidate(i, xc, half, margin) ? 1 : 0);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kBroadWarps)
+    k_box_cand_emit(int n, const float *__restrict__ xc, const float *__restrict__ half,
+                    const int *__restrict__ start, const int *__restrict__ sorted, BoxGrid g, float margin,
+                    const int *__restrict__ offset, int cap, int *__restrict__ ca, int *__restrict__ cb,
+                    b2c_header *hdr)
+{
+    __shared__ int s_js[kBroadWarps][kMaxBoxCandidates];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kBroadWarps + w;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && offset[n] > cap) atomicOr(&hdr->error, B2C_ERR_PAIR_OVERFLOW);
+    if (i >= n) return;  // warp-uniform
+    int m = 0;  // partners collected so far (warp-uniform)
+    warp_box_neighbors(i, xc, half, start, sorted, g, margin, [&](int j, bool pass) {
+        const unsigned bal = __ballot_sync(0xffffffffu, pass);
+        const int pos = m + __popc(bal & ((1u << lane) - 1u));
+        if (pass && pos < kMaxBoxCandidates) s_js[w][pos] = j;
+        m += __popc(bal);
+    });
+    __syncwarp();
+    m = min(m, kMaxBoxCandidates);
     int k = offset[i];
     if (ground_candidate(i, xc, half, margin)) {
-        if (k < cap) {
+        if (lane == 0 && k < cap) {
             ca[k] = i;
             cb[k] = -1;
         }
         ++k;
     }
-    int js[kMaxBoxCandidates];
-    int m = 0;
-    for_each_box_neighbor(i, xc, half, start, sorted, g, margin, [&](int j) {
-        if (m < kMaxBoxCandidates) {
-            int t = m++;
-            while (t > 0 && js[t - 1] > j) {
-                js[t] = js[t - 1];
-                --t;
-            }
-            js[t] = j;
+    // ascending partner order: each entry's rank is the number of smaller entries (ids are unique)
+    for (int e = lane; e < m; e += 32) {
+        const int j = s_js[w][e];
+        int rank = 0;
+        for (int q = 0; q < m; ++q) rank += s_js[w][q] < j ? 1 : 0;
+        if (k + rank < cap) {
+            ca[k + rank] = i;
+            cb[k + rank] = j;
         }
-    });
-    for (int t = 0; t < m; ++t, ++k)
-        if (k < cap) {
-            ca[k] = i;
-            cb[k] = js[t];
-        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -537,13 +568,14 @@ int box_candidates(const b2c_bodies *b, b2c_boxes *bx, b2c_header *hdr, cudaStre
     if ((rc = exclusive_scan(bx->cursor, bx->start, nbk + 1, nullptr, bx->scan_tmp, s))) return rc;
     cudaMemsetAsync(bx->cursor, 0, sizeof(int) * (size_t)nbk, s);
     if (n > 0) k_box_scatter<<<blocks_for(n), kThreads, 0, s>>>(n, bx->bucket, bx->start, bx->cursor, bx->sorted);
-    k_box_cand_count<<<blocks_for(n + 1, 128), 128, 0, s>>>(n, b->xc, b->q, bx->half, bx->start, bx->sorted, g,
-                                                            bx->margin, bx->cand_count, hdr);
+    const int bgrid = std::max(1, (n + kBroadWarps - 1) / kBroadWarps);
+    k_box_cand_count<<<bgrid, 32 * kBroadWarps, 0, s>>>(n, b->xc, bx->half, bx->start, bx->sorted, g, bx->margin,
+                                                         bx->cand_count, hdr);
     if ((rc = check_launch("box_cand_count"))) return rc;
     if ((rc = exclusive_scan(bx->cand_count, bx->cand_offset, n + 1, nullptr, bx->scan_tmp, s))) return rc;
-    k_box_cand_emit<<<blocks_for(n + 1, 128), 128, 0, s>>>(n, b->xc, b->q, bx->half, bx->start, bx->sorted, g,
-                                                           bx->margin, bx->cand_offset, bx->cand_capacity, bx->cand_a,
-                                                           bx->cand_b, hdr);
+    k_box_cand_emit<<<bgrid, 32 * kBroadWarps, 0, s>>>(n, b->xc, bx->half, bx->start, bx->sorted, g, bx->margin,
+                                                        bx->cand_offset, bx->cand_capacity, bx->cand_a, bx->cand_b,
+                                                        hdr);
     return check_launch("box_cand_emit");
 }
 

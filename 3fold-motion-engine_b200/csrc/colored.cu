@@ -15,6 +15,8 @@
 //   6. warm store.
 // Every float32 expression follows the reference kernels with the contraction pattern of
 // b2c_math.cuh; the selection is float64 without contraction, as the reference compiled it.
+#include <cooperative_groups.h>
+
 #include "b2c_grid.cuh"
 
 namespace b2c {
@@ -422,30 +424,48 @@ __device__ __forceinline__ uint32_t pcg_hash(uint32_t state)
     const uint32_t c = ((b >> ((b >> 28u) + 4u)) ^ b) * 277803737u;
     return (c >> 22u) ^ c;
 }
-// k_prio, COL:136-148: |int32(randi(rand_init(7919, p)))| << 32 | p
-__device__ __forceinline__ long long jp_priority(int p)
-{
-    const uint32_t st = pcg_hash(pcg_hash(7919u + pcg_hash((uint32_t)p)));
-    long long v = (long long)(int32_t)st;
-    if (v < 0) v = -v;
-    return v * 4294967296LL + (long long)p;
-}
 
 constexpr int kColorThreads = 1024;
 constexpr int kMaxColorsCap = 512;
+constexpr int kColorSub = 16;  // buckets inside a colour: 8 contact counts (descending) x ground / box pair
+constexpr int kColorClusterMax = 16;
+constexpr int kPrioPairBits = 22;  // pair index bits of the compact priority (capacity <= 4M pairs)
 
+// Round-tagged claim of pair p in round r: a larger key wins atomicMax.  The priority of a pair
+// is k_prio's (COL:136-148) |int32(randi(rand_init(7919, p)))| << 32 | p, the smaller first; it is
+// packed here as |h| << 22 | p (the same order while p < 2^22).  The round tag makes the claims
+// of earlier rounds lose without clearing them; inside a round the smaller priority gives the
+// larger key.
+__device__ __forceinline__ unsigned long long claim_key(int p, int r)
+{
+    const uint32_t st = pcg_hash(pcg_hash(7919u + pcg_hash((uint32_t)p)));
+    long long h = (long long)(int32_t)st;
+    if (h < 0) h = -h;  // <= 2^31: 32 bits
+    const unsigned long long prio = ((unsigned long long)h << kPrioPairBits) | (unsigned long long)p;  // < 2^54
+    return ((unsigned long long)(r + 1) << 54) | ((1ull << 54) - 1ull - prio);
+}
+
+// Jones-Plassmann colouring of the pair graph behind the colour cache, on one thread-block
+// cluster (CTAs synchronised by cluster barriers, sums and histograms in distributed shared
+// memory).  Every round: each uncoloured pair claims its dynamic bodies (atomicMax of the
+// round-tagged key); a pair that holds all its claims takes the round number as its colour
+// (k_win, COL:163-181) or, with first_fit, the smallest colour not used around its bodies.  The
+// pairs are then grouped by colour, inside a colour by contact count (descending) and ground
+// pairs first, so the lanes of a warp of the solve run similar code.
 __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, int nbodies,
                                                                 const float *__restrict__ invM, b2c_pairs pr,
                                                                 int use_cache, int color_cap, int max_rounds,
                                                                 int first_fit)
 {
+    namespace cgc = cooperative_groups;
+    cgc::cluster_group cluster = cgc::this_cluster();
     __shared__ int s_flag;
-    __shared__ int s_left;
+    __shared__ int s_left[2];
     __shared__ int s_ncol;
-    __shared__ int s_cnt[kMaxColorsCap];
-    __shared__ int s_cur[kMaxColorsCap];
+    __shared__ int s_hist[kMaxColorsCap * kColorSub];  // rank 0 only: bucket counts, then cursors
+    const int rank = (int)cluster.block_rank(), nrank = (int)cluster.num_blocks();
+    const int tid = rank * kColorThreads + threadIdx.x, nth = nrank * kColorThreads;
     const int P = hdr->n_pairs;
-    const int tid = threadIdx.x;
     if (P == 0) {
         if (tid == 0) {
             hdr->n_colors = 0;
@@ -454,17 +474,18 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         return;
     }
     // colour cache: reuse while the pair count, pbi, pbj and invM are unchanged
-    if (use_cache) {
-        if (tid == 0) s_flag = (pr.cache_state[2] == 1 && pr.cache_state[0] == P) ? 0 : 1;
+    if (use_cache && pr.cache_state[2] == 1 && pr.cache_state[0] == P) {
+        if (threadIdx.x == 0) s_flag = 0;
         __syncthreads();
-        if (s_flag == 0) {
-            int mism = 0;
-            for (int p = tid; p < P; p += kColorThreads) mism |= (pr.pbi[p] != pr.cached_a[p]) | (pr.pbj[p] != pr.cached_b[p]);
-            for (int i = tid; i < nbodies; i += kColorThreads) mism |= (invM[i] != pr.cached_mass[i]);
-            if (mism) atomicOr(&s_flag, 1);
-        }
-        __syncthreads();
-        if (s_flag == 0) {
+        int mism = 0;
+        for (int p = tid; p < P; p += nth) mism |= (pr.pbi[p] != pr.cached_a[p]) | (pr.pbj[p] != pr.cached_b[p]);
+        for (int i = tid; i < nbodies; i += nth) mism |= (invM[i] != pr.cached_mass[i]);
+        if (mism) atomicOr(&s_flag, 1);
+        cluster.sync();
+        int any = 0;
+        for (int r = 0; r < nrank; ++r) any |= *cluster.map_shared_rank(&s_flag, r);
+        cluster.sync();  // no CTA leaves while another still reads its shared memory
+        if (!any) {
             if (tid == 0) {
                 hdr->n_colors = pr.cache_state[1];
                 pr.cache_state[3] += 1;
@@ -473,39 +494,40 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
             return;
         }
     }
-    for (int p = tid; p < P; p += kColorThreads) pr.col[p] = -1;
+    unsigned long long *claim = reinterpret_cast<unsigned long long *>(pr.claim);
     unsigned long long *used = reinterpret_cast<unsigned long long *>(pr.body_colors);
-    if (first_fit)
-        for (int i = tid; i < nbodies; i += kColorThreads) used[i] = 0ull;
-    if (tid == 0) s_ncol = 0;
+    for (int p = tid; p < P; p += nth) pr.col[p] = -1;
+    for (int i = tid; i < nbodies; i += nth) {
+        claim[i] = 0ull;
+        if (first_fit) used[i] = 0ull;
+    }
+    if (threadIdx.x == 0) s_ncol = 0;
+    cluster.sync();
     int r = 0;
     bool done = false;
     for (; r < max_rounds; ++r) {
-        for (int i = tid; i < nbodies; i += kColorThreads) pr.claim[i] = LLONG_MAX;
-        __syncthreads();  // also: every thread has read s_left of the previous round
-        if (tid == 0) s_left = 0;
-        for (int p = tid; p < P; p += kColorThreads) {
+        const int b = r & 1;
+        if (threadIdx.x == 0) s_left[b] = 0;  // last read two rounds ago, before two cluster barriers
+        for (int p = tid; p < P; p += nth) {
             if (pr.col[p] >= 0) continue;
-            const long long k = jp_priority(p);
+            const unsigned long long k = claim_key(p, r);
             const int bi = pr.pbi[p], bj = pr.pbj[p];
-            if (invM[bi] > 0.0f) atomicMin(reinterpret_cast<long long *>(pr.claim) + bi, k);
-            if (bj >= 0 && invM[bj] > 0.0f) atomicMin(reinterpret_cast<long long *>(pr.claim) + bj, k);
+            if (invM[bi] > 0.0f) atomicMax(claim + bi, k);
+            if (bj >= 0 && invM[bj] > 0.0f) atomicMax(claim + bj, k);
         }
-        __syncthreads();
-        for (int p = tid; p < P; p += kColorThreads) {
+        cluster.sync();
+        int left = 0;
+        for (int p = tid; p < P; p += nth) {
             if (pr.col[p] >= 0) continue;
-            const long long k = jp_priority(p);
+            const unsigned long long k = claim_key(p, r);
             const int bi = pr.pbi[p], bj = pr.pbj[p];
-            bool ok = true;
-            if (invM[bi] > 0.0f && pr.claim[bi] != k) ok = false;
-            if (bj >= 0 && invM[bj] > 0.0f && pr.claim[bj] != k) ok = false;
-            if (!ok) {
-                atomicAdd(&s_left, 1);
+            const bool da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
+            if ((da && __ldcg(claim + bi) != k) || (db && __ldcg(claim + bj) != k)) {
+                ++left;
             } else if (!first_fit) {
                 pr.col[p] = r;
             } else {
                 // the winners of a round share no dynamic body: their masks are theirs alone
-                const bool da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
                 const unsigned long long m = (da ? used[bi] : 0ull) | (db ? used[bj] : 0ull);
                 const int c = (~m == 0ull) ? 64 : __ffsll((long long)~m) - 1;
                 pr.col[p] = c;
@@ -516,13 +538,21 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
                 atomicMax(&s_ncol, c + 1);
             }
         }
-        __syncthreads();
-        if (s_left == 0) {
+        if (left) atomicAdd(&s_left[b], left);
+        cluster.sync();
+        int total = 0;
+        for (int q = 0; q < nrank; ++q) total += *cluster.map_shared_rank(&s_left[b], q);
+        if (total == 0) {
             done = true;
             break;
         }
     }
-    const int ncol = first_fit ? s_ncol : (done ? r + 1 : r);
+    int ncol = done ? r + 1 : r;
+    if (first_fit) {
+        ncol = 0;
+        for (int q = 0; q < nrank; ++q) ncol = max(ncol, *cluster.map_shared_rank(&s_ncol, q));
+    }
+    cluster.sync();  // every CTA has read the others' s_left and s_ncol
     if (!done || ncol > color_cap || ncol > pr.max_colors || ncol > kMaxColorsCap) {
         if (tid == 0) {
             atomicOr(&hdr->error, done ? B2C_ERR_COLOR_OVERFLOW : B2C_ERR_COLOR_TIMEOUT);
@@ -533,43 +563,88 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         }
         return;
     }
-    // group the pairs by colour (order inside a colour is free: its pairs share no dynamic body)
-    for (int c = tid; c < ncol; c += kColorThreads) s_cnt[c] = 0;
-    __syncthreads();
-    for (int p = tid; p < P; p += kColorThreads) atomicAdd(&s_cnt[pr.col[p]], 1);
-    __syncthreads();
-    if (tid == 0) {
-        int acc = 0;
-        for (int c = 0; c < ncol; ++c) {
+    // group by (colour, bucket): counts in rank 0's shared memory, scanned there, then cursors
+    int *hist0 = cluster.map_shared_rank(s_hist, 0);
+    if (rank == 0)
+        for (int k = threadIdx.x; k < ncol * kColorSub; k += kColorThreads) s_hist[k] = 0;
+    cluster.sync();
+    for (int p = tid; p < P; p += nth) {
+        const int n = min(max(pr.kcount[p], 1), 8);
+        atomicAdd(hist0 + pr.col[p] * kColorSub + (8 - n) * 2 + (pr.pbj[p] >= 0 ? 1 : 0), 1);
+    }
+    cluster.sync();
+    if (rank == 0) {
+        __shared__ int s_ctot[kMaxColorsCap];
+        for (int c = threadIdx.x; c < ncol; c += kColorThreads) {
+            int t = 0;
+            for (int k = 0; k < kColorSub; ++k) t += s_hist[c * kColorSub + k];
+            s_ctot[c] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int c = 0; c < ncol; ++c) {
+                const int t = s_ctot[c];
+                s_ctot[c] = acc;
+                acc += t;
+            }
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < ncol; c += kColorThreads) {
+            int acc = s_ctot[c];
             pr.cstart[c] = acc;
-            pr.ccount[c] = s_cnt[c];
-            s_cur[c] = acc;
-            acc += s_cnt[c];
+            for (int k = 0; k < kColorSub; ++k) {
+                const int t = s_hist[c * kColorSub + k];
+                s_hist[c * kColorSub + k] = acc;
+                acc += t;
+            }
+            pr.ccount[c] = acc - s_ctot[c];
         }
     }
-    __syncthreads();
-    // ground pairs first inside every colour, so a warp of the solve mostly runs one code path
-    for (int p = tid; p < P; p += kColorThreads)
-        if (pr.pbj[p] < 0) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
-    __syncthreads();
-    for (int p = tid; p < P; p += kColorThreads)
-        if (pr.pbj[p] >= 0) pr.porder[atomicAdd(&s_cur[pr.col[p]], 1)] = p;
+    cluster.sync();
+    for (int p = tid; p < P; p += nth) {
+        const int n = min(max(pr.kcount[p], 1), 8);
+        const int slot = atomicAdd(hist0 + pr.col[p] * kColorSub + (8 - n) * 2 + (pr.pbj[p] >= 0 ? 1 : 0), 1);
+        pr.porder[slot] = p;
+    }
     if (use_cache) {
-        for (int p = tid; p < P; p += kColorThreads) {
+        for (int p = tid; p < P; p += nth) {
             pr.cached_a[p] = pr.pbi[p];
             pr.cached_b[p] = pr.pbj[p];
         }
-        for (int i = tid; i < nbodies; i += kColorThreads) pr.cached_mass[i] = invM[i];
+        for (int i = tid; i < nbodies; i += nth) pr.cached_mass[i] = invM[i];
     }
     if (tid == 0) {
         hdr->n_colors = ncol;
         hdr->cache_hit = 0;
-        hdr->rounds = ncol;
+        hdr->rounds = r + 1;
         pr.cache_state[0] = P;
         pr.cache_state[1] = ncol;
         pr.cache_state[2] = 1;
         if (use_cache) pr.cache_state[4] += 1;  // cumulative misses ([3] counts hits)
     }
+    cluster.sync();  // rank 0's shared cursors stay alive until every CTA is done with them
+}
+
+// largest power-of-two cluster (<= 16) of colouring CTAs the device co-schedules; cached
+static int color_cluster_size()
+{
+    static int cached = -1;
+    if (cached < 0) {
+        cudaFuncSetAttribute(k_color_pairs, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kColorClusterMax);
+        cfg.blockDim = dim3(kColorThreads);
+        int cs = 0;
+        if (cudaOccupancyMaxPotentialClusterSize(&cs, k_color_pairs, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            cs = 1;
+        }
+        int p2 = 1;
+        for (int c = 1; c <= std::min(cs, kColorClusterMax); c *= 2) p2 = c;
+        cached = p2;
+    }
+    return cached;
 }
 
 int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
@@ -663,8 +738,29 @@ int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_c
         set_error("color_pairs: B2C_COLOR_FIRST_FIT needs pairs->body_colors");
         return B2C_EARG;
     }
-    k_color_pairs<<<1, kColorThreads, 0, s>>>(hdr, b->n, b->invM, *pr, (p->flags & B2C_COLOR_CACHE) ? 1 : 0,
-                                              first_fit ? std::min(cap, 64) : cap, kMaxColorsCap + 1, first_fit);
+    if (pr->capacity > (1 << kPrioPairBits)) {
+        set_error("color_pairs: pair capacity %d above %d", pr->capacity, 1 << kPrioPairBits);
+        return B2C_EARG;
+    }
+    const int cs = color_cluster_size();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kColorThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_pairs, hdr, b->n, (const float *)b->invM, *pr,
+                                       (p->flags & B2C_COLOR_CACHE) ? 1 : 0, first_fit ? std::min(cap, 64) : cap,
+                                       kMaxColorsCap + 1, first_fit);
+    if (e != cudaSuccess) {
+        set_error("color_pairs: cluster launch of %d CTAs: %s", cs, cudaGetErrorString(e));
+        return B2C_ECUDA;
+    }
     return check_launch("color_pairs");
 }
 

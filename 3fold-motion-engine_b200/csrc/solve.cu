@@ -257,6 +257,17 @@ __device__ __forceinline__ CRec load_contact(const Records &R, int s, int k)
                 R.contact(kCImp, k)[s]};
 }
 
+// The impulse word of a contact is (jn, jt1, jt2, jp).  A phase can run the velocity chunk and
+// the position chunk of the same pair on two threads (they read and write disjoint state), so the
+// velocity chunk stores only x, y, z and the position chunk only w.
+__device__ __forceinline__ void store_imp_xyz(float4 *p, float4 im)
+{
+    float *f = reinterpret_cast<float *>(p);
+    *reinterpret_cast<float2 *>(f) = make_float2(im.x, im.y);
+    f[2] = im.z;
+}
+__device__ __forceinline__ void store_imp_w(float4 *p, float jp) { reinterpret_cast<float *>(p)[3] = jp; }
+
 // apply_warm, contact_engine_gpu_applied_warm.py:5-54
 template <class BA>
 __device__ void pair_apply_warm(const SolveArgs &a, int s, const BA &BS)
@@ -384,7 +395,7 @@ __device__ void pair_velocity(const SolveArgs &a, int s, const BA &B)
                     wB = sub3(wB, matvec(q.IB, cross3(rB, Jt)));
                 }
             }
-            a.rec.contact(kCImp, k)[s] = im;
+            store_imp_xyz(&a.rec.contact(kCImp, k)[s], im);
         }
         cur = nxt;
     }
@@ -422,11 +433,10 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
         if (meff >= 1e-12f) {
             const float bias = B2C_BETA * fmaxf(cur.n.w - B2C_SLOP, 0.0f) / a.dt;
             float dj = (bias - dot3(rel, nrm)) / meff;
-            float4 im = cur.im;
-            const float nw = fmaxf(0.0f, im.w + dj);
-            dj = nw - im.w;
-            im.w = nw;
-            a.rec.contact(kCImp, k)[s] = im;
+            const float jp = cur.im.w;
+            const float nw = fmaxf(0.0f, jp + dj);
+            dj = nw - jp;
+            store_imp_w(&a.rec.contact(kCImp, k)[s], nw);
             const f3 Jn = scale3(nrm, dj);
             if (iMA > 0.0f) {
                 pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
@@ -450,33 +460,47 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 }
 
 // ---------------------------------------------------------------------------------------------
-// the persistent kernels: record slot cstart[ci] + t of colour ci on thread t mod (threads)
+// the persistent kernels
+//
+// Phase schedule.  The position sweeps read and write only pv, po and the contacts' jp, which no
+// velocity sweep or warm application touches, and the velocity sweeps never read them; so
+// position sweep k runs in the same phase as the k-th (warm application, velocity sweep 0,
+// velocity sweep 1, ...) pass over the colours, on other threads.  Every pair still sees the
+// same values in the same order as in the sequential schedule (warm; vit velocity sweeps; pit
+// position sweeps), so the results are identical, with (warm + max(vit, pit)) x colours phases
+// instead of (warm + vit + pit) x colours.
+//
+// Task t of a phase (velocity/warm tasks first, then position tasks) runs on lane t mod 32 of
+// warp chunk c = t div 32, and chunk c on CTA c mod CTAs: a warp reads 32 consecutive record
+// slots (coalesced), and a colour narrower than the launch is spread over all of its SMs.
 // ---------------------------------------------------------------------------------------------
 template <int kKind, bool kFixed, class BA>
 __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
     if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    if (a.apply_warm) {
+    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
+    const int me = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);  // task slot
+    const int vpasses = (a.apply_warm ? 1 : 0) + a.vit;
+    const int passes = vpasses > a.pit ? vpasses : a.pit;
+    for (int pass = 0; pass < passes; ++pass) {
+        const bool vel = pass < vpasses;
+        const bool warm = a.apply_warm && pass == 0;
+        const bool pos = pass < a.pit;
         for (int ci = 0; ci < nc; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_apply_warm(a, s0 + t, B);
+            const int nv = vel ? cnt : 0, ntask = nv + (pos ? cnt : 0);
+            for (int t = me; t < ntask; t += nth) {
+                if (t < nv) {
+                    if (warm) pair_apply_warm(a, s0 + t, B);
+                    else pair_velocity<BA, kFixed>(a, s0 + t, B);
+                } else {
+                    pair_position(a, s0 + (t - nv), B);
+                }
+            }
             if (!solve_barrier<kKind>(a)) return;
         }
     }
-    for (int it = 0; it < a.vit; ++it)
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_velocity<BA, kFixed>(a, s0 + t, B);
-            if (!solve_barrier<kKind>(a)) return;
-        }
-    for (int it = 0; it < a.pit; ++it)
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) pair_position(a, s0 + t, B);
-            if (!solve_barrier<kKind>(a)) return;
-        }
 }
 
 constexpr int kClusterThreads = 512;

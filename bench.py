@@ -256,6 +256,11 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--save-state", default=None,
+                    help="write the body state after the set-up steps to this .npz (profiling aid)")
+    ap.add_argument("--load-state", default=None,
+                    help="start from a state written by --save-state instead of running the set-up steps "
+                         "(profiling aid: short runs with few launches before the captured ones)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.steps is None:
@@ -296,8 +301,16 @@ def main():
 
     e = make_engine(me, wl, scene)
     dt, S = wl["dt"], wl["substeps"]
-    for _ in range(wl["preroll"]):
-        e.step(dt, S)
+    if args.load_state:
+        d = np.load(args.load_state)
+        e.set_body_state(d["xc"], d["q"], d["v"], d["w"])
+    else:
+        for _ in range(wl["preroll"]):
+            e.step(dt, S)
+    if args.save_state:
+        torch.cuda.synchronize()
+        np.savez(args.save_state, xc=e.xc[:, :3].cpu().numpy(), q=e.q.cpu().numpy(), v=e.v[:, :3].cpu().numpy(),
+                 w=e.w[:, :3].cpu().numpy())
     for _ in range(args.warmup):
         e.step(dt, S)
     e.check_errors()
