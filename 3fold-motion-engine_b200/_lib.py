@@ -69,6 +69,7 @@ COLOR_CACHE = 4
 COLOR_WARM_START = 8
 COLOR_PER_CONTACT = 16
 COLOR_FIRST_FIT = 32
+COLOR_ROW_FORM = 64
 
 
 class Grid(ctypes.Structure):

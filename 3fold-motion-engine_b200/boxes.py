@@ -51,7 +51,7 @@ class BoxContactEngine(_BeadEngineBase):
 
     def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, fixed_frame=True, apply_warm=True,
                  color_cache=True, warm_start=True, margin=MARGIN, device="cuda", color_cap=NCOLMAX,
-                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16, first_fit=True):
+                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16, first_fit=True, row_form=True):
         super().__init__(dims=dims, mu=mu, device=device, graph=True)
         self.vit, self.pit = int(vit), int(pit)
         self.fixed_frame, self.apply_warm = bool(fixed_frame), bool(apply_warm)
@@ -62,6 +62,7 @@ class BoxContactEngine(_BeadEngineBase):
         self.barrier_timeout_ns = int(barrier_timeout_s * 1e9)
         self.cand_per_body = int(cand_per_body)
         self.first_fit = bool(first_fit)
+        self.row_form = bool(row_form) and self.fixed_frame
         self._halves, self._mus = [], []
         self._has_manifold = True
 
@@ -147,7 +148,7 @@ class BoxContactEngine(_BeadEngineBase):
                                     _ptr(self.po), _ptr(self.invM), _ptr(self.IbInv), _ptr(self.kin), _ptr(self.invIw))
         flags = ((_lib.COLOR_FIXED_FRAME if self.fixed_frame else 0) | (_lib.COLOR_APPLY_WARM if self.apply_warm else 0)
                  | (_lib.COLOR_CACHE if self.color_cache else 0) | (_lib.COLOR_WARM_START if self.warm_start else 0)
-                 | (_lib.COLOR_FIRST_FIT if self.first_fit else 0))
+                 | (_lib.COLOR_FIRST_FIT if self.first_fit else 0) | (_lib.COLOR_ROW_FORM if self.row_form else 0))
         self.c_params = _lib.ColorParams(self.vit, self.pit, 8, flags, self.mu, 1.0, min(self.color_cap, NCOLMAX),
                                          self.solve_blocks, self.barrier_timeout_ns,
                                          _ptr(self.body_mu) if self.per_body_mu else None)

@@ -40,6 +40,11 @@ __device__ __forceinline__ f3 ldcg3(const float *p, int i) { return xyz(ldcg4(p,
 // record fields (float4 units)
 enum { kRecBody = 7, kRecContact = 5 };
 enum { kCN = 0, kCRA = 1, kCRB = 2, kCT1 = 3, kCImp = 4 };
+// row form (B2C_COLOR_ROW_FORM): per contact n|inv_n, rA|bias, rB, t1|inv_1, t2|inv_2, the
+// angular responses kAn, kA1, kA2, kBn, kB1, kB2 and the impulses
+enum { kRecContactRow = 12 };
+enum { kRN = 0, kRRA = 1, kRRB = 2, kRT1 = 3, kRT2 = 4, kRKAN = 5, kRKA1 = 6, kRKA2 = 7, kRKBN = 8, kRKB1 = 9,
+       kRKB2 = 10, kRImp = 11 };
 
 struct Records {
     float4 *base;
@@ -59,7 +64,7 @@ struct SolveArgs {
     Records rec;
     float *v, *w, *pv, *po;
     float mu, t2d, dt;
-    int vit, pit, fixed_frame, apply_warm;
+    int vit, pit, fixed_frame, apply_warm, row;
     unsigned int *bar_count, *bar_gen;
     long long timeout_ns;
 };
@@ -142,14 +147,89 @@ __global__ void k_pair_gather(const b2c_header *__restrict__ hdr, const int *__r
     }
 }
 
+// row form: the same header and masses, and per contact the constants of the substep
+__global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int *__restrict__ porder,
+                                  const int *__restrict__ pstart, const int *__restrict__ pcount,
+                                  const int *__restrict__ pidx, const int *__restrict__ pbi,
+                                  const int *__restrict__ pbj, b2c_contacts kept, const float *__restrict__ xc,
+                                  const float *__restrict__ invIw, const float *__restrict__ invM,
+                                  const float *__restrict__ body_mu, float mu, float dt, Records R, b2c_header *hdr_w)
+{
+    const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
+        const int p = porder[s];
+        const int bi = pbi[p], bj = pbj[p];
+        int n = pcount[p];
+        if (n > R.K) {
+            atomicOr(&hdr_w->error, B2C_ERR_CHUNK_OVERFLOW);
+            n = R.K;
+        }
+        R.hdr()[s] = make_int4(bi, bj, n, p);
+        const m3 IA = ldm(invIw, bi);
+        const float iMA = invM[bi];
+        m3 IB = IA;
+        float iMB = 0.0f;
+        if (bj >= 0) {
+            IB = ldm(invIw, bj);
+            iMB = invM[bj];
+        }
+        float mu_p = mu;
+        if (body_mu) mu_p = bj >= 0 ? sqrtf(body_mu[bi] * body_mu[bj]) : body_mu[bi];
+        R.body(6)[s] = make_float4(iMA, iMB, mu_p, 0.0f);
+        const f3 xA = ld3(xc, bi);
+        f3 xB{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) xB = ld3(xc, bj);
+        const int st = pstart[p];
+        for (int j = 0; j < n; ++j) {
+            const int c = pidx[st + j];
+            const float4 pA4 = ld4(kept.pA, c);
+            const f3 nrm = ld3(kept.n, c);
+            const f3 rA = sub3(xyz(pA4), xA);
+            f3 rB{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) rB = sub3(ld3(kept.pB, c), xB);
+            f3 aa{1.0f, 0.0f, 0.0f};
+            if (fabsf(nrm.x) >= 0.9f) aa = f3{0.0f, 1.0f, 0.0f};
+            const float dd = dot3(aa, nrm);
+            const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
+            const f3 t2 = cross3(nrm, t1);
+            const f3 rnA = cross3(rA, nrm), rtA1 = cross3(rA, t1), rtA2 = cross3(rA, t2);
+            const f3 kAn = matvec(IA, rnA), kA1 = matvec(IA, rtA1), kA2 = matvec(IA, rtA2);
+            float meff = iMA + dot3(rnA, kAn), meft1 = iMA + dot3(rtA1, kA1), meft2 = iMA + dot3(rtA2, kA2);
+            if (bj >= 0) {
+                const f3 rnB = cross3(rB, nrm), rtB1 = cross3(rB, t1), rtB2 = cross3(rB, t2);
+                const f3 kBn = matvec(IB, rnB), kB1 = matvec(IB, rtB1), kB2 = matvec(IB, rtB2);
+                meff = (meff + iMB) + dot3(rnB, kBn);
+                meft1 = (meft1 + iMB) + dot3(rtB1, kB1);
+                meft2 = (meft2 + iMB) + dot3(rtB2, kB2);
+                R.contact(kRRB, j)[s] = f4(rB, 0.0f);
+                R.contact(kRKBN, j)[s] = f4(kBn, 0.0f);
+                R.contact(kRKB1, j)[s] = f4(kB1, 0.0f);
+                R.contact(kRKB2, j)[s] = f4(kB2, 0.0f);
+            }
+            const float inv_n = meff >= 1e-12f ? 1.0f / meff : 0.0f;
+            const float inv_1 = meft1 >= 1e-12f ? 1.0f / meft1 : 0.0f;
+            const float inv_2 = meft2 >= 1e-12f ? 1.0f / meft2 : 0.0f;
+            const float bias = B2C_BETA * fmaxf(pA4.w - B2C_SLOP, 0.0f) / dt;
+            R.contact(kRN, j)[s] = f4(nrm, inv_n);
+            R.contact(kRRA, j)[s] = f4(rA, bias);
+            R.contact(kRT1, j)[s] = f4(t1, inv_1);
+            R.contact(kRT2, j)[s] = f4(t2, inv_2);
+            R.contact(kRKAN, j)[s] = f4(kAn, 0.0f);
+            R.contact(kRKA1, j)[s] = f4(kA1, 0.0f);
+            R.contact(kRKA2, j)[s] = f4(kA2, 0.0f);
+            R.contact(kRImp, j)[s] = ld4(kept.imp, c);
+        }
+    }
+}
+
 __global__ void k_imp_scatter(const b2c_header *__restrict__ hdr, const int *__restrict__ pstart,
-                              const int *__restrict__ pidx, Records R, float *__restrict__ imp)
+                              const int *__restrict__ pidx, Records R, int imp_field, float *__restrict__ imp)
 {
     const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
         const int4 h = R.hdr()[s];
         const int st = pstart[h.w];
-        for (int j = 0; j < h.z; ++j) st4(imp, pidx[st + j], R.contact(kCImp, j)[s]);
+        for (int j = 0; j < h.z; ++j) st4(imp, pidx[st + j], R.contact(imp_field, j)[s]);
     }
 }
 
@@ -460,6 +540,230 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 }
 
 // ---------------------------------------------------------------------------------------------
+// row form of the three chunks (B2C_COLOR_ROW_FORM; not in the reference): the same sweep with
+// the substep constants of k_pair_gather_row.  The contact loop prefetches the next contact's
+// record, as above.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ f3 fma3s(float s, f3 a, f3 b) { return f3{fmaf(s, a.x, b.x), fmaf(s, a.y, b.y), fmaf(s, a.z, b.z)}; }
+
+struct RowVel {
+    float4 n, ra, rb, t1, t2, kan, ka1, ka2, kbn, kb1, kb2, im;
+};
+__device__ __forceinline__ RowVel load_row_vel(const Records &R, int s, int k, bool has_b)
+{
+    RowVel c;
+    c.n = R.contact(kRN, k)[s];
+    c.ra = R.contact(kRRA, k)[s];
+    c.t1 = R.contact(kRT1, k)[s];
+    c.t2 = R.contact(kRT2, k)[s];
+    c.kan = R.contact(kRKAN, k)[s];
+    c.ka1 = R.contact(kRKA1, k)[s];
+    c.ka2 = R.contact(kRKA2, k)[s];
+    c.im = R.contact(kRImp, k)[s];
+    if (has_b) {
+        c.rb = R.contact(kRRB, k)[s];
+        c.kbn = R.contact(kRKBN, k)[s];
+        c.kb1 = R.contact(kRKB1, k)[s];
+        c.kb2 = R.contact(kRKB2, k)[s];
+    } else {
+        c.rb = c.kbn = c.kb1 = c.kb2 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    return c;
+}
+
+template <class BA>
+__device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS)
+{
+    const int4 h = a.rec.hdr()[s];
+    const float4 mm = a.rec.body(6)[s];
+    const int A = h.x, B = h.y, n = h.z;
+    const float iMA = mm.x, iMB = mm.y;
+    RowVel cur = load_row_vel(a.rec, s, 0, B >= 0);
+    f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
+    if (B >= 0) {
+        vb = BS.get(B, 0);
+        wb = BS.get(B, 1);
+    }
+    for (int k = 0; k < n; ++k) {
+        RowVel nxt;
+        if (k + 1 < n) nxt = load_row_vel(a.rec, s, k + 1, B >= 0);
+        const f3 nrm = xyz(cur.n), t1 = xyz(cur.t1), t2 = xyz(cur.t2);
+        const float jn = cur.im.x, j1 = cur.im.y, j2 = cur.im.z;
+        const f3 J{fmaf(j2, t2.x, fmaf(jn, nrm.x, j1 * t1.x)), fmaf(j2, t2.y, fmaf(jn, nrm.y, j1 * t1.y)),
+                   fmaf(j2, t2.z, fmaf(jn, nrm.z, j1 * t1.z))};
+        if (iMA > 0.0f) {
+            const f3 kn = xyz(cur.kan), k1 = xyz(cur.ka1), k2 = xyz(cur.ka2);
+            va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
+            wa = add3(wa, f3{fmaf(j2, k2.x, fmaf(jn, kn.x, j1 * k1.x)), fmaf(j2, k2.y, fmaf(jn, kn.y, j1 * k1.y)),
+                             fmaf(j2, k2.z, fmaf(jn, kn.z, j1 * k1.z))});
+        }
+        if (B >= 0 && iMB > 0.0f) {
+            const f3 kn = xyz(cur.kbn), k1 = xyz(cur.kb1), k2 = xyz(cur.kb2);
+            vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
+            wb = sub3(wb, f3{fmaf(j2, k2.x, fmaf(jn, kn.x, j1 * k1.x)), fmaf(j2, k2.y, fmaf(jn, kn.y, j1 * k1.y)),
+                             fmaf(j2, k2.z, fmaf(jn, kn.z, j1 * k1.z))});
+        }
+        cur = nxt;
+    }
+    if (iMA > 0.0f) {
+        BS.set(A, 0, va);
+        BS.set(A, 1, wa);
+    }
+    if (B >= 0 && iMB > 0.0f) {
+        BS.set(B, 0, vb);
+        BS.set(B, 1, wb);
+    }
+}
+
+template <class BA>
+__device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B)
+{
+    const int4 h = a.rec.hdr()[s];
+    const float4 mm = a.rec.body(6)[s];
+    const int bi = h.x, bj = h.y, n = h.z;
+    const float iMA = mm.x, iMB = mm.y, mu = mm.z;
+    RowVel cur = load_row_vel(a.rec, s, 0, bj >= 0);
+    f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
+    f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        vB = B.get(bj, 0);
+        wB = B.get(bj, 1);
+    }
+    for (int k = 0; k < n; ++k) {
+        RowVel nxt;
+        if (k + 1 < n) nxt = load_row_vel(a.rec, s, k + 1, bj >= 0);
+        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
+        f3 va = add3(vA, cross3(wA, rA));
+        f3 vb{0.0f, 0.0f, 0.0f};
+        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+        f3 vrel = sub3(va, vb);
+        const float vn = dot3(vrel, nrm);
+        if (cur.n.w > 0.0f) {
+            float4 im = cur.im;
+            float dj = -vn * cur.n.w;
+            const float nw = fmaxf(0.0f, im.x + dj);
+            dj = nw - im.x;
+            im.x = nw;
+            const f3 Jn = scale3(nrm, dj);
+            if (iMA > 0.0f) {
+                vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
+                wA = fma3s(dj, xyz(cur.kan), wA);
+            }
+            if (bj >= 0 && iMB > 0.0f) {
+                vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
+                wB = fma3s(-dj, xyz(cur.kbn), wB);
+            }
+            va = add3(vA, cross3(wA, rA));
+            vb = f3{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+            vrel = sub3(va, vb);
+            if (cur.t1.w > 0.0f && cur.t2.w > 0.0f) {
+                const f3 t1 = xyz(cur.t1), t2 = xyz(cur.t2);
+                const float o1 = im.y, o2 = im.z;
+                float a1 = o1 - dot3(vrel, t1) * cur.t1.w;
+                float a2 = o2 - dot3(vrel, t2) * cur.t2.w;
+                const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+                const float lim = mu * im.x;
+                if (mag > lim && mag > 1e-12f) {
+                    const float sc = lim / mag;
+                    a1 = a1 * sc;
+                    a2 = a2 * sc;
+                }
+                im.y = a1;
+                im.z = a2;
+                const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+                const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+                if (iMA > 0.0f) {
+                    vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
+                    wA = fma3s(e1, xyz(cur.ka1), fma3s(e2, xyz(cur.ka2), wA));
+                }
+                if (bj >= 0 && iMB > 0.0f) {
+                    vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
+                    wB = fma3s(-e1, xyz(cur.kb1), fma3s(-e2, xyz(cur.kb2), wB));
+                }
+            }
+            store_imp_xyz(&a.rec.contact(kRImp, k)[s], im);
+        }
+        cur = nxt;
+    }
+    if (iMA > 0.0f) {
+        B.set(bi, 0, vA);
+        B.set(bi, 1, wA);
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        B.set(bj, 0, vB);
+        B.set(bj, 1, wB);
+    }
+}
+
+struct RowPos {
+    float4 n, ra, rb, kan, kbn;
+    float jp;
+};
+__device__ __forceinline__ RowPos load_row_pos(const Records &R, int s, int k, bool has_b)
+{
+    RowPos c;
+    c.n = R.contact(kRN, k)[s];
+    c.ra = R.contact(kRRA, k)[s];
+    c.kan = R.contact(kRKAN, k)[s];
+    c.jp = reinterpret_cast<const float *>(&R.contact(kRImp, k)[s])[3];
+    if (has_b) {
+        c.rb = R.contact(kRRB, k)[s];
+        c.kbn = R.contact(kRKBN, k)[s];
+    } else {
+        c.rb = c.kbn = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    return c;
+}
+
+template <class BA>
+__device__ void pair_position_row(const SolveArgs &a, int s, const BA &B)
+{
+    const int4 h = a.rec.hdr()[s];
+    const float4 mm = a.rec.body(6)[s];
+    const int bi = h.x, bj = h.y, n = h.z;
+    const float iMA = mm.x, iMB = mm.y;
+    RowPos cur = load_row_pos(a.rec, s, 0, bj >= 0);
+    f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
+    f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        pvB = B.get(bj, 2);
+        poB = B.get(bj, 3);
+    }
+    for (int k = 0; k < n; ++k) {
+        RowPos nxt;
+        if (k + 1 < n) nxt = load_row_pos(a.rec, s, k + 1, bj >= 0);
+        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
+        f3 rel = add3(pvA, cross3(poA, rA));
+        if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
+        if (cur.n.w > 0.0f) {
+            float dj = (cur.ra.w - dot3(rel, nrm)) * cur.n.w;
+            const float nw = fmaxf(0.0f, cur.jp + dj);
+            dj = nw - cur.jp;
+            store_imp_w(&a.rec.contact(kRImp, k)[s], nw);
+            const f3 Jn = scale3(nrm, dj);
+            if (iMA > 0.0f) {
+                pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
+                poA = fma3s(dj, xyz(cur.kan), poA);
+            }
+            if (bj >= 0 && iMB > 0.0f) {
+                pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
+                poB = fma3s(-dj, xyz(cur.kbn), poB);
+            }
+        }
+        cur = nxt;
+    }
+    if (iMA > 0.0f) {
+        B.set(bi, 2, pvA);
+        B.set(bi, 3, poA);
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        B.set(bj, 2, pvB);
+        B.set(bj, 3, poB);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // the persistent kernels
 //
 // Phase schedule.  The position sweeps read and write only pv, po and the contacts' jp, which no
@@ -474,7 +778,7 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 // warp chunk c = t div 32, and chunk c on CTA c mod CTAs: a warp reads 32 consecutive record
 // slots (coalesced), and a colour narrower than the launch is spread over all of its SMs.
 // ---------------------------------------------------------------------------------------------
-template <int kKind, bool kFixed, class BA>
+template <int kKind, bool kFixed, bool kRow, class BA>
 __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
@@ -491,11 +795,20 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
             const int nv = vel ? cnt : 0, ntask = nv + (pos ? cnt : 0);
             for (int t = me; t < ntask; t += nth) {
-                if (t < nv) {
-                    if (warm) pair_apply_warm(a, s0 + t, B);
-                    else pair_velocity<BA, kFixed>(a, s0 + t, B);
+                if (kRow) {
+                    if (t < nv) {
+                        if (warm) pair_apply_warm_row(a, s0 + t, B);
+                        else pair_velocity_row(a, s0 + t, B);
+                    } else {
+                        pair_position_row(a, s0 + (t - nv), B);
+                    }
                 } else {
-                    pair_position(a, s0 + (t - nv), B);
+                    if (t < nv) {
+                        if (warm) pair_apply_warm(a, s0 + t, B);
+                        else pair_velocity<BA, kFixed>(a, s0 + t, B);
+                    } else {
+                        pair_position(a, s0 + (t - nv), B);
+                    }
                 }
             }
             if (!solve_barrier<kKind>(a)) return;
@@ -503,28 +816,37 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
     }
 }
 
-constexpr int kClusterThreads = 512;
+constexpr int kClusterThreads = 512;     // reference form
+constexpr int kClusterThreadsRow = 384;  // row form: more live record registers per thread
 constexpr int kClusterMax = 16;
 
 __global__ void __launch_bounds__(256) k_color_solve_block(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.fixed_frame) solve_body<kBlock, true>(a, B);
-    else solve_body<kBlock, false>(a, B);
+    if (a.row) solve_body<kBlock, true, true>(a, B);
+    else if (a.fixed_frame) solve_body<kBlock, true, false>(a, B);
+    else solve_body<kBlock, false, false>(a, B);
 }
 __global__ void __launch_bounds__(256) k_color_solve_grid(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.fixed_frame) solve_body<kGrid, true>(a, B);
-    else solve_body<kGrid, false>(a, B);
+    if (a.row) solve_body<kGrid, true, true>(a, B);
+    else if (a.fixed_frame) solve_body<kGrid, true, false>(a, B);
+    else solve_body<kGrid, false, false>(a, B);
 }
-// Cluster solve.  (Holding the body state in distributed shared memory instead measured slower
-// on B200 for this access pattern: 1.25 ms against 0.78 ms on the 10k-box lattice.)
+// Cluster solve, one kernel per form so each gets the registers it needs.  (Holding the body
+// state in distributed shared memory instead measured slower on B200 for this access pattern:
+// 1.25 ms against 0.78 ms on the 10k-box lattice.)
 __global__ void __launch_bounds__(kClusterThreads) k_color_solve_cluster(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.fixed_frame) solve_body<kCluster, true>(a, B);
-    else solve_body<kCluster, false>(a, B);
+    if (a.fixed_frame) solve_body<kCluster, true, false>(a, B);
+    else solve_body<kCluster, false, false>(a, B);
+}
+__global__ void __launch_bounds__(kClusterThreadsRow) k_color_solve_cluster_row(SolveArgs a)
+{
+    const GlobalBodies B{a.v, a.w, a.pv, a.po};
+    solve_body<kCluster, true, true>(a, B);
 }
 
 static int max_coresident_grid_blocks()
@@ -540,43 +862,28 @@ static int max_coresident_grid_blocks()
     return cached;
 }
 
-static int max_dyn_smem()
+// largest power-of-two cluster (<= 16) of a cluster-solve kernel that the device can
+// co-schedule; a host-side occupancy query, cached per form (an engine's first step runs
+// eagerly, before any graph capture)
+static int max_cluster_size(int row)
 {
-    static int cached = -1;
-    if (cached < 0) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-        cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cached = v;
-    }
-    return cached;
-}
-
-// largest power-of-two cluster (<= 16) of k_color_solve_cluster CTAs with `smem` bytes of
-// shared memory each that the device can co-schedule; a host-side occupancy query, cached per
-// size (an engine's first step runs eagerly, before any graph capture)
-static int max_cluster_size(int smem)
-{
-    static int cached_smem = -1, cached = 0;
-    if (smem != cached_smem) {
-        max_dyn_smem();
+    static int cached[2] = {-1, -1};
+    if (cached[row] < 0) {
+        const void *fn = row ? (const void *)k_color_solve_cluster_row : (const void *)k_color_solve_cluster;
+        cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kClusterMax);
-        cfg.blockDim = dim3(kClusterThreads);
-        cfg.dynamicSmemBytes = smem;
+        cfg.blockDim = dim3(row ? kClusterThreadsRow : kClusterThreads);
         int cs = 0;
-        if (cudaOccupancyMaxPotentialClusterSize(&cs, k_color_solve_cluster, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxPotentialClusterSize(&cs, fn, &cfg) != cudaSuccess) {
             cudaGetLastError();
             cs = 0;
         }
         int p2 = 0;
         for (int c = 1; c <= std::min(cs, kClusterMax); c *= 2) p2 = c;
-        cached = p2 >= 2 ? p2 : 0;
-        cached_smem = smem;
+        cached[row] = p2 >= 2 ? p2 : 0;
     }
-    return cached;
+    return cached[row];
 }
 
 int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
@@ -599,13 +906,23 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     a.pit = p->pit;
     a.fixed_frame = (p->flags & B2C_COLOR_FIXED_FRAME) ? 1 : 0;
     a.apply_warm = (p->flags & B2C_COLOR_APPLY_WARM) ? 1 : 0;
+    a.row = (p->flags & B2C_COLOR_ROW_FORM) ? 1 : 0;
+    if (a.row && !a.fixed_frame) {
+        set_error("color_solve: B2C_COLOR_ROW_FORM needs B2C_COLOR_FIXED_FRAME");
+        return B2C_EARG;
+    }
     a.bar_count = pr->barrier;
     a.bar_gen = pr->barrier + 1;
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
-    k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
-                                             *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, a.rec, hdr);
+    if (a.row)
+        k_pair_gather_row<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi,
+                                                     pr->pbj, *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, dt,
+                                                     a.rec, hdr);
+    else
+        k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
+                                                 *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, a.rec, hdr);
     int rc = check_launch("pair_gather");
     if (rc) return rc;
 
@@ -615,11 +932,11 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
         else mode = -kClusterMax;
     }
     if (mode < 0) {
-        const int cs = std::min(-mode, max_cluster_size(0));
+        const int cs = std::min(-mode, max_cluster_size(a.row));
         if (cs >= 2) {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(cs);
-            cfg.blockDim = dim3(kClusterThreads);
+            cfg.blockDim = dim3(a.row ? kClusterThreadsRow : kClusterThreads);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -628,7 +945,8 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             attr[0].val.clusterDim.z = 1;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
-            cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_solve_cluster, a);
+            cudaError_t e = a.row ? cudaLaunchKernelEx(&cfg, k_color_solve_cluster_row, a)
+                                  : cudaLaunchKernelEx(&cfg, k_color_solve_cluster, a);
             if (e != cudaSuccess) {
                 set_error("color_solve: cluster launch of %d CTAs: %s", cs, cudaGetErrorString(e));
                 return B2C_ECUDA;
@@ -662,7 +980,8 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             if ((rc = check_launch("color_solve_grid"))) return rc;
         }
     }
-    k_imp_scatter<<<pgrid, kThreads, 0, s>>>(hdr, pr->pstart, pr->pidx, a.rec, kept->imp);
+    k_imp_scatter<<<pgrid, kThreads, 0, s>>>(hdr, pr->pstart, pr->pidx, a.rec, a.row ? (int)kRImp : (int)kCImp,
+                                             kept->imp);
     return check_launch("imp_scatter");
 }
 
@@ -671,5 +990,6 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
 extern "C" int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots)
 {
     if (pair_capacity < 0 || kslots < 1) return -1;
-    return 4LL * (int64_t)pair_capacity * (1 + b2c::kRecBody + b2c::kRecContact * (int64_t)kslots);
+    // room for either layout: the reference form (kRecContact fields per contact) or the row form
+    return 4LL * (int64_t)pair_capacity * (1 + b2c::kRecBody + b2c::kRecContactRow * (int64_t)kslots);
 }

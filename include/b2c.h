@@ -220,6 +220,12 @@ typedef struct b2c_boxes {
                                      pair count D of one body, at most 2D - 1 colours, and <= 64)
                                      instead of the round number.  Not in the reference; the box
                                      engine's default, as it needs fewer colour phases. */
+#define B2C_COLOR_ROW_FORM 64     /* pair solve in row form: the angular response IA (r x d) of every
+                                     contact direction, the reciprocal effective masses and the
+                                     position bias computed once per substep, so an impulse j along
+                                     d changes w by j k.  Not in the reference (whose chunks recompute
+                                     IA (r x (j d)) and divide by the effective mass every sweep);
+                                     needs B2C_COLOR_FIXED_FRAME.  The box engine's default. */
 #define B2C_COLOR_PER_CONTACT 16 /* no manifold reduction; every contact is its own chunk and is
                                     coloured on the contact graph (the plain coloured engine) */
 

@@ -337,10 +337,10 @@ class BoxOracle:
     """CPU restatement of the box engine: box/plane + box/box narrowphase (BoxWorld.contacts,
     ncp_gpu.py:1273-1280) over the pairs whose bounding spheres are within the margin, with the
     ColorCache pair solve of the coloured chain and per-body friction.  flags: 1 fixed frame,
-    2 applied warm, 4 colour cache, 8 warm start, 32 first-fit colours."""
+    2 applied warm, 4 colour cache, 8 warm start, 32 first-fit colours, 64 row form."""
     name = "box_color_cache_oracle"
 
-    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=47, margin=2e-3, cap=MAXC):
+    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=111, margin=2e-3, cap=MAXC):
         self.dims = dims; self.mu = mu; self.vit = vit; self.pit = pit; self.flags = flags; self.margin = margin
         self.cap = cap
         self._centers, self._halves, self._dens, self._mus, self._kin = [], [], [], [], []

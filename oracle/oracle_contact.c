@@ -1421,6 +1421,179 @@ OR_API int or_box_box(const double *ha_, const double *xa_, const double *qa, co
 static inline int64_t box_key(int a, int b, int f, int N) { return ((int64_t)a * (N + 1) + (int64_t)(b + 1)) * 256 + f; }
 
 /* flags: 1 fixed frame, 2 applied warm start, 4 colour cache, 8 warm start (as B2C_COLOR_*) */
+/* ---- row form of the pair solve (box engine) ------------------------------------------------
+ * Not in the reference.  The same Gauss-Seidel pair chunks (fixed tangent frame, applied warm
+ * impulses, Baumgarte position pass) with the per-contact constants of a substep computed once:
+ * the angular response k = IA (r x d) of every direction d in {n, t1, t2}, the reciprocal
+ * effective masses and the position bias.  An impulse j along d then changes w by j k (one fma
+ * per component) instead of IA (r x (j d)).  The GPU's row-form kernels compute the same
+ * expressions in the same order. */
+typedef struct {
+    v3 n, rA, rB, t1, t2, kAn, kA1, kA2, kBn, kB1, kB2;
+    float inv_n, inv_1, inv_2, bias;
+} row_t;
+
+static void row_precompute(int P, const int *pidx, const int *pstart, const int *pcount, const int *pbi,
+                           const int *pbj, const float *cpA, const float *cpB, const float *cn, const float *cpen,
+                           const float *xc, const float *invIw, const float *invM, float dt, row_t *rows)
+{
+    for (int p = 0; p < P; ++p) {
+        int bi = pbi[p], bj = pbj[p];
+        float iMA = invM[bi], iMB = bj >= 0 ? invM[bj] : 0.0f;
+        m33 IA = ldm(invIw, bi), IB = IA;
+        if (bj >= 0) IB = ldm(invIw, bj);
+        for (int k = 0; k < pcount[p]; ++k) {
+            int c = pidx[pstart[p] + k];
+            row_t *r = &rows[c];
+            v3 nrm = ld3(cn, c);
+            r->n = nrm;
+            r->rA = vsub(ld3(cpA, c), ld3(xc, bi));
+            r->rB = bj >= 0 ? vsub(ld3(cpB, c), ld3(xc, bj)) : V(0, 0, 0);
+            v3 aa = V(1.0f, 0.0f, 0.0f);
+            if (fabsf(nrm.x) >= 0.9f) aa = V(0.0f, 1.0f, 0.0f);
+            float dd = dot3(aa, nrm);
+            r->t1 = vnormalize(V(fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)));
+            r->t2 = cross3(nrm, r->t1);
+            v3 rnA = cross3(r->rA, nrm), rtA1 = cross3(r->rA, r->t1), rtA2 = cross3(r->rA, r->t2);
+            r->kAn = matvec(&IA, rnA); r->kA1 = matvec(&IA, rtA1); r->kA2 = matvec(&IA, rtA2);
+            float meff = iMA + dot3(rnA, r->kAn), meft1 = iMA + dot3(rtA1, r->kA1), meft2 = iMA + dot3(rtA2, r->kA2);
+            r->kBn = r->kB1 = r->kB2 = V(0, 0, 0);
+            if (bj >= 0) {
+                v3 rnB = cross3(r->rB, nrm), rtB1 = cross3(r->rB, r->t1), rtB2 = cross3(r->rB, r->t2);
+                r->kBn = matvec(&IB, rnB); r->kB1 = matvec(&IB, rtB1); r->kB2 = matvec(&IB, rtB2);
+                meff = (meff + iMB) + dot3(rnB, r->kBn);
+                meft1 = (meft1 + iMB) + dot3(rtB1, r->kB1);
+                meft2 = (meft2 + iMB) + dot3(rtB2, r->kB2);
+            }
+            r->inv_n = meff >= 1e-12f ? 1.0f / meff : 0.0f;
+            r->inv_1 = meft1 >= 1e-12f ? 1.0f / meft1 : 0.0f;
+            r->inv_2 = meft2 >= 1e-12f ? 1.0f / meft2 : 0.0f;
+            r->bias = K_BETA * fmaxf(cpen[c] - K_SLOP, 0.0f) / dt;
+        }
+    }
+}
+
+static inline v3 fma3s(float s, v3 a, v3 b) { return V(fmaf(s, a.x, b.x), fmaf(s, a.y, b.y), fmaf(s, a.z, b.z)); }
+
+static void row_warm(int p, const int *pidx, const int *pstart, const int *pcount, const int *pbi, const int *pbj,
+                     const row_t *rows, const float *jn, const float *jt1, const float *jt2, float *v, float *w,
+                     const float *invM)
+{
+    int bi = pbi[p], bj = pbj[p];
+    float iMA = invM[bi], iMB = bj >= 0 ? invM[bj] : 0.0f;
+    v3 vA = ld3(v, bi), wA = ld3(w, bi), vB = V(0, 0, 0), wB = V(0, 0, 0);
+    if (bj >= 0) { vB = ld3(v, bj); wB = ld3(w, bj); }
+    for (int k = 0; k < pcount[p]; ++k) {
+        int c = pidx[pstart[p] + k];
+        const row_t *r = &rows[c];
+        float a = jn[c], b = jt1[c], d = jt2[c];
+        v3 J = V(fmaf(d, r->t2.x, fmaf(a, r->n.x, b * r->t1.x)), fmaf(d, r->t2.y, fmaf(a, r->n.y, b * r->t1.y)),
+                 fmaf(d, r->t2.z, fmaf(a, r->n.z, b * r->t1.z)));
+        if (iMA > 0.0f) {
+            vA = V(fmaf(iMA, J.x, vA.x), fmaf(iMA, J.y, vA.y), fmaf(iMA, J.z, vA.z));
+            wA = vadd(wA, V(fmaf(d, r->kA2.x, fmaf(a, r->kAn.x, b * r->kA1.x)),
+                            fmaf(d, r->kA2.y, fmaf(a, r->kAn.y, b * r->kA1.y)),
+                            fmaf(d, r->kA2.z, fmaf(a, r->kAn.z, b * r->kA1.z))));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = V(fmaf(-iMB, J.x, vB.x), fmaf(-iMB, J.y, vB.y), fmaf(-iMB, J.z, vB.z));
+            wB = vsub(wB, V(fmaf(d, r->kB2.x, fmaf(a, r->kBn.x, b * r->kB1.x)),
+                            fmaf(d, r->kB2.y, fmaf(a, r->kBn.y, b * r->kB1.y)),
+                            fmaf(d, r->kB2.z, fmaf(a, r->kBn.z, b * r->kB1.z))));
+        }
+    }
+    if (iMA > 0.0f) { st3(v, bi, vA); st3(w, bi, wA); }
+    if (bj >= 0 && iMB > 0.0f) { st3(v, bj, vB); st3(w, bj, wB); }
+}
+
+static void row_velocity(int p, const int *pidx, const int *pstart, const int *pcount, const int *pbi,
+                         const int *pbj, const row_t *rows, float *jn, float *jt1, float *jt2, float *v, float *w,
+                         const float *invM, float mu, float t2d)
+{
+    int bi = pbi[p], bj = pbj[p];
+    float iMA = invM[bi], iMB = bj >= 0 ? invM[bj] : 0.0f;
+    v3 vA = ld3(v, bi), wA = ld3(w, bi), vB = V(0, 0, 0), wB = V(0, 0, 0);
+    if (bj >= 0) { vB = ld3(v, bj); wB = ld3(w, bj); }
+    for (int k = 0; k < pcount[p]; ++k) {
+        int c = pidx[pstart[p] + k];
+        const row_t *r = &rows[c];
+        v3 va = vadd(vA, cross3(wA, r->rA)), vb = V(0, 0, 0);
+        if (bj >= 0) vb = vadd(vB, cross3(wB, r->rB));
+        v3 vrel = vsub(va, vb);
+        float vn = dot3(vrel, r->n);
+        if (!(r->inv_n > 0.0f)) continue;
+        float dj = -vn * r->inv_n;
+        float nw = fmaxf(0.0f, jn[c] + dj);
+        dj = nw - jn[c];
+        jn[c] = nw;
+        v3 Jn = vscale(r->n, dj);
+        if (iMA > 0.0f) {
+            vA = V(fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z));
+            wA = fma3s(dj, r->kAn, wA);
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = V(fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z));
+            wB = fma3s(-dj, r->kBn, wB);
+        }
+        va = vadd(vA, cross3(wA, r->rA));
+        vb = V(0, 0, 0);
+        if (bj >= 0) vb = vadd(vB, cross3(wB, r->rB));
+        vrel = vsub(va, vb);
+        if (!(r->inv_1 > 0.0f) || !(r->inv_2 > 0.0f)) continue;
+        float o1 = jt1[c], o2 = jt2[c];
+        float a1 = o1 - dot3(vrel, r->t1) * r->inv_1;
+        float a2 = o2 - dot3(vrel, r->t2) * r->inv_2;
+        float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+        float lim = mu * jn[c];
+        if (mag > lim && mag > 1e-12f) { float sc = lim / mag; a1 = a1 * sc; a2 = a2 * sc; }
+        jt1[c] = a1;
+        jt2[c] = a2;
+        float e1 = a1 - o1, e2 = t2d * (a2 - o2);
+        v3 Jt = V(fmaf(e1, r->t1.x, e2 * r->t2.x), fmaf(e1, r->t1.y, e2 * r->t2.y), fmaf(e1, r->t1.z, e2 * r->t2.z));
+        if (iMA > 0.0f) {
+            vA = V(fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z));
+            wA = fma3s(e1, r->kA1, fma3s(e2, r->kA2, wA));
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            vB = V(fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z));
+            wB = fma3s(-e1, r->kB1, fma3s(-e2, r->kB2, wB));
+        }
+    }
+    if (iMA > 0.0f) { st3(v, bi, vA); st3(w, bi, wA); }
+    if (bj >= 0 && iMB > 0.0f) { st3(v, bj, vB); st3(w, bj, wB); }
+}
+
+static void row_position(int p, const int *pidx, const int *pstart, const int *pcount, const int *pbi,
+                         const int *pbj, const row_t *rows, float *jp, float *pv, float *po, const float *invM)
+{
+    int bi = pbi[p], bj = pbj[p];
+    float iMA = invM[bi], iMB = bj >= 0 ? invM[bj] : 0.0f;
+    v3 pvA = ld3(pv, bi), poA = ld3(po, bi), pvB = V(0, 0, 0), poB = V(0, 0, 0);
+    if (bj >= 0) { pvB = ld3(pv, bj); poB = ld3(po, bj); }
+    for (int k = 0; k < pcount[p]; ++k) {
+        int c = pidx[pstart[p] + k];
+        const row_t *r = &rows[c];
+        v3 rel = vadd(pvA, cross3(poA, r->rA));
+        if (bj >= 0) rel = vsub(rel, vadd(pvB, cross3(poB, r->rB)));
+        if (!(r->inv_n > 0.0f)) continue;
+        float dj = (r->bias - dot3(rel, r->n)) * r->inv_n;
+        float nw = fmaxf(0.0f, jp[c] + dj);
+        dj = nw - jp[c];
+        jp[c] = nw;
+        v3 Jn = vscale(r->n, dj);
+        if (iMA > 0.0f) {
+            pvA = V(fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z));
+            poA = fma3s(dj, r->kAn, poA);
+        }
+        if (bj >= 0 && iMB > 0.0f) {
+            pvB = V(fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z));
+            poB = fma3s(-dj, r->kBn, poB);
+        }
+    }
+    if (iMA > 0.0f) { st3(pv, bi, pvA); st3(po, bi, poA); }
+    if (bj >= 0 && iMB > 0.0f) { st3(pv, bj, pvB); st3(po, bj, poB); }
+}
+
 /* ---- box engine pair enumeration ------------------------------------------------------------
  * The pair test of the box engine: bounding spheres at most the margin apart,
  * |xb - xa|^2 <= (ra + rb + margin)^2 in float64 (the same expression, in the same order, as the
@@ -1513,6 +1686,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
     float *jp = malloc(sizeof(float) * cap), *pmu = malloc(sizeof(float) * cap);
     int *pidx = malloc(sizeof(int) * cap), *pstart = malloc(sizeof(int) * cap), *pcount = malloc(sizeof(int) * cap);
     int *pbi = malloc(sizeof(int) * cap), *pbj = malloc(sizeof(int) * cap);
+    row_t *rows = (flags & 64) ? malloc(sizeof(row_t) * cap) : NULL;
     int rc = 0;
     double *rad = malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
     int *partners = malloc(sizeof(int) * (size_t)(N > 0 ? N : 1));
@@ -1593,6 +1767,27 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             }
             e->n_colors = ncol;
             int fixed = flags & 1;
+            if (flags & 64) {
+                /* row form: constants once per substep, then the same sweep schedule */
+                row_precompute(P, pidx, pstart, pcount, pbi, pbj, spA, spB, sn, spen, xc, invIw, invM, sdt, rows);
+                if (flags & 2)
+                    for (int ci = 0; ci < ncol; ++ci)
+                        for (int t = 0; t < e->ccount[ci]; ++t)
+                            row_warm(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, rows, jn, jt1, jt2,
+                                     v, w, invM);
+                for (int it = 0; it < e->vit; ++it)
+                    for (int ci = 0; ci < ncol; ++ci)
+                        for (int t = 0; t < e->ccount[ci]; ++t) {
+                            int p = e->porder[e->cstart[ci] + t];
+                            row_velocity(p, pidx, pstart, pcount, pbi, pbj, rows, jn, jt1, jt2, v, w, invM, pmu[p],
+                                         e->t2d);
+                        }
+                for (int it = 0; it < e->pit; ++it)
+                    for (int ci = 0; ci < ncol; ++ci)
+                        for (int t = 0; t < e->ccount[ci]; ++t)
+                            row_position(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, rows, jp, pv,
+                                         po, invM);
+            } else {
             if (flags & 2)
                 for (int ci = 0; ci < ncol; ++ci)
                     for (int t = 0; t < e->ccount[ci]; ++t)
@@ -1610,6 +1805,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
                     for (int t = 0; t < e->ccount[ci]; ++t)
                         chunk_position(e->porder[e->cstart[ci] + t], pidx, pstart, pcount, pbi, pbj, spA, spB, sn,
                                        spen, jp, xc, pv, po, invIw, invM, sdt);
+            }
         } else {
             e->n_colors = 0;
         }
@@ -1625,6 +1821,6 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
     }
     free(invIw); free(keys); free(sbi); free(sbj); free(spA); free(spB); free(sn); free(spen);
     free(jn); free(jt1); free(jt2); free(jp); free(pmu); free(pidx); free(pstart); free(pcount); free(pbi); free(pbj);
-    free(rad); free(partners); free(bc.start); free(bc.items);
+    free(rad); free(partners); free(bc.start); free(bc.items); free(rows);
     return rc;
 }

@@ -93,10 +93,11 @@ def _state(e):
     return s.xc, s.Rm, s.vc, s.om
 
 
-def test_box_engine_matches_oracle(me, oracle_mod):
+@pytest.mark.parametrize("row_form", [True, False])
+def test_box_engine_matches_oracle(me, oracle_mod, row_form):
     S = _pile()
-    g = _fill(me.BoxContactEngine(mu=0.5, vit=16, pit=10), S)
-    o = _fill(oracle_mod.BoxOracle(mu=0.5, vit=16, pit=10), S)
+    g = _fill(me.BoxContactEngine(mu=0.5, vit=16, pit=10, row_form=row_form), S)
+    o = _fill(oracle_mod.BoxOracle(mu=0.5, vit=16, pit=10, flags=111 if row_form else 47), S)
     for step in range(240):
         g.step(DT, 2)
         o.step(DT, 2)
