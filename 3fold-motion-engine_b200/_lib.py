@@ -63,6 +63,27 @@ class Boxes(ctypes.Structure):
                 ("scan_tmp", c_void_p)]
 
 
+class NcpScene(ctypes.Structure):
+    _fields_ = [("n_c", c_int32), ("n_b", c_int32), ("dtype", c_int32), ("Ja", c_void_p), ("Jb", c_void_p),
+                ("Minv", c_void_p), ("v_free", c_void_p), ("mu", c_void_p), ("bias", c_void_p), ("sep", c_void_p),
+                ("pa", c_void_p), ("pb", c_void_p), ("feature", c_void_p)]
+
+
+class NcpState(ctypes.Structure):
+    _fields_ = [("max_contacts", c_int32), ("n_bodies", c_int32), ("max_colors", c_int32), ("rho", c_void_p),
+                ("lam", c_void_p), ("v", c_void_p), ("acc", c_void_p), ("res", c_void_p), ("u", c_void_p),
+                ("col", c_void_p), ("order", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p),
+                ("claim", c_void_p), ("dyn", c_void_p), ("cache_pa", c_void_p), ("cache_pb", c_void_p),
+                ("cache_feat", c_void_p), ("cache_minv", c_void_p), ("stats", c_void_p), ("res_max", c_void_p),
+                ("barrier", c_void_p)]
+
+
+class NcpParams(ctypes.Structure):
+    _fields_ = [("desaxce", c_int32), ("soft", c_int32), ("use_bias", c_int32), ("color_cache", c_int32),
+                ("solve_blocks", c_int32), ("pad", c_int32), ("softp", ctypes.c_double * 5),
+                ("barrier_timeout_ns", ctypes.c_int64)]
+
+
 COLOR_FIXED_FRAME = 1
 COLOR_APPLY_WARM = 2
 COLOR_CACHE = 4
@@ -124,6 +145,10 @@ _SIGS = {
                           _P(ColorParams), c_void_p], c_int32),
     "b2c_box_substep": ([_P(Bodies), _P(Boxes), _P(Contacts), c_void_p, _P(Pairs), _P(Warm), c_void_p,
                          _P(ColorParams), c_float, c_void_p, c_void_p], c_int32),
+    "b2c_ncp_setup": ([_P(NcpScene), _P(NcpState), c_int32, c_void_p], c_int32),
+    "b2c_ncp_color": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
+    "b2c_ncp_sweeps": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p], c_int32),
+    "b2c_ncp_residual": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
     "b2c_box_narrowphase_test": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
 }

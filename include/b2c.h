@@ -345,6 +345,70 @@ B2C_API int32_t b2c_box_narrowphase_test(int32_t n, const float *a_half, const f
                                          const float *b_half, const float *b_x, const float *b_q, float margin,
                                          double *pts, double *nrm, int32_t *fid, int32_t *count, b2c_stream s);
 
+/* ---------------------------------------------------------------------------------------------
+ * Exact-cone NCP solve (src/motion_engine/ncp/ncp_gpu.py:361-1063, NCPSolverGPU): per-contact
+ * 3x6 Jacobian blocks, per-body 6x6 inverse mass, coloured projected Gauss-Seidel on the
+ * Coulomb cone with the de Saxce correction, int64 fixed-point per-body accumulation of
+ * Minv J^T lambda, optional soft step.  Reals are float32 or float64 (dtype = 4 or 8 bytes).
+ * ------------------------------------------------------------------------------------------- */
+/* The scene (BlockScene, ncp_gpu.py:193-260), device pointers. */
+typedef struct b2c_ncp_scene {
+    int32_t n_c, n_b;
+    int32_t dtype;             /* bytes of a real: 4 or 8 */
+    const void *Ja, *Jb;       /* (n_c,3,6) blocks of body A and B (B carries the minus sign) */
+    const void *Minv;          /* (n_b,6,6) */
+    const void *v_free;        /* (n_b,6) */
+    const void *mu;            /* (n_c) */
+    const void *bias;          /* (n_c,3) added to u */
+    const void *sep;           /* (n_c) separation, read by the soft step only; may be NULL */
+    const int32_t *pa, *pb;    /* (n_c) bodies, -1 = static */
+    const int32_t *feature;    /* (n_c) stable feature id (< 2^20), unique per (pa, pb) */
+} b2c_ncp_scene;
+
+/* Solver state, device pointers sized by the capacities (NCPSolverGPU.__init__, :799-846). */
+typedef struct b2c_ncp_state {
+    int32_t max_contacts, n_bodies, max_colors;
+    void *rho;                 /* (max_contacts) step 1/lambda_max(W_cc) */
+    void *lam;                 /* (max_contacts,3) impulses (n, t1, t2); the warm start on entry */
+    void *v;                   /* (n_bodies,6) velocity */
+    int64_t *acc;              /* (n_bodies*6) sum_c round(1e10 Minv J_c^T lambda_c) */
+    void *res;                 /* (max_contacts) per-contact natural-map residual */
+    void *u;                   /* (max_contacts,3) contact velocity of the last residual */
+    int32_t *col, *order;      /* (max_contacts) colour of each contact; contacts grouped by colour */
+    int32_t *cstart, *ccount;  /* (max_colors) */
+    uint64_t *claim;           /* (n_bodies) colouring claims */
+    int32_t *dyn;              /* (n_bodies) 1 = dynamic (Minv != 0) */
+    int32_t *cache_pa, *cache_pb, *cache_feat; /* (max_contacts) inputs of the cached colouring */
+    void *cache_minv;          /* (n_bodies,4) Minv[0][0], [1][1], [2][2] and the dynamic flag */
+    int32_t *stats;            /* (8) n_colors, cache_valid, cached_C, cache_hit, hits, misses,
+                                  rounds, error bits */
+    uint64_t *res_max;         /* (1) bits of max_c residual_c (non-negative reals) */
+    uint32_t *barrier;         /* (2) grid barrier of the persistent sweep */
+} b2c_ncp_state;
+
+/* Per-call parameters: de Saxce correction, soft step (SoftStep.params: bias_rate, mass_scale,
+ * impulse_scale, inv_h, contact_speed) and its pass flag, colour cache, launch form. */
+typedef struct b2c_ncp_params {
+    int32_t desaxce, soft, use_bias, color_cache;
+    int32_t solve_blocks;      /* 0 auto, 1 one CTA, -n a cluster of n CTAs */
+    int32_t pad;
+    double softp[5];
+    int64_t barrier_timeout_ns;
+} b2c_ncp_params;
+
+/* rho (k_rho), dynamic flags, acc = 0 or the warm start scattered (k_scatter), v = v_free +
+ * acc / 1e10 (k_apply).  warm != 0: state->lam holds the warm start. */
+B2C_API int32_t b2c_ncp_setup(const b2c_ncp_scene *sc, b2c_ncp_state *st, int32_t warm, b2c_stream s);
+/* Colouring behind the colour cache (NCPSolverGPU._color_cached / _color, :876-963). */
+B2C_API int32_t b2c_ncp_color(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                              b2c_stream s);
+/* iters sweeps over the colours in one persistent launch (k_sweep + k_apply_c per colour). */
+B2C_API int32_t b2c_ncp_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                               int32_t iters, b2c_stream s);
+/* Natural-map residual per contact, its maximum and the contact velocity u (k_resid). */
+B2C_API int32_t b2c_ncp_residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                 b2c_stream s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -422,3 +422,44 @@ class BoxOracle:
         nk = self.b.kin == 0
         f[nk] = self.b.M[nk, None] * (self.b.v[nk] - self.vgrav[nk]) / self._force_dt
         return f
+
+
+# ---- exact-cone NCP (oracle_ncp.c) ----
+def _ncp_sigs(L):
+    P = ctypes.c_void_p
+    for suf in ("_f", "_d"):
+        f = getattr(L, "or_ncp_solve" + suf)
+        f.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 11 + [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                               ctypes.c_int, P, P, P, P, P]
+        f.restype = ctypes.c_double
+
+
+def ncp_solve(bs, iters, dtype="float64", warm=None, desaxce=True, softp=None, use_bias=True):
+    """The oracle's coloured PGS on a block scene (any object with Ja, Jb, Minv, v_free, mu,
+    body_pairs, bias, feature, sep).  Returns dict(lam (n_c,3), v (n_b,6), res (n_c), residual,
+    col (n_c), n_colors); arrays in the solve's dtype."""
+    L = lib()
+    _ncp_sigs(L)
+    nt = np.float32 if dtype == "float32" else np.float64
+    fn = L.or_ncp_solve_f if dtype == "float32" else L.or_ncp_solve_d
+    Ja = np.ascontiguousarray(bs.Ja, nt)
+    n_c, n_b = Ja.shape[0], np.shape(bs.Minv)[0]
+    Jb = np.ascontiguousarray(bs.Jb, nt)
+    Minv = np.ascontiguousarray(bs.Minv, nt)
+    vf = np.ascontiguousarray(bs.v_free, nt)
+    mu = np.ascontiguousarray(bs.mu, nt)
+    pairs = np.ascontiguousarray(bs.body_pairs, np.int32).reshape(n_c, 2)
+    pa, pb = np.ascontiguousarray(pairs[:, 0]), np.ascontiguousarray(pairs[:, 1])
+    feat = np.ascontiguousarray(bs.feature, np.int32)
+    bias = np.ascontiguousarray(bs.bias, nt)
+    sep = None if getattr(bs, "sep", None) is None else np.ascontiguousarray(bs.sep, nt)
+    sp = None if softp is None else np.ascontiguousarray(softp, nt)
+    lam = np.zeros((n_c, 3), nt) if warm is None else np.array(warm, nt).reshape(n_c, 3)
+    v = np.zeros((n_b, 6), nt)
+    res = np.zeros(n_c, nt)
+    col = np.zeros(n_c, np.int32)
+    ncol = np.zeros(1, np.int32)
+    r = fn(n_c, n_b, _p(Ja), _p(Jb), _p(Minv), _p(vf), _p(mu), _p(pa), _p(pb), _p(feat), _p(bias),
+           None if sep is None else _p(sep), None if sp is None else _p(sp), 1 if use_bias else 0,
+           1 if desaxce else 0, int(iters), 0 if warm is None else 1, _p(lam), _p(v), _p(res), _p(col), _p(ncol))
+    return dict(lam=lam, v=v, res=res, residual=float(r), col=col, n_colors=int(ncol[0]))
