@@ -122,6 +122,8 @@ _SIGS = {
     "b2c_last_error": ([], ctypes.c_char_p),
     "b2c_scan_scratch_ints": ([c_int32], c_int32),
     "b2c_exclusive_scan": ([c_void_p, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
+    "b2c_exclusive_scan_noalloc": ([c_void_p, c_void_p, c_int32, c_void_p], c_int32),
+    "b2c_scan_noalloc_max_n": ([], c_int32),
     "b2c_body_predict": ([_P(Bodies), c_float, c_void_p], c_int32),
     "b2c_body_integrate": ([_P(Bodies), c_float, c_void_p], c_int32),
     "b2c_bead_world": ([_P(Bodies), _P(Beads), _P(Grid), c_void_p], c_int32),

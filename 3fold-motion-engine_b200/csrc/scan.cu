@@ -3,6 +3,8 @@
 // offsets of contact generation and the compaction of kept contacts.  The element count can
 // be read from the device (`dn`), so a scan inside a captured step needs no host read-back:
 // elements at or beyond *dn read as zero.
+#include <mutex>
+
 #include "b2c_common.cuh"
 
 namespace b2c {
@@ -102,7 +104,65 @@ int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, 
     return check_launch("scan_add");
 }
 
+// Scratch of b2c_exclusive_scan_noalloc: one file-scope device array, sized for the largest
+// scan it accepts (kNoAllocMaxN elements: 2 x 8192 tile sums and offsets plus 8 for the second
+// level = 16,392 ints, 64 KiB).  It keeps its contents between calls; nothing in it has to
+// start at zero (every tile sum is written before it is read).
+constexpr int kNoAllocMaxN = 1 << 24;
+constexpr int noalloc_scratch_ints(int n)
+{
+    return n <= kScanTile ? 0 : 2 * ((n + kScanTile - 1) / kScanTile) + noalloc_scratch_ints((n + kScanTile - 1) / kScanTile);
+}
+constexpr int kNoAllocScratchInts = noalloc_scratch_ints(kNoAllocMaxN);
+static __device__ __align__(256) int g_noalloc_scan_scratch[kNoAllocScratchInts];
+
+// Device address of the scratch array for the current device, looked up once per device (with
+// that device current) and cached.
+static int noalloc_scratch(int **out)
+{
+    static std::mutex mu;
+    static int *addr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error("b2c_exclusive_scan_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+        return B2C_ECUDA;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("b2c_exclusive_scan_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return B2C_ECUDA;
+        }
+        addr[dev] = static_cast<int *>(p);
+    }
+    *out = addr[dev];
+    return B2C_OK;
+}
+
 }  // namespace b2c
+
+extern "C" int32_t b2c_scan_noalloc_max_n(void) { return b2c::kNoAllocMaxN; }
+
+extern "C" int32_t b2c_exclusive_scan_noalloc(const int32_t *in, int32_t *out, int32_t n, b2c_stream s)
+{
+    if (!in || !out || n < 0) {
+        b2c::set_error("b2c_exclusive_scan_noalloc: bad argument");
+        return B2C_EARG;
+    }
+    if (n > b2c::kNoAllocMaxN) {
+        b2c::set_error("b2c_exclusive_scan_noalloc: n = %d exceeds the maximum %d of its built-in scratch; "
+                       "use b2c_exclusive_scan with a caller scratch buffer",
+                       n, b2c::kNoAllocMaxN);
+        return B2C_EARG;
+    }
+    int *scratch = nullptr;
+    const int rc = b2c::noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return b2c::exclusive_scan(in, out, n, nullptr, scratch, b2c::stream_of(s));
+}
 
 extern "C" int32_t b2c_scan_scratch_ints(int32_t n) { return b2c::scan_scratch_ints(n); }
 

@@ -256,6 +256,17 @@ B2C_API int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots);
 B2C_API int32_t b2c_scan_scratch_ints(int32_t n);
 /* exclusive prefix sum of n int32 (device pointers); out may alias nothing */
 B2C_API int32_t b2c_exclusive_scan(const int32_t *in, int32_t *out, int32_t n, int32_t *scratch, b2c_stream s);
+/* Exclusive scan that allocates nothing and takes no scratch argument: for callers that cannot
+ * allocate device memory or own a scratch buffer -- a foreign-language binding that holds only
+ * the two arrays it passes, or a host loop that must not allocate once it runs.  No counterpart
+ * in the reference (its scans are Warp's array_scan on Warp-allocated arrays).  The scratch is
+ * one library-owned device array per device for at most b2c_scan_noalloc_max_n() = 2^24
+ * elements; larger n returns B2C_EARG with a message.  Calls share that array: two calls that
+ * overlap in time (concurrent streams or host threads) race, so order them on one stream.  The
+ * first call on a device looks up the array's address; make it (n = 0 is enough) before any
+ * stream capture begins on that device. */
+B2C_API int32_t b2c_exclusive_scan_noalloc(const int32_t *in, int32_t *out, int32_t n, b2c_stream s);
+B2C_API int32_t b2c_scan_noalloc_max_n(void);
 
 /* ---- per-body stages ---- */
 /* k_grav + k_invIw (contact_engine_gpu.py:40-53): v += g dt for dynamic bodies;
