@@ -9,11 +9,11 @@ The directory name is not a Python identifier, so the package is imported under 
 ``motion_engine_b200`` (see ``__graft_entry__.load_package``).
 """
 from . import _lib, build
-from .boxes import BoxContactEngine
+from .boxes import BatchedBoxEngine, BoxContactEngine, autotune, partition_scenes
 from .colored import (AppliedWarmContactEngine, ColorCacheContactEngine, DeferredForceContactEngine,
                       FixedFrameContactEngine, GraphColoredContactEngine)
 from .engine import BodyState, ContactEngine, RelaxedJacobiContactEngine, quat_to_R, voxbox
 
 __all__ = ["BodyState", "ContactEngine", "RelaxedJacobiContactEngine", "GraphColoredContactEngine",
            "FixedFrameContactEngine", "AppliedWarmContactEngine", "DeferredForceContactEngine",
-           "ColorCacheContactEngine", "BoxContactEngine", "quat_to_R", "voxbox", "build", "_lib"]
+           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "_lib"]

@@ -40,7 +40,7 @@ class Pairs(ctypes.Structure):
                 ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
                 ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
                 ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
-                ("body_colors", c_void_p)]
+                ("body_colors", c_void_p), ("body_local", c_void_p)]
 
 
 class Warm(ctypes.Structure):
@@ -60,7 +60,7 @@ class Boxes(ctypes.Structure):
                 ("cand_count", c_void_p), ("cand_offset", c_void_p), ("cand_a", c_void_p), ("cand_b", c_void_p),
                 ("cont_count", c_void_p), ("cont_offset", c_void_p), ("pair_flag", c_void_p),
                 ("pair_offset", c_void_p), ("slot_p", c_void_p), ("slot_n", c_void_p), ("slot_f", c_void_p),
-                ("scan_tmp", c_void_p)]
+                ("scan_tmp", c_void_p), ("scene", c_void_p)]
 
 
 class NcpScene(ctypes.Structure):

@@ -24,6 +24,19 @@ from .engine import _BeadEngineBase, _pad4, _ptr
 MARGIN = 2e-3
 
 
+def scene_local_index(scene):
+    """Index of every body among the bodies of its scene, in body order."""
+    scene = np.asarray(scene, np.int64)
+    out = np.zeros(len(scene), np.int32)
+    if len(scene):
+        order = np.argsort(scene, kind="stable")
+        ss = scene[order]
+        first = np.r_[0, np.flatnonzero(np.diff(ss)) + 1]
+        run_start = np.repeat(first, np.diff(np.r_[first, len(ss)]))
+        out[order] = (np.arange(len(ss)) - run_start).astype(np.int32)
+    return out
+
+
 def box_body_arrays(centers, halves, dens, kin):
     """Solid boxes (Box.Ib, ncp_gpu.py:1105-1109): mass = density * 8 hx hy hz,
     Ib = m/12 diag(h_y^2 + h_z^2, ...) with full edges h = 2 half; float64, cast to float32."""
@@ -63,16 +76,19 @@ class BoxContactEngine(_BeadEngineBase):
         self.cand_per_body = int(cand_per_body)
         self.first_fit = bool(first_fit)
         self.row_form = bool(row_form) and self.fixed_frame
-        self._halves, self._mus = [], []
+        self._halves, self._mus, self._scenes = [], [], []
         self._has_manifold = True
 
     def add_body(self, center, density=700.0, kin=False):
         return self.add_box(center, dims=self.dims, density=density, kin=kin)
 
-    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False):
+    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False, scene=0):
+        """Add a solid box.  `scene` groups bodies into independent scenes (a batch): bodies of
+        different scenes never touch, whatever their positions."""
         d = self.dims if dims is None else tuple(float(x) for x in dims)
         self._halves.append([0.5 * d[0], 0.5 * d[1], 0.5 * d[2]])
         self._mus.append(self.mu if mu is None else float(mu))
+        self._scenes.append(int(scene))
         return super().add_body(center, density=density, kin=kin)
 
     def _build(self):
@@ -103,7 +119,14 @@ class BoxContactEngine(_BeadEngineBase):
         # broadphase grid over body centres
         hmax = float(np.max(np.linalg.norm(A["half"], axis=1))) if N else 0.5
         cell = 1.01 * (2.0 * hmax + self.margin)  # every sphere-test pair lies in adjacent cells
-        dims = (32, 32, 16) if N > 2000 else (16, 16, 8)
+        dims = (16, 16, 8) if N <= 2000 else (32, 32, 16) if N <= 20000 else (64, 64, 32) if N <= 500000 \
+            else (128, 128, 64)
+        # scenes of a batch: the scene of every body, and its index among its scene's bodies (the
+        # colouring priority uses scene-local indices, so a scene colours alike alone or batched)
+        sc = np.array(self._scenes, np.int32)
+        self.n_scenes = int(sc.max()) + 1 if N else 0
+        self.scene_t = torch.from_numpy(sc).to(dev) if self.n_scenes > 1 else None
+        self.local_t = torch.from_numpy(scene_local_index(sc)).to(dev)
         nbk = dims[0] * dims[1] * dims[2]
         cand_cap = max(self.cand_per_body * N + N, 64)
         kept_cap = 4 * cand_cap + 8 * N
@@ -120,7 +143,8 @@ class BoxContactEngine(_BeadEngineBase):
                                   cand_cap, *(_ptr(b[k]) for k in (
                                       "bucket", "start", "cursor", "sorted", "cand_count", "cand_offset", "cand_a",
                                       "cand_b", "cont_count", "cont_offset", "pair_flag", "pair_offset", "slot_p",
-                                      "slot_n", "slot_f", "scan_tmp")))
+                                      "slot_n", "slot_f", "scan_tmp")),
+                                  _ptr(self.scene_t) if self.scene_t is not None else None)
         # kept contacts, pairs, colouring, records, warm store
         i64 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int64, device=dev)
         f4 = lambda n: torch.zeros((max(int(n), 1), 4), dtype=torch.float32, device=dev)
@@ -141,7 +165,8 @@ class BoxContactEngine(_BeadEngineBase):
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
-            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots, _ptr(pb["body_colors"]))
+            "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots, _ptr(pb["body_colors"]),
+            _ptr(self.local_t))
         self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
         self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
         self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
@@ -173,6 +198,14 @@ class BoxContactEngine(_BeadEngineBase):
         self._graph_step(("box", float(sdt), int(substeps)), lambda: self._launch_step(sdt, substeps))
         self._force_dt = sdt
         self._fetch_header()
+
+    def set_solve_blocks(self, n: int):
+        """Launch form of the persistent solve: 0 auto, 1 one CTA, n > 1 a cooperative grid of n
+        CTAs, -n a cluster of n CTAs.  Results do not depend on it.  Drops captured graphs."""
+        self.solve_blocks = int(n)
+        if self._built:
+            self.c_params.solve_blocks = self.solve_blocks
+            self._graphs = {}
 
     def set_kinematic(self, i, xc):
         super().set_kinematic(i, xc)
@@ -245,3 +278,82 @@ class BoxContactEngine(_BeadEngineBase):
         warm = per_pos if self.apply_warm else 0
         return dict(pairs=P, kept=Ck, endpoints=E, colors=h["n_colors"],
                     bytes=warm + self.vit * per_vel + self.pit * per_pos)
+
+
+class BatchedBoxEngine(BoxContactEngine):
+    """Many independent box scenes advanced together: one body array, scene ids that keep the
+    scenes apart in the broadphase, and every stage of a substep -- the broadphase, the
+    narrowphase, the colouring and the persistent solve -- launched once for all scenes.  Each
+    scene's slice of the result is bytewise the scene advanced alone (its colouring uses
+    scene-local priorities; nothing else couples scenes).  The scenes may overlap in space."""
+    name = "box_color_cache_batched_b200"
+
+    def __init__(self, scenes=(), **kw):
+        kw.setdefault("cand_per_body", 12)
+        super().__init__(**kw)
+        self.scene_start = [0]
+        for sc in scenes:
+            self.add_scene(sc)
+
+    def add_scene(self, sc) -> int:
+        """sc: dict(centers, dims, density, mu[, kin]).  Returns the scene index."""
+        s = len(self.scene_start) - 1
+        kin = sc.get("kin", np.zeros(len(sc["centers"]), bool))
+        for c, d, de, m, k in zip(sc["centers"], sc["dims"], sc["density"], sc["mu"], kin):
+            self.add_box(c, dims=d, density=de, mu=m, kin=bool(k), scene=s)
+        self.scene_start.append(len(self._centers))
+        return s
+
+    def scene_slice(self, s) -> slice:
+        return slice(self.scene_start[s], self.scene_start[s + 1])
+
+    def scene_state(self, s):
+        st = self.get_state()
+        sl = self.scene_slice(s)
+        return type(st)(xc=st.xc[sl], Rm=st.Rm[sl], vc=st.vc[sl], om=st.om[sl])
+
+
+_TUNED = {}
+
+
+def autotune(engine, dt, substeps=1, candidates=(-16, -8, 148, 74), steps=2):
+    """Pick the persistent solve's launch form (a cluster of 16 or 8 CTAs, or a cooperative grid
+    of 148 or 74 CTAs) by timing `steps` live steps of each.  The launch forms give bit-identical
+    results (the tests check it), so tuning on live steps does not change the trajectory.  The
+    choice is cached per (bodies, scenes, colours) and applied to the engine."""
+    import torch
+    h = engine.header_dict() if engine._built else {"n_colors": 0}
+    key = (engine.N if engine._built else len(engine._centers), getattr(engine, "n_scenes", 1), h["n_colors"])
+    if key in _TUNED:
+        engine.set_solve_blocks(_TUNED[key][0])
+        return _TUNED[key]
+    times = {}
+    for cand in candidates:
+        engine.set_solve_blocks(cand)
+        engine.step(dt, substeps)  # capture / first run of this form
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            engine.step(dt, substeps)
+        b.record()
+        b.synchronize()
+        times[cand] = a.elapsed_time(b) / steps
+        engine.check_errors()
+    best = min(times, key=times.get)
+    engine.set_solve_blocks(best)
+    _TUNED[key] = (best, times)
+    return _TUNED[key]
+
+
+def partition_scenes(counts, parts):
+    """Longest-processing-time assignment of scenes (by body count) to `parts` workers (GPUs or
+    processes): scenes in decreasing size, each to the currently lightest worker; ties by index.
+    Returns one ascending index list per worker.  Scenes are independent, so a shard needs no
+    data exchange with the others."""
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for i in sorted(range(len(counts)), key=lambda i: (-counts[i], i)):
+        k = min(range(parts), key=lambda k: (load[k], k))
+        out[k].append(i)
+        load[k] += counts[i]
+    return [sorted(x) for x in out]

@@ -276,6 +276,7 @@ __device__ int box_box(float4 haf, float4 xaf, float4 qaf, float4 hbf, float4 xb
 struct BoxGrid {
     int dx, dy, dz;
     float inv;
+    const int *scene;  // scene of each body (NULL: one scene)
 };
 __device__ __forceinline__ int bwrap(int a, int m)
 {
@@ -283,10 +284,15 @@ __device__ __forceinline__ int bwrap(int a, int m)
     return r < 0 ? r + m : r;
 }
 __device__ __forceinline__ int bcell(float x, float inv) { return (int)floorf(x * inv); }
-__device__ __forceinline__ int bbucket(const BoxGrid &g, int ix, int iy, int iz)
+// bucket of a cell; in a batch the scene shifts it (the 27 buckets of a query stay distinct, and
+// scenes that overlap in space mostly fall into different buckets)
+__device__ __forceinline__ int bbucket(const BoxGrid &g, int ix, int iy, int iz, int sc)
 {
-    return (bwrap(ix, g.dx) * g.dy + bwrap(iy, g.dy)) * g.dz + bwrap(iz, g.dz);
+    const int nb = g.dx * g.dy * g.dz;
+    const int b = (bwrap(ix, g.dx) * g.dy + bwrap(iy, g.dy)) * g.dz + bwrap(iz, g.dz);
+    return sc ? (int)(((long long)b + (long long)sc * 40503LL) % nb) : b;
 }
+__device__ __forceinline__ int scene_of(const BoxGrid &g, int i) { return g.scene ? g.scene[i] : 0; }
 // bounding-sphere radius of a box, float64 from the float32 half extents
 __device__ __forceinline__ double bound_radius(float4 hf)
 {
@@ -311,7 +317,7 @@ __global__ void k_box_cells(int n, const float *__restrict__ xc, BoxGrid g, int 
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const f3 x = ld3(xc, i);
-    const int b = bbucket(g, bcell(x.x, g.inv), bcell(x.y, g.inv), bcell(x.z, g.inv));
+    const int b = bbucket(g, bcell(x.x, g.inv), bcell(x.y, g.inv), bcell(x.z, g.inv), scene_of(g, i));
     bucket[i] = b;
     atomicAdd(count + b, 1);
 }
@@ -345,9 +351,10 @@ __device__ __forceinline__ void warp_box_neighbors(int i, const float *__restric
     const f3 xi = ld3(xc, i);
     const double ri = bound_radius(ld4(half, i));
     const int cx = bcell(xi.x, g.inv), cy = bcell(xi.y, g.inv), cz = bcell(xi.z, g.inv);
+    const int si = scene_of(g, i);
     int lo = 0, cnt = 0;
     if (lane < 27) {
-        const int b = bbucket(g, cx + lane % 3 - 1, cy + (lane / 3) % 3 - 1, cz + lane / 9 - 1);
+        const int b = bbucket(g, cx + lane % 3 - 1, cy + (lane / 3) % 3 - 1, cz + lane / 9 - 1, si);
         lo = start[b];
         cnt = start[b + 1] - lo;
     }
@@ -368,7 +375,7 @@ __device__ __forceinline__ void warp_box_neighbors(int i, const float *__restric
         int j = -1;
         if (k < total) {
             j = sorted[t];
-            pass = j > i && sphere_pair(xi, ri, ld3(xc, j), bound_radius(ld4(half, j)), margin);
+            pass = j > i && scene_of(g, j) == si && sphere_pair(xi, ri, ld3(xc, j), bound_radius(ld4(half, j)), margin);
         }
         f(j, pass);
     }
@@ -554,7 +561,10 @@ __global__ void k_pstart_from_offsets(const int *__restrict__ cand_offset, int n
 // ---------------------------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------------------------
-static BoxGrid box_grid_of(const b2c_boxes *bx) { return BoxGrid{bx->dim_x, bx->dim_y, bx->dim_z, 1.0f / bx->cell}; }
+static BoxGrid box_grid_of(const b2c_boxes *bx)
+{
+    return BoxGrid{bx->dim_x, bx->dim_y, bx->dim_z, 1.0f / bx->cell, bx->scene};
+}
 
 int box_candidates(const b2c_bodies *b, b2c_boxes *bx, b2c_header *hdr, cudaStream_t s)
 {

@@ -436,13 +436,32 @@ constexpr int kPrioPairBits = 22;  // pair index bits of the compact priority (c
 // packed here as |h| << 22 | p (the same order while p < 2^22).  The round tag makes the claims
 // of earlier rounds lose without clearing them; inside a round the smaller priority gives the
 // larger key.
-__device__ __forceinline__ unsigned long long claim_key(int p, int r)
+__device__ __forceinline__ unsigned long long claim_key(int p, int r, unsigned long long h)
 {
+    const unsigned long long prio = (h << kPrioPairBits) | (unsigned long long)p;  // < 2^54
+    return ((unsigned long long)(r + 1) << 54) | ((1ull << 54) - 1ull - prio);
+}
+// The hash part of a pair's priority (<= 2^31).  Without body_local: k_prio's hash of the pair
+// index.  With body_local (the box engine): a hash of the pair's two scene-local body indices,
+// so the colouring of a scene does not depend on where its pairs sit in a batch of scenes (ties
+// fall back to the pair index, whose order inside a scene is the same either way).
+__device__ __forceinline__ unsigned long long pair_hash(int p, int a, int b, const int *__restrict__ body_local)
+{
+    if (body_local) {
+        const unsigned long long key = ((unsigned long long)(unsigned)(body_local[a] + 1) << 32) |
+                                       (unsigned long long)(unsigned)(b >= 0 ? body_local[b] + 1 : 0);
+        unsigned long long z = key;
+        z ^= z >> 30;
+        z *= 0xbf58476d1ce4e5b9ULL;
+        z ^= z >> 27;
+        z *= 0x94d049bb133111ebULL;
+        z ^= z >> 31;
+        return z >> 33;
+    }
     const uint32_t st = pcg_hash(pcg_hash(7919u + pcg_hash((uint32_t)p)));
     long long h = (long long)(int32_t)st;
     if (h < 0) h = -h;  // <= 2^31: 32 bits
-    const unsigned long long prio = ((unsigned long long)h << kPrioPairBits) | (unsigned long long)p;  // < 2^54
-    return ((unsigned long long)(r + 1) << 54) | ((1ull << 54) - 1ull - prio);
+    return (unsigned long long)h;
 }
 
 // Jones-Plassmann colouring of the pair graph behind the colour cache, on one thread-block
@@ -510,8 +529,8 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         if (threadIdx.x == 0) s_left[b] = 0;  // last read two rounds ago, before two cluster barriers
         for (int p = tid; p < P; p += nth) {
             if (pr.col[p] >= 0) continue;
-            const unsigned long long k = claim_key(p, r);
             const int bi = pr.pbi[p], bj = pr.pbj[p];
+            const unsigned long long k = claim_key(p, r, pair_hash(p, bi, bj, pr.body_local));
             if (invM[bi] > 0.0f) atomicMax(claim + bi, k);
             if (bj >= 0 && invM[bj] > 0.0f) atomicMax(claim + bj, k);
         }
@@ -519,8 +538,8 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         int left = 0;
         for (int p = tid; p < P; p += nth) {
             if (pr.col[p] >= 0) continue;
-            const unsigned long long k = claim_key(p, r);
             const int bi = pr.pbi[p], bj = pr.pbj[p];
+            const unsigned long long k = claim_key(p, r, pair_hash(p, bi, bj, pr.body_local));
             const bool da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
             if ((da && __ldcg(claim + bi) != k) || (db && __ldcg(claim + bj) != k)) {
                 ++left;

@@ -72,3 +72,40 @@ def random_boxes(n=10000, edge=(0.2, 0.6), box=(20.0, 20.0, 10.0), mu=(0.3, 0.8)
         centers[i] = c
         grid.setdefault(key, []).append(i)
     return dict(dims=dims, centers=centers, mu=rm.uniform(mu[0], mu[1], size=n), density=np.full(n, density))
+
+
+def jittered_boxes(n, edge=(0.2, 0.6), height=10.0, mu=(0.3, 0.8), density=1000.0, rng=None, pitch=None):
+    """n random boxes in a footprint scaled to n (the 10 000-box, 20 x 20 x 10 m drop's body
+    density: side 20 sqrt(n / 10^4) m, at least 2 m), without overlap: each box gets its own cell
+    of a lattice of pitch > the largest edge, drawn uniformly without replacement, and a uniform
+    jitter that keeps it inside the cell.  Vectorised, so hundreds of scenes build in seconds."""
+    rng = rng if rng is not None else np.random.default_rng(0)
+    pitch = pitch if pitch is not None else edge[1] * 1.0 + 0.02
+    side = max(2.0, 20.0 * np.sqrt(n / 1e4))
+    nx = max(1, int(side / pitch))
+    nz = max(1, int(height / pitch))
+    while nx * nx * nz < n:
+        nx += 1
+    dims = rng.uniform(edge[0], edge[1], size=(n, 3))
+    cells = rng.choice(nx * nx * nz, size=n, replace=False)
+    ix, iy, iz = cells // (nx * nz), (cells // nz) % nx, cells % nz
+    centers = np.stack([(ix + 0.5) * pitch - nx * pitch / 2, (iy + 0.5) * pitch - nx * pitch / 2,
+                        (iz + 0.5) * pitch], axis=1)
+    centers += rng.uniform(-1.0, 1.0, size=(n, 3)) * (pitch - dims) / 2
+    return dict(dims=dims, centers=centers, mu=rng.uniform(mu[0], mu[1], size=n), density=np.full(n, density))
+
+
+def batched_scenes(n_scenes=512, nmin=8, nmax=2000, seed_n=5, seed_mass=6, seed_boxes=1, heavy_frac=0.1,
+                   heavy_factor=100.0):
+    """The batched workload: body counts log-uniform in [nmin, nmax] (round(exp(U[ln nmin,
+    ln nmax]))), boxes sized and placed as the random-box drop scaled to each scene's footprint,
+    and heavy_frac of each scene's bodies at heavy_factor x density (mass ratios 100:1)."""
+    rn, rm, rb = (np.random.default_rng(s) for s in (seed_n, seed_mass, seed_boxes))
+    counts = np.round(np.exp(rn.uniform(np.log(nmin), np.log(nmax), n_scenes))).astype(int)
+    out = []
+    for n in counts:
+        sc = jittered_boxes(int(n), rng=rb)
+        heavy = rm.random(int(n)) < heavy_frac
+        sc["density"] = np.where(heavy, sc["density"] * heavy_factor, sc["density"])
+        out.append(sc)
+    return out

@@ -45,6 +45,11 @@ WORKLOADS = {
     # the reference's ColorCache timing fixture (reports/innovation_stack_color_cache_l4.json):
     # lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5, 40 velocity / 20 position sweeps,
     # 1 substep, dt 1/240
+    # 512 independent box scenes of 8..2000 bodies (log-uniform), ~180k bodies, 10 % of each scene
+    # 100x denser, advanced together by one batched engine; scenes are sharded over GPUs
+    "batched512": dict(engine="batched", scene="batched", n_scenes=512, nmin=8, nmax=2000, edge=(0.2, 0.6),
+                       mu_range=(0.3, 0.8), density=1000.0, vit=16, pit=10, substeps=2, dt=1 / 240, color_cap=32,
+                       preroll=300, steps=100, warmup=3),
     "colorcache_lattice10k": dict(engine="color_cache", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5,
                                   vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20),
     "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
@@ -68,12 +73,17 @@ def _scenes():
 
 def scene_of(wl):
     sc = _scenes()
+    if wl["scene"] == "batched":
+        return {"scenes": sc.batched_scenes(n_scenes=wl["n_scenes"], nmin=wl["nmin"], nmax=wl["nmax"])}
     if wl["scene"] == "random_boxes":
         return sc.random_boxes(n=wl["n"], edge=wl["edge"], box=wl["box"], mu=wl["mu_range"], density=wl["density"])
     return {"centers": sc.lattice(wl["n"]) if wl["scene"] == "lattice" else sc.stack(wl["n"])}
 
 
 def make_engine(me, wl, scene):
+    if wl["engine"] == "batched":
+        return me.BatchedBoxEngine(scene["scenes"], mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
+                                   color_cap=wl["color_cap"])
     if wl["engine"] == "box":
         e = me.BoxContactEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
                                 color_cap=wl["color_cap"])
@@ -179,6 +189,92 @@ def cpu_baseline_sample(wl, scene, state=None, max_seconds=20.0):
     return wl["n"] * n / el, n, el
 
 
+def partition_scenes(counts, parts):
+    from importlib import import_module
+    return import_module("motion_engine_b200.boxes").partition_scenes(counts, parts)
+
+
+def _box_oracle(wl, sc):
+    from oracle import oracle as O
+    o = O.BoxOracle(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"])
+    for c, d, m, de in zip(sc["centers"], sc["dims"], sc["mu"], sc["density"]):
+        o.add_box(c, dims=d, density=de, mu=m)
+    return o
+
+
+def batched_cpu_sample(wl, scenes, states, max_seconds=20.0):
+    """The oracle, one scene at a time from the GPU's state of that scene, one step each, scenes
+    in order until max_seconds of CPU work: body-steps/s on one core."""
+    bs, t_busy, n_sc = 0, 0.0, 0
+    for sc, st in zip(scenes, states):
+        o = _box_oracle(wl, sc)
+        o.set_body_state(*st)
+        t0 = time.perf_counter()
+        o.step(wl["dt"], wl["substeps"])
+        t_busy += time.perf_counter() - t0
+        bs += len(sc["centers"])
+        n_sc += 1
+        if t_busy > max_seconds:
+            break
+    return bs / t_busy, n_sc, t_busy
+
+
+def _ref_batched_worker(workload, idx, steps, warmup, budget):
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ge.load_package()
+    wl = WORKLOADS[workload]
+    scenes = scene_of(wl)["scenes"]
+    oracles = [_box_oracle(wl, scenes[i]) for i in idx]
+    for o in oracles:
+        for _ in range(wl["preroll"] + warmup):
+            o.step(wl["dt"], wl["substeps"])
+    bs, n = 0, 0
+    t0 = time.perf_counter()
+    while n < steps:
+        for o, i in zip(oracles, idx):
+            o.step(wl["dt"], wl["substeps"])
+            bs += len(scenes[i]["centers"])
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return bs, time.perf_counter() - t0, n
+
+
+def run_reference_batched(args, wl):
+    """--impl reference for the batched workload: the oracle on every host core, the scenes
+    split over the processes (LPT on body counts); each process advances its scenes through the
+    set-up and warm-up steps, then times whole batch steps for up to ~60 s."""
+    import multiprocessing as mp
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    scenes = scene_of(wl)["scenes"]
+    counts = [len(sc["centers"]) for sc in scenes]
+    procs = max(1, min(os.cpu_count() or 1, 64, len(scenes)))
+    parts = [p for p in partition_scenes(counts, procs) if p]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(len(parts)) as pool:
+        t0 = time.perf_counter()
+        res = pool.starmap(_ref_batched_worker, [(args.workload, p, args.steps, args.warmup, 60.0) for p in parts])
+        wall = time.perf_counter() - t0
+    steps_min = min(r[2] for r in res)
+    # whole-job rate: every process's body-steps over the slowest process's busy time
+    value = sum(r[0] for r in res) / max(r[1] for r in res)
+    line = {"impl": "reference", "metric": "body-steps/s", "value": value, "unit": "body-steps/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload, "bodies": sum(counts), "scenes": len(scenes),
+                       **{k: v for k, v in wl.items() if k not in ("warmup", "steps")}},
+            "dtype": "f32", "data": "synthetic",
+            "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": len(parts), "kind": "port",
+                             "sample": f"{len(parts)} processes, each advancing its share of the {len(scenes)} "
+                                       f"scenes (LPT on body counts) by >= {steps_min} timed batch steps after the "
+                                       f"{wl['preroll']} set-up and {args.warmup} warm-up steps, capped at ~60 s; "
+                                       f"the oracle restatement, the reference's Warp CPU path is not installed"},
+            "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, wl):
     """--impl reference: the oracle port on every host core (one independent replica per
     process, spawn start method), each timed over a bounded number of steps from the workload's
@@ -248,6 +344,40 @@ def _ref_worker(workload, path, steps, warmup, budget):
     return _time_oracle(o, wl, budget, steps)
 
 
+def per_scene_sequential(me, wl, scenes, batch, dt, S, stream, steps=3):
+    """The same scenes advanced one engine per scene, one after another (per-scene launches), from
+    the batch's current state and for the same sweeps: body-steps/s on this GPU.  Each engine
+    first runs one untimed step (its CUDA graph capture; it starts without the batch's warm
+    impulses)."""
+    import torch
+    engines = []
+    st = batch.get_state()
+    q = batch.q.cpu().numpy()
+    for k, sc in enumerate(scenes):
+        e = me.BoxContactEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
+                                color_cap=wl["color_cap"], cand_per_body=12)
+        for c, d, de, m in zip(sc["centers"], sc["dims"], sc["density"], sc["mu"]):
+            e.add_box(c, dims=d, density=de, mu=m)
+        sl = batch.scene_slice(k)
+        e.set_body_state(st.xc[sl], q[sl], st.vc[sl], st.om[sl])
+        e.step(dt, S)
+        engines.append(e)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        for e in engines:
+            e.step(dt, S)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    for e in engines:
+        e.check_errors()
+    n = sum(len(sc["centers"]) for sc in scenes)
+    return {"value": n / (ms / 1e3), "unit": "body-steps/s", "ms_per_step": ms, "steps": steps,
+            "engines": len(engines), "note": "same sweeps per scene; each scene's arithmetic is bytewise the batch's"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -271,16 +401,22 @@ def main():
     import __graft_entry__ as ge
     if args.impl == "reference":
         ge.load_package()
-        return run_reference(args, wl)
+        return run_reference_batched(args, wl) if wl["engine"] == "batched" else run_reference(args, wl)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     ge.load_package()
     scene = scene_of(wl)
+    n_job = wl.get("n", 0) * world  # replicas: every rank runs the whole workload
+    if wl["engine"] == "batched":  # scenes sharded over the ranks, no data-path collective
+        counts = [len(sc["centers"]) for sc in scene["scenes"]]
+        n_job = sum(counts)
+        mine = partition_scenes(counts, world)[rank]
+        scene = {"scenes": [scene["scenes"][i] for i in mine]}
     cpu_base = None
     do_cpu = rank == 0 and not args.no_cpu_baseline
-    if do_cpu and wl["engine"] != "box":
+    if do_cpu and wl["engine"] not in ("box", "batched"):
         ge.load_package()
         v, n, el = cpu_baseline_sample(wl, scene)  # before the first GPU call
         cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
@@ -311,12 +447,16 @@ def main():
         torch.cuda.synchronize()
         np.savez(args.save_state, xc=e.xc[:, :3].cpu().numpy(), q=e.q.cpu().numpy(), v=e.v[:, :3].cpu().numpy(),
                  w=e.w[:, :3].cpu().numpy())
+    tuned = None
+    if wl["engine"] == "batched":  # the launch form of the solve, picked on live (untimed) steps
+        best, times = me.autotune(e, dt, S)
+        tuned = {"solve_blocks": best, "ms_per_step": {str(k): round(v, 4) for k, v in times.items()}}
     for _ in range(args.warmup):
         e.step(dt, S)
     e.check_errors()
     torch.cuda.synchronize()
     start_state = None
-    if do_cpu and wl["engine"] == "box":
+    if do_cpu and wl["engine"] in ("box", "batched"):
         start_state = (e.xc[:, :3].cpu().numpy(), e.q.cpu().numpy(), e.v[:, :3].cpu().numpy(),
                        e.w[:, :3].cpu().numpy())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
@@ -363,6 +503,10 @@ def main():
     e.check_errors()
     bytes_io = N * (3 + 4 + 3 + 3) * 4
 
+    per_scene = None
+    if wl["engine"] == "batched":
+        per_scene = per_scene_sequential(me, wl, scene["scenes"], e, dt, S, stream)
+
     # the dominant kernel (the persistent chunk solve), timed live on its launching stream
     solve_ms, solve_bytes, stage_ms = [], [], {}
     if hasattr(e, "profile_substep"):
@@ -381,6 +525,13 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
+    if do_cpu and wl["engine"] == "batched":
+        sl = [e.scene_slice(k) for k in range(len(scene["scenes"]))]
+        v, nsc, el = batched_cpu_sample(wl, scene["scenes"], [tuple(a[x] for a in start_state) for x in sl])
+        cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
+                    "sample": f"one step of each of the first {nsc} scenes from the GPU's state of that scene at the "
+                              f"start of the timed region, on one host core ({el:.1f} s of stepping; the oracle "
+                              f"restatement, not the reference's Warp CPU path)"}
     if do_cpu and wl["engine"] == "box":
         v, n, el = cpu_baseline_sample(wl, scene, state=start_state)
         cpu_base = {"value": v, "unit": "body-steps/s", "cores": 1, "kind": "port",
@@ -388,7 +539,7 @@ def main():
                               f"region, on one host core ({el:.1f} s; the oracle restatement, not the reference's "
                               f"Warp CPU path)"}
     peaks, peak_kind = _peaks()
-    value = wl["n"] * world * args.steps / (ms / 1e3)
+    value = n_job * args.steps / (ms / 1e3)
     roof = None
     if solve_ms:
         avg_ms = float(np.mean(solve_ms))
@@ -405,22 +556,30 @@ def main():
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "k_color_solve (persistent chunk solve, one launch per substep)",
                 "launch_ms": avg_ms, "algorithmic_bytes_per_launch": avg_b, "counts": solve_bytes[-1]}
-    cfg = {"workload": args.workload, "bodies": wl["n"], "substeps": S, "vit": wl["vit"], "pit": wl["pit"], "dt": dt,
-           "setup_steps": wl["preroll"], "l2": "flushed between timed steps (256 MiB write)",
-           "parallelism": f"replicas x{world}"}
+    cfg = {"workload": args.workload, "bodies": n_job if wl["engine"] == "batched" else wl["n"], "substeps": S,
+           "vit": wl["vit"], "pit": wl["pit"], "dt": dt, "setup_steps": wl["preroll"],
+           "l2": "flushed between timed steps (256 MiB write)",
+           "parallelism": f"scenes sharded x{world} (LPT)" if wl["engine"] == "batched" else f"replicas x{world}"}
+    if wl["engine"] == "batched":
+        cfg.update(scenes=wl["n_scenes"], bodies_per_scene=[wl["nmin"], wl["nmax"]], edge=wl["edge"],
+                   mu=wl["mu_range"], density=wl["density"], heavy="10 % of each scene at 100 x density",
+                   color_cap=wl["color_cap"], autotuned=tuned)
     if wl["engine"] == "box":
         cfg.update(edge=wl["edge"], volume=wl["box"], mu=wl["mu_range"], density=wl["density"],
                    color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3")
     line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "strong" if wl["engine"] == "batched" else "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene builders)", "config": cfg,
             "clocks": clk.summary(),
-            "e2e": {"value": wl["n"] * world * K2 / (e2e_ms / 1e3), "unit": "body-steps/s",
+            "e2e": {"value": n_job * K2 / (e2e_ms / 1e3), "unit": "body-steps/s",
                     "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io, "steps": K2},
             "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
             "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h_end,
             "colors_e2e_steps": {"max": max(colors), "mean": float(np.mean(colors))}}
+    if per_scene is not None:
+        line["per_scene_sequential"] = per_scene
+        line["batched_over_sequential"] = (N * args.steps / (ms / 1e3)) / per_scene["value"]
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

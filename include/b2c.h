@@ -172,6 +172,10 @@ typedef struct b2c_pairs {
     int32_t kslots;          /* contact slots per record (>= the most contacts one pair keeps) */
     uint64_t *body_colors;   /* (bodies) colours used around each body; needed with
                                 B2C_COLOR_FIRST_FIT only, else NULL */
+    const int32_t *body_local; /* (bodies) index of each body inside its scene, or NULL.  Set:
+                                the colouring priority hashes the pair's scene-local bodies
+                                (a scene colours alike alone or in a batch); NULL: the
+                                reference's hash of the pair index (COL:136-148). */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -207,6 +211,9 @@ typedef struct b2c_boxes {
     float *slot_n;            /* (cand cap, 4) normal from b to a */
     int32_t *slot_f;          /* (cand cap x 8) feature id */
     int32_t *scan_tmp;        /* b2c_scan_scratch_ints(max(dims, n, cand cap) + 1) */
+    const int32_t *scene;     /* (n) scene of each body for a batch of independent scenes, or
+                                 NULL (one scene).  Bodies of different scenes never pair; the
+                                 scenes may overlap in space (the grid hash includes the scene). */
 } b2c_boxes;
 
 /* Flags of b2c_color_params.flags */

@@ -307,7 +307,7 @@ class ColoredOracle:
 def _box_sigs(L):
     P = ctypes.c_void_p
     L.or_box_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_float, P, P, P, P, P, P, P, P, P,
-                              ctypes.c_double, ctypes.c_int, ctypes.c_double, P]
+                              ctypes.c_double, ctypes.c_int, ctypes.c_double, P, P, P]
     L.or_box_step.restype = ctypes.c_int
     L.or_box_box.argtypes = [P, P, P, P, P, P, ctypes.c_double, P, P, P, P]
     L.or_box_box.restype = ctypes.c_int
@@ -333,6 +333,17 @@ def box_box(ha, xa, qa, hb, xb, qb, margin=2e-3):
     return po[:3 * m].reshape(m, 3), no, go[:m], fo[:m]
 
 
+def scene_local_index(scene):
+    """Index of every body among the bodies of its scene, in body order."""
+    scene = np.asarray(scene, np.int64)
+    out = np.zeros(len(scene), np.int32)
+    seen = {}
+    for i, s in enumerate(scene.tolist()):
+        out[i] = seen.get(s, 0)
+        seen[s] = out[i] + 1
+    return out
+
+
 class BoxOracle:
     """CPU restatement of the box engine: box/plane + box/box narrowphase (BoxWorld.contacts,
     ncp_gpu.py:1273-1280) over the pairs whose bounding spheres are within the margin, with the
@@ -344,13 +355,15 @@ class BoxOracle:
         self.dims = dims; self.mu = mu; self.vit = vit; self.pit = pit; self.flags = flags; self.margin = margin
         self.cap = cap
         self._centers, self._halves, self._dens, self._mus, self._kin = [], [], [], [], []
+        self._scenes = []
         self.b = None; self._h = None; self._force_dt = None
 
-    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False):
+    def add_box(self, center, dims=None, density=1000.0, mu=None, kin=False, scene=0):
         d = self.dims if dims is None else dims
         self._centers.append(list(center)); self._halves.append([0.5 * d[0], 0.5 * d[1], 0.5 * d[2]])
         self._dens.append(float(density)); self._mus.append(self.mu if mu is None else float(mu))
         self._kin.append(1 if kin else 0)
+        self._scenes.append(int(scene))
         self.b = None
         return len(self._centers) - 1
 
@@ -377,6 +390,9 @@ class BoxOracle:
         self.per_body = bool(np.any(self.mus != np.float32(self.mu)))
         self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
         self.vgrav = np.zeros((N, 3), np.float32)
+        sc = np.array(self._scenes, np.int32)
+        self.scene = sc if len(sc) and sc.max() > 0 else None
+        self.local = scene_local_index(sc)
         self._h = L.or_col_create(1, self.vit, self.pit, 4, self.mu, 1.0, self.cap, N)
 
     def step(self, dt, substeps=1):
@@ -386,7 +402,8 @@ class BoxOracle:
         rc = lib().or_box_step(self._h, self.flags, self.N, _p(self.half4), _p(self.mus) if self.per_body else None,
                                float(self.mu), _p(b.xc), _p(b.q), _p(b.v), _p(b.w), _p(self.pv), _p(self.po),
                                _p(b.invM), _p(b.IbInv), _p(b.kin), float(dt), int(substeps),
-                               float(np.float32(self.margin)), _p(self.vgrav))
+                               float(np.float32(self.margin)), _p(self.vgrav),
+                               None if self.scene is None else _p(self.scene), _p(self.local))
         if rc != 0:
             raise RuntimeError(f"oracle box step failed with status {rc}")
         self._force_dt = dt / substeps

@@ -769,15 +769,28 @@ static void select_segment(int i, int L, int mx, const int *gorder, const int *c
 
 /* JP colouring of the pair graph, COL:1178-1208 (k_prio, k_clear_claim, k_claim, k_win) plus the
  * stable grouping by colour.  Returns the colour count. */
+/* priority of a pair from its two scene-local bodies (the box engine): a 31-bit splitmix64 hash
+ * of (local a + 1, local b + 1 or 0), ties broken by the pair index */
+static int64_t local_priority(int p, int a, int b, const int *local)
+{
+    uint64_t z = ((uint64_t)(uint32_t)(local[a] + 1) << 32) | (uint64_t)(uint32_t)(b >= 0 ? local[b] + 1 : 0);
+    z ^= z >> 30;
+    z *= 0xbf58476d1ce4e5b9ULL;
+    z ^= z >> 27;
+    z *= 0x94d049bb133111ebULL;
+    z ^= z >> 31;
+    return (int64_t)((z >> 33) << 32) | (int64_t)p;
+}
+
 static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int *pbj, const float *invM,
-                       int first_fit)
+                       int first_fit, const int *local)
 {
     int *col = malloc(sizeof(int) * (P > 0 ? P : 1));
     uint64_t *used = calloc((size_t)(N > 0 ? N : 1), sizeof(uint64_t));
     int ncol_ff = 0;
     int64_t *key = malloc(sizeof(int64_t) * (P > 0 ? P : 1));
     int64_t *claim = malloc(sizeof(int64_t) * (N > 0 ? N : 1));
-    for (int p = 0; p < P; ++p) { col[p] = -1; key[p] = jp_priority(p); }
+    for (int p = 0; p < P; ++p) { col[p] = -1; key[p] = local ? local_priority(p, pbi[p], pbj[p], local) : jp_priority(p); }
     int cur = 0;
     for (;;) {
         for (int i = 0; i < N; ++i) claim[i] = INT64_MAX;
@@ -1149,7 +1162,7 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
                 ncol = e->cached_colors;
                 e->hits++;
             } else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM, 0);
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, 0, NULL);
                 e->has_colors = 1;
                 if (e->mode == 1) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
@@ -1653,7 +1666,8 @@ static void box_cells_build(box_cells_t *g, int N, const float *xc, const double
     free(fill);
 }
 static int box_int_cmp(const void *a, const void *b) { return *(const int *)a - *(const int *)b; }
-static int box_cells_partners(const box_cells_t *g, int a, const float *xc, const double *rad, double margin, int *out)
+static int box_cells_partners(const box_cells_t *g, int a, const float *xc, const double *rad, double margin,
+                              const int *scene, int *out)
 {
     int ca[3], n = 0;
     for (int k = 0; k < 3; ++k) ca[k] = box_cell_axis(g, xc[3 * a + k], k);
@@ -1664,7 +1678,9 @@ static int box_cells_partners(const box_cells_t *g, int a, const float *xc, cons
                 int c = (x * g->dim[1] + y) * g->dim[2] + z;
                 for (int t = g->start[c]; t < g->start[c + 1]; ++t) {
                     int b = g->items[t];
-                    if (b > a && box_sphere_pair(xc + 3 * a, rad[a], xc + 3 * b, rad[b], margin)) out[n++] = b;
+                    if (b > a && (!scene || scene[b] == scene[a]) &&
+                        box_sphere_pair(xc + 3 * a, rad[a], xc + 3 * b, rad[b], margin))
+                        out[n++] = b;
                 }
             }
     qsort(out, n, sizeof(int), box_int_cmp);
@@ -1673,7 +1689,8 @@ static int box_cells_partners(const box_cells_t *g, int a, const float *xc, cons
 
 OR_API int or_box_step(void *h, int flags, int N, const float *half, const float *body_mu, float mu, float *xc,
                        float *q, float *v, float *w, float *pv, float *po, const float *invM, const float *IbInv,
-                       const int *kin, double dt, int substeps, double margin, float *vgrav)
+                       const int *kin, double dt, int substeps, double margin, float *vgrav, const int *scene,
+                       const int *local)
 {
     col_engine_t *e = h;
     int cap = e->cap;
@@ -1708,7 +1725,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             double ha[3] = {half[4 * a], half[4 * a + 1], half[4 * a + 2]};
             double xa[3] = {xc[3 * a], xc[3 * a + 1], xc[3 * a + 2]};
             double qa[4] = {q[4 * a], q[4 * a + 1], q[4 * a + 2], q[4 * a + 3]};
-            int nb = box_cells_partners(&bc, a, xc, rad, margin, partners);
+            int nb = box_cells_partners(&bc, a, xc, rad, margin, scene, partners);
             for (int t = -1; t < nb; ++t) {
                 int b = t < 0 ? -1 : partners[t];
                 double pts[24], nrm[3] = {0.0, 0.0, 1.0}, gs[8];
@@ -1757,7 +1774,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             }
             if (hit) { ncol = e->cached_colors; e->hits++; }
             else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM, (flags & 32) ? 1 : 0);
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, (flags & 32) ? 1 : 0, local);
                 e->has_colors = 1;
                 if (flags & 4) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
