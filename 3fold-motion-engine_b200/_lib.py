@@ -84,6 +84,12 @@ class NcpParams(ctypes.Structure):
                 ("barrier_timeout_ns", ctypes.c_int64)]
 
 
+class Bncp(ctypes.Structure):
+    _fields_ = [("n_env", c_int32), ("n_max", c_int32), ("nc", c_void_p), ("G", c_void_p), ("b", c_void_p),
+                ("mu", c_void_p), ("lam", c_void_p), ("res", c_void_p), ("iters", c_void_p), ("labels", c_void_p),
+                ("status", c_void_p)]
+
+
 COLOR_FIXED_FRAME = 1
 COLOR_APPLY_WARM = 2
 COLOR_CACHE = 4
@@ -151,6 +157,10 @@ _SIGS = {
     "b2c_ncp_color": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
     "b2c_ncp_sweeps": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p], c_int32),
     "b2c_ncp_residual": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
+    "b2c_bncp_max_rows": ([], c_int32),
+    "b2c_bncp_solve": ([_P(Bncp), c_int32, ctypes.c_double, c_int32, c_void_p], c_int32),
+    "b2c_bncp_sensitivity": ([_P(Bncp), c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_bncp_vjp": ([_P(Bncp), c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
     "b2c_box_narrowphase_test": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
 }

@@ -427,6 +427,37 @@ B2C_API int32_t b2c_ncp_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const
 B2C_API int32_t b2c_ncp_residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
                                  b2c_stream s);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched exact-cone NCP in Delassus form and its implicit adjoint (the reference's batched
+ * adjoint BatchProxADMMGPU, src/motion_engine/ncp/ncp_batch_gpu.py:918-1313, and its CPU
+ * implicit-function sensitivity, src/motion_engine/ncp/ncp_ref.py:786-959).  float64.  Every
+ * environment e has n_c[e] <= 16 contacts; arrays are padded to n_max = 3 x (max n_c) rows.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct b2c_bncp {
+    int32_t n_env;
+    int32_t n_max;          /* rows per environment, a multiple of 3, <= b2c_bncp_max_rows() */
+    const int32_t *nc;      /* (n_env) contacts of each environment */
+    const double *G;        /* (n_env, n_max, n_max) Delassus J Minv J^T, row-major */
+    const double *b;        /* (n_env, n_max) free contact velocity J v_free + bias */
+    const double *mu;       /* (n_env, n_max/3) friction */
+    double *lam;            /* (n_env, n_max) warm start in, solution out (n, t1, t2 per contact) */
+    double *res;            /* (n_env) natural residual of the returned lambda */
+    int32_t *iters;         /* (n_env) sweeps run (the convergence mask: < max_iters = converged) */
+    int32_t *labels;        /* (n_env, n_max/3) 0 open, 1 stick, 2 slip (written by the adjoint) */
+    int32_t *status;        /* (n_env) 1 = singular branch, 2 = branch boundary (responses NaN) */
+} b2c_bncp;
+
+B2C_API int32_t b2c_bncp_max_rows(void);
+/* Projected Gauss-Seidel per environment until the natural residual < tol (checked every
+ * `check` sweeps) or max_iters (ncp_batch_gpu.py's convergence mask; ncp_gpu.py:485-568 sweep). */
+B2C_API int32_t b2c_bncp_solve(const b2c_bncp *p, int32_t max_iters, double tol, int32_t check, b2c_stream s);
+/* Full fixed-branch responses dlam/dmu (n_env, n_max, n_max/3) and dlam/db (n_env, n_max, n_max)
+ * at p->lam (ncp_ref.sensitivity, :907-959); NaN where the branch is singular or on a boundary. */
+B2C_API int32_t b2c_bncp_sensitivity(const b2c_bncp *p, double *dlam_dmu, double *dlam_db, b2c_stream s);
+/* Vector-Jacobian product at p->lam: gb = (dlam/db)^T glam, gmu = (dlam/dmu)^T glam (the
+ * backward of the batched adjoint, ncp_batch_gpu.py:1172-1186). */
+B2C_API int32_t b2c_bncp_vjp(const b2c_bncp *p, const double *glam, double *gb, double *gmu, b2c_stream s);
+
 #ifdef __cplusplus
 }
 #endif
