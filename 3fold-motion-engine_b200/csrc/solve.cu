@@ -560,14 +560,13 @@ __device__ __forceinline__ RowVel load_row_vel(const Records &R, int s, int k, b
     c.ka1 = R.contact(kRKA1, k)[s];
     c.ka2 = R.contact(kRKA2, k)[s];
     c.im = R.contact(kRImp, k)[s];
-    if (has_b) {
-        c.rb = R.contact(kRRB, k)[s];
-        c.kbn = R.contact(kRKBN, k)[s];
-        c.kb1 = R.contact(kRKB1, k)[s];
-        c.kb2 = R.contact(kRKB2, k)[s];
-    } else {
-        c.rb = c.kbn = c.kb1 = c.kb2 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    }
+    // body B's fields are loaded whether or not the pair has a body B (a ground pair never
+    // reads them): the loads then do not wait for the pair header
+    (void)has_b;
+    c.rb = R.contact(kRRB, k)[s];
+    c.kbn = R.contact(kRKBN, k)[s];
+    c.kb1 = R.contact(kRKB1, k)[s];
+    c.kb2 = R.contact(kRKB2, k)[s];
     return c;
 }
 
@@ -707,12 +706,9 @@ __device__ __forceinline__ RowPos load_row_pos(const Records &R, int s, int k, b
     c.ra = R.contact(kRRA, k)[s];
     c.kan = R.contact(kRKAN, k)[s];
     c.jp = reinterpret_cast<const float *>(&R.contact(kRImp, k)[s])[3];
-    if (has_b) {
-        c.rb = R.contact(kRRB, k)[s];
-        c.kbn = R.contact(kRKBN, k)[s];
-    } else {
-        c.rb = c.kbn = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    }
+    (void)has_b;  // loaded unconditionally, as in load_row_vel
+    c.rb = R.contact(kRRB, k)[s];
+    c.kbn = R.contact(kRKBN, k)[s];
     return c;
 }
 
@@ -778,11 +774,20 @@ __device__ void pair_position_row(const SolveArgs &a, int s, const BA &B)
 // warp chunk c = t div 32, and chunk c on CTA c mod CTAs: a warp reads 32 consecutive record
 // slots (coalesced), and a colour narrower than the launch is spread over all of its SMs.
 // ---------------------------------------------------------------------------------------------
+constexpr int kMaxSolveColors = 512;  // the colouring's cap (kMaxColorsCap)
+
 template <int kKind, bool kFixed, bool kRow, class BA>
 __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
     if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
+    // the colour table in shared memory: a phase's first load then depends on nothing
+    __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors];
+    for (int c = threadIdx.x; c < nc && c < kMaxSolveColors; c += blockDim.x) {
+        s_cstart[c] = a.cstart[c];
+        s_ccount[c] = a.ccount[c];
+    }
+    __syncthreads();
     const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
     const int me = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);  // task slot
     const int vpasses = (a.apply_warm ? 1 : 0) + a.vit;
@@ -792,7 +797,7 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
         const bool warm = a.apply_warm && pass == 0;
         const bool pos = pass < a.pit;
         for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            const int s0 = s_cstart[ci], cnt = s_ccount[ci];
             const int nv = vel ? cnt : 0, ntask = nv + (pos ? cnt : 0);
             for (int t = me; t < ntask; t += nth) {
                 if (kRow) {
