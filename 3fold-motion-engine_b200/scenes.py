@@ -109,3 +109,23 @@ def batched_scenes(n_scenes=512, nmin=8, nmax=2000, seed_n=5, seed_mass=6, seed_
         sc["density"] = np.where(heavy, sc["density"] * heavy_factor, sc["density"])
         out.append(sc)
     return out
+
+
+def box_lattice(n=100000, edge=0.25, extent=(50.0, 50.0, 10.0), jitter=0.05, mu=0.6, density=1000.0, seed=4):
+    """The stress scene: n cubes of one edge on a seeded random subset of a lattice filling
+    extent (pitch >= 1.05 x edge), each displaced by up to jitter x pitch per axis (uniform), the
+    lowest layer resting just above the ground."""
+    rng = np.random.default_rng(seed)
+    vol = extent[0] * extent[1] * extent[2]
+    pitch = max(edge * 1.05, (vol / n) ** (1.0 / 3.0))
+    nx, ny, nz = (max(1, int(e / pitch)) for e in extent)
+    while nx * ny * nz < n:
+        pitch *= 0.99
+        nx, ny, nz = (max(1, int(e / pitch)) for e in extent)
+    cells = np.sort(rng.choice(nx * ny * nz, size=n, replace=False))
+    ix, iy, iz = cells // (ny * nz), (cells // nz) % ny, cells % nz
+    j = jitter * min(pitch - edge, pitch) / 2 if pitch > edge else 0.0
+    centers = np.stack([(ix + 0.5) * pitch - nx * pitch / 2, (iy + 0.5) * pitch - ny * pitch / 2,
+                        edge / 2 + 1e-3 + iz * pitch], axis=1) + rng.uniform(-1.0, 1.0, (n, 3)) * j
+    centers[:, 2] = np.maximum(centers[:, 2], edge / 2 + 1e-3)
+    return dict(dims=np.full((n, 3), edge), centers=centers, mu=np.full(n, mu), density=np.full(n, density))

@@ -45,6 +45,11 @@ WORKLOADS = {
     # the reference's ColorCache timing fixture (reports/innovation_stack_color_cache_l4.json):
     # lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5, 40 velocity / 20 position sweeps,
     # 1 substep, dt 1/240
+    # stress: 100 000 cubes of edge 0.25 on a seeded, jittered lattice in 50 x 50 x 10 m, mu 0.6,
+    # 2 substeps x (16 velocity + 16 position sweeps), broadphase rebuilt every substep, 200 steps
+    "stress100k": dict(engine="box", scene="box_lattice", n=100000, edge=(0.25, 0.25), box=(50.0, 50.0, 10.0),
+                       mu_range=(0.6, 0.6), density=1000.0, vit=16, pit=16, substeps=2, dt=1 / 240, color_cap=32,
+                       preroll=100, steps=100, warmup=3),
     # 512 independent box scenes of 8..2000 bodies (log-uniform), ~180k bodies, 10 % of each scene
     # 100x denser, advanced together by one batched engine; scenes are sharded over GPUs
     "batched512": dict(engine="batched", scene="batched", n_scenes=512, nmin=8, nmax=2000, edge=(0.2, 0.6),
@@ -75,6 +80,9 @@ def scene_of(wl):
     sc = _scenes()
     if wl["scene"] == "batched":
         return {"scenes": sc.batched_scenes(n_scenes=wl["n_scenes"], nmin=wl["nmin"], nmax=wl["nmax"])}
+    if wl["scene"] == "box_lattice":
+        return sc.box_lattice(n=wl["n"], edge=wl["edge"][0], extent=wl["box"], mu=wl["mu_range"][0],
+                              density=wl["density"])
     if wl["scene"] == "random_boxes":
         return sc.random_boxes(n=wl["n"], edge=wl["edge"], box=wl["box"], mu=wl["mu_range"], density=wl["density"])
     return {"centers": sc.lattice(wl["n"]) if wl["scene"] == "lattice" else sc.stack(wl["n"])}
