@@ -155,7 +155,7 @@ class BoxContactEngine(_BeadEngineBase):
                                     _ptr(self.k_n), _ptr(self.k_fa), _ptr(self.k_fb), _ptr(self.k_imp))
         pcap, kslots = cand_cap, 8
         self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(kept_cap),
-                           col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
+                           col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(2 * N),
                            cached_a=i32(pcap), cached_b=i32(pcap),
                            cached_mass=torch.zeros(max(N, 1), dtype=torch.float32, device=dev), cache_state=i32(8),
                            body_colors=i64(N),

@@ -127,7 +127,7 @@ class GraphColoredContactEngine(_BeadEngineBase):
             "praw_start", "praw_count", "jn_in", "jn_red", "jt_in", "keep", "kidx", "scan_tmp")))
         # pairs, colouring, colour cache, barrier
         self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(cap),
-                           col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(N),
+                           col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(2 * N),
                            cached_a=i32(pcap), cached_b=i32(pcap), cached_mass=f32(N), cache_state=i32(8),
                            barrier=torch.zeros(2, dtype=torch.int32, device=dev),
                            rec=f32(self.L.b2c_pair_record_floats(pcap, kslots)))

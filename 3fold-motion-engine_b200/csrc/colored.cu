@@ -430,6 +430,7 @@ constexpr int kMaxColorsCap = 512;
 constexpr int kColorSub = 16;  // buckets inside a colour: 8 contact counts (descending) x ground / box pair
 constexpr int kColorClusterMax = 16;
 constexpr int kPrioPairBits = 22;  // pair index bits of the compact priority (capacity <= 4M pairs)
+constexpr int kJPRegPairs = 4;     // pairs per colouring thread whose round state lives in registers
 
 // Round-tagged claim of pair p in round r: a larger key wins atomicMax.  The priority of a pair
 // is k_prio's (COL:136-148) |int32(randi(rand_init(7919, p)))| << 32 | p, the smaller first; it is
@@ -464,6 +465,73 @@ __device__ __forceinline__ unsigned long long pair_hash(int p, int a, int b, con
     return (unsigned long long)h;
 }
 
+// One pair's part in the Jones-Plassmann rounds: the bodies it claims (the dynamic ones; -1
+// for a static or absent body), its colour (-1 while uncoloured) and the low 54 bits of its
+// claim key, which carry the priority (the round tag sits above them).
+struct JPPair {
+    int bi, bj, col;
+    unsigned long long low;
+};
+__device__ __forceinline__ JPPair jp_pair(int p, const b2c_pairs &pr, const float *__restrict__ invM)
+{
+    const int a = pr.pbi[p], b = pr.pbj[p];
+    const unsigned long long h = pair_hash(p, a, b, pr.body_local);
+    JPPair q;
+    q.bi = invM[a] > 0.0f ? a : -1;
+    q.bj = (b >= 0 && invM[b] > 0.0f) ? b : -1;
+    q.col = -1;
+    q.low = claim_key(p, -1, h);  // round tag 0: the low bits alone
+    return q;
+}
+__device__ __forceinline__ unsigned long long jp_key(const JPPair &q, int r)
+{
+    return ((unsigned long long)(r + 1) << 54) | q.low;
+}
+__device__ __forceinline__ void jp_claim(const JPPair &q, int r, unsigned long long *claim)
+{
+    const unsigned long long k = jp_key(q, r);
+    if (q.bi >= 0) atomicMax(claim + q.bi, k);
+    if (q.bj >= 0) atomicMax(claim + q.bj, k);
+}
+// Pair q's turn in round r: it wins if it holds every claim it made in `cur`, and then takes
+// the round number or, with first_fit, the smallest colour not used around its bodies (the
+// masks are read together with the claims: the winners of a round share no dynamic body, so a
+// winner's masks hold exactly the colours of the earlier rounds).  A pair that loses claims
+// its bodies for round r + 1 in `nxt`.  Returns 1 while the pair is uncoloured.
+__device__ __forceinline__ int jp_turn(JPPair &q, int p, int r, const unsigned long long *cur,
+                                       unsigned long long *nxt, unsigned long long *used, int first_fit,
+                                       int *__restrict__ col, int *s_ncol)
+{
+    if (q.col >= 0) return 0;
+    const unsigned long long k = jp_key(q, r);
+    unsigned long long ca = k, cb = k, ua = 0ull, ub = 0ull;
+    if (q.bi >= 0) {
+        ca = __ldcg(cur + q.bi);
+        if (first_fit) ua = __ldcg(used + q.bi);
+    }
+    if (q.bj >= 0) {
+        cb = __ldcg(cur + q.bj);
+        if (first_fit) ub = __ldcg(used + q.bj);
+    }
+    if (ca != k || cb != k) {
+        jp_claim(q, r + 1, nxt);
+        return 1;
+    }
+    int c = r;
+    if (first_fit) {
+        const unsigned long long m = ua | ub;
+        c = (~m == 0ull) ? 64 : __ffsll((long long)~m) - 1;
+        if (c < 64) {
+            if (q.bi >= 0) __stcg(used + q.bi, ua | (1ull << c));
+            if (q.bj >= 0) __stcg(used + q.bj, ub | (1ull << c));
+        }
+        atomicMax(s_ncol, c + 1);
+    }
+    q.col = c;
+    col[p] = c;
+    return 0;
+}
+
 // Jones-Plassmann colouring of the pair graph behind the colour cache, on one thread-block
 // cluster (CTAs synchronised by cluster barriers, sums and histograms in distributed shared
 // memory).  Every round: each uncoloured pair claims its dynamic bodies (atomicMax of the
@@ -471,6 +539,14 @@ __device__ __forceinline__ unsigned long long pair_hash(int p, int a, int b, con
 // (k_win, COL:163-181) or, with first_fit, the smallest colour not used around its bodies.  The
 // pairs are then grouped by colour, inside a colour by contact count (descending) and ground
 // pairs first, so the lanes of a warp of the solve run similar code.
+//
+// A round costs one cluster barrier.  The claims alternate between two body arrays (pr.claim
+// holds 2 x bodies): the pairs that lose round r claim for round r + 1 in the other array in the
+// same pass, and a round's winners are decided only after the barrier that follows every claim
+// of that round.  Each thread's pairs are fixed (p = thread + k x threads), and their static
+// part (claimed bodies, priority) is computed once: in registers for the first kJPRegPairs of
+// them, and in the record buffer's header words beyond that (scratch until the solve's gather
+// rewrites them).  The winners and colours of every round are those of the two-barrier form.
 __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, int nbodies,
                                                                 const float *__restrict__ invM, b2c_pairs pr,
                                                                 int use_cache, int color_cap, int max_rounds,
@@ -479,7 +555,7 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
     namespace cgc = cooperative_groups;
     cgc::cluster_group cluster = cgc::this_cluster();
     __shared__ int s_flag;
-    __shared__ int s_left[2];
+    __shared__ int s_left[3];
     __shared__ int s_ncol;
     __shared__ int s_hist[kMaxColorsCap * kColorSub];  // rank 0 only: bucket counts, then cursors
     const int rank = (int)cluster.block_rank(), nrank = (int)cluster.num_blocks();
@@ -513,54 +589,65 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
             return;
         }
     }
-    unsigned long long *claim = reinterpret_cast<unsigned long long *>(pr.claim);
+    unsigned long long *claim0 = reinterpret_cast<unsigned long long *>(pr.claim);
+    unsigned long long *claim1 = claim0 + nbodies;
     unsigned long long *used = reinterpret_cast<unsigned long long *>(pr.body_colors);
+    int4 *pstate = reinterpret_cast<int4 *>(pr.rec);
+    JPPair rq[kJPRegPairs];
+#pragma unroll
+    for (int k = 0; k < kJPRegPairs; ++k) {
+        const int p = tid + k * nth;
+        if (p < P) rq[k] = jp_pair(p, pr, invM);
+    }
+    for (int p = tid + kJPRegPairs * nth; p < P; p += nth) {
+        const JPPair q = jp_pair(p, pr, invM);
+        pstate[p] = make_int4(q.bi, q.bj, (int)(unsigned)q.low, (int)(unsigned)(q.low >> 32));
+    }
     for (int p = tid; p < P; p += nth) pr.col[p] = -1;
     for (int i = tid; i < nbodies; i += nth) {
-        claim[i] = 0ull;
+        claim0[i] = 0ull;
+        claim1[i] = 0ull;
         if (first_fit) used[i] = 0ull;
     }
-    if (threadIdx.x == 0) s_ncol = 0;
+    if (threadIdx.x == 0) {
+        s_ncol = 0;
+        s_left[0] = 0;
+    }
+    cluster.sync();
+    // the claims of round 0
+#pragma unroll
+    for (int k = 0; k < kJPRegPairs; ++k)
+        if (tid + k * nth < P) jp_claim(rq[k], 0, claim0);
+    for (int p = tid + kJPRegPairs * nth; p < P; p += nth) {
+        const int4 st = pstate[p];
+        jp_claim(JPPair{st.x, st.y, -1, (unsigned long long)(unsigned)st.z | ((unsigned long long)(unsigned)st.w << 32)},
+                 0, claim0);
+    }
     cluster.sync();
     int r = 0;
     bool done = false;
     for (; r < max_rounds; ++r) {
-        const int b = r & 1;
-        if (threadIdx.x == 0) s_left[b] = 0;  // last read two rounds ago, before two cluster barriers
-        for (int p = tid; p < P; p += nth) {
-            if (pr.col[p] >= 0) continue;
-            const int bi = pr.pbi[p], bj = pr.pbj[p];
-            const unsigned long long k = claim_key(p, r, pair_hash(p, bi, bj, pr.body_local));
-            if (invM[bi] > 0.0f) atomicMax(claim + bi, k);
-            if (bj >= 0 && invM[bj] > 0.0f) atomicMax(claim + bj, k);
-        }
-        cluster.sync();
+        const unsigned long long *cur = (r & 1) ? claim1 : claim0;
+        unsigned long long *nxt = (r & 1) ? claim0 : claim1;
+        // s_left[r % 3] counts this round; the next round's counter is cleared here (every CTA
+        // read it two barriers ago)
+        if (threadIdx.x == 0) s_left[(r + 1) % 3] = 0;
         int left = 0;
-        for (int p = tid; p < P; p += nth) {
-            if (pr.col[p] >= 0) continue;
-            const int bi = pr.pbi[p], bj = pr.pbj[p];
-            const unsigned long long k = claim_key(p, r, pair_hash(p, bi, bj, pr.body_local));
-            const bool da = invM[bi] > 0.0f, db = bj >= 0 && invM[bj] > 0.0f;
-            if ((da && __ldcg(claim + bi) != k) || (db && __ldcg(claim + bj) != k)) {
-                ++left;
-            } else if (!first_fit) {
-                pr.col[p] = r;
-            } else {
-                // the winners of a round share no dynamic body: their masks are theirs alone
-                const unsigned long long m = (da ? used[bi] : 0ull) | (db ? used[bj] : 0ull);
-                const int c = (~m == 0ull) ? 64 : __ffsll((long long)~m) - 1;
-                pr.col[p] = c;
-                if (c < 64) {
-                    if (da) used[bi] |= 1ull << c;
-                    if (db) used[bj] |= 1ull << c;
-                }
-                atomicMax(&s_ncol, c + 1);
-            }
+#pragma unroll
+        for (int k = 0; k < kJPRegPairs; ++k) {
+            const int p = tid + k * nth;
+            if (p < P) left += jp_turn(rq[k], p, r, cur, nxt, used, first_fit, pr.col, &s_ncol);
         }
-        if (left) atomicAdd(&s_left[b], left);
+        for (int p = tid + kJPRegPairs * nth; p < P; p += nth) {
+            if (pr.col[p] >= 0) continue;
+            const int4 st = pstate[p];
+            JPPair q{st.x, st.y, -1, (unsigned long long)(unsigned)st.z | ((unsigned long long)(unsigned)st.w << 32)};
+            left += jp_turn(q, p, r, cur, nxt, used, first_fit, pr.col, &s_ncol);
+        }
+        if (left) atomicAdd(&s_left[r % 3], left);
         cluster.sync();
         int total = 0;
-        for (int q = 0; q < nrank; ++q) total += *cluster.map_shared_rank(&s_left[b], q);
+        for (int q = 0; q < nrank; ++q) total += *cluster.map_shared_rank(&s_left[r % 3], q);
         if (total == 0) {
             done = true;
             break;
@@ -755,6 +842,10 @@ int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_c
     const int first_fit = (p->flags & B2C_COLOR_FIRST_FIT) ? 1 : 0;
     if (first_fit && !pr->body_colors) {
         set_error("color_pairs: B2C_COLOR_FIRST_FIT needs pairs->body_colors");
+        return B2C_EARG;
+    }
+    if (!pr->claim || !pr->rec || !pr->col || !pr->porder) {
+        set_error("color_pairs: pairs->claim, rec, col and porder are required");
         return B2C_EARG;
     }
     if (pr->capacity > (1 << kPrioPairBits)) {

@@ -40,11 +40,25 @@ __device__ __forceinline__ f3 ldcg3(const float *p, int i) { return xyz(ldcg4(p,
 // record fields (float4 units)
 enum { kRecBody = 7, kRecContact = 5 };
 enum { kCN = 0, kCRA = 1, kCRB = 2, kCT1 = 3, kCImp = 4 };
-// row form (B2C_COLOR_ROW_FORM): per contact n|inv_n, rA|bias, rB, t1|inv_1, t2|inv_2, the
-// angular responses kAn, kA1, kA2, kBn, kB1, kB2 and the impulses
-enum { kRecContactRow = 12 };
-enum { kRN = 0, kRRA = 1, kRRB = 2, kRT1 = 3, kRT2 = 4, kRKAN = 5, kRKA1 = 6, kRKA2 = 7, kRKBN = 8, kRKB1 = 9,
-       kRKB2 = 10, kRImp = 11 };
+// row form (B2C_COLOR_ROW_FORM): the reference form's header and inverse-inertia rows, and per
+// contact n|inv_n, rA|bias, rB|inv_2, t1|inv_1 and the impulses.  The second tangent t2 = n x t1
+// and the angular responses k = I^-1 (r x d) are not stored: the sweeps recompute them with the
+// gather's own expressions (row_responses), which gives the same bits, and do so off the
+// velocity chain.  Five words per contact let a pair's first kRowBatch contacts load in one
+// batch of independent 128-bit loads.
+enum { kRecContactRow = 5 };
+enum { kRN = 0, kRRA = 1, kRRB = 2, kRT1 = 3, kRImp = 4 };
+constexpr int kRowBatch = 4;
+
+// the angular responses of one contact's three rows on one body: I^-1 (r x n), I^-1 (r x t1),
+// I^-1 (r x t2)
+struct RowResp {
+    f3 n, t1, t2;
+};
+__device__ __forceinline__ RowResp row_responses(const m3 &I, f3 r, f3 nrm, f3 t1, f3 t2)
+{
+    return RowResp{matvec(I, cross3(r, nrm)), matvec(I, cross3(r, t1)), matvec(I, cross3(r, t2))};
+}
 
 struct Records {
     float4 *base;
@@ -147,7 +161,8 @@ __global__ void k_pair_gather(const b2c_header *__restrict__ hdr, const int *__r
     }
 }
 
-// row form: the same header and masses, and per contact the constants of the substep
+// row form: the reference form's header, inertia rows and masses, and per contact the constants
+// of the substep
 __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int *__restrict__ porder,
                                   const int *__restrict__ pstart, const int *__restrict__ pcount,
                                   const int *__restrict__ pidx, const int *__restrict__ pbi,
@@ -175,6 +190,12 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
         }
         float mu_p = mu;
         if (body_mu) mu_p = bj >= 0 ? sqrtf(body_mu[bi] * body_mu[bj]) : body_mu[bi];
+        R.body(0)[s] = f4(IA.r0, 0.0f);
+        R.body(1)[s] = f4(IA.r1, 0.0f);
+        R.body(2)[s] = f4(IA.r2, 0.0f);
+        R.body(3)[s] = f4(IB.r0, 0.0f);
+        R.body(4)[s] = f4(IB.r1, 0.0f);
+        R.body(5)[s] = f4(IB.r2, 0.0f);
         R.body(6)[s] = make_float4(iMA, iMB, mu_p, 0.0f);
         const f3 xA = ld3(xc, bi);
         f3 xB{0.0f, 0.0f, 0.0f};
@@ -193,18 +214,14 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
             const f3 t1 = normalize3(f3{fmaf(-dd, nrm.x, aa.x), fmaf(-dd, nrm.y, aa.y), fmaf(-dd, nrm.z, aa.z)});
             const f3 t2 = cross3(nrm, t1);
             const f3 rnA = cross3(rA, nrm), rtA1 = cross3(rA, t1), rtA2 = cross3(rA, t2);
-            const f3 kAn = matvec(IA, rnA), kA1 = matvec(IA, rtA1), kA2 = matvec(IA, rtA2);
-            float meff = iMA + dot3(rnA, kAn), meft1 = iMA + dot3(rtA1, kA1), meft2 = iMA + dot3(rtA2, kA2);
+            const RowResp kA = row_responses(IA, rA, nrm, t1, t2);
+            float meff = iMA + dot3(rnA, kA.n), meft1 = iMA + dot3(rtA1, kA.t1), meft2 = iMA + dot3(rtA2, kA.t2);
             if (bj >= 0) {
                 const f3 rnB = cross3(rB, nrm), rtB1 = cross3(rB, t1), rtB2 = cross3(rB, t2);
-                const f3 kBn = matvec(IB, rnB), kB1 = matvec(IB, rtB1), kB2 = matvec(IB, rtB2);
-                meff = (meff + iMB) + dot3(rnB, kBn);
-                meft1 = (meft1 + iMB) + dot3(rtB1, kB1);
-                meft2 = (meft2 + iMB) + dot3(rtB2, kB2);
-                R.contact(kRRB, j)[s] = f4(rB, 0.0f);
-                R.contact(kRKBN, j)[s] = f4(kBn, 0.0f);
-                R.contact(kRKB1, j)[s] = f4(kB1, 0.0f);
-                R.contact(kRKB2, j)[s] = f4(kB2, 0.0f);
+                const RowResp kB = row_responses(IB, rB, nrm, t1, t2);
+                meff = (meff + iMB) + dot3(rnB, kB.n);
+                meft1 = (meft1 + iMB) + dot3(rtB1, kB.t1);
+                meft2 = (meft2 + iMB) + dot3(rtB2, kB.t2);
             }
             const float inv_n = meff >= 1e-12f ? 1.0f / meff : 0.0f;
             const float inv_1 = meft1 >= 1e-12f ? 1.0f / meft1 : 0.0f;
@@ -212,11 +229,8 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
             const float bias = B2C_BETA * fmaxf(pA4.w - B2C_SLOP, 0.0f) / dt;
             R.contact(kRN, j)[s] = f4(nrm, inv_n);
             R.contact(kRRA, j)[s] = f4(rA, bias);
+            R.contact(kRRB, j)[s] = f4(rB, inv_2);
             R.contact(kRT1, j)[s] = f4(t1, inv_1);
-            R.contact(kRT2, j)[s] = f4(t2, inv_2);
-            R.contact(kRKAN, j)[s] = f4(kAn, 0.0f);
-            R.contact(kRKA1, j)[s] = f4(kA1, 0.0f);
-            R.contact(kRKA2, j)[s] = f4(kA2, 0.0f);
             R.contact(kRImp, j)[s] = ld4(kept.imp, c);
         }
     }
@@ -541,68 +555,108 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 
 // ---------------------------------------------------------------------------------------------
 // row form of the three chunks (B2C_COLOR_ROW_FORM; not in the reference): the same sweep with
-// the substep constants of k_pair_gather_row.  The contact loop prefetches the next contact's
-// record, as above.
+// the substep constants of k_pair_gather_row.  A pair's contacts are loaded kRowBatch at a time,
+// the first batch together with the pair's header (without waiting for it: the slots exist
+// whatever the pair's count), so a pair of up to kRowBatch contacts pays two dependent round
+// trips (record, then the bodies' velocities) however many contacts it has.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ f3 fma3s(float s, f3 a, f3 b) { return f3{fmaf(s, a.x, b.x), fmaf(s, a.y, b.y), fmaf(s, a.z, b.z)}; }
 
-struct RowVel {
-    float4 n, ra, rb, t1, t2, kan, ka1, ka2, kbn, kb1, kb2, im;
+struct RowC {
+    float4 n, ra, rb, t1, im;
 };
-__device__ __forceinline__ RowVel load_row_vel(const Records &R, int s, int k, bool has_b)
+
+// Staging.  A batch of a pair's contact records is copied into this thread's part of the
+// dynamic shared memory with cp.async (no registers held while the copies are in flight), and
+// each contact is read from there when its turn comes: field f of batch contact j sits at
+// s_stage[(f * kRowBatch + j) * blockDim.x + threadIdx.x], so a warp's reads are consecutive.
+// A thread only ever reads its own words after its own cp.async.wait_group, so no block-level
+// synchronisation is involved.
+extern __shared__ float4 s_stage[];
+constexpr int kStageBytesPerThread = kRecContactRow * kRowBatch * 16;
+
+__device__ __forceinline__ float4 *stage_word(int f, int j)
 {
-    RowVel c;
-    c.n = R.contact(kRN, k)[s];
-    c.ra = R.contact(kRRA, k)[s];
-    c.t1 = R.contact(kRT1, k)[s];
-    c.t2 = R.contact(kRT2, k)[s];
-    c.kan = R.contact(kRKAN, k)[s];
-    c.ka1 = R.contact(kRKA1, k)[s];
-    c.ka2 = R.contact(kRKA2, k)[s];
-    c.im = R.contact(kRImp, k)[s];
-    // body B's fields are loaded whether or not the pair has a body B (a ground pair never
-    // reads them): the loads then do not wait for the pair header
-    (void)has_b;
-    c.rb = R.contact(kRRB, k)[s];
-    c.kbn = R.contact(kRKBN, k)[s];
-    c.kb1 = R.contact(kRKB1, k)[s];
-    c.kb2 = R.contact(kRKB2, k)[s];
-    return c;
+    return s_stage + ((f * kRowBatch + j) * (int)blockDim.x + (int)threadIdx.x);
+}
+__device__ __forceinline__ void cp_async16(float4 *dst, const float4 *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+// issue the copies of contacts k0 .. k0 + kRowBatch - 1 of slot s (those below the slot count
+// K; a slot beyond the pair's count holds stale words that are never read); the position chunk
+// skips t1
+__device__ __forceinline__ void stage_rows(const Records &R, int s, int k0, bool pos)
+{
+#pragma unroll
+    for (int j = 0; j < kRowBatch; ++j) {
+        if (k0 + j < R.K) {
+            cp_async16(stage_word(kRN, j), &R.contact(kRN, k0 + j)[s]);
+            cp_async16(stage_word(kRRA, j), &R.contact(kRRA, k0 + j)[s]);
+            cp_async16(stage_word(kRRB, j), &R.contact(kRRB, k0 + j)[s]);
+            if (!pos) cp_async16(stage_word(kRT1, j), &R.contact(kRT1, k0 + j)[s]);
+            cp_async16(stage_word(kRImp, j), &R.contact(kRImp, k0 + j)[s]);
+        }
+    }
+}
+__device__ __forceinline__ RowC staged_row(int j)
+{
+    return RowC{*stage_word(kRN, j), *stage_word(kRRA, j), *stage_word(kRRB, j), *stage_word(kRT1, j),
+                *stage_word(kRImp, j)};
+}
+__device__ __forceinline__ m3 load_inertia(const Records &R, int s, int f0)
+{
+    return m3{xyz(R.body(f0)[s]), xyz(R.body(f0 + 1)[s]), xyz(R.body(f0 + 2)[s])};
 }
 
 template <class BA>
 __device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS)
 {
+    stage_rows(a.rec, s, 0, false);
     const int4 h = a.rec.hdr()[s];
     const float4 mm = a.rec.body(6)[s];
+    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
     const int A = h.x, B = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y;
-    RowVel cur = load_row_vel(a.rec, s, 0, B >= 0);
     f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
     if (B >= 0) {
         vb = BS.get(B, 0);
         wb = BS.get(B, 1);
     }
-    for (int k = 0; k < n; ++k) {
-        RowVel nxt;
-        if (k + 1 < n) nxt = load_row_vel(a.rec, s, k + 1, B >= 0);
-        const f3 nrm = xyz(cur.n), t1 = xyz(cur.t1), t2 = xyz(cur.t2);
-        const float jn = cur.im.x, j1 = cur.im.y, j2 = cur.im.z;
-        const f3 J{fmaf(j2, t2.x, fmaf(jn, nrm.x, j1 * t1.x)), fmaf(j2, t2.y, fmaf(jn, nrm.y, j1 * t1.y)),
-                   fmaf(j2, t2.z, fmaf(jn, nrm.z, j1 * t1.z))};
-        if (iMA > 0.0f) {
-            const f3 kn = xyz(cur.kan), k1 = xyz(cur.ka1), k2 = xyz(cur.ka2);
-            va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
-            wa = add3(wa, f3{fmaf(j2, k2.x, fmaf(jn, kn.x, j1 * k1.x)), fmaf(j2, k2.y, fmaf(jn, kn.y, j1 * k1.y)),
-                             fmaf(j2, k2.z, fmaf(jn, kn.z, j1 * k1.z))});
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, false);
+            cp_async_wait_all();
         }
-        if (B >= 0 && iMB > 0.0f) {
-            const f3 kn = xyz(cur.kbn), k1 = xyz(cur.kb1), k2 = xyz(cur.kb2);
-            vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
-            wb = sub3(wb, f3{fmaf(j2, k2.x, fmaf(jn, kn.x, j1 * k1.x)), fmaf(j2, k2.y, fmaf(jn, kn.y, j1 * k1.y)),
-                             fmaf(j2, k2.z, fmaf(jn, kn.z, j1 * k1.z))});
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const RowC cur = staged_row(j);
+            const f3 nrm = xyz(cur.n), t1 = xyz(cur.t1), t2 = cross3(nrm, t1);
+            const float jn = cur.im.x, j1 = cur.im.y, j2 = cur.im.z;
+            const f3 J{fmaf(j2, t2.x, fmaf(jn, nrm.x, j1 * t1.x)), fmaf(j2, t2.y, fmaf(jn, nrm.y, j1 * t1.y)),
+                       fmaf(j2, t2.z, fmaf(jn, nrm.z, j1 * t1.z))};
+            if (iMA > 0.0f) {
+                const RowResp k = row_responses(IA, xyz(cur.ra), nrm, t1, t2);
+                va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
+                wa = add3(wa, f3{fmaf(j2, k.t2.x, fmaf(jn, k.n.x, j1 * k.t1.x)),
+                                 fmaf(j2, k.t2.y, fmaf(jn, k.n.y, j1 * k.t1.y)),
+                                 fmaf(j2, k.t2.z, fmaf(jn, k.n.z, j1 * k.t1.z))});
+            }
+            if (B >= 0 && iMB > 0.0f) {
+                const RowResp k = row_responses(IB, xyz(cur.rb), nrm, t1, t2);
+                vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
+                wb = sub3(wb, f3{fmaf(j2, k.t2.x, fmaf(jn, k.n.x, j1 * k.t1.x)),
+                                 fmaf(j2, k.t2.y, fmaf(jn, k.n.y, j1 * k.t1.y)),
+                                 fmaf(j2, k.t2.z, fmaf(jn, k.n.z, j1 * k.t1.z))});
+            }
         }
-        cur = nxt;
     }
     if (iMA > 0.0f) {
         BS.set(A, 0, va);
@@ -617,73 +671,83 @@ __device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS)
 template <class BA>
 __device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B)
 {
+    stage_rows(a.rec, s, 0, false);
     const int4 h = a.rec.hdr()[s];
     const float4 mm = a.rec.body(6)[s];
+    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
     const int bi = h.x, bj = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y, mu = mm.z;
-    RowVel cur = load_row_vel(a.rec, s, 0, bj >= 0);
     f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
     f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
     if (bj >= 0) {
         vB = B.get(bj, 0);
         wB = B.get(bj, 1);
     }
-    for (int k = 0; k < n; ++k) {
-        RowVel nxt;
-        if (k + 1 < n) nxt = load_row_vel(a.rec, s, k + 1, bj >= 0);
-        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
-        f3 va = add3(vA, cross3(wA, rA));
-        f3 vb{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-        f3 vrel = sub3(va, vb);
-        const float vn = dot3(vrel, nrm);
-        if (cur.n.w > 0.0f) {
-            float4 im = cur.im;
-            float dj = -vn * cur.n.w;
-            const float nw = fmaxf(0.0f, im.x + dj);
-            dj = nw - im.x;
-            im.x = nw;
-            const f3 Jn = scale3(nrm, dj);
-            if (iMA > 0.0f) {
-                vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
-                wA = fma3s(dj, xyz(cur.kan), wA);
-            }
-            if (bj >= 0 && iMB > 0.0f) {
-                vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
-                wB = fma3s(-dj, xyz(cur.kbn), wB);
-            }
-            va = add3(vA, cross3(wA, rA));
-            vb = f3{0.0f, 0.0f, 0.0f};
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, false);
+            cp_async_wait_all();
+        }
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const RowC cur = staged_row(j);
+            const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb), t1 = xyz(cur.t1), t2 = cross3(nrm, t1);
+            // the responses depend on the record only, so they are computed off the velocity chain
+            const RowResp kA = row_responses(IA, rA, nrm, t1, t2);
+            RowResp kB{};
+            if (bj >= 0) kB = row_responses(IB, rB, nrm, t1, t2);
+            f3 va = add3(vA, cross3(wA, rA));
+            f3 vb{0.0f, 0.0f, 0.0f};
             if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-            vrel = sub3(va, vb);
-            if (cur.t1.w > 0.0f && cur.t2.w > 0.0f) {
-                const f3 t1 = xyz(cur.t1), t2 = xyz(cur.t2);
-                const float o1 = im.y, o2 = im.z;
-                float a1 = o1 - dot3(vrel, t1) * cur.t1.w;
-                float a2 = o2 - dot3(vrel, t2) * cur.t2.w;
-                const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-                const float lim = mu * im.x;
-                if (mag > lim && mag > 1e-12f) {
-                    const float sc = lim / mag;
-                    a1 = a1 * sc;
-                    a2 = a2 * sc;
-                }
-                im.y = a1;
-                im.z = a2;
-                const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
-                const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+            f3 vrel = sub3(va, vb);
+            const float vn = dot3(vrel, nrm);
+            if (cur.n.w > 0.0f) {
+                float4 im = cur.im;
+                float dj = -vn * cur.n.w;
+                const float nw = fmaxf(0.0f, im.x + dj);
+                dj = nw - im.x;
+                im.x = nw;
+                const f3 Jn = scale3(nrm, dj);
                 if (iMA > 0.0f) {
-                    vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
-                    wA = fma3s(e1, xyz(cur.ka1), fma3s(e2, xyz(cur.ka2), wA));
+                    vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
+                    wA = fma3s(dj, kA.n, wA);
                 }
                 if (bj >= 0 && iMB > 0.0f) {
-                    vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
-                    wB = fma3s(-e1, xyz(cur.kb1), fma3s(-e2, xyz(cur.kb2), wB));
+                    vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
+                    wB = fma3s(-dj, kB.n, wB);
                 }
+                va = add3(vA, cross3(wA, rA));
+                vb = f3{0.0f, 0.0f, 0.0f};
+                if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+                vrel = sub3(va, vb);
+                if (cur.t1.w > 0.0f && cur.rb.w > 0.0f) {
+                    const float o1 = im.y, o2 = im.z;
+                    float a1 = o1 - dot3(vrel, t1) * cur.t1.w;
+                    float a2 = o2 - dot3(vrel, t2) * cur.rb.w;
+                    const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+                    const float lim = mu * im.x;
+                    if (mag > lim && mag > 1e-12f) {
+                        const float sc = lim / mag;
+                        a1 = a1 * sc;
+                        a2 = a2 * sc;
+                    }
+                    im.y = a1;
+                    im.z = a2;
+                    const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+                    const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+                    if (iMA > 0.0f) {
+                        vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
+                        wA = fma3s(e1, kA.t1, fma3s(e2, kA.t2, wA));
+                    }
+                    if (bj >= 0 && iMB > 0.0f) {
+                        vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
+                        wB = fma3s(-e1, kB.t1, fma3s(-e2, kB.t2, wB));
+                    }
+                }
+                store_imp_xyz(&a.rec.contact(kRImp, k0 + j)[s], im);
             }
-            store_imp_xyz(&a.rec.contact(kRImp, k)[s], im);
         }
-        cur = nxt;
     }
     if (iMA > 0.0f) {
         B.set(bi, 0, vA);
@@ -695,59 +759,53 @@ __device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B)
     }
 }
 
-struct RowPos {
-    float4 n, ra, rb, kan, kbn;
-    float jp;
-};
-__device__ __forceinline__ RowPos load_row_pos(const Records &R, int s, int k, bool has_b)
-{
-    RowPos c;
-    c.n = R.contact(kRN, k)[s];
-    c.ra = R.contact(kRRA, k)[s];
-    c.kan = R.contact(kRKAN, k)[s];
-    c.jp = reinterpret_cast<const float *>(&R.contact(kRImp, k)[s])[3];
-    (void)has_b;  // loaded unconditionally, as in load_row_vel
-    c.rb = R.contact(kRRB, k)[s];
-    c.kbn = R.contact(kRKBN, k)[s];
-    return c;
-}
-
 template <class BA>
 __device__ void pair_position_row(const SolveArgs &a, int s, const BA &B)
 {
+    stage_rows(a.rec, s, 0, true);
     const int4 h = a.rec.hdr()[s];
     const float4 mm = a.rec.body(6)[s];
+    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
     const int bi = h.x, bj = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y;
-    RowPos cur = load_row_pos(a.rec, s, 0, bj >= 0);
     f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
     f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
     if (bj >= 0) {
         pvB = B.get(bj, 2);
         poB = B.get(bj, 3);
     }
-    for (int k = 0; k < n; ++k) {
-        RowPos nxt;
-        if (k + 1 < n) nxt = load_row_pos(a.rec, s, k + 1, bj >= 0);
-        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
-        f3 rel = add3(pvA, cross3(poA, rA));
-        if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
-        if (cur.n.w > 0.0f) {
-            float dj = (cur.ra.w - dot3(rel, nrm)) * cur.n.w;
-            const float nw = fmaxf(0.0f, cur.jp + dj);
-            dj = nw - cur.jp;
-            store_imp_w(&a.rec.contact(kRImp, k)[s], nw);
-            const f3 Jn = scale3(nrm, dj);
-            if (iMA > 0.0f) {
-                pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
-                poA = fma3s(dj, xyz(cur.kan), poA);
-            }
-            if (bj >= 0 && iMB > 0.0f) {
-                pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
-                poB = fma3s(-dj, xyz(cur.kbn), poB);
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, true);
+            cp_async_wait_all();
+        }
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const float4 wn = *stage_word(kRN, j), wa = *stage_word(kRRA, j), wb = *stage_word(kRRB, j);
+            const float jp = stage_word(kRImp, j)->w;
+            const f3 nrm = xyz(wn), rA = xyz(wa), rB = xyz(wb);
+            const f3 kAn = matvec(IA, cross3(rA, nrm));
+            f3 kBn{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) kBn = matvec(IB, cross3(rB, nrm));
+            f3 rel = add3(pvA, cross3(poA, rA));
+            if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
+            if (wn.w > 0.0f) {
+                float dj = (wa.w - dot3(rel, nrm)) * wn.w;
+                const float nw = fmaxf(0.0f, jp + dj);
+                dj = nw - jp;
+                store_imp_w(&a.rec.contact(kRImp, k0 + j)[s], nw);
+                const f3 Jn = scale3(nrm, dj);
+                if (iMA > 0.0f) {
+                    pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
+                    poA = fma3s(dj, kAn, poA);
+                }
+                if (bj >= 0 && iMB > 0.0f) {
+                    pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
+                    poB = fma3s(-dj, kBn, poB);
+                }
             }
         }
-        cur = nxt;
     }
     if (iMA > 0.0f) {
         B.set(bi, 2, pvA);
@@ -822,7 +880,7 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 }
 
 constexpr int kClusterThreads = 512;     // reference form
-constexpr int kClusterThreadsRow = 384;  // row form: more live record registers per thread
+constexpr int kClusterThreadsRow = 384;  // row form (123 registers; 120 KB of contact staging)
 constexpr int kClusterMax = 16;
 
 __global__ void __launch_bounds__(256) k_color_solve_block(SolveArgs a)
@@ -854,17 +912,33 @@ __global__ void __launch_bounds__(kClusterThreadsRow) k_color_solve_cluster_row(
     solve_body<kCluster, true, true>(a, B);
 }
 
-static int max_coresident_grid_blocks()
+// dynamic shared memory of a solve launch: the row form's contact staging
+static size_t stage_bytes(int row, int threads) { return row ? (size_t)kStageBytesPerThread * threads : 0; }
+
+// the row-form kernels' dynamic shared memory exceeds the 48 KB default: opt in once
+static void allow_stage_smem()
 {
-    static int cached = -1;
-    if (cached < 0) {
+    static bool done = false;
+    if (done) return;
+    const int bytes = (int)stage_bytes(1, 256 > kClusterThreadsRow ? 256 : kClusterThreadsRow);
+    cudaFuncSetAttribute(k_color_solve_block, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_color_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_color_solve_cluster_row, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    done = true;
+}
+
+static int max_coresident_grid_blocks(int row)
+{
+    static int cached[2] = {-1, -1};
+    if (cached[row] < 0) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve_grid, 256, 0);
-        cached = std::max(1, sms * std::max(per, 1));
+        allow_stage_smem();
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve_grid, 256, stage_bytes(row, 256));
+        cached[row] = std::max(1, sms * std::max(per, 1));
     }
-    return cached;
+    return cached[row];
 }
 
 // largest power-of-two cluster (<= 16) of a cluster-solve kernel that the device can
@@ -876,9 +950,11 @@ static int max_cluster_size(int row)
     if (cached[row] < 0) {
         const void *fn = row ? (const void *)k_color_solve_cluster_row : (const void *)k_color_solve_cluster;
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        allow_stage_smem();
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kClusterMax);
         cfg.blockDim = dim3(row ? kClusterThreadsRow : kClusterThreads);
+        cfg.dynamicSmemBytes = stage_bytes(row, kClusterThreadsRow);
         int cs = 0;
         if (cudaOccupancyMaxPotentialClusterSize(&cs, fn, &cfg) != cudaSuccess) {
             cudaGetLastError();
@@ -942,6 +1018,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(cs);
             cfg.blockDim = dim3(a.row ? kClusterThreadsRow : kClusterThreads);
+            cfg.dynamicSmemBytes = stage_bytes(a.row, kClusterThreadsRow);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -958,19 +1035,21 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             }
             if ((rc = check_launch("color_solve_cluster"))) return rc;
         } else {
-            mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks());
+            mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks(a.row));
         }
     }
     if (mode > 0) {
-        const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks()));
+        allow_stage_smem();
+        const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks(a.row)));
         if (nblocks == 1) {
-            k_color_solve_block<<<1, 256, 0, s>>>(a);
+            k_color_solve_block<<<1, 256, stage_bytes(a.row, 256), s>>>(a);
             if ((rc = check_launch("color_solve_block"))) return rc;
         } else {
             cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (generation keeps counting)
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(256);
+            cfg.dynamicSmemBytes = stage_bytes(a.row, 256);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeCooperative;
@@ -996,5 +1075,6 @@ extern "C" int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots)
 {
     if (pair_capacity < 0 || kslots < 1) return -1;
     // room for either layout: the reference form (kRecContact fields per contact) or the row form
-    return 4LL * (int64_t)pair_capacity * (1 + b2c::kRecBody + b2c::kRecContactRow * (int64_t)kslots);
+    const int64_t per_contact = (int)b2c::kRecContact > (int)b2c::kRecContactRow ? (int)b2c::kRecContact : (int)b2c::kRecContactRow;
+    return 4LL * (int64_t)pair_capacity * (1 + b2c::kRecBody + per_contact * (int64_t)kslots);
 }

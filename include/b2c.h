@@ -160,7 +160,7 @@ typedef struct b2c_pairs {
     int32_t *col;            /* colour of each pair */
     int32_t *porder;         /* pairs grouped by colour */
     int32_t *cstart, *ccount;/* (max_colors) per-colour offset and count into porder */
-    int64_t *claim;          /* (bodies) Jones-Plassmann claims */
+    int64_t *claim;          /* (2 x bodies) Jones-Plassmann claims, two alternating arrays */
     int32_t *cached_a, *cached_b; /* colour cache: pbi / pbj of the cached colouring */
     float *cached_mass;      /* (bodies) invM of the cached colouring */
     int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
@@ -168,7 +168,8 @@ typedef struct b2c_pairs {
     float *rec;              /* colour-major pair records of the solve, b2c_pair_record_floats()
                                 floats: per slot a header, both bodies' inverse inertia and mass,
                                 and per contact its normal|depth, the terms that stay fixed
-                                during a solve (rA|meff, rB|meft1, t1|meft2, t2) and its impulses */
+                                during a solve (rA|meff, rB|meft1, t1|meft2) and its impulses.
+                                The colouring uses the header words as scratch. */
     int32_t kslots;          /* contact slots per record (>= the most contacts one pair keeps) */
     uint64_t *body_colors;   /* (bodies) colours used around each body; needed with
                                 B2C_COLOR_FIRST_FIT only, else NULL */
