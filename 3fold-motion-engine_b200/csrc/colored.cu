@@ -497,10 +497,11 @@ __device__ __forceinline__ void jp_claim(const JPPair &q, int r, unsigned long l
 // the round number or, with first_fit, the smallest colour not used around its bodies (the
 // masks are read together with the claims: the winners of a round share no dynamic body, so a
 // winner's masks hold exactly the colours of the earlier rounds).  A pair that loses claims
-// its bodies for round r + 1 in `nxt`.  Returns 1 while the pair is uncoloured.
+// its bodies for round r + 1 in `nxt`.  Returns 1 while the pair is uncoloured; `ncol` keeps
+// the thread's colour count.
 __device__ __forceinline__ int jp_turn(JPPair &q, int p, int r, const unsigned long long *cur,
                                        unsigned long long *nxt, unsigned long long *used, int first_fit,
-                                       int *__restrict__ col, int *s_ncol)
+                                       int *__restrict__ col, int &ncol)
 {
     if (q.col >= 0) return 0;
     const unsigned long long k = jp_key(q, r);
@@ -525,12 +526,54 @@ __device__ __forceinline__ int jp_turn(JPPair &q, int p, int r, const unsigned l
             if (q.bi >= 0) __stcg(used + q.bi, ua | (1ull << c));
             if (q.bj >= 0) __stcg(used + q.bj, ub | (1ull << c));
         }
-        atomicMax(s_ncol, c + 1);
+        ncol = max(ncol, c + 1);
     }
     q.col = c;
     col[p] = c;
     return 0;
 }
+
+// exclusive scan of a[0, E) in shared memory by the whole CTA (E <= 8 x blockDim.x); ends with a
+// __syncthreads
+__device__ void block_exclusive_scan(int *a, int E)
+{
+    __shared__ int s_w[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (E + (int)blockDim.x - 1) / (int)blockDim.x, b0 = (int)threadIdx.x * per;
+    int sum = 0;
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < E) sum += a[b0 + i];
+    int x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? s_w[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_w[lane] = w;
+    }
+    __syncthreads();
+    int base = x - sum + (warp > 0 ? s_w[warp - 1] : 0);
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < E) {
+            const int v = a[b0 + i];
+            a[b0 + i] = base;
+            base += v;
+        }
+    __syncthreads();
+}
+__device__ __forceinline__ int color_bucket(const b2c_pairs &pr, int p)
+{
+    const int n = min(max(pr.kcount[p], 1), 8);
+    return pr.col[p] * kColorSub + (8 - n) * 2 + (pr.pbj[p] >= 0 ? 1 : 0);
+}
+constexpr int kColorDynSmem = 2 * kMaxColorsCap * kColorSub * (int)sizeof(int);  // counts + cursors
 
 // Jones-Plassmann colouring of the pair graph behind the colour cache, on one thread-block
 // cluster (CTAs synchronised by cluster barriers, sums and histograms in distributed shared
@@ -556,8 +599,9 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
     cgc::cluster_group cluster = cgc::this_cluster();
     __shared__ int s_flag;
     __shared__ int s_left[3];
+    __shared__ int s_total[2];
     __shared__ int s_ncol;
-    __shared__ int s_hist[kMaxColorsCap * kColorSub];  // rank 0 only: bucket counts, then cursors
+    extern __shared__ int s_dyn[];  // this CTA's bucket counts, then its cursors
     const int rank = (int)cluster.block_rank(), nrank = (int)cluster.num_blocks();
     const int tid = rank * kColorThreads + threadIdx.x, nth = nrank * kColorThreads;
     const int P = hdr->n_pairs;
@@ -624,7 +668,7 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
                  0, claim0);
     }
     cluster.sync();
-    int r = 0;
+    int r = 0, my_ncol = 0;
     bool done = false;
     for (; r < max_rounds; ++r) {
         const unsigned long long *cur = (r & 1) ? claim1 : claim0;
@@ -636,19 +680,30 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
 #pragma unroll
         for (int k = 0; k < kJPRegPairs; ++k) {
             const int p = tid + k * nth;
-            if (p < P) left += jp_turn(rq[k], p, r, cur, nxt, used, first_fit, pr.col, &s_ncol);
+            if (p < P) left += jp_turn(rq[k], p, r, cur, nxt, used, first_fit, pr.col, my_ncol);
         }
         for (int p = tid + kJPRegPairs * nth; p < P; p += nth) {
             if (pr.col[p] >= 0) continue;
             const int4 st = pstate[p];
             JPPair q{st.x, st.y, -1, (unsigned long long)(unsigned)st.z | ((unsigned long long)(unsigned)st.w << 32)};
-            left += jp_turn(q, p, r, cur, nxt, used, first_fit, pr.col, &s_ncol);
+            left += jp_turn(q, p, r, cur, nxt, used, first_fit, pr.col, my_ncol);
         }
-        if (left) atomicAdd(&s_left[r % 3], left);
+        // one shared-memory atomic per warp for the count and the colour number
+        left = __reduce_add_sync(0xffffffffu, left);
+        const int wcol = __reduce_max_sync(0xffffffffu, my_ncol);
+        if ((threadIdx.x & 31) == 0) {
+            if (left) atomicAdd(&s_left[r % 3], left);
+            if (wcol > 0) atomicMax(&s_ncol, wcol);
+        }
         cluster.sync();
-        int total = 0;
-        for (int q = 0; q < nrank; ++q) total += *cluster.map_shared_rank(&s_left[r % 3], q);
-        if (total == 0) {
+        // the cluster-wide count: one warp reads the CTAs' counters and shares the sum
+        if (threadIdx.x < 32) {
+            int v = (int)threadIdx.x < nrank ? *cluster.map_shared_rank(&s_left[r % 3], (int)threadIdx.x) : 0;
+            v = __reduce_add_sync(0xffffffffu, v);
+            if (threadIdx.x == 0) s_total[r & 1] = v;
+        }
+        __syncthreads();
+        if (s_total[r & 1] == 0) {
             done = true;
             break;
         }
@@ -669,50 +724,37 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         }
         return;
     }
-    // group by (colour, bucket): counts in rank 0's shared memory, scanned there, then cursors
-    int *hist0 = cluster.map_shared_rank(s_hist, 0);
+    // group by (colour, bucket).  Each CTA counts its own pairs in its shared memory; the bucket
+    // starts are a scan of the cluster-wide totals, and a CTA's cursors start after the pairs of
+    // the same bucket held by the lower ranks.  (The order inside a bucket is free: the pairs of
+    // a colour share no dynamic body.)
+    const int E = ncol * kColorSub;
+    int *s_hist = s_dyn, *s_cur = s_dyn + kMaxColorsCap * kColorSub;
+    for (int k = threadIdx.x; k < E; k += kColorThreads) s_hist[k] = 0;
+    __syncthreads();
+    for (int p = tid; p < P; p += nth) atomicAdd(&s_hist[color_bucket(pr, p)], 1);
+    cluster.sync();
+    for (int k = threadIdx.x; k < E; k += kColorThreads) {
+        int t = 0;
+        for (int q = 0; q < nrank; ++q) t += cluster.map_shared_rank(s_hist, q)[k];
+        s_cur[k] = t;
+    }
+    __syncthreads();
+    block_exclusive_scan(s_cur, E);
     if (rank == 0)
-        for (int k = threadIdx.x; k < ncol * kColorSub; k += kColorThreads) s_hist[k] = 0;
-    cluster.sync();
-    for (int p = tid; p < P; p += nth) {
-        const int n = min(max(pr.kcount[p], 1), 8);
-        atomicAdd(hist0 + pr.col[p] * kColorSub + (8 - n) * 2 + (pr.pbj[p] >= 0 ? 1 : 0), 1);
-    }
-    cluster.sync();
-    if (rank == 0) {
-        __shared__ int s_ctot[kMaxColorsCap];
         for (int c = threadIdx.x; c < ncol; c += kColorThreads) {
-            int t = 0;
-            for (int k = 0; k < kColorSub; ++k) t += s_hist[c * kColorSub + k];
-            s_ctot[c] = t;
+            const int st = s_cur[c * kColorSub];
+            pr.cstart[c] = st;
+            pr.ccount[c] = (c + 1 < ncol ? s_cur[(c + 1) * kColorSub] : P) - st;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int c = 0; c < ncol; ++c) {
-                const int t = s_ctot[c];
-                s_ctot[c] = acc;
-                acc += t;
-            }
-        }
-        __syncthreads();
-        for (int c = threadIdx.x; c < ncol; c += kColorThreads) {
-            int acc = s_ctot[c];
-            pr.cstart[c] = acc;
-            for (int k = 0; k < kColorSub; ++k) {
-                const int t = s_hist[c * kColorSub + k];
-                s_hist[c * kColorSub + k] = acc;
-                acc += t;
-            }
-            pr.ccount[c] = acc - s_ctot[c];
-        }
+    __syncthreads();
+    for (int k = threadIdx.x; k < E; k += kColorThreads) {
+        int t = 0;
+        for (int q = 0; q < rank; ++q) t += cluster.map_shared_rank(s_hist, q)[k];
+        s_cur[k] += t;
     }
-    cluster.sync();
-    for (int p = tid; p < P; p += nth) {
-        const int n = min(max(pr.kcount[p], 1), 8);
-        const int slot = atomicAdd(hist0 + pr.col[p] * kColorSub + (8 - n) * 2 + (pr.pbj[p] >= 0 ? 1 : 0), 1);
-        pr.porder[slot] = p;
-    }
+    __syncthreads();
+    for (int p = tid; p < P; p += nth) pr.porder[atomicAdd(&s_cur[color_bucket(pr, p)], 1)] = p;
     if (use_cache) {
         for (int p = tid; p < P; p += nth) {
             pr.cached_a[p] = pr.pbi[p];
@@ -729,7 +771,7 @@ __global__ void __launch_bounds__(kColorThreads) k_color_pairs(b2c_header *hdr, 
         pr.cache_state[2] = 1;
         if (use_cache) pr.cache_state[4] += 1;  // cumulative misses ([3] counts hits)
     }
-    cluster.sync();  // rank 0's shared cursors stay alive until every CTA is done with them
+    cluster.sync();  // every CTA's counts stay alive until the others are done reading them
 }
 
 // largest power-of-two cluster (<= 16) of colouring CTAs the device co-schedules; cached
@@ -738,9 +780,11 @@ static int color_cluster_size()
     static int cached = -1;
     if (cached < 0) {
         cudaFuncSetAttribute(k_color_pairs, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(k_color_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, kColorDynSmem);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kColorClusterMax);
         cfg.blockDim = dim3(kColorThreads);
+        cfg.dynamicSmemBytes = kColorDynSmem;
         int cs = 0;
         if (cudaOccupancyMaxPotentialClusterSize(&cs, k_color_pairs, &cfg) != cudaSuccess) {
             cudaGetLastError();
@@ -856,6 +900,7 @@ int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_c
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs);
     cfg.blockDim = dim3(kColorThreads);
+    cfg.dynamicSmemBytes = kColorDynSmem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
