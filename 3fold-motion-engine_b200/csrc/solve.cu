@@ -301,6 +301,64 @@ __device__ __forceinline__ bool solve_barrier(const SolveArgs &a)
     return s_ok != 0;
 }
 
+// The same barriers split into an arrive and a wait, so that a thread can issue loads that do
+// not depend on the other CTAs' work of the phase (its next task's fixed record words) in
+// between.  The grid form's arrive count and generation are the solve_barrier's.
+struct BarTok {
+    unsigned int gen;
+};
+template <int kKind>
+__device__ __forceinline__ BarTok bar_arrive(const SolveArgs &a)
+{
+    BarTok tok{0u};
+    if (kKind == kCluster) {
+        asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
+    } else if (kKind == kGrid) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tok.gen = *(volatile unsigned int *)a.bar_gen;
+            __threadfence();
+            const unsigned int prev = atomicAdd(a.bar_count, 1u);
+            if (prev == gridDim.x - 1) {
+                atomicExch(a.bar_count, 0u);
+                __threadfence();
+                atomicAdd(a.bar_gen, 1u);
+            }
+        }
+    }
+    return tok;
+}
+template <int kKind>
+__device__ __forceinline__ bool bar_wait(const SolveArgs &a, BarTok tok)
+{
+    if (kKind == kBlock) {
+        __syncthreads();
+        return true;
+    }
+    if (kKind == kCluster) {
+        asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
+        return true;
+    }
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned long long t0 = global_ns();
+        while (*(volatile unsigned int *)a.bar_gen == tok.gen) {
+            if (global_ns() - t0 > (unsigned long long)a.timeout_ns) {
+                atomicOr(a.err, B2C_ERR_BARRIER_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        if (*(volatile int *)a.err & B2C_ERR_BARRIER_TIMEOUT) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // ---------------------------------------------------------------------------------------------
 // one pair record of a colour.  The contact loop is software-pipelined: contact k+1's record is
 // loaded before contact k is computed, and contact 0's together with the pair's header, so a
@@ -614,14 +672,32 @@ __device__ __forceinline__ m3 load_inertia(const Records &R, int s, int f0)
 {
     return m3{xyz(R.body(f0)[s]), xyz(R.body(f0 + 1)[s]), xyz(R.body(f0 + 2)[s])};
 }
+// The words of a task that stay fixed during the solve (header, masses, inertia rows) in
+// registers, and its first kRowBatch contacts on their way into the staging area.  Issued either
+// at the start of the task or, for a thread's first task of the next phase, between the arrive
+// and the wait of the barrier before it.
+struct RowPre {
+    int4 h;
+    float4 mm;
+    m3 IA, IB;
+};
+__device__ __forceinline__ RowPre row_pre(const Records &R, int s, bool pos)
+{
+    stage_rows(R, s, 0, pos);
+    RowPre q;
+    q.h = R.hdr()[s];
+    q.mm = R.body(6)[s];
+    q.IA = load_inertia(R, s, 0);
+    q.IB = load_inertia(R, s, 3);
+    return q;
+}
 
 template <class BA>
-__device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS)
+__device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS, const RowPre &pre)
 {
-    stage_rows(a.rec, s, 0, false);
-    const int4 h = a.rec.hdr()[s];
-    const float4 mm = a.rec.body(6)[s];
-    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
+    const int4 h = pre.h;
+    const float4 mm = pre.mm;
+    const m3 &IA = pre.IA, &IB = pre.IB;
     const int A = h.x, B = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y;
     f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
@@ -669,12 +745,11 @@ __device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS)
 }
 
 template <class BA>
-__device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B)
+__device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B, const RowPre &pre)
 {
-    stage_rows(a.rec, s, 0, false);
-    const int4 h = a.rec.hdr()[s];
-    const float4 mm = a.rec.body(6)[s];
-    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
+    const int4 h = pre.h;
+    const float4 mm = pre.mm;
+    const m3 &IA = pre.IA, &IB = pre.IB;
     const int bi = h.x, bj = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y, mu = mm.z;
     f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
@@ -760,12 +835,11 @@ __device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B)
 }
 
 template <class BA>
-__device__ void pair_position_row(const SolveArgs &a, int s, const BA &B)
+__device__ void pair_position_row(const SolveArgs &a, int s, const BA &B, const RowPre &pre)
 {
-    stage_rows(a.rec, s, 0, true);
-    const int4 h = a.rec.hdr()[s];
-    const float4 mm = a.rec.body(6)[s];
-    const m3 IA = load_inertia(a.rec, s, 0), IB = load_inertia(a.rec, s, 3);
+    const int4 h = pre.h;
+    const float4 mm = pre.mm;
+    const m3 &IA = pre.IA, &IB = pre.IB;
     const int bi = h.x, bj = h.y, n = h.z;
     const float iMA = mm.x, iMB = mm.y;
     f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
@@ -858,23 +932,88 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
             const int s0 = s_cstart[ci], cnt = s_ccount[ci];
             const int nv = vel ? cnt : 0, ntask = nv + (pos ? cnt : 0);
             for (int t = me; t < ntask; t += nth) {
-                if (kRow) {
-                    if (t < nv) {
-                        if (warm) pair_apply_warm_row(a, s0 + t, B);
-                        else pair_velocity_row(a, s0 + t, B);
-                    } else {
-                        pair_position_row(a, s0 + (t - nv), B);
-                    }
+                if (t < nv) {
+                    if (warm) pair_apply_warm(a, s0 + t, B);
+                    else pair_velocity<BA, kFixed>(a, s0 + t, B);
                 } else {
-                    if (t < nv) {
-                        if (warm) pair_apply_warm(a, s0 + t, B);
-                        else pair_velocity<BA, kFixed>(a, s0 + t, B);
-                    } else {
-                        pair_position(a, s0 + (t - nv), B);
-                    }
+                    pair_position(a, s0 + (t - nv), B);
                 }
             }
             if (!solve_barrier<kKind>(a)) return;
+        }
+    }
+}
+
+// The row form's phases.  Task layout of a colour of cnt pairs: velocity (or warm) tasks
+// [0, cnt) and position tasks [P0, P0 + cnt) with P0 = cnt rounded up to a warp, in every pass
+// (a pass without the velocity sweep leaves [0, P0) idle).  So no warp mixes the two kinds,
+// and a pair's velocity task and its position task each stay on one thread in every pass: the
+// impulse words a task reads are written only by the thread that runs it.  A thread's first
+// task of the next phase has its fixed words loaded between the barrier's arrive and wait.
+// Those words do not change during the solve, and its contact words were last written by this
+// same thread.  With a single colour the next phase revisits this phase's pairs, so nothing is
+// prefetched then.
+template <int kKind, class BA>
+__device__ __forceinline__ void solve_body_row(const SolveArgs &a, const BA &B)
+{
+    const int nc = a.hdr->n_colors;
+    if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
+    __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors];
+    for (int c = threadIdx.x; c < nc && c < kMaxSolveColors; c += blockDim.x) {
+        s_cstart[c] = a.cstart[c];
+        s_ccount[c] = a.ccount[c];
+    }
+    __syncthreads();
+    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
+    const int me = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);  // task slot
+    const int vpasses = (a.apply_warm ? 1 : 0) + a.vit;
+    const int passes = vpasses > a.pit ? vpasses : a.pit;
+    // task t of phase (pass, ci): its record slot, or -1 for none; pos tells the kind
+    auto task_slot = [&](int pass, int ci, int t, bool &pos) -> int {
+        const int cnt = s_ccount[ci], p0 = (cnt + 31) & ~31;
+        if (t < cnt) {
+            pos = false;
+            return pass < vpasses ? s_cstart[ci] + t : -1;
+        }
+        pos = true;
+        return (pass < a.pit && t >= p0 && t < p0 + cnt) ? s_cstart[ci] + (t - p0) : -1;
+    };
+    RowPre pre;
+    int pre_t = -1;
+    bool pos;
+    {
+        const int sl = task_slot(0, 0, me, pos);
+        if (sl >= 0) {
+            pre = row_pre(a.rec, sl, pos);
+            pre_t = me;
+        }
+    }
+    for (int pass = 0; pass < passes; ++pass) {
+        const bool warm = a.apply_warm && pass == 0;
+        for (int ci = 0; ci < nc; ++ci) {
+            const int cnt = s_ccount[ci], ntask = ((cnt + 31) & ~31) + cnt;
+            for (int t = me; t < ntask; t += nth) {
+                const int sl = task_slot(pass, ci, t, pos);
+                if (sl < 0) continue;
+                const RowPre q = (t == pre_t) ? pre : row_pre(a.rec, sl, pos);
+                if (!pos) {
+                    if (warm) pair_apply_warm_row(a, sl, B, q);
+                    else pair_velocity_row(a, sl, B, q);
+                } else {
+                    pair_position_row(a, sl, B, q);
+                }
+            }
+            pre_t = -1;
+            const BarTok tok = bar_arrive<kKind>(a);
+            const int np = ci + 1 < nc ? pass : pass + 1, nci = ci + 1 < nc ? ci + 1 : 0;
+            if (nc > 1 && np < passes) {
+                const int sl = task_slot(np, nci, me, pos);
+                if (sl >= 0) {
+                    pre = row_pre(a.rec, sl, pos);
+                    pre_t = me;
+                }
+            }
+            if (!bar_wait<kKind>(a, tok)) return;
         }
     }
 }
@@ -883,17 +1022,17 @@ constexpr int kClusterThreads = 512;     // reference form
 constexpr int kClusterThreadsRow = 384;  // row form (123 registers; 120 KB of contact staging)
 constexpr int kClusterMax = 16;
 
-__global__ void __launch_bounds__(256) k_color_solve_block(SolveArgs a)
+__global__ void __launch_bounds__(256, 1) k_color_solve_block(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.row) solve_body<kBlock, true, true>(a, B);
+    if (a.row) solve_body_row<kBlock>(a, B);
     else if (a.fixed_frame) solve_body<kBlock, true, false>(a, B);
     else solve_body<kBlock, false, false>(a, B);
 }
-__global__ void __launch_bounds__(256) k_color_solve_grid(SolveArgs a)
+__global__ void __launch_bounds__(256, 1) k_color_solve_grid(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.row) solve_body<kGrid, true, true>(a, B);
+    if (a.row) solve_body_row<kGrid>(a, B);
     else if (a.fixed_frame) solve_body<kGrid, true, false>(a, B);
     else solve_body<kGrid, false, false>(a, B);
 }
@@ -909,7 +1048,7 @@ __global__ void __launch_bounds__(kClusterThreads) k_color_solve_cluster(SolveAr
 __global__ void __launch_bounds__(kClusterThreadsRow) k_color_solve_cluster_row(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    solve_body<kCluster, true, true>(a, B);
+    solve_body_row<kCluster>(a, B);
 }
 
 // dynamic shared memory of a solve launch: the row form's contact staging
