@@ -619,6 +619,7 @@ __device__ void pair_position(const SolveArgs &a, int s, const BA &B)
 // trips (record, then the bodies' velocities) however many contacts it has.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ f3 fma3s(float s, f3 a, f3 b) { return f3{fmaf(s, a.x, b.x), fmaf(s, a.y, b.y), fmaf(s, a.z, b.z)}; }
+__device__ __forceinline__ f3 sel3(bool c, f3 a, f3 b) { return f3{c ? a.x : b.x, c ? a.y : b.y, c ? a.z : b.z}; }
 
 struct RowC {
     float4 n, ra, rb, t1, im;
@@ -772,56 +773,55 @@ __device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B, const 
             const RowResp kA = row_responses(IA, rA, nrm, t1, t2);
             RowResp kB{};
             if (bj >= 0) kB = row_responses(IB, rB, nrm, t1, t2);
+            // The guarded updates below are written as selects of the updated and the old value
+            // (exactly the values of the branches they replace), so the chain has no branches
+            // but the friction clamp's.
+            const bool hasB = bj >= 0, dynA = iMA > 0.0f, dynB = hasB && iMB > 0.0f;
+            const bool act = cur.n.w > 0.0f, fric = cur.t1.w > 0.0f && cur.rb.w > 0.0f;
+            const f3 zero{0.0f, 0.0f, 0.0f};
             f3 va = add3(vA, cross3(wA, rA));
-            f3 vb{0.0f, 0.0f, 0.0f};
-            if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+            f3 vb = sel3(hasB, add3(vB, cross3(wB, rB)), zero);
             f3 vrel = sub3(va, vb);
             const float vn = dot3(vrel, nrm);
-            if (cur.n.w > 0.0f) {
-                float4 im = cur.im;
-                float dj = -vn * cur.n.w;
-                const float nw = fmaxf(0.0f, im.x + dj);
-                dj = nw - im.x;
-                im.x = nw;
-                const f3 Jn = scale3(nrm, dj);
-                if (iMA > 0.0f) {
-                    vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
-                    wA = fma3s(dj, kA.n, wA);
-                }
-                if (bj >= 0 && iMB > 0.0f) {
-                    vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
-                    wB = fma3s(-dj, kB.n, wB);
-                }
-                va = add3(vA, cross3(wA, rA));
-                vb = f3{0.0f, 0.0f, 0.0f};
-                if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-                vrel = sub3(va, vb);
-                if (cur.t1.w > 0.0f && cur.rb.w > 0.0f) {
-                    const float o1 = im.y, o2 = im.z;
-                    float a1 = o1 - dot3(vrel, t1) * cur.t1.w;
-                    float a2 = o2 - dot3(vrel, t2) * cur.rb.w;
-                    const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-                    const float lim = mu * im.x;
-                    if (mag > lim && mag > 1e-12f) {
-                        const float sc = lim / mag;
-                        a1 = a1 * sc;
-                        a2 = a2 * sc;
-                    }
-                    im.y = a1;
-                    im.z = a2;
-                    const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
-                    const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
-                    if (iMA > 0.0f) {
-                        vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
-                        wA = fma3s(e1, kA.t1, fma3s(e2, kA.t2, wA));
-                    }
-                    if (bj >= 0 && iMB > 0.0f) {
-                        vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
-                        wB = fma3s(-e1, kB.t1, fma3s(-e2, kB.t2, wB));
-                    }
-                }
-                store_imp_xyz(&a.rec.contact(kRImp, k0 + j)[s], im);
+            float4 im = cur.im;
+            float dj = -vn * cur.n.w;
+            const float nw = fmaxf(0.0f, im.x + dj);
+            dj = nw - im.x;
+            im.x = nw;
+            const f3 Jn = scale3(nrm, dj);
+            const f3 vA1 = sel3(dynA, f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)}, vA);
+            const f3 wA1 = sel3(dynA, fma3s(dj, kA.n, wA), wA);
+            const f3 vB1 = sel3(dynB, f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)}, vB);
+            const f3 wB1 = sel3(dynB, fma3s(-dj, kB.n, wB), wB);
+            va = add3(vA1, cross3(wA1, rA));
+            vb = sel3(hasB, add3(vB1, cross3(wB1, rB)), zero);
+            vrel = sub3(va, vb);
+            const float o1 = im.y, o2 = im.z;
+            float a1 = o1 - dot3(vrel, t1) * cur.t1.w;
+            float a2 = o2 - dot3(vrel, t2) * cur.rb.w;
+            const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+            const float lim = mu * im.x;
+            if (fric && mag > lim && mag > 1e-12f) {
+                const float sc = lim / mag;
+                a1 = a1 * sc;
+                a2 = a2 * sc;
             }
+            const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+            const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+            const bool fA = fric && dynA, fB = fric && dynB;
+            const f3 vA2 = sel3(fA, f3{fmaf(Jt.x, iMA, vA1.x), fmaf(Jt.y, iMA, vA1.y), fmaf(Jt.z, iMA, vA1.z)}, vA1);
+            const f3 wA2 = sel3(fA, fma3s(e1, kA.t1, fma3s(e2, kA.t2, wA1)), wA1);
+            const f3 vB2 = sel3(fB, f3{fmaf(-Jt.x, iMB, vB1.x), fmaf(-Jt.y, iMB, vB1.y), fmaf(-Jt.z, iMB, vB1.z)}, vB1);
+            const f3 wB2 = sel3(fB, fma3s(-e1, kB.t1, fma3s(-e2, kB.t2, wB1)), wB1);
+            if (fric) {
+                im.y = a1;
+                im.z = a2;
+            }
+            vA = sel3(act, vA2, vA);
+            wA = sel3(act, wA2, wA);
+            vB = sel3(act, vB2, vB);
+            wB = sel3(act, wB2, wB);
+            if (act) store_imp_xyz(&a.rec.contact(kRImp, k0 + j)[s], im);
         }
     }
     if (iMA > 0.0f) {
