@@ -862,23 +862,20 @@ __device__ void pair_position_row(const SolveArgs &a, int s, const BA &B, const 
             const f3 kAn = matvec(IA, cross3(rA, nrm));
             f3 kBn{0.0f, 0.0f, 0.0f};
             if (bj >= 0) kBn = matvec(IB, cross3(rB, nrm));
+            // selects of the updated and the old values, as in the velocity chunk
+            const bool hasB = bj >= 0, act = wn.w > 0.0f;
+            const bool uA = act && iMA > 0.0f, uB = act && hasB && iMB > 0.0f;
             f3 rel = add3(pvA, cross3(poA, rA));
-            if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
-            if (wn.w > 0.0f) {
-                float dj = (wa.w - dot3(rel, nrm)) * wn.w;
-                const float nw = fmaxf(0.0f, jp + dj);
-                dj = nw - jp;
-                store_imp_w(&a.rec.contact(kRImp, k0 + j)[s], nw);
-                const f3 Jn = scale3(nrm, dj);
-                if (iMA > 0.0f) {
-                    pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
-                    poA = fma3s(dj, kAn, poA);
-                }
-                if (bj >= 0 && iMB > 0.0f) {
-                    pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
-                    poB = fma3s(-dj, kBn, poB);
-                }
-            }
+            rel = sel3(hasB, sub3(rel, add3(pvB, cross3(poB, rB))), rel);
+            float dj = (wa.w - dot3(rel, nrm)) * wn.w;
+            const float nw = fmaxf(0.0f, jp + dj);
+            dj = nw - jp;
+            if (act) store_imp_w(&a.rec.contact(kRImp, k0 + j)[s], nw);
+            const f3 Jn = scale3(nrm, dj);
+            pvA = sel3(uA, f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)}, pvA);
+            poA = sel3(uA, fma3s(dj, kAn, poA), poA);
+            pvB = sel3(uB, f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)}, pvB);
+            poB = sel3(uB, fma3s(-dj, kBn, poB), poB);
         }
     }
     if (iMA > 0.0f) {
