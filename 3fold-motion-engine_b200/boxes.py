@@ -218,13 +218,6 @@ class BoxContactEngine(_BeadEngineBase):
     def color_cache_misses(self):
         return int(self.p_bufs["cache_state"][4].item()) if self._built else 0
 
-    def set_body_state(self, xc, q, v, w):
-        if not self._built:
-            self._build()
-        for dst, src, k in ((self.xc, xc, 3), (self.q, q, 4), (self.v, v, 3), (self.w, w, 3)):
-            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float32))
-            dst[:, :k].copy_(t, non_blocking=True)
-
     # staged substep with CUDA events (profiling); same launches as b2c_box_substep
     STAGES = ("predict", "candidates", "narrowphase", "colour", "solve", "warm_store", "integrate")
 

@@ -285,6 +285,16 @@ class _BeadEngineBase:
             self._kinarr[i] = 1
             self._M[i] = np.inf
 
+    # ---- host state I/O ----
+    def set_body_state(self, xc, q, v, w):
+        """Overwrite the body state from host arrays ((N,3), (N,4), (N,3), (N,3) float32; pinned
+        torch tensors are copied asynchronously on the engine's stream)."""
+        if not self._built:
+            self._build()
+        for dst, src, k in ((self.xc, xc, 3), (self.q, q, 4), (self.v, v, 3), (self.w, w, 3)):
+            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float32))
+            dst[:, :k].copy_(t, non_blocking=True)
+
     # ---- data out ----
     def get_state(self) -> BodyState:
         if not self._built:

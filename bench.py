@@ -42,9 +42,6 @@ WORKLOADS = {
     "boxes10k": dict(engine="box", scene="random_boxes", n=10000, edge=(0.2, 0.6), box=(20.0, 20.0, 10.0),
                      mu_range=(0.3, 0.8), density=1000.0, vit=16, pit=10, substeps=2, dt=1 / 240, color_cap=32,
                      preroll=300, steps=300, warmup=3),
-    # the reference's ColorCache timing fixture (reports/innovation_stack_color_cache_l4.json):
-    # lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5, 40 velocity / 20 position sweeps,
-    # 1 substep, dt 1/240
     # stress: 100 000 cubes of edge 0.25 on a seeded, jittered lattice in 50 x 50 x 10 m, mu 0.6,
     # 2 substeps x (16 velocity + 16 position sweeps), broadphase rebuilt every substep, 200 steps
     "stress100k": dict(engine="box", scene="box_lattice", n=100000, edge=(0.25, 0.25), box=(50.0, 50.0, 10.0),
@@ -55,10 +52,20 @@ WORKLOADS = {
     "batched512": dict(engine="batched", scene="batched", n_scenes=512, nmin=8, nmax=2000, edge=(0.2, 0.6),
                        mu_range=(0.3, 0.8), density=1000.0, vit=16, pit=10, substeps=2, dt=1 / 240, color_cap=32,
                        preroll=300, steps=100, warmup=3),
+    # the reference's ColorCache timing fixture: lattice(10000) of (0.3, 0.3, 0.2) bead boxes, mu 0.5,
+    # 40 velocity / 20 position sweeps, 1 substep, dt 1/240 (87 716 raw -> 40 000 kept contacts,
+    # 10 000 pairs, 2 colours); published: 3.684 ms per step on an NVIDIA L4
+    # (reports/innovation_stack_color_cache_l4.json, "timing")
     "colorcache_lattice10k": dict(engine="color_cache", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5,
-                                  vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20),
+                                  vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
+                                  published=(1e4 / 3.684e-3, "reference ColorCache, 3.684 ms/step, NVIDIA L4 "
+                                             "(reports/innovation_stack_color_cache_l4.json)")),
+    # the same lattice under relaxed Jacobi; published: 5.599 ms per step at N = 10 000 on an RTX 5070
+    # (docs/RUNNING.md:374-379)
     "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
-                              pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20),
+                              pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
+                              published=(1e4 / 5.599e-3, "reference relaxed Jacobi, 5.599 ms/step, RTX 5070 "
+                                         "(docs/RUNNING.md:374-379)")),
 }
 DEFAULT_WORKLOAD = "boxes10k"
 
@@ -577,7 +584,8 @@ def main():
                    color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3")
     line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "strong" if wl["engine"] == "batched" else "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "strong" if wl["engine"] == "batched" else "weak",
+            "vs_baseline": value / wl["published"][0] if "published" in wl else None, "dtype": "f32",
             "data": "synthetic (seeded scene builders)", "config": cfg,
             "clocks": clk.summary(),
             "e2e": {"value": n_job * K2 / (e2e_ms / 1e3), "unit": "body-steps/s",
@@ -585,6 +593,8 @@ def main():
             "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
             "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h_end,
             "colors_e2e_steps": {"max": max(colors), "mean": float(np.mean(colors))}}
+    if "published" in wl:
+        line["baseline"] = {"value": wl["published"][0], "unit": "body-steps/s", "source": wl["published"][1]}
     if per_scene is not None:
         line["per_scene_sequential"] = per_scene
         line["batched_over_sequential"] = (N * args.steps / (ms / 1e3)) / per_scene["value"]
