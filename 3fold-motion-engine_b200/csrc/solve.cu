@@ -360,10 +360,7 @@ __device__ __forceinline__ bool bar_wait(const SolveArgs &a, BarTok tok)
 }
 
 // ---------------------------------------------------------------------------------------------
-// one pair record of a colour.  The contact loop is software-pipelined: contact k+1's record is
-// loaded before contact k is computed, and contact 0's together with the pair's header, so a
-// phase pays about two dependent round trips (record, then the bodies' velocities) instead of
-// one per contact.
+// pair tasks
 // ---------------------------------------------------------------------------------------------
 // Body state access through L2 (a policy class, so the pair physics is written once).
 struct GlobalBodies {
@@ -379,35 +376,6 @@ struct GlobalBodies {
         stcg4(p, b, f4(x, 0.0f));
     }
 };
-struct PairBodies {
-    int bi, bj, n;
-    m3 IA, IB;
-    float iMA, iMB, mu;
-};
-__device__ __forceinline__ PairBodies load_pair(const Records &R, int s)
-{
-    PairBodies q;
-    const int4 h = R.hdr()[s];
-    q.bi = h.x;
-    q.bj = h.y;
-    q.n = h.z;
-    const float4 i0 = R.body(0)[s], i1 = R.body(1)[s], i2 = R.body(2)[s];
-    const float4 j0 = R.body(3)[s], j1 = R.body(4)[s], j2 = R.body(5)[s], mm = R.body(6)[s];
-    q.IA = m3{xyz(i0), xyz(i1), xyz(i2)};
-    q.IB = m3{xyz(j0), xyz(j1), xyz(j2)};
-    q.iMA = mm.x;
-    q.iMB = mm.y;
-    q.mu = mm.z;
-    return q;
-}
-struct CRec {
-    float4 n, ra, rb, t1, im;
-};
-__device__ __forceinline__ CRec load_contact(const Records &R, int s, int k)
-{
-    return CRec{R.contact(kCN, k)[s], R.contact(kCRA, k)[s], R.contact(kCRB, k)[s], R.contact(kCT1, k)[s],
-                R.contact(kCImp, k)[s]};
-}
 
 // The impulse word of a contact is (jn, jt1, jt2, jp).  A phase can run the velocity chunk and
 // the position chunk of the same pair on two threads (they read and write disjoint state), so the
@@ -419,197 +387,6 @@ __device__ __forceinline__ void store_imp_xyz(float4 *p, float4 im)
     f[2] = im.z;
 }
 __device__ __forceinline__ void store_imp_w(float4 *p, float jp) { reinterpret_cast<float *>(p)[3] = jp; }
-
-// apply_warm, contact_engine_gpu_applied_warm.py:5-54
-template <class BA>
-__device__ void pair_apply_warm(const SolveArgs &a, int s, const BA &BS)
-{
-    const PairBodies q = load_pair(a.rec, s);
-    CRec cur = load_contact(a.rec, s, 0);
-    const int A = q.bi, B = q.bj;
-    f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
-    if (B >= 0) {
-        vb = BS.get(B, 0);
-        wb = BS.get(B, 1);
-    }
-    for (int k = 0; k < q.n; ++k) {
-        CRec nxt;
-        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
-        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb), t1 = xyz(cur.t1);
-        const f3 t2 = cross3(nrm, t1);
-        const float4 im = cur.im;
-        const f3 J{fmaf(im.z, t2.x, fmaf(im.x, nrm.x, im.y * t1.x)), fmaf(im.z, t2.y, fmaf(im.x, nrm.y, im.y * t1.y)),
-                   fmaf(im.z, t2.z, fmaf(im.x, nrm.z, im.y * t1.z))};
-        if (q.iMA > 0.0f) {
-            va = f3{fmaf(q.iMA, J.x, va.x), fmaf(q.iMA, J.y, va.y), fmaf(q.iMA, J.z, va.z)};
-            wa = add3(wa, matvec(q.IA, cross3(rA, J)));
-        }
-        if (B >= 0 && q.iMB > 0.0f) {
-            vb = f3{fmaf(-q.iMB, J.x, vb.x), fmaf(-q.iMB, J.y, vb.y), fmaf(-q.iMB, J.z, vb.z)};
-            wb = sub3(wb, matvec(q.IB, cross3(rB, J)));
-        }
-        cur = nxt;
-    }
-    if (q.iMA > 0.0f) {
-        BS.set(A, 0, va);
-        BS.set(A, 1, wa);
-    }
-    if (B >= 0 && q.iMB > 0.0f) {
-        BS.set(B, 0, vb);
-        BS.set(B, 1, wb);
-    }
-}
-
-// velocity chunk: k_fixed_frame (fixed_frame.py:7-77) or k_chunk_vel_r (COL:413-490)
-template <class BA, bool kFixed>
-__device__ void pair_velocity(const SolveArgs &a, int s, const BA &B)
-{
-    const PairBodies q = load_pair(a.rec, s);
-    CRec cur = load_contact(a.rec, s, 0);
-    const int bi = q.bi, bj = q.bj;
-    const float iMA = q.iMA, iMB = q.iMB;
-    f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
-    f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) {
-        vB = B.get(bj, 0);
-        wB = B.get(bj, 1);
-    }
-    for (int k = 0; k < q.n; ++k) {
-        CRec nxt;
-        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
-        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
-        const float meff = cur.ra.w;
-        f3 va = add3(vA, cross3(wA, rA));
-        f3 vb{0.0f, 0.0f, 0.0f};
-        if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-        f3 vrel = sub3(va, vb);
-        const float vn = dot3(vrel, nrm);
-        f3 t1 = xyz(cur.t1);
-        f3 t2 = cross3(nrm, t1);
-        float meft1 = cur.rb.w, meft2 = cur.t1.w;
-        if (!kFixed) {
-            const f3 vt{fmaf(-vn, nrm.x, vrel.x), fmaf(-vn, nrm.y, vrel.y), fmaf(-vn, nrm.z, vrel.z)};
-            const float mt = len3(vt);
-            if (!(mt <= 5e-3f)) {  // slip basis t1 = vt / |vt|; otherwise the axis frame of the record
-                t1 = div3(vt, mt);
-                t2 = cross3(nrm, t1);
-                const f3 rtA1 = cross3(rA, t1);
-                meft1 = iMA + dot3(rtA1, matvec(q.IA, rtA1));
-                const f3 rtA2 = cross3(rA, t2);
-                meft2 = iMA + dot3(rtA2, matvec(q.IA, rtA2));
-                if (bj >= 0) {
-                    const f3 rtB1 = cross3(rB, t1);
-                    meft1 = (meft1 + iMB) + dot3(rtB1, matvec(q.IB, rtB1));
-                    const f3 rtB2 = cross3(rB, t2);
-                    meft2 = (meft2 + iMB) + dot3(rtB2, matvec(q.IB, rtB2));
-                }
-            }
-        }
-        if (meff >= 1e-12f) {
-            float4 im = cur.im;
-            float dj = -vn / meff;
-            const float nw = fmaxf(0.0f, im.x + dj);
-            dj = nw - im.x;
-            im.x = nw;
-            const f3 Jn = scale3(nrm, dj);
-            if (iMA > 0.0f) {
-                vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
-                wA = add3(wA, matvec(q.IA, cross3(rA, Jn)));
-            }
-            if (bj >= 0 && iMB > 0.0f) {
-                vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
-                wB = sub3(wB, matvec(q.IB, cross3(rB, Jn)));
-            }
-            va = add3(vA, cross3(wA, rA));
-            vb = f3{0.0f, 0.0f, 0.0f};
-            if (bj >= 0) vb = add3(vB, cross3(wB, rB));
-            vrel = sub3(va, vb);
-            if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
-                const float o1 = im.y, o2 = im.z;
-                float a1 = o1 - dot3(vrel, t1) / meft1;
-                float a2 = o2 - dot3(vrel, t2) / meft2;
-                const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
-                const float lim = q.mu * im.x;
-                if (mag > lim && mag > 1e-12f) {
-                    a1 = a1 * lim / mag;
-                    a2 = a2 * lim / mag;
-                }
-                im.y = a1;
-                im.z = a2;
-                const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
-                const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
-                if (iMA > 0.0f) {
-                    vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
-                    wA = add3(wA, matvec(q.IA, cross3(rA, Jt)));
-                }
-                if (bj >= 0 && iMB > 0.0f) {
-                    vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
-                    wB = sub3(wB, matvec(q.IB, cross3(rB, Jt)));
-                }
-            }
-            store_imp_xyz(&a.rec.contact(kCImp, k)[s], im);
-        }
-        cur = nxt;
-    }
-    if (iMA > 0.0f) {
-        B.set(bi, 0, vA);
-        B.set(bi, 1, wA);
-    }
-    if (bj >= 0 && iMB > 0.0f) {
-        B.set(bj, 0, vB);
-        B.set(bj, 1, wB);
-    }
-}
-
-// position chunk, k_chunk_pos_r (COL:510-554)
-template <class BA>
-__device__ void pair_position(const SolveArgs &a, int s, const BA &B)
-{
-    const PairBodies q = load_pair(a.rec, s);
-    CRec cur = load_contact(a.rec, s, 0);
-    const int bi = q.bi, bj = q.bj;
-    const float iMA = q.iMA, iMB = q.iMB;
-    f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
-    f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
-    if (bj >= 0) {
-        pvB = B.get(bj, 2);
-        poB = B.get(bj, 3);
-    }
-    for (int k = 0; k < q.n; ++k) {
-        CRec nxt;
-        if (k + 1 < q.n) nxt = load_contact(a.rec, s, k + 1);
-        const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
-        f3 rel = add3(pvA, cross3(poA, rA));
-        if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
-        const float meff = cur.ra.w;
-        if (meff >= 1e-12f) {
-            const float bias = B2C_BETA * fmaxf(cur.n.w - B2C_SLOP, 0.0f) / a.dt;
-            float dj = (bias - dot3(rel, nrm)) / meff;
-            const float jp = cur.im.w;
-            const float nw = fmaxf(0.0f, jp + dj);
-            dj = nw - jp;
-            store_imp_w(&a.rec.contact(kCImp, k)[s], nw);
-            const f3 Jn = scale3(nrm, dj);
-            if (iMA > 0.0f) {
-                pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
-                poA = add3(poA, matvec(q.IA, cross3(rA, Jn)));
-            }
-            if (bj >= 0 && iMB > 0.0f) {
-                pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
-                poB = sub3(poB, matvec(q.IB, cross3(rB, Jn)));
-            }
-        }
-        cur = nxt;
-    }
-    if (iMA > 0.0f) {
-        B.set(bi, 2, pvA);
-        B.set(bi, 3, poA);
-    }
-    if (bj >= 0 && iMB > 0.0f) {
-        B.set(bj, 2, pvB);
-        B.set(bj, 3, poB);
-    }
-}
 
 // ---------------------------------------------------------------------------------------------
 // row form of the three chunks (B2C_COLOR_ROW_FORM; not in the reference): the same sweep with
@@ -691,6 +468,214 @@ __device__ __forceinline__ RowPre row_pre(const Records &R, int s, bool pos)
     q.IA = load_inertia(R, s, 0);
     q.IB = load_inertia(R, s, 3);
     return q;
+}
+
+// apply_warm, contact_engine_gpu_applied_warm.py:5-54.  The reference form's chunks take the
+// pair's fixed words from a RowPre and its contacts from the staging area, as the row form's do
+// (the record layouts share the header, the inertia rows, the masses and the five-word contact).
+template <class BA>
+__device__ void pair_apply_warm(const SolveArgs &a, int s, const BA &BS, const RowPre &pre)
+{
+    const int A = pre.h.x, B = pre.h.y, n = pre.h.z;
+    const float iMA = pre.mm.x, iMB = pre.mm.y;
+    f3 va = BS.get(A, 0), wa = BS.get(A, 1), vb{0.0f, 0.0f, 0.0f}, wb{0.0f, 0.0f, 0.0f};
+    if (B >= 0) {
+        vb = BS.get(B, 0);
+        wb = BS.get(B, 1);
+    }
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, false);
+            cp_async_wait_all();
+        }
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const RowC cur = staged_row(j);
+            const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb), t1 = xyz(cur.t1);
+            const f3 t2 = cross3(nrm, t1);
+            const float4 im = cur.im;
+            const f3 J{fmaf(im.z, t2.x, fmaf(im.x, nrm.x, im.y * t1.x)),
+                       fmaf(im.z, t2.y, fmaf(im.x, nrm.y, im.y * t1.y)),
+                       fmaf(im.z, t2.z, fmaf(im.x, nrm.z, im.y * t1.z))};
+            if (iMA > 0.0f) {
+                va = f3{fmaf(iMA, J.x, va.x), fmaf(iMA, J.y, va.y), fmaf(iMA, J.z, va.z)};
+                wa = add3(wa, matvec(pre.IA, cross3(rA, J)));
+            }
+            if (B >= 0 && iMB > 0.0f) {
+                vb = f3{fmaf(-iMB, J.x, vb.x), fmaf(-iMB, J.y, vb.y), fmaf(-iMB, J.z, vb.z)};
+                wb = sub3(wb, matvec(pre.IB, cross3(rB, J)));
+            }
+        }
+    }
+    if (iMA > 0.0f) {
+        BS.set(A, 0, va);
+        BS.set(A, 1, wa);
+    }
+    if (B >= 0 && iMB > 0.0f) {
+        BS.set(B, 0, vb);
+        BS.set(B, 1, wb);
+    }
+}
+
+// velocity chunk: k_fixed_frame (fixed_frame.py:7-77) or k_chunk_vel_r (COL:413-490)
+template <class BA, bool kFixed>
+__device__ void pair_velocity(const SolveArgs &a, int s, const BA &B, const RowPre &pre)
+{
+    const int bi = pre.h.x, bj = pre.h.y, n = pre.h.z;
+    const float iMA = pre.mm.x, iMB = pre.mm.y, mu = pre.mm.z;
+    const m3 &IA = pre.IA, &IB = pre.IB;
+    f3 vA = B.get(bi, 0), wA = B.get(bi, 1);
+    f3 vB{0.0f, 0.0f, 0.0f}, wB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        vB = B.get(bj, 0);
+        wB = B.get(bj, 1);
+    }
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, false);
+            cp_async_wait_all();
+        }
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const RowC cur = staged_row(j);
+            const f3 nrm = xyz(cur.n), rA = xyz(cur.ra), rB = xyz(cur.rb);
+            const float meff = cur.ra.w;
+            f3 va = add3(vA, cross3(wA, rA));
+            f3 vb{0.0f, 0.0f, 0.0f};
+            if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+            f3 vrel = sub3(va, vb);
+            const float vn = dot3(vrel, nrm);
+            f3 t1 = xyz(cur.t1);
+            f3 t2 = cross3(nrm, t1);
+            float meft1 = cur.rb.w, meft2 = cur.t1.w;
+            if (!kFixed) {
+                const f3 vt{fmaf(-vn, nrm.x, vrel.x), fmaf(-vn, nrm.y, vrel.y), fmaf(-vn, nrm.z, vrel.z)};
+                const float mt = len3(vt);
+                if (!(mt <= 5e-3f)) {  // slip basis t1 = vt / |vt|; otherwise the axis frame of the record
+                    t1 = div3(vt, mt);
+                    t2 = cross3(nrm, t1);
+                    const f3 rtA1 = cross3(rA, t1);
+                    meft1 = iMA + dot3(rtA1, matvec(IA, rtA1));
+                    const f3 rtA2 = cross3(rA, t2);
+                    meft2 = iMA + dot3(rtA2, matvec(IA, rtA2));
+                    if (bj >= 0) {
+                        const f3 rtB1 = cross3(rB, t1);
+                        meft1 = (meft1 + iMB) + dot3(rtB1, matvec(IB, rtB1));
+                        const f3 rtB2 = cross3(rB, t2);
+                        meft2 = (meft2 + iMB) + dot3(rtB2, matvec(IB, rtB2));
+                    }
+                }
+            }
+            if (meff >= 1e-12f) {
+                float4 im = cur.im;
+                float dj = -vn / meff;
+                const float nw = fmaxf(0.0f, im.x + dj);
+                dj = nw - im.x;
+                im.x = nw;
+                const f3 Jn = scale3(nrm, dj);
+                if (iMA > 0.0f) {
+                    vA = f3{fmaf(Jn.x, iMA, vA.x), fmaf(Jn.y, iMA, vA.y), fmaf(Jn.z, iMA, vA.z)};
+                    wA = add3(wA, matvec(IA, cross3(rA, Jn)));
+                }
+                if (bj >= 0 && iMB > 0.0f) {
+                    vB = f3{fmaf(-Jn.x, iMB, vB.x), fmaf(-Jn.y, iMB, vB.y), fmaf(-Jn.z, iMB, vB.z)};
+                    wB = sub3(wB, matvec(IB, cross3(rB, Jn)));
+                }
+                va = add3(vA, cross3(wA, rA));
+                vb = f3{0.0f, 0.0f, 0.0f};
+                if (bj >= 0) vb = add3(vB, cross3(wB, rB));
+                vrel = sub3(va, vb);
+                if (meft1 >= 1e-12f && meft2 >= 1e-12f) {
+                    const float o1 = im.y, o2 = im.z;
+                    float a1 = o1 - dot3(vrel, t1) / meft1;
+                    float a2 = o2 - dot3(vrel, t2) / meft2;
+                    const float mag = sqrtf(fmaf(a1, a1, a2 * a2));
+                    const float lim = mu * im.x;
+                    if (mag > lim && mag > 1e-12f) {
+                        a1 = a1 * lim / mag;
+                        a2 = a2 * lim / mag;
+                    }
+                    im.y = a1;
+                    im.z = a2;
+                    const float e1 = a1 - o1, e2 = a.t2d * (a2 - o2);
+                    const f3 Jt{fmaf(e1, t1.x, e2 * t2.x), fmaf(e1, t1.y, e2 * t2.y), fmaf(e1, t1.z, e2 * t2.z)};
+                    if (iMA > 0.0f) {
+                        vA = f3{fmaf(Jt.x, iMA, vA.x), fmaf(Jt.y, iMA, vA.y), fmaf(Jt.z, iMA, vA.z)};
+                        wA = add3(wA, matvec(IA, cross3(rA, Jt)));
+                    }
+                    if (bj >= 0 && iMB > 0.0f) {
+                        vB = f3{fmaf(-Jt.x, iMB, vB.x), fmaf(-Jt.y, iMB, vB.y), fmaf(-Jt.z, iMB, vB.z)};
+                        wB = sub3(wB, matvec(IB, cross3(rB, Jt)));
+                    }
+                }
+                store_imp_xyz(&a.rec.contact(kCImp, k0 + j)[s], im);
+            }
+        }
+    }
+    if (iMA > 0.0f) {
+        B.set(bi, 0, vA);
+        B.set(bi, 1, wA);
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        B.set(bj, 0, vB);
+        B.set(bj, 1, wB);
+    }
+}
+
+// position chunk, k_chunk_pos_r (COL:510-554)
+template <class BA>
+__device__ void pair_position(const SolveArgs &a, int s, const BA &B, const RowPre &pre)
+{
+    const int bi = pre.h.x, bj = pre.h.y, n = pre.h.z;
+    const float iMA = pre.mm.x, iMB = pre.mm.y;
+    f3 pvA = B.get(bi, 2), poA = B.get(bi, 3);
+    f3 pvB{0.0f, 0.0f, 0.0f}, poB{0.0f, 0.0f, 0.0f};
+    if (bj >= 0) {
+        pvB = B.get(bj, 2);
+        poB = B.get(bj, 3);
+    }
+    cp_async_wait_all();
+    for (int k0 = 0; k0 < n; k0 += kRowBatch) {
+        if (k0 > 0) {
+            stage_rows(a.rec, s, k0, true);
+            cp_async_wait_all();
+        }
+        for (int j = 0; j < kRowBatch; ++j) {
+            if (k0 + j >= n) break;
+            const float4 wn = *stage_word(kCN, j), wa = *stage_word(kCRA, j), wb = *stage_word(kCRB, j);
+            const float jp = stage_word(kCImp, j)->w;
+            const f3 nrm = xyz(wn), rA = xyz(wa), rB = xyz(wb);
+            f3 rel = add3(pvA, cross3(poA, rA));
+            if (bj >= 0) rel = sub3(rel, add3(pvB, cross3(poB, rB)));
+            const float meff = wa.w;
+            if (meff >= 1e-12f) {
+                const float bias = B2C_BETA * fmaxf(wn.w - B2C_SLOP, 0.0f) / a.dt;
+                float dj = (bias - dot3(rel, nrm)) / meff;
+                const float nw = fmaxf(0.0f, jp + dj);
+                dj = nw - jp;
+                store_imp_w(&a.rec.contact(kCImp, k0 + j)[s], nw);
+                const f3 Jn = scale3(nrm, dj);
+                if (iMA > 0.0f) {
+                    pvA = f3{fmaf(Jn.x, iMA, pvA.x), fmaf(Jn.y, iMA, pvA.y), fmaf(Jn.z, iMA, pvA.z)};
+                    poA = add3(poA, matvec(pre.IA, cross3(rA, Jn)));
+                }
+                if (bj >= 0 && iMB > 0.0f) {
+                    pvB = f3{fmaf(-Jn.x, iMB, pvB.x), fmaf(-Jn.y, iMB, pvB.y), fmaf(-Jn.z, iMB, pvB.z)};
+                    poB = sub3(poB, matvec(pre.IB, cross3(rB, Jn)));
+                }
+            }
+        }
+    }
+    if (iMA > 0.0f) {
+        B.set(bi, 2, pvA);
+        B.set(bi, 3, poA);
+    }
+    if (bj >= 0 && iMB > 0.0f) {
+        B.set(bj, 2, pvB);
+        B.set(bj, 3, poB);
+    }
 }
 
 template <class BA>
@@ -905,43 +890,7 @@ __device__ void pair_position_row(const SolveArgs &a, int s, const BA &B, const 
 // ---------------------------------------------------------------------------------------------
 constexpr int kMaxSolveColors = 512;  // the colouring's cap (kMaxColorsCap)
 
-template <int kKind, bool kFixed, bool kRow, class BA>
-__device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
-{
-    const int nc = a.hdr->n_colors;
-    if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
-    // the colour table in shared memory: a phase's first load then depends on nothing
-    __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors];
-    for (int c = threadIdx.x; c < nc && c < kMaxSolveColors; c += blockDim.x) {
-        s_cstart[c] = a.cstart[c];
-        s_ccount[c] = a.ccount[c];
-    }
-    __syncthreads();
-    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
-    const int me = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);  // task slot
-    const int vpasses = (a.apply_warm ? 1 : 0) + a.vit;
-    const int passes = vpasses > a.pit ? vpasses : a.pit;
-    for (int pass = 0; pass < passes; ++pass) {
-        const bool vel = pass < vpasses;
-        const bool warm = a.apply_warm && pass == 0;
-        const bool pos = pass < a.pit;
-        for (int ci = 0; ci < nc; ++ci) {
-            const int s0 = s_cstart[ci], cnt = s_ccount[ci];
-            const int nv = vel ? cnt : 0, ntask = nv + (pos ? cnt : 0);
-            for (int t = me; t < ntask; t += nth) {
-                if (t < nv) {
-                    if (warm) pair_apply_warm(a, s0 + t, B);
-                    else pair_velocity<BA, kFixed>(a, s0 + t, B);
-                } else {
-                    pair_position(a, s0 + (t - nv), B);
-                }
-            }
-            if (!solve_barrier<kKind>(a)) return;
-        }
-    }
-}
-
-// The row form's phases.  Task layout of a colour of cnt pairs: velocity (or warm) tasks
+// The phases of the persistent solve (both forms).  Task layout of a colour of cnt pairs: velocity (or warm) tasks
 // [0, cnt) and position tasks [P0, P0 + cnt) with P0 = cnt rounded up to a warp, in every pass
 // (a pass without the velocity sweep leaves [0, P0) idle).  So no warp mixes the two kinds,
 // and a pair's velocity task and its position task each stay on one thread in every pass: the
@@ -950,8 +899,8 @@ __device__ __forceinline__ void solve_body(const SolveArgs &a, const BA &B)
 // Those words do not change during the solve, and its contact words were last written by this
 // same thread.  With a single colour the next phase revisits this phase's pairs, so nothing is
 // prefetched then.
-template <int kKind, class BA>
-__device__ __forceinline__ void solve_body_row(const SolveArgs &a, const BA &B)
+template <int kKind, bool kRow, bool kFixed, class BA>
+__device__ __forceinline__ void solve_phases(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
     if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
@@ -993,11 +942,20 @@ __device__ __forceinline__ void solve_body_row(const SolveArgs &a, const BA &B)
                 const int sl = task_slot(pass, ci, t, pos);
                 if (sl < 0) continue;
                 const RowPre q = (t == pre_t) ? pre : row_pre(a.rec, sl, pos);
-                if (!pos) {
-                    if (warm) pair_apply_warm_row(a, sl, B, q);
-                    else pair_velocity_row(a, sl, B, q);
+                if (kRow) {
+                    if (!pos) {
+                        if (warm) pair_apply_warm_row(a, sl, B, q);
+                        else pair_velocity_row(a, sl, B, q);
+                    } else {
+                        pair_position_row(a, sl, B, q);
+                    }
                 } else {
-                    pair_position_row(a, sl, B, q);
+                    if (!pos) {
+                        if (warm) pair_apply_warm(a, sl, B, q);
+                        else pair_velocity<BA, kFixed>(a, sl, B, q);
+                    } else {
+                        pair_position(a, sl, B, q);
+                    }
                 }
             }
             pre_t = -1;
@@ -1015,23 +973,23 @@ __device__ __forceinline__ void solve_body_row(const SolveArgs &a, const BA &B)
     }
 }
 
-constexpr int kClusterThreads = 512;     // reference form
+constexpr int kClusterThreads = 384;     // reference form (contact staging as the row form)
 constexpr int kClusterThreadsRow = 384;  // row form (123 registers; 120 KB of contact staging)
 constexpr int kClusterMax = 16;
 
 __global__ void __launch_bounds__(256, 1) k_color_solve_block(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.row) solve_body_row<kBlock>(a, B);
-    else if (a.fixed_frame) solve_body<kBlock, true, false>(a, B);
-    else solve_body<kBlock, false, false>(a, B);
+    if (a.row) solve_phases<kBlock, true, true>(a, B);
+    else if (a.fixed_frame) solve_phases<kBlock, false, true>(a, B);
+    else solve_phases<kBlock, false, false>(a, B);
 }
 __global__ void __launch_bounds__(256, 1) k_color_solve_grid(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.row) solve_body_row<kGrid>(a, B);
-    else if (a.fixed_frame) solve_body<kGrid, true, false>(a, B);
-    else solve_body<kGrid, false, false>(a, B);
+    if (a.row) solve_phases<kGrid, true, true>(a, B);
+    else if (a.fixed_frame) solve_phases<kGrid, false, true>(a, B);
+    else solve_phases<kGrid, false, false>(a, B);
 }
 // Cluster solve, one kernel per form so each gets the registers it needs.  (Holding the body
 // state in distributed shared memory instead measured slower on B200 for this access pattern:
@@ -1039,42 +997,44 @@ __global__ void __launch_bounds__(256, 1) k_color_solve_grid(SolveArgs a)
 __global__ void __launch_bounds__(kClusterThreads) k_color_solve_cluster(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    if (a.fixed_frame) solve_body<kCluster, true, false>(a, B);
-    else solve_body<kCluster, false, false>(a, B);
+    if (a.fixed_frame) solve_phases<kCluster, false, true>(a, B);
+    else solve_phases<kCluster, false, false>(a, B);
 }
 __global__ void __launch_bounds__(kClusterThreadsRow) k_color_solve_cluster_row(SolveArgs a)
 {
     const GlobalBodies B{a.v, a.w, a.pv, a.po};
-    solve_body_row<kCluster>(a, B);
+    solve_phases<kCluster, true, true>(a, B);
 }
 
-// dynamic shared memory of a solve launch: the row form's contact staging
-static size_t stage_bytes(int row, int threads) { return row ? (size_t)kStageBytesPerThread * threads : 0; }
+// dynamic shared memory of a solve launch: the contact staging of its threads
+static size_t stage_bytes(int threads) { return (size_t)kStageBytesPerThread * threads; }
 
-// the row-form kernels' dynamic shared memory exceeds the 48 KB default: opt in once
+// the solve kernels' dynamic shared memory exceeds the 48 KB default: opt in once
 static void allow_stage_smem()
 {
     static bool done = false;
     if (done) return;
-    const int bytes = (int)stage_bytes(1, 256 > kClusterThreadsRow ? 256 : kClusterThreadsRow);
-    cudaFuncSetAttribute(k_color_solve_block, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_color_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(k_color_solve_cluster_row, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_color_solve_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes(256));
+    cudaFuncSetAttribute(k_color_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes(256));
+    cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)stage_bytes(kClusterThreads));
+    cudaFuncSetAttribute(k_color_solve_cluster_row, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)stage_bytes(kClusterThreadsRow));
     done = true;
 }
 
-static int max_coresident_grid_blocks(int row)
+static int max_coresident_grid_blocks()
 {
-    static int cached[2] = {-1, -1};
-    if (cached[row] < 0) {
+    static int cached = -1;
+    if (cached < 0) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         allow_stage_smem();
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve_grid, 256, stage_bytes(row, 256));
-        cached[row] = std::max(1, sms * std::max(per, 1));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve_grid, 256, stage_bytes(256));
+        cached = std::max(1, sms * std::max(per, 1));
     }
-    return cached[row];
+    return cached;
 }
 
 // largest power-of-two cluster (<= 16) of a cluster-solve kernel that the device can
@@ -1090,7 +1050,7 @@ static int max_cluster_size(int row)
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kClusterMax);
         cfg.blockDim = dim3(row ? kClusterThreadsRow : kClusterThreads);
-        cfg.dynamicSmemBytes = stage_bytes(row, kClusterThreadsRow);
+        cfg.dynamicSmemBytes = stage_bytes(row ? kClusterThreadsRow : kClusterThreads);
         int cs = 0;
         if (cudaOccupancyMaxPotentialClusterSize(&cs, fn, &cfg) != cudaSuccess) {
             cudaGetLastError();
@@ -1154,7 +1114,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(cs);
             cfg.blockDim = dim3(a.row ? kClusterThreadsRow : kClusterThreads);
-            cfg.dynamicSmemBytes = stage_bytes(a.row, kClusterThreadsRow);
+            cfg.dynamicSmemBytes = stage_bytes(a.row ? kClusterThreadsRow : kClusterThreads);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1171,21 +1131,21 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             }
             if ((rc = check_launch("color_solve_cluster"))) return rc;
         } else {
-            mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks(a.row));
+            mode = std::min((b->n + 255) / 256, max_coresident_grid_blocks());
         }
     }
     if (mode > 0) {
         allow_stage_smem();
-        const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks(a.row)));
+        const int nblocks = std::max(1, std::min(mode, max_coresident_grid_blocks()));
         if (nblocks == 1) {
-            k_color_solve_block<<<1, 256, stage_bytes(a.row, 256), s>>>(a);
+            k_color_solve_block<<<1, 256, stage_bytes(256), s>>>(a);
             if ((rc = check_launch("color_solve_block"))) return rc;
         } else {
             cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (generation keeps counting)
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(256);
-            cfg.dynamicSmemBytes = stage_bytes(a.row, 256);
+            cfg.dynamicSmemBytes = stage_bytes(256);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeCooperative;
