@@ -237,6 +237,14 @@ class GraphColoredContactEngine(_BeadEngineBase):
         return dict(pairs=P, kept=Ck, endpoints=E, colors=h["n_colors"],
                     bytes=warm + self.vit * per_vel + self.pit * per_pos)
 
+    def set_solve_blocks(self, n: int):
+        """Launch form of the persistent solve: 0 auto, 1 one CTA, n > 1 a cooperative grid of n
+        CTAs, -n a cluster of n CTAs.  Results do not depend on it.  Drops captured graphs."""
+        self.solve_blocks = int(n)
+        if self._built:
+            self.c_params.solve_blocks = self.solve_blocks
+            self._graphs = {}
+
     # ---- diagnostics ----
     @property
     def color_cache_hits(self):

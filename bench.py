@@ -462,11 +462,14 @@ def main():
         torch.cuda.synchronize()
         np.savez(args.save_state, xc=e.xc[:, :3].cpu().numpy(), q=e.q.cpu().numpy(), v=e.v[:, :3].cpu().numpy(),
                  w=e.w[:, :3].cpu().numpy())
-    tuned = None
-    if wl["engine"] == "batched":  # the launch form of the solve, picked on live (untimed) steps
-        best, times = me.autotune(e, dt, S)
-        tuned = {"solve_blocks": best, "ms_per_step": {str(k): round(v, 4) for k, v in times.items()}}
     for _ in range(args.warmup):
+        e.step(dt, S)
+    tuned = None
+    if wl["engine"] in ("batched", "color_cache"):
+        # the solve's launch form, picked on live (untimed) steps after the warm-up, then one more
+        # untimed step on the chosen form (its graph capture)
+        best, times = me.autotune(e, dt, S, steps=4)
+        tuned = {"solve_blocks": best, "ms_per_step": {str(k): round(v, 4) for k, v in times.items()}}
         e.step(dt, S)
     e.check_errors()
     torch.cuda.synchronize()
@@ -579,6 +582,8 @@ def main():
         cfg.update(scenes=wl["n_scenes"], bodies_per_scene=[wl["nmin"], wl["nmax"]], edge=wl["edge"],
                    mu=wl["mu_range"], density=wl["density"], heavy="10 % of each scene at 100 x density",
                    color_cap=wl["color_cap"], autotuned=tuned)
+    if tuned is not None and wl["engine"] != "batched":
+        cfg.update(autotuned=tuned)
     if wl["engine"] == "box":
         cfg.update(edge=wl["edge"], volume=wl["box"], mu=wl["mu_range"], density=wl["density"],
                    color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3")

@@ -122,6 +122,24 @@ def test_single_cta_equals_grid_solve(me):
         assert s.xc.tobytes() == states[0].xc.tobytes() and s.om.tobytes() == states[0].om.tobytes()
 
 
+def test_set_solve_blocks_mid_run_keeps_bits(me):
+    """Switching the launch form between steps (what the autotuner does on live steps) leaves
+    the trajectory bit-identical to a run on one form."""
+    runs = []
+    for forms in ((1, 1), (-16, 148)):
+        e = _make(me, "color_cache", vit=16, pit=8, solve_blocks=forms[0])
+        for c in lattice(400):
+            e.add_body(c)
+        for _ in range(10):
+            e.step(DT, 1)
+        e.set_solve_blocks(forms[1])
+        for _ in range(10):
+            e.step(DT, 1)
+        runs.append(e.get_state())
+    for n in ("xc", "Rm", "vc", "om"):
+        assert getattr(runs[0], n).tobytes() == getattr(runs[1], n).tobytes(), n
+
+
 def test_contract_checks(me):
     """contact_engine_gpu_colored.py:1414-1515 on the engines built here."""
     for engine in ("plain", "pair_chunks", "color_cache"):
