@@ -102,7 +102,7 @@ COLOR_ROW_FORM = 64
 class Grid(ctypes.Structure):
     _fields_ = [("dim_x", c_int32), ("dim_y", c_int32), ("dim_z", c_int32), ("cell", c_float),
                 ("bucket", c_void_p), ("start", c_void_p), ("cursor", c_void_p), ("sorted", c_void_p),
-                ("scan_tmp", c_void_p)]
+                ("scan_tmp", c_void_p), ("sorted_pos", c_void_p)]
 
 
 class Contacts(ctypes.Structure):

@@ -40,29 +40,52 @@ __device__ __forceinline__ QueryRange query_range(f3 p, float r, float inv)
 }
 
 inline GridView view_of(const b2c_grid *g) { return GridView{g->dim_x, g->dim_y, g->dim_z, 1.0f / g->cell}; }
+// every array of a grid present and its dims at least 8 per axis (the wrap-around query needs it)
+inline bool grid_valid(const b2c_grid *g)
+{
+    return g && g->dim_x >= 8 && g->dim_y >= 8 && g->dim_z >= 8 && g->cell > 0.0f && g->bucket && g->start &&
+           g->cursor && g->sorted && g->scan_tmp && g->sorted_pos;
+}
 
-// Visit every bead j > i of another body within (1e-9, 2R) of xi, in bucket order.
+// Visit every bead j > i of another body within (1e-9, 2R) of xi.  z is the innermost bucket
+// coordinate, so each (x, y) column of the query block is one run of consecutive buckets, and
+// its slots one range of `sorted`, unless the column wraps around the grid (then cell by cell).
+// A candidate's id and its slot-ordered position and owner (spos) are independent loads.  The
+// visiting order is not the bucket order; callers that emit in order sort by bead id.
 template <class F>
-__device__ __forceinline__ void for_each_bead_neighbor(int i, f3 xi, int bi, const float *__restrict__ world,
-                                                       const int *__restrict__ owner, const int *__restrict__ start,
-                                                       const int *__restrict__ sorted, const GridView &g, F &&f)
+__device__ __forceinline__ void visit_slots(int i, f3 xi, int bi, const float4 *__restrict__ spos,
+                                            const int *__restrict__ sorted, int t0, int t1, F &&f)
+{
+    for (int t = t0; t < t1; ++t) {
+        const int j = sorted[t];
+        const float4 p = spos[t];
+        if (j > i && __float_as_int(p.w) != bi) {
+            const f3 xj = xyz(p);
+            const f3 dvec = sub3(xi, xj);
+            const float dist = len3(dvec);
+            if (dist < B2C_2R && dist > 1e-9f) f(j, xj, dvec, dist);
+        }
+    }
+}
+template <class F>
+__device__ __forceinline__ void for_each_bead_neighbor(int i, f3 xi, int bi, const float4 *__restrict__ spos,
+                                                       const int *__restrict__ start, const int *__restrict__ sorted,
+                                                       const GridView &g, F &&f)
 {
     const QueryRange qr = query_range(xi, B2C_2R, g.inv);
-    for (int iz = qr.lo[2]; iz <= qr.hi[2]; ++iz)
-        for (int iy = qr.lo[1]; iy <= qr.hi[1]; ++iy)
-            for (int ix = qr.lo[0]; ix <= qr.hi[0]; ++ix) {
-                const int b = bucket_of(g, ix, iy, iz);
-                const int e = start[b + 1];
-                for (int t = start[b]; t < e; ++t) {
-                    const int j = sorted[t];
-                    if (j > i && owner[j] != bi) {
-                        const f3 xj = ld3(world, j);
-                        const f3 dvec = sub3(xi, xj);
-                        const float dist = len3(dvec);
-                        if (dist < B2C_2R && dist > 1e-9f) f(j, xj, dvec, dist);
-                    }
+    const int nz = qr.hi[2] - qr.lo[2];
+    for (int iy = qr.lo[1]; iy <= qr.hi[1]; ++iy)
+        for (int ix = qr.lo[0]; ix <= qr.hi[0]; ++ix) {
+            const int b0 = bucket_of(g, ix, iy, qr.lo[2]), b1 = bucket_of(g, ix, iy, qr.hi[2]);
+            if (b1 - b0 == nz) {
+                visit_slots(i, xi, bi, spos, sorted, start[b0], start[b1 + 1], f);
+            } else {
+                for (int iz = qr.lo[2]; iz <= qr.hi[2]; ++iz) {
+                    const int b = bucket_of(g, ix, iy, iz);
+                    visit_slots(i, xi, bi, spos, sorted, start[b], start[b + 1], f);
                 }
             }
+        }
 }
 
 }  // namespace b2c

@@ -24,13 +24,17 @@ __global__ void k_grid_count(int nb, const int *__restrict__ bucket, int *__rest
     if (i < nb) atomicAdd(count + bucket[i], 1);
 }
 
+// slot of bead i in its bucket; the slot also receives the bead's position and owner
 __global__ void k_grid_scatter(int nb, const int *__restrict__ bucket, const int *__restrict__ start,
-                               int *__restrict__ cursor, int *__restrict__ sorted)
+                               int *__restrict__ cursor, int *__restrict__ sorted, const float *__restrict__ world,
+                               const int *__restrict__ owner, float4 *__restrict__ spos)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     const int b = bucket[i];
-    sorted[start[b] + atomicAdd(cursor + b, 1)] = i;
+    const int t = start[b] + atomicAdd(cursor + b, 1);
+    sorted[t] = i;
+    spos[t] = f4(ld3(world, i), __int_as_float(owner[i]));
 }
 
 __device__ __forceinline__ void append_contact(b2c_contacts c, int *n_raw, int bi, int bj, f3 pA, f3 pB, f3 nrm,
@@ -51,8 +55,8 @@ __device__ __forceinline__ void append_contact(b2c_contacts c, int *n_raw, int b
 // Ground: z - R < 0 -> normal +z, depth R - z.  Bead pairs: j > i, other body,
 // 1e-9 < |xi - xj| < 2R -> normal (xi - xj)/dist, depth 2R - dist, body A owns bead i.
 __global__ void k_bead_contacts(int nb, const float *__restrict__ world, const int *__restrict__ owner,
-                                const int *__restrict__ start, const int *__restrict__ sorted, GridView g,
-                                b2c_contacts c, b2c_header *hdr)
+                                const int *__restrict__ start, const int *__restrict__ sorted,
+                                const float4 *__restrict__ spos, GridView g, b2c_contacts c, b2c_header *hdr)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
@@ -60,7 +64,7 @@ __global__ void k_bead_contacts(int nb, const float *__restrict__ world, const i
     const int bi = owner[i];
     const float s = xi.z - B2C_R;
     if (s < 0.0f) append_contact(c, &hdr->n_raw, bi, -1, xi, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 1.0f}, -s, i, -1);
-    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int j, f3 xj, f3 dvec, float dist) {
+    for_each_bead_neighbor(i, xi, bi, spos, start, sorted, g, [&](int j, f3 xj, f3 dvec, float dist) {
         append_contact(c, &hdr->n_raw, bi, owner[j], xi, xj, div3(dvec, dist), B2C_2R - dist, i, j);
     });
 }
@@ -99,7 +103,9 @@ int grid_build(const b2c_beads *beads, b2c_grid *g, cudaStream_t s)
     if (rc) return rc;
     cudaMemsetAsync(g->cursor, 0, sizeof(int) * (size_t)nbk, s);
     if (beads->n > 0)
-        k_grid_scatter<<<blocks_for(beads->n), kThreads, 0, s>>>(beads->n, g->bucket, g->start, g->cursor, g->sorted);
+        k_grid_scatter<<<blocks_for(beads->n), kThreads, 0, s>>>(beads->n, g->bucket, g->start, g->cursor, g->sorted,
+                                                                 beads->world, beads->owner,
+                                                                 reinterpret_cast<float4 *>(g->sorted_pos));
     return check_launch("grid_scatter");
 }
 
@@ -107,19 +113,16 @@ int bead_contacts(const b2c_beads *beads, const b2c_grid *g, b2c_contacts *c, b2
 {
     k_header_reset_contacts<<<1, 1, 0, s>>>(hdr);
     if (beads->n > 0)
-        k_bead_contacts<<<blocks_for(beads->n, 128), 128, 0, s>>>(beads->n, beads->world, beads->owner, g->start,
-                                                                  g->sorted, view_of(g), *c, hdr);
+        k_bead_contacts<<<blocks_for(beads->n, 128), 128, 0, s>>>(
+            beads->n, beads->world, beads->owner, g->start, g->sorted,
+            reinterpret_cast<const float4 *>(g->sorted_pos), view_of(g), *c, hdr);
     k_header_finish_contacts<<<1, 1, 0, s>>>(hdr, c->capacity);
     return check_launch("bead_contacts");
 }
 
 }  // namespace b2c
 
-static bool grid_ok(const b2c_grid *g)
-{
-    return g && g->dim_x >= 8 && g->dim_y >= 8 && g->dim_z >= 8 && g->cell > 0.0f && g->bucket && g->start &&
-           g->cursor && g->sorted;
-}
+static bool grid_ok(const b2c_grid *g) { return b2c::grid_valid(g); }
 
 extern "C" int32_t b2c_bead_world(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, b2c_stream s)
 {

@@ -33,8 +33,8 @@ constexpr int kMaxNeighbors = 64;
 // 1. contact generation in feature order (k_gen_fid COL:102-122 + k_fkey/radix sort/k_gather)
 // ---------------------------------------------------------------------------------------------
 __global__ void k_bead_count(int nb, const float *__restrict__ world, const int *__restrict__ owner,
-                             const int *__restrict__ start, const int *__restrict__ sorted, GridView g,
-                             int *__restrict__ count, b2c_header *hdr)
+                             const int *__restrict__ start, const int *__restrict__ sorted,
+                             const float4 *__restrict__ spos, GridView g, int *__restrict__ count, b2c_header *hdr)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) count[nb] = 0;
@@ -42,7 +42,7 @@ __global__ void k_bead_count(int nb, const float *__restrict__ world, const int 
     const f3 xi = ld3(world, i);
     const int bi = owner[i];
     int nn = 0;
-    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int, f3, f3, float) { ++nn; });
+    for_each_bead_neighbor(i, xi, bi, spos, start, sorted, g, [&](int, f3, f3, float) { ++nn; });
     if (nn > kMaxNeighbors) {
         atomicOr(&hdr->error, B2C_ERR_NEIGHBOR_OVERFLOW);
         nn = kMaxNeighbors;
@@ -63,8 +63,9 @@ __device__ __forceinline__ void put_contact(b2c_contacts &c, int k, int bi, int 
 }
 
 __global__ void k_bead_emit(int nb, const float *__restrict__ world, const int *__restrict__ owner,
-                            const int *__restrict__ start, const int *__restrict__ sorted, GridView g,
-                            const int *__restrict__ offset, b2c_contacts c, b2c_header *hdr)
+                            const int *__restrict__ start, const int *__restrict__ sorted,
+                            const float4 *__restrict__ spos, GridView g, const int *__restrict__ offset,
+                            b2c_contacts c, b2c_header *hdr)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -86,7 +87,7 @@ __global__ void k_bead_emit(int nb, const float *__restrict__ world, const int *
     if (offset[i + 1] == k) return;  // no bead neighbours
     int js[kMaxNeighbors];
     int n = 0;
-    for_each_bead_neighbor(i, xi, bi, world, owner, start, sorted, g, [&](int j, f3, f3, float) {
+    for_each_bead_neighbor(i, xi, bi, spos, start, sorted, g, [&](int j, f3, f3, float) {
         if (n < kMaxNeighbors) {  // insertion into ascending order of bead id
             int t = n++;
             while (t > 0 && js[t - 1] > j) {
@@ -825,13 +826,14 @@ int bead_contacts_sorted(const b2c_beads *beads, const b2c_grid *g, b2c_contacts
                          b2c_header *hdr, cudaStream_t s)
 {
     const int nb = beads->n;
-    k_bead_count<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted,
+    const float4 *spos = reinterpret_cast<const float4 *>(g->sorted_pos);
+    k_bead_count<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted, spos,
                                                          view_of(g), m->bead_count, hdr);
     int rc = check_launch("bead_count");
     if (rc) return rc;
     rc = exclusive_scan(m->bead_count, m->bead_offset, nb + 1, nullptr, m->scan_tmp, s);
     if (rc) return rc;
-    k_bead_emit<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted,
+    k_bead_emit<<<blocks_for(nb + 1, 128), 128, 0, s>>>(nb, beads->world, beads->owner, g->start, g->sorted, spos,
                                                         view_of(g), m->bead_offset, *c, hdr);
     return check_launch("bead_emit");
 }
@@ -942,7 +944,7 @@ static bool color_params_ok(const b2c_color_params *p)
 extern "C" int32_t b2c_bead_contacts_sorted(const b2c_beads *beads, const b2c_grid *g, b2c_contacts *c,
                                             b2c_manifold *m, b2c_header *hdr, b2c_stream s)
 {
-    if (!beads || !g || !c || !m || !hdr || !m->bead_count || !m->bead_offset) {
+    if (!beads || !b2c::grid_valid(g) || !c || !m || !hdr || !m->bead_count || !m->bead_offset) {
         b2c::set_error("b2c_bead_contacts_sorted: bad argument");
         return B2C_EARG;
     }
@@ -996,7 +998,8 @@ extern "C" int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads
                                      b2c_warm *warm, b2c_header *hdr, const b2c_color_params *p, float dt,
                                      float *vgrav, b2c_stream s)
 {
-    if (!b || !beads || !beads->bead_start || !g || !c || !m || !kept || !kept_keys || !pr || !warm || !hdr ||
+    if (!b || !beads || !beads->bead_start || !b2c::grid_valid(g) || !c || !m || !kept || !kept_keys || !pr ||
+        !warm || !hdr ||
         !color_params_ok(p) || !vgrav || !(dt > 0.0f) || kept->capacity < c->capacity ||
         warm->capacity < kept->capacity || !pr->barrier || !pr->rec || pr->kslots < 1) {
         b2c::set_error("b2c_color_substep: bad argument");

@@ -9,6 +9,7 @@
 // accumulators.  Counts are read from the device header, launches are fixed-size grid-stride
 // loops, so the whole solve is capturable into one graph.
 #include "b2c_common.cuh"
+#include "b2c_grid.cuh"
 
 namespace b2c {
 
@@ -251,7 +252,7 @@ extern "C" int32_t b2c_jacobi_substep(const b2c_bodies *b, const b2c_beads *bead
                                       b2c_header *hdr, int64_t *acc, const b2c_jacobi_params *p, float dt,
                                       float *vgrav, b2c_stream s)
 {
-    if (!b || !beads || !g || !c || !hdr || !acc || !p || !vgrav || !(dt > 0.0f)) {
+    if (!b || !beads || !b2c::grid_valid(g) || !c || !hdr || !acc || !p || !vgrav || !(dt > 0.0f)) {
         b2c::set_error("b2c_jacobi_substep: bad argument");
         return B2C_EARG;
     }

@@ -180,8 +180,9 @@ class _BeadEngineBase:
         self.g_bucket, self.g_start, self.g_cursor, self.g_sorted = i32(max(self.NB, 1)), i32(nbk + 1), i32(nbk + 1), \
             i32(max(self.NB, 1))
         self.g_scan = i32(max(self.L.b2c_scan_scratch_ints(nbk + 1), 1))
+        self.g_spos = torch.zeros((max(self.NB, 1), 4), dtype=torch.float32, device=dev)
         self.c_grid = _lib.Grid(dims[0], dims[1], dims[2], 2.0 * R, _ptr(self.g_bucket), _ptr(self.g_start),
-                                _ptr(self.g_cursor), _ptr(self.g_sorted), _ptr(self.g_scan))
+                                _ptr(self.g_cursor), _ptr(self.g_sorted), _ptr(self.g_scan), _ptr(self.g_spos))
 
     def _setup_contacts(self, cap=MAXC):
         dev = self.dev

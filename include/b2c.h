@@ -93,6 +93,8 @@ typedef struct b2c_grid {
     int32_t *cursor;    /* (dims+1) bucket counts, then scatter cursors */
     int32_t *sorted;    /* (beads) bead ids grouped by bucket */
     int32_t *scan_tmp;  /* scan scratch, b2c_scan_scratch_ints(dims+1) ints */
+    float *sorted_pos;  /* (beads x 4) per slot of `sorted`: the bead's world position and, as the
+                           bit pattern of .w, its owner body (written by b2c_grid_build) */
 } b2c_grid;
 
 /* Contacts, structure of arrays of float4 records. */
