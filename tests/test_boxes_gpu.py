@@ -140,3 +140,29 @@ def test_box_engine_rests(me):
     f = e.contact_forces()
     M = e._M
     np.testing.assert_allclose(f[:, 2], M * 9.81, rtol=0.05)
+
+
+def test_colouring_beyond_register_pairs(me, oracle_mod):
+    """More pairs than the colouring keeps in registers (4 per thread of a 16 x 1024-thread
+    cluster, 65 536): the rest take its scratch path.  Three layers of 105 x 105 cubes with a
+    1.6 mm face gap (inside the 2 mm contact margin; edge and corner neighbours are not) give
+    about 98 000 pairs from the first step; colours, counts and states equal the oracle's."""
+    n, layers, edge, gap = 105, 3, 0.25, 1.6e-3
+    pitch = edge + gap
+    g = me.BoxContactEngine(mu=0.5, vit=8, pit=4)
+    o = oracle_mod.BoxOracle(mu=0.5, vit=8, pit=4)
+    for k in range(layers):
+        for j in range(n):
+            for i in range(n):
+                c = ((i - n / 2) * pitch, (j - n / 2) * pitch, 0.5 * edge + gap / 2 + k * pitch)
+                g.add_box(c, dims=(edge, edge, edge), density=1000.0, mu=0.5)
+                o.add_box(c, dims=(edge, edge, edge), density=1000.0, mu=0.5)
+    for _ in range(2):
+        g.step(1 / 240, 1)
+        o.step(1 / 240, 1)
+    h, st = g.check_errors(), o.stats()
+    assert h["n_pairs"] > 65536, h
+    assert (h["n_contacts"], h["n_pairs"], h["n_colors"]) == (st["n_contacts"], st["n_pairs"], st["n_colors"])
+    sg, so = g.get_state(), o.get_state()
+    for name in ("xc", "Rm", "vc", "om"):
+        np.testing.assert_array_equal(getattr(sg, name), getattr(so, name), err_msg=name)
