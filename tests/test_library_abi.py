@@ -36,3 +36,18 @@ def test_bad_arguments_rejected_without_gpu(me):
     assert L.b2c_body_predict(None, ctypes.c_float(0.01), None) == 1
     assert b"bad" in L.b2c_last_error()
     assert L.b2c_exclusive_scan(None, None, 5, None, None) == 1
+
+
+def test_grid_without_sorted_positions_rejected(me):
+    """Every entry point that takes a bead grid checks all of its arrays, slot-ordered positions
+    included, before touching the device."""
+    import ctypes
+    L = me._lib.load()
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the check fails first
+    g = me._lib.Grid(8, 8, 8, 0.1, dummy, dummy, dummy, dummy, dummy, None)
+    beads = me._lib.Beads()
+    assert L.b2c_grid_build(ctypes.byref(beads), ctypes.byref(g), None) == 1
+    assert b"b2c_grid_build" in L.b2c_last_error()
+    g.sorted_pos = dummy
+    g.dim_z = 4  # below the 8 cells per axis the wrap-around query needs
+    assert L.b2c_grid_build(ctypes.byref(beads), ctypes.byref(g), None) == 1
