@@ -129,3 +129,33 @@ def box_lattice(n=100000, edge=0.25, extent=(50.0, 50.0, 10.0), jitter=0.05, mu=
                         edge / 2 + 1e-3 + iz * pitch], axis=1) + rng.uniform(-1.0, 1.0, (n, 3)) * j
     centers[:, 2] = np.maximum(centers[:, 2], edge / 2 + 1e-3)
     return dict(dims=np.full((n, 3), edge), centers=centers, mu=np.full(n, mu), density=np.full(n, density))
+
+
+def stance_batch(B=4096, nv=18, nc=4, mu=0.5, seed=8, slide=(0.3, 0.1)):
+    """B seeded contact problems of a legged stance: a floating base (6 velocity coordinates)
+    and nc legs of (nv - 6) / nc joints each, every leg touching the ground once.  Per problem
+    an SPD mass matrix M = A A^T / nv + diag(U[0.5, 2]); per contact the rows (normal, t1, t2) of
+    J act on the base (linear part along the frame, angular part through a random lever arm)
+    and on that leg's joints (Gaussian), nothing else.  The free velocity slides the base
+    tangentially by `slide` (plus noise) and presses it into the ground, so most contacts slip.
+    Returns J (B, 3 nc, nv), Minv (B, nv, nv), v_free (B, nv), mu (B, nc) as float64 arrays."""
+    rng = np.random.default_rng(seed)
+    per_leg = (nv - 6) // nc
+    A = rng.standard_normal((B, nv, nv))
+    M = A @ A.transpose(0, 2, 1) / nv + np.einsum("bi,ij->bij", rng.uniform(0.5, 2.0, (B, nv)), np.eye(nv))
+    Minv = np.linalg.inv(M)
+    J = np.zeros((B, 3 * nc, nv))
+    frame = np.eye(3)[[2, 0, 1]]  # rows n = z, t1 = x, t2 = y
+    for c in range(nc):
+        r = rng.uniform(-0.4, 0.4, (B, 3))
+        r[:, 2] = -0.3
+        for k in range(3):
+            d = frame[k]
+            J[:, 3 * c + k, 0:3] = d
+            J[:, 3 * c + k, 3:6] = np.cross(r, d)  # angular part: (r x d) . w
+            J[:, 3 * c + k, 6 + per_leg * c:6 + per_leg * (c + 1)] = rng.standard_normal((B, per_leg)) * 0.3
+    v_free = rng.standard_normal((B, nv)) * 0.05
+    v_free[:, 0] += slide[0]
+    v_free[:, 1] += slide[1]
+    v_free[:, 2] -= 0.2
+    return J, Minv, v_free, np.full((B, nc), float(mu))

@@ -62,6 +62,16 @@ WORKLOADS = {
                                              "(reports/innovation_stack_color_cache_l4.json)")),
     # the same lattice under relaxed Jacobi; published: 5.599 ms per step at N = 10 000 on an RTX 5070
     # (docs/RUNNING.md:374-379)
+    # the batched exact-cone NCP and its adjoint at the shape of the reference's batched-adjoint
+    # benchmark (B = 4096 legged-stance problems, nv = 18, 4 contacts, mu 0.5, sliding): one step
+    # is a forward solve of the whole batch to a natural residual of 1e-6, and the gradient is
+    # two vector-Jacobian-product directions; published: forward 428.49 ms (9 559 env-steps/s),
+    # grad (2 directions) 119.61 ms on an RTX 5070
+    # (reproducibility/p2/data/reference/batch_throughput_slip.txt)
+    "adjoint4096": dict(engine="bncp", B=4096, nv=18, nc=4, mu=0.5, tol=1e-6, max_iters=5000, steps=200, warmup=3,
+                        published=(4096 / 428.49e-3, "reference batched ADMM forward, 428.49 ms at B = 4096, "
+                                   "RTX 5070 (reproducibility/p2/data/reference/batch_throughput_slip.txt)"),
+                        published_grad_ms=119.61, published_fwd_ms=428.49),
     "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
                               pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                               published=(1e4 / 5.599e-3, "reference relaxed Jacobi, 5.599 ms/step, RTX 5070 "
@@ -393,6 +403,168 @@ def per_scene_sequential(me, wl, scenes, batch, dt, S, stream, steps=3):
             "engines": len(engines), "note": "same sweeps per scene; each scene's arithmetic is bytewise the batch's"}
 
 
+def _stance(wl, B=None):
+    sc = _scenes()
+    return sc.stance_batch(B=wl["B"] if B is None else B, nv=wl["nv"], nc=wl["nc"], mu=wl["mu"])
+
+
+def _bncp_cpu_worker(args_):
+    """Oracle PGS plus two VJP directions on problems [lo, hi) of the stance batch; returns
+    (problems done, seconds)."""
+    workload, lo, hi, budget = args_
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ge.load_package()
+    from oracle import oracle_bncp as OB
+    wl = WORKLOADS[workload]
+    J, Minv, v, mu = _stance(wl)
+    G = J[lo:hi] @ Minv[lo:hi] @ J[lo:hi].transpose(0, 2, 1)
+    b = (J[lo:hi] @ v[lo:hi, :, None])[..., 0]
+    done, t0 = 0, time.perf_counter()
+    for e in range(hi - lo):
+        OB.pgs(G[e], b[e], mu[lo + e], iters=wl["max_iters"], tol=wl["tol"])
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return done, time.perf_counter() - t0
+
+
+def run_reference_adjoint(args, wl):
+    """--impl reference for the adjoint workload: the oracle's PGS (numpy) on every host core,
+    each process on its share of the batch, bounded to ~30 s."""
+    import multiprocessing as mp
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    B = wl["B"]
+    cuts = [B * k // procs for k in range(procs + 1)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_bncp_cpu_worker, [(args.workload, cuts[k], cuts[k + 1], 30.0) for k in range(procs)])
+    value = sum(r[0] for r in res) / max(r[1] for r in res)
+    line = {"impl": "reference", "metric": "env-steps/s", "value": value, "unit": "env-steps/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup", "steps")}},
+            "dtype": "f64", "data": "synthetic",
+            "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": procs, "kind": "port",
+                             "sample": f"{sum(r[0] for r in res)} of the {B} problems, forward solves to the "
+                                       f"same residual, {procs} processes capped at ~30 s (the oracle's numpy "
+                                       f"PGS; the reference's Warp path is not installed)"},
+            "e2e": {"value": value, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, wl):
+    """The batched NCP forward solve and its adjoint.  A step solves the whole batch (from zero)
+    to the workload's residual; the gradient is two vector-Jacobian products (two seeds), as the
+    reference's "grad (2 dir)".  With N ranks every rank solves its own batch (weak scaling)."""
+    import torch
+    import __graft_entry__ as ge
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    me = ge.load_package()
+    from motion_engine_b200 import bncp
+    cpu_base = None
+    if rank == 0 and not args.no_cpu_baseline:  # before the first GPU call
+        n, el = _bncp_cpu_worker((args.workload, 0, wl["B"], 20.0))
+        cpu_base = {"value": n / el, "unit": "env-steps/s", "cores": 1, "kind": "port",
+                    "sample": f"{n} problems of the batch solved to the same residual on one host core "
+                              f"({el:.1f} s; the oracle's numpy PGS)"}
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    J, Minv, v, mu = _stance(wl)
+    B, n = wl["B"], 3 * wl["nc"]
+    f64 = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    G, b = bncp.delassus(f64(J), f64(Minv), f64(v))
+    mu_d = f64(mu)
+    s = bncp.BatchNCP(G, b, mu_d)
+    gen = torch.Generator(device="cpu").manual_seed(11)
+    seeds = [torch.randn((B, n), generator=gen, dtype=torch.float64).to(dev) for _ in range(2)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        s.solve(wl["max_iters"], wl["tol"])
+        for g in seeds:
+            s.vjp(g)
+    torch.cuda.synchronize()
+    fwd, grad = [], []
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            s.solve(wl["max_iters"], wl["tol"])
+            e1.record()
+            for g in seeds:
+                s.vjp(g)
+            e2.record()
+            e2.synchronize()
+            fwd.append(e0.elapsed_time(e1))
+            grad.append(e1.elapsed_time(e2))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    fwd_ms, grad_ms = float(np.mean(fwd)), float(np.mean(grad))
+    t = torch.tensor([fwd_ms, grad_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    fwd_ms, grad_ms = float(t[0]), float(t[1])
+    value = B * world / (fwd_ms / 1e3)
+    res = s.res
+    conv = int((s.iters < wl["max_iters"]).sum())
+    labels = torch.bincount(s.labels.flatten().long(), minlength=3).tolist()
+    # end to end through the public autograd entry: pinned host problems in, lambda out, every step
+    hG, hb, hmu = (x.cpu().pin_memory() for x in (G, b, mu_d))
+    hlam = torch.empty((B, n), dtype=torch.float64).pin_memory()
+    K2 = max(3, min(args.steps, 10))
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(K2):
+        lam = bncp.ncp_solve(hG.to(dev, non_blocking=True), hb.to(dev, non_blocking=True),
+                             hmu.to(dev, non_blocking=True), wl["max_iters"], wl["tol"])
+        hlam.copy_(lam, non_blocking=True)
+    z.record()
+    z.synchronize()
+    e2e_ms = a.elapsed_time(z) / K2
+    peaks, peak_kind = _peaks()
+    alg = B * (n * n + n + n // 3 + n) * 8  # G, b, mu read, lambda written, per launch
+    roof = {"bound": "hbm", "achieved": alg / (fwd_ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": alg / (fwd_ms / 1e3) / 1e9 / peaks["hbm_gbs"], "traffic": None, "peak_kind": peak_kind,
+            "kernel": "k_bncp_solve (one warp per problem, PGS sweeps to the residual)",
+            "launch_ms": fwd_ms, "algorithmic_bytes_per_launch": alg,
+            "note": "latency-bound: each warp iterates its problem in shared memory; the bytes are read once"}
+    if rank == 0:
+        line = {"metric": "env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": fwd_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": value / wl["published"][0], "dtype": "f64",
+                "data": "synthetic (seeded legged-stance batch, the reference's shapes)",
+                "config": {"workload": args.workload, "B": B, "nv": wl["nv"], "contacts": wl["nc"], "mu": wl["mu"],
+                           "tol": wl["tol"], "max_iters": wl["max_iters"],
+                           "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"batches x{world}"},
+                "baseline": {"value": wl["published"][0], "unit": "env-steps/s", "source": wl["published"][1]},
+                "adjoint": {"fwd_ms": fwd_ms, "grad_ms_2dir": grad_ms, "grad_over_fwd": grad_ms / fwd_ms,
+                            "reference": {"fwd_ms": wl["published_fwd_ms"], "grad_ms_2dir": wl["published_grad_ms"],
+                                          "grad_over_fwd": wl["published_grad_ms"] / wl["published_fwd_ms"]}},
+                "residual": {"max": float(res.max()), "median": float(res.median()), "converged": conv,
+                             "iters_mean": float(s.iters.double().mean()), "iters_max": int(s.iters.max())},
+                "contacts_by_label": dict(zip(("open", "stick", "slip"), labels)),
+                "clocks": clk.summary(),
+                "e2e": {"value": B / (e2e_ms / 1e3), "unit": "env-steps/s",
+                        "h2d_bytes_per_step": int(hG.numel() * 8 + hb.numel() * 8 + hmu.numel() * 8),
+                        "d2h_bytes_per_step": int(hlam.numel() * 8), "steps": K2},
+                "gpu_launches": args.steps * 3, "launches_per_step": 3,
+                "roofline": roof, "cpu_baseline": cpu_base}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,6 +586,9 @@ def main():
         args.warmup = wl["warmup"]
     args.warmup = max(args.warmup, 3)
     import __graft_entry__ as ge
+    if wl["engine"] == "bncp":
+        ge.load_package()
+        return run_reference_adjoint(args, wl) if args.impl == "reference" else run_adjoint(args, wl)
     if args.impl == "reference":
         ge.load_package()
         return run_reference_batched(args, wl) if wl["engine"] == "batched" else run_reference(args, wl)
