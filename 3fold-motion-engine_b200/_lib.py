@@ -40,7 +40,7 @@ class Pairs(ctypes.Structure):
                 ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
                 ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
                 ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
-                ("body_colors", c_void_p), ("body_local", c_void_p)]
+                ("body_colors", c_void_p), ("body_local", c_void_p), ("body_slots", c_void_p)]
 
 
 class Warm(ctypes.Structure):

@@ -158,7 +158,7 @@ class BoxContactEngine(_BeadEngineBase):
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(2 * N),
                            cached_a=i32(pcap), cached_b=i32(pcap),
                            cached_mass=torch.zeros(max(N, 1), dtype=torch.float32, device=dev), cache_state=i32(8),
-                           body_colors=i64(N),
+                           body_colors=i64(N), body_slots=i32(64 * N),
                            barrier=torch.zeros(2, dtype=torch.int32, device=dev),
                            rec=torch.zeros(max(int(self.L.b2c_pair_record_floats(pcap, kslots)), 1),
                                            dtype=torch.float32, device=dev))
@@ -166,7 +166,7 @@ class BoxContactEngine(_BeadEngineBase):
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
             "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots, _ptr(pb["body_colors"]),
-            _ptr(self.local_t))
+            _ptr(self.local_t), _ptr(pb["body_slots"]))
         self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
         self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
         self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),

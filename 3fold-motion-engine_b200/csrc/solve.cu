@@ -168,7 +168,8 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
                                   const int *__restrict__ pidx, const int *__restrict__ pbi,
                                   const int *__restrict__ pbj, b2c_contacts kept, const float *__restrict__ xc,
                                   const float *__restrict__ invIw, const float *__restrict__ invM,
-                                  const float *__restrict__ body_mu, float mu, float dt, Records R, b2c_header *hdr_w)
+                                  const float *__restrict__ body_mu, float mu, float dt, Records R, b2c_header *hdr_w,
+                                  const int *__restrict__ col, int *__restrict__ body_slots)
 {
     const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
@@ -190,6 +191,13 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
         }
         float mu_p = mu;
         if (body_mu) mu_p = bj >= 0 ? sqrtf(body_mu[bi] * body_mu[bj]) : body_mu[bi];
+        if (body_slots) {  // this pair's slot under its colour, for each dynamic side
+            const int c = col[p];
+            if (c >= 0 && c < 64) {
+                if (iMA > 0.0f) body_slots[64 * bi + c] = 2 * s;
+                if (bj >= 0 && iMB > 0.0f) body_slots[64 * bj + c] = 2 * s + 1;
+            }
+        }
         R.body(0)[s] = f4(IA.r0, 0.0f);
         R.body(1)[s] = f4(IA.r1, 0.0f);
         R.body(2)[s] = f4(IA.r2, 0.0f);
@@ -730,6 +738,55 @@ __device__ void pair_apply_warm_row(const SolveArgs &a, int s, const BA &BS, con
     }
 }
 
+// The row form's warm start applied body by body: each dynamic body walks its pairs in colour
+// order (the set bits of its first-fit colour mask, the slots from body_slots) and applies
+// every contact of each with pair_apply_warm_row's expressions for its side.  A body's pairs
+// have distinct colours and the colour phases visit them in colour order, so the result is
+// the same bits as the warm pass of colour phases, in one launch.
+__global__ void k_warm_gather_row(const b2c_header *__restrict__ hdr, int nbodies,
+                                  const unsigned long long *__restrict__ body_colors,
+                                  const int *__restrict__ body_slots, Records R, float *v, float *w)
+{
+    if (hdr->n_pairs == 0 || hdr->n_colors == 0) return;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbodies; b += gridDim.x * blockDim.x) {
+        unsigned long long m = body_colors[b];
+        if (!m) continue;
+        f3 vv = ld3(v, b), ww = ld3(w, b);
+        while (m) {
+            const int c = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            const int e = body_slots[64 * b + c];
+            const int s = e >> 1;
+            const bool sideB = (e & 1) != 0;
+            const int4 h = R.hdr()[s];
+            const float4 mm = R.body(6)[s];
+            const m3 I = load_inertia(R, s, sideB ? 3 : 0);
+            const float iM = sideB ? mm.y : mm.x;
+            for (int k = 0; k < h.z; ++k) {
+                const float4 cn = R.contact(kRN, k)[s], ct1 = R.contact(kRT1, k)[s], im = R.contact(kRImp, k)[s];
+                const f3 nrm = xyz(cn), t1 = xyz(ct1), t2 = cross3(nrm, t1);
+                const f3 r = xyz(sideB ? R.contact(kRRB, k)[s] : R.contact(kRRA, k)[s]);
+                const float jn = im.x, j1 = im.y, j2 = im.z;
+                const f3 J{fmaf(j2, t2.x, fmaf(jn, nrm.x, j1 * t1.x)), fmaf(j2, t2.y, fmaf(jn, nrm.y, j1 * t1.y)),
+                           fmaf(j2, t2.z, fmaf(jn, nrm.z, j1 * t1.z))};
+                const RowResp kr = row_responses(I, r, nrm, t1, t2);
+                const f3 dw{fmaf(j2, kr.t2.x, fmaf(jn, kr.n.x, j1 * kr.t1.x)),
+                            fmaf(j2, kr.t2.y, fmaf(jn, kr.n.y, j1 * kr.t1.y)),
+                            fmaf(j2, kr.t2.z, fmaf(jn, kr.n.z, j1 * kr.t1.z))};
+                if (!sideB) {
+                    vv = f3{fmaf(iM, J.x, vv.x), fmaf(iM, J.y, vv.y), fmaf(iM, J.z, vv.z)};
+                    ww = add3(ww, dw);
+                } else {
+                    vv = f3{fmaf(-iM, J.x, vv.x), fmaf(-iM, J.y, vv.y), fmaf(-iM, J.z, vv.z)};
+                    ww = sub3(ww, dw);
+                }
+            }
+        }
+        st4(v, b, f4(vv, 0.0f));
+        st4(w, b, f4(ww, 0.0f));
+    }
+}
+
 template <class BA>
 __device__ void pair_velocity_row(const SolveArgs &a, int s, const BA &B, const RowPre &pre)
 {
@@ -1093,15 +1150,25 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
+    // the warm start body by body (one launch) instead of a pass of colour phases
+    const bool warm_bodies = a.row && a.apply_warm && (p->flags & B2C_COLOR_FIRST_FIT) && pr->body_slots &&
+                             pr->body_colors;
     if (a.row)
         k_pair_gather_row<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi,
                                                      pr->pbj, *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, dt,
-                                                     a.rec, hdr);
+                                                     a.rec, hdr, pr->col, warm_bodies ? pr->body_slots : nullptr);
     else
         k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
                                                  *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, a.rec, hdr);
     int rc = check_launch("pair_gather");
     if (rc) return rc;
+    if (warm_bodies) {
+        k_warm_gather_row<<<std::min(blocks_for(b->n), kSMs * 8), kThreads, 0, s>>>(
+            hdr, b->n, reinterpret_cast<const unsigned long long *>(pr->body_colors), pr->body_slots, a.rec, b->v,
+            b->w);
+        if ((rc = check_launch("warm_gather"))) return rc;
+        a.apply_warm = 0;
+    }
 
     int mode = p->solve_blocks;
     if (mode == 0) {  // auto: one CTA for tiny scenes, else a cluster (colours wider than it loop)

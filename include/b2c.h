@@ -179,6 +179,13 @@ typedef struct b2c_pairs {
                                 the colouring priority hashes the pair's scene-local bodies
                                 (a scene colours alike alone or in a batch); NULL: the
                                 reference's hash of the pair index (COL:136-148). */
+    int32_t *body_slots;     /* (bodies x 64) or NULL.  With B2C_COLOR_FIRST_FIT, B2C_COLOR_ROW_FORM
+                                and B2C_COLOR_APPLY_WARM the solve's record gather writes, for
+                                each dynamic body b and colour c of one of its pairs, that
+                                pair's record slot x 2 + side (0: body A, 1: body B) at
+                                [64 b + c]; the warm start is then applied body by body in
+                                colour order (the same bits as colour by colour) instead of in
+                                one pass of colour phases. */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
