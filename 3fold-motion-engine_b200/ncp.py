@@ -357,6 +357,24 @@ class NCPSolverB200:
                            contact_model="SOFT_STEP" if soft is not None else ("NCP_RIGID" if self.desaxce else "CCP"),
                            bias_applied=relax_iters <= 0)
 
+    def solve_resident(self, iters: int, soft: Optional[np.ndarray] = None) -> None:
+        """Solve the last uploaded scene again on the device, without host transfers: setup
+        (lambda from zero), the colouring through the colour cache, and `iters` sweeps.  The
+        results stay in self.lam and self.v."""
+        if self.C == 0:
+            return
+        params = self._params(soft, True)
+        s = self._stream()
+        _lib.check(self.L.b2c_ncp_setup(ctypes.byref(self.c_scene), ctypes.byref(self.c_state), 0, s),
+                   "b2c_ncp_setup")
+        _lib.check(self.L.b2c_ncp_color(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                        ctypes.byref(params), s), "b2c_ncp_color")
+        self._sweeps(params, iters)
+
+    def residual(self, soft: Optional[np.ndarray] = None) -> float:
+        """Natural-map residual of the current lambda (one device reduction)."""
+        return self._residual(self._params(soft, True))
+
     def coloring(self):
         """(colour per contact, colour-grouped order, per-colour offset, per-colour count)."""
         C, k = self.C, self.n_colors

@@ -159,3 +159,58 @@ def stance_batch(B=4096, nv=18, nc=4, mu=0.5, seed=8, slide=(0.3, 0.1)):
     v_free[:, 1] += slide[1]
     v_free[:, 2] -= 0.2
     return J, Minv, v_free, np.full((B, nc), float(mu))
+
+
+def ncp_lattice(n=10000, half=0.1, spacing=0.35, z0=0.0999, dz=0.1999, mass=1.0, dt=1.0 / 240.0, mu=0.5):
+    """The reference's exact-cone NCP timing fixture, LatticeWorld (ncp/ncp_gpu.py:1556-1665), as
+    the arrays of one BlockScene: a two-layer lattice of n cubes of half-edge `half` at rest
+    (ceil(sqrt(n / 2))^2 lower bodies on the ground, the rest stacked on the first of them), one
+    ground pair per lower body and one stacking pair per upper body, each expanded to its four
+    bottom corners (n_c = 4 n).  Normals are +z, the interface plane of a stacked pair passes
+    through the lower centre + half, Ja/Jb are the rows (n, t1, t2) = (z, x, y) on (v, w), the
+    free velocity is gravity's, and the bias is gap/dt when open, else the Baumgarte term.
+    Returns a dict of BlockScene's fields (float64)."""
+    g = int(np.ceil(np.sqrt(n / 2.0)))
+    n_low = min(g * g, n)
+    n_up = n - n_low
+    ix, iy = np.divmod(np.arange(n_low), g)
+    x = np.zeros((n, 3))
+    x[:n_low, 0] = (ix - (g - 1) / 2.0) * spacing
+    x[:n_low, 1] = (iy - (g - 1) / 2.0) * spacing
+    x[:n_low, 2] = z0
+    x[n_low:, :2] = x[:n_up, :2]
+    x[n_low:, 2] = z0 + dz
+    h = float(half)
+    Ib = mass / 12.0 * ((2 * h) ** 2 + (2 * h) ** 2)
+    off = np.array([[-h, -h, -h], [h, -h, -h], [-h, h, -h], [h, h, -h]])
+    K = len(off)
+    ca = np.concatenate([np.repeat(np.arange(n_low), K), np.repeat(np.arange(n_low, n), K)])
+    cb = np.concatenate([np.full(n_low * K, -1), np.repeat(np.arange(n_up), K)])
+    offs = np.tile(off, (n_low + n_up, 1))
+    feat = (np.arange(len(ca)) % K).astype(np.int32) + 8 * (cb + 1).astype(np.int32)
+    pa = x[ca] + offs  # identity orientations
+    gap = np.empty(len(ca))
+    gnd = cb < 0
+    gap[gnd] = pa[gnd, 2]
+    gap[~gnd] = pa[~gnd, 2] - (x[cb[~gnd], 2] + h)
+    Minv = np.zeros((n, 6, 6))
+    Minv[:, 0, 0] = Minv[:, 1, 1] = Minv[:, 2, 2] = 1.0 / mass
+    Minv[:, 3, 3] = Minv[:, 4, 4] = Minv[:, 5, 5] = 1.0 / Ib
+    vf = np.zeros((n, 6))
+    vf[:, 2] = dt * (-9.81)
+    D = np.array([[0.0, 0.0, 1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
+    nc = len(ca)
+    ra = pa - x[ca]
+    Ja = np.zeros((nc, 3, 6))
+    Jb = np.zeros((nc, 3, 6))
+    Ja[:, :, :3] = D
+    Ja[:, :, 3:] = np.cross(ra[:, None, :], D[None, :, :])
+    hasb = cb >= 0
+    rb = np.zeros((nc, 3))
+    rb[hasb] = pa[hasb] - x[cb[hasb]]
+    Jb[hasb, :, :3] = -D
+    Jb[hasb, :, 3:] = -np.cross(rb[hasb][:, None, :], D[None, :, :])
+    bias = np.zeros((nc, 3))
+    bias[:, 0] = np.where(gap > 0, gap / dt, -0.2 * np.maximum(-gap - 1e-4, 0.0) / dt)
+    return dict(Ja=Ja, Jb=Jb, Minv=Minv, v_free=vf, mu=np.full(nc, float(mu)),
+                body_pairs=np.stack([ca, cb], axis=1).astype(np.int32), dt=dt, bias=bias, feature=feat)

@@ -72,6 +72,13 @@ WORKLOADS = {
                         published=(4096 / 428.49e-3, "reference batched ADMM forward, 428.49 ms at B = 4096, "
                                    "RTX 5070 (reproducibility/p2/data/reference/batch_throughput_slip.txt)"),
                         published_grad_ms=119.61, published_fwd_ms=428.49),
+    # the reference's exact-cone NCP timing fixture (LatticeWorld, N = 10 000, n_c = 40 000, float64,
+    # 40 PGS sweeps: residual 7.778e-05, 8 colours); one step solves the resident scene again
+    # (setup, colouring through the cache, 40 sweeps); published: 11.21 ms per step = 280.2 us per
+    # sweep on an RTX 5070 (reproducibility/p2/data/reference/lattice_producer_shared.txt)
+    "ncp_lattice10k": dict(engine="ncp", n=10000, iters=40, steps=200, warmup=3,
+                           published=(40000 * 40 / 11.21e-3, "reference NCPSolverGPU PGS, 40 sweeps in 11.21 ms, "
+                                      "RTX 5070 (reproducibility/p2/data/reference/lattice_producer_shared.txt)")),
     "jacobi_lattice10k": dict(engine="jacobi", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5, vit=40,
                               pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                               published=(1e4 / 5.599e-3, "reference relaxed Jacobi, 5.599 ms/step, RTX 5070 "
@@ -565,6 +572,144 @@ def run_adjoint(args, wl):
         dist.destroy_process_group()
 
 
+def _ncp_scene(wl):
+    from motion_engine_b200 import ncp
+    return ncp.BlockScene(**_scenes().ncp_lattice(n=wl["n"]))
+
+
+def _ncp_cpu_worker(args_):
+    """The oracle's exact-cone NCP solve of the lattice, repeated for ~budget seconds on one
+    core; returns (solves, seconds)."""
+    workload, budget = args_
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ge.load_package()
+    from oracle import oracle as O
+    wl = WORKLOADS[workload]
+    bs = _ncp_scene(wl)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.ncp_solve(bs, wl["iters"], dtype="float64")
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    return done, time.perf_counter() - t0
+
+
+def run_reference_ncp(args, wl):
+    """--impl reference for the NCP lattice: independent replicas of the oracle's solve, one per
+    host core, each for ~30 s."""
+    import multiprocessing as mp
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ncp_cpu_worker, [(args.workload, 30.0)] * procs)
+    nc = 4 * wl["n"]
+    value = sum(r[0] for r in res) * nc * wl["iters"] / max(r[1] for r in res)
+    line = {"impl": "reference", "metric": "contact-sweeps/s", "value": value, "unit": "contact-sweeps/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup", "steps")}},
+            "dtype": "f64", "data": "synthetic",
+            "cpu_baseline": {"value": value, "unit": "contact-sweeps/s", "cores": procs, "kind": "port",
+                             "sample": f"{sum(r[0] for r in res)} solves of {wl['iters']} sweeps over {procs} "
+                                       f"independent replicas, ~30 s each (the oracle's C restatement; the "
+                                       f"reference's Warp path is not installed)"},
+            "e2e": {"value": value, "unit": "contact-sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ncp(args, wl):
+    """The exact-cone NCP solver on the reference's lattice fixture (float64).  A step solves the
+    resident scene again: setup, colouring through the cache, `iters` sweeps, in CUDA events.
+    With N ranks every rank solves its own replica."""
+    import torch
+    import __graft_entry__ as ge
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ge.load_package()
+    from motion_engine_b200 import ncp
+    cpu_base = None
+    if rank == 0 and not args.no_cpu_baseline:  # before the first GPU call
+        n, el = _ncp_cpu_worker((args.workload, 15.0))
+        cpu_base = {"value": n * 4 * wl["n"] * wl["iters"] / el, "unit": "contact-sweeps/s", "cores": 1,
+                    "kind": "port", "sample": f"{n} solves of {wl['iters']} sweeps of the same scene on one host "
+                                              f"core ({el:.1f} s; the oracle's C restatement)"}
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    bs = _ncp_scene(wl)
+    it = wl["iters"]
+    s = ncp.NCPSolverB200(bs.n_b, bs.n_c, dtype="float64", solve_blocks=wl.get("solve_blocks", 0))
+    first = s.solve(bs, iters=it)  # upload, colouring (cache miss), sweeps
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        s.solve_resident(it)
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            s.solve_resident(it)
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = float(np.mean(times))
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t[0])
+    res = s.residual()
+    nc, nb = bs.n_c, bs.n_b
+    value = nc * it * world / (ms / 1e3)
+    # end to end through the public solve(): host scene up, lambda and v down, every step
+    K2 = 10
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(K2):
+        s.solve(bs, iters=it, measure_residual=False)
+    b.record()
+    b.synchronize()
+    e2e_ms = a.elapsed_time(b) / K2
+    peaks, peak_kind = _peaks()
+    alg = it * (nc * (2 * 18 + 3 + 3 + 1 + 1) * 8 + nb * 6 * 8 * 2)  # per sweep: J rows, lambda, rho, mu; bodies
+    if rank == 0:
+        line = {"metric": "contact-sweeps/s", "value": value, "unit": "contact-sweeps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": value / wl["published"][0], "dtype": "f64",
+                "data": "synthetic (the reference's LatticeWorld geometry, restated)",
+                "config": {"workload": args.workload, "bodies": nb, "contacts": nc, "sweeps": it,
+                           "colours": int(first.n_colors), "l2": "flushed between timed steps (256 MiB write)",
+                           "parallelism": f"replicas x{world}"},
+                "baseline": {"value": wl["published"][0], "unit": "contact-sweeps/s", "source": wl["published"][1]},
+                "us_per_sweep": ms * 1e3 / it, "residual": res, "reference_residual": 7.778e-05,
+                "clocks": clk.summary(),
+                "e2e": {"value": nc * it / (e2e_ms / 1e3), "unit": "contact-sweeps/s",
+                        "h2d_bytes_per_step": int(nc * (2 * 18 + 1 + 3 + 1) * 8 + nc * 3 * 4 + nb * (36 + 6) * 8),
+                        "d2h_bytes_per_step": int(nc * 3 * 8 + nb * 6 * 8), "steps": K2},
+                "gpu_launches": args.steps * 3, "launches_per_step": 3,
+                "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"],
+                             "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                             "peak_kind": peak_kind, "kernel": "k_sweeps<double> (persistent coloured PGS)",
+                             "launch_ms": ms, "algorithmic_bytes_per_launch": alg},
+                "cpu_baseline": cpu_base}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -589,6 +734,9 @@ def main():
     if wl["engine"] == "bncp":
         ge.load_package()
         return run_reference_adjoint(args, wl) if args.impl == "reference" else run_adjoint(args, wl)
+    if wl["engine"] == "ncp":
+        ge.load_package()
+        return run_reference_ncp(args, wl) if args.impl == "reference" else run_ncp(args, wl)
     if args.impl == "reference":
         ge.load_package()
         return run_reference_batched(args, wl) if wl["engine"] == "batched" else run_reference(args, wl)

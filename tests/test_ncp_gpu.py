@@ -146,3 +146,16 @@ def _block_diag(M):
     for i in range(n):
         out[6 * i:6 * i + 6, 6 * i:6 * i + 6] = M[i]
     return out
+
+
+def test_resident_resolve_equals_full_solve(me):
+    """solve_resident (the scene kept on the device, the colour cache hit) gives the same bytes
+    as a full solve of the same scene."""
+    from motion_engine_b200 import ncp, scenes
+    bs = ncp.BlockScene(**scenes.ncp_lattice(n=2000))
+    s = ncp.NCPSolverB200(bs.n_b, bs.n_c, dtype="float64")
+    s.solve(bs, iters=40)
+    lam0, v0 = s.raw_bytes()
+    s.solve_resident(40)
+    lam1, v1 = s.raw_bytes()
+    assert lam0 == lam1 and v0 == v1

@@ -86,3 +86,15 @@ def test_soft_step_runs_and_relax_converges():
     r1 = O.ncp_solve(bs, 300, dtype="float64", softp=soft, use_bias=True)
     r2 = O.ncp_solve(bs, 3000, dtype="float64", softp=soft, use_bias=False, warm=r1["lam"])
     assert np.all(np.isfinite(r1["lam"])) and r2["residual"] < 1e-8
+
+
+def test_lattice_fixture_matches_the_reference_record(me):
+    """The restated LatticeWorld fixture (N = 10 000, n_c = 40 000, float64) reproduces the
+    reference's own record of it: 8 colours and a natural residual of 7.778e-05 after 40 PGS
+    sweeps (reproducibility/p2/data/reference/lattice_producer_shared.txt, first line)."""
+    from motion_engine_b200 import ncp, scenes
+    bs = ncp.BlockScene(**scenes.ncp_lattice())
+    assert (bs.n_b, bs.n_c) == (10000, 40000)
+    r = O.ncp_solve(bs, 40, dtype="float64")
+    assert r["n_colors"] == 8
+    assert abs(r["residual"] - 7.778e-05) < 5e-9
