@@ -275,13 +275,58 @@ struct SweepArgs {
     Soft soft;
 };
 
-enum Kind { kBlock = 0, kCluster = 1 };
+enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
-template <int kKind>
-__device__ __forceinline__ void phase_barrier()
+__device__ __forceinline__ unsigned long long ncp_global_ns()
 {
-    if (kKind == kBlock) __syncthreads();
-    else cg::this_cluster().sync();
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident)
+// counts arrivals in a.bar[0] and releases through the generation in a.bar[1]; its wait is
+// bounded by a.timeout_ns, after which it sets kErrBarrier and every CTA leaves the sweep.
+template <int kKind, typename T>
+__device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a)
+{
+    if (kKind == kBlock) {
+        __syncthreads();
+        return true;
+    }
+    if (kKind == kCluster) {
+        cg::this_cluster().sync();
+        return true;
+    }
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned int *gen = a.bar + 1;
+        const unsigned int my_gen = *gen;
+        __threadfence();
+        const unsigned int prev = atomicAdd(a.bar, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(a.bar, 0u);
+            __threadfence();
+            atomicAdd(a.bar + 1, 1u);
+        } else {
+            const unsigned long long t0 = ncp_global_ns();
+            while (*gen == my_gen) {
+                if (ncp_global_ns() - t0 > (unsigned long long)a.timeout_ns) {
+                    atomicOr(a.stats + kError, kErrBarrier);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        if (*(volatile int *)(a.stats + kError) & kErrBarrier) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
 }
 
 template <typename T>
@@ -316,12 +361,16 @@ template <typename T, int kKind>
 __global__ void __launch_bounds__(kSweepThreads) k_sweeps(SweepArgs<T> a)
 {
     const int ncol = a.stats[kNColors];
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    // Task slot: chunk k = t / 32 of a colour runs on CTA k mod gridDim, so a colour narrower
+    // than the launch is spread over every SM of it (contiguous slots would give all of a
+    // colour's float64 work to its first CTAs).  A contact keeps its thread in every sweep.
+    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
+    const int tid = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);
     for (int it = 0; it < a.iters; ++it)
         for (int ci = 0; ci < ncol; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
             for (int t = tid; t < cnt; t += nth) sweep_contact(a, a.order[s0 + t]);
-            phase_barrier<kKind>();
+            if (!phase_barrier<kKind>(a)) return;
         }
 }
 
@@ -546,13 +595,57 @@ int cluster_size()
     return cached;
 }
 
+// CTAs of the grid sweep the device holds at once (SMs x resident CTAs per SM); cached per type
+template <typename T>
+int grid_blocks()
+{
+    static int cached = -1;
+    if (cached < 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweeps<T, kGrid>, kSweepThreads, 0);
+        cached = std::max(1, sms * per);
+    }
+    return cached;
+}
+
 template <typename T>
 int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, int iters, cudaStream_t s)
 {
     if (iters <= 0 || sc->n_c == 0) return B2C_OK;
     const SweepArgs<T> a = sweep_args<T>(sc, st, p, iters);
     int mode = p->solve_blocks;
-    if (mode == 0) mode = sc->n_c <= 16384 ? 1 : -kClusterMax;
+    // auto: one CTA for small scenes; else every SM (the sweep's float64 work needs their issue
+    // rate: on the 40 000-contact lattice a grid of 148 CTAs takes 4.6 ms for 40 sweeps, a
+    // 16-CTA cluster 6.6 ms)
+    if (mode == 0) mode = sc->n_c <= 16384 ? 1 : grid_blocks<T>();
+    if (mode > 1) {  // a cooperative grid of at most the co-resident CTAs
+        const int nblocks = std::min(mode, grid_blocks<T>());
+        if (nblocks > 1) {
+            if (!(a.timeout_ns > 0)) {
+                set_error("ncp_sweeps: a grid launch needs barrier_timeout_ns > 0");
+                return B2C_EARG;
+            }
+            cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nblocks);
+            cfg.blockDim = dim3(kSweepThreads);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, k_sweeps<T, kGrid>, a);
+            if (e != cudaSuccess) {
+                set_error("ncp_sweeps: cooperative launch of %d CTAs: %s", nblocks, cudaGetErrorString(e));
+                return B2C_ECUDA;
+            }
+            return check_launch("ncp_sweeps_grid");
+        }
+        mode = 1;
+    }
     if (mode < 0) {
         const int cs = std::min(-mode, cluster_size<T>());
         if (cs >= 2) {

@@ -295,7 +295,8 @@ class NCPSolverB200:
             bits = int(st[7])
             self.stats[7] = 0
             raise RuntimeError("NCPSolverB200: " + ("colour count exceeds capacity" if bits & 1 else
-                                                    "colouring did not terminate"))
+                                                    "colouring did not terminate" if bits & 2 else
+                                                    "a sweep barrier timed out"))
         return st
 
     # ---- solve ----
@@ -348,6 +349,7 @@ class NCPSolverB200:
                 self._sweeps(self._params(soft, False), relax_iters)
             return vb
         v_bias = self._t("iter", run)
+        self._check_stats()
         r = 0.0
         if measure_residual:
             r = self._t("resid", lambda: self._residual(self._params(soft, relax_iters <= 0)))

@@ -418,7 +418,9 @@ typedef struct b2c_ncp_state {
  * impulse_scale, inv_h, contact_speed) and its pass flag, colour cache, launch form. */
 typedef struct b2c_ncp_params {
     int32_t desaxce, soft, use_bias, color_cache;
-    int32_t solve_blocks;      /* 0 auto, 1 one CTA, -n a cluster of n CTAs */
+    int32_t solve_blocks;      /* 0 auto (one CTA up to 16 384 contacts, else a grid of every
+                                  co-resident CTA), 1 one CTA, -n a cluster of n CTAs, n > 1 a
+                                  cooperative grid of n CTAs (at most the co-resident count) */
     int32_t pad;
     double softp[5];
     int64_t barrier_timeout_ns;
