@@ -572,6 +572,16 @@ def run_adjoint(args, wl):
         dist.destroy_process_group()
 
 
+def _traffic(workload):
+    """DRAM bytes per launch of the workload's dominant kernel, from the committed ncu summary
+    (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(workload)
+    except Exception:
+        return None
+
+
 def _ncp_scene(wl):
     from motion_engine_b200 import ncp
     return ncp.BlockScene(**_scenes().ncp_lattice(n=wl["n"]))
@@ -716,7 +726,8 @@ def run_ncp(args, wl):
                         "d2h_bytes_per_step": int(nc * 3 * 8 + nb * 6 * 8), "steps": K2},
                 "gpu_launches": args.steps * 3, "launches_per_step": 3,
                 "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"],
-                             "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"], "traffic": None,
+                             "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+                             "traffic": _traffic(args.workload),
                              "peak_kind": peak_kind, "kernel": "k_sweeps<double> (persistent coloured PGS)",
                              "launch_ms": ms, "algorithmic_bytes_per_launch": alg},
                 "cpu_baseline": cpu_base}
