@@ -20,6 +20,12 @@ every step uploads the state (set_body_state), steps, and downloads it again.
 `--impl reference` times the CPU restatement of the same algorithm (the oracle; the reference
 runs these engines through Warp, which is not installed) on the same workload, one replica per
 host core, rank 0 only.
+
+Other workloads (--workload): stress100k (100 000-cube lattice), batched512 (512 uneven
+scenes in one engine), colorcache_lattice10k and jacobi_lattice10k (the reference's 10k bead
+lattice, with vs_baseline against its published timings), ncp_lattice10k (the exact-cone NCP
+solve of the reference's LatticeWorld fixture) and adjoint4096 (the batched NCP forward solve
+and its adjoint at the reference's batched-adjoint shape).
 """
 from __future__ import annotations
 
