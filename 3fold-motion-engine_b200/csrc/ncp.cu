@@ -537,7 +537,7 @@ SweepArgs<T> sweep_args(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_nc
     a.acc = reinterpret_cast<long long *>(st->acc);
     a.stats = st->stats;
     a.bar = st->barrier;
-    a.timeout_ns = p ? p->barrier_timeout_ns : 0;
+    a.timeout_ns = (p && p->barrier_timeout_ns > 0) ? p->barrier_timeout_ns : 1000000000LL;  // default 1 s
     a.iters = iters;
     a.desaxce = p ? p->desaxce : 1;
     a.soft.on = p ? p->soft : 0;
@@ -623,10 +623,6 @@ int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, 
     if (mode > 1) {  // a cooperative grid of at most the co-resident CTAs
         const int nblocks = std::min(mode, grid_blocks<T>());
         if (nblocks > 1) {
-            if (!(a.timeout_ns > 0)) {
-                set_error("ncp_sweeps: a grid launch needs barrier_timeout_ns > 0");
-                return B2C_EARG;
-            }
             cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);

@@ -423,7 +423,7 @@ typedef struct b2c_ncp_params {
                                   cooperative grid of n CTAs (at most the co-resident count) */
     int32_t pad;
     double softp[5];
-    int64_t barrier_timeout_ns;
+    int64_t barrier_timeout_ns; /* grid-barrier wait limit (<= 0: 1 s) */
 } b2c_ncp_params;
 
 /* rho (k_rho), dynamic flags, acc = 0 or the warm start scattered (k_scatter), v = v_free +
