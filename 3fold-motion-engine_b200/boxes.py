@@ -100,10 +100,13 @@ class BoxContactEngine(_BeadEngineBase):
         dev = self.dev
         f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
         i32 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int32, device=dev)
-        self.xc = f32(_pad4(A["xc"]))
-        self.q = f32(np.tile(np.array([0, 0, 0, 1.0], np.float32), (N, 1)))
+        # positions, quaternions, velocities, angular velocities: four planes of one tensor
+        self.state = torch.zeros((4, N, 4), dtype=torch.float32, device=dev)
+        self.xc, self.q, self.v, self.w = self.state[0], self.state[1], self.state[2], self.state[3]
+        self.xc.copy_(f32(_pad4(A["xc"])))
+        self.q.copy_(f32(np.tile(np.array([0, 0, 0, 1.0], np.float32), (N, 1))))
         z4 = lambda: torch.zeros((N, 4), dtype=torch.float32, device=dev)
-        self.v, self.w, self.pv, self.po, self.vgrav = z4(), z4(), z4(), z4(), z4()
+        self.pv, self.po, self.vgrav = z4(), z4(), z4()
         self.invM = f32(A["invM"])
         Ib12 = np.zeros((N, 3, 4), np.float32)
         Ib12[:, :, :3] = A["IbInv"]

@@ -152,10 +152,14 @@ class _BeadEngineBase:
         self._kinarr = A["kin"].astype(int)
         dev = self.dev
         f32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
-        self.xc = f32(_pad4(A["xc"]))
-        self.q = f32(A["q"])
+        # positions, quaternions, velocities and angular velocities as the four contiguous
+        # (N, 4) planes of one tensor, so the whole state moves in one copy (set/get_state_packed)
+        self.state = torch.zeros((4, N, 4), dtype=torch.float32, device=dev)
+        self.xc, self.q, self.v, self.w = self.state[0], self.state[1], self.state[2], self.state[3]
+        self.xc.copy_(f32(_pad4(A["xc"])))
+        self.q.copy_(f32(A["q"]))
         z4 = lambda: torch.zeros((N, 4), dtype=torch.float32, device=dev)
-        self.v, self.w, self.pv, self.po = z4(), z4(), z4(), z4()
+        self.pv, self.po = z4(), z4()
         self.vgrav = z4()
         self.invM = f32(A["invM"])
         Ib12 = np.zeros((N, 3, 4), np.float32)
@@ -295,6 +299,26 @@ class _BeadEngineBase:
         for dst, src, k in ((self.xc, xc, 3), (self.q, q, 4), (self.v, v, 3), (self.w, w, 3)):
             t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float32))
             dst[:, :k].copy_(t, non_blocking=True)
+
+    def set_state_packed(self, state):
+        """Overwrite the whole body state with one (4, N, 4) float32 array: the planes are the
+        positions, the quaternions (x, y, z, w), the velocities and the angular velocities, each
+        row padded to four floats (the kernels read the first three of a vector row).  One copy;
+        a pinned torch tensor is copied asynchronously on the current stream."""
+        if not self._built:
+            self._build()
+        t = state if isinstance(state, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(state, np.float32))
+        self.state.copy_(t.reshape(self.state.shape), non_blocking=True)
+
+    def get_state_packed(self, out=None):
+        """The whole body state as one (4, N, 4) float32 array (see set_state_packed): a new host
+        tensor, or copied into `out` (asynchronously when it is pinned)."""
+        if not self._built:
+            self._build()
+        if out is None:
+            return self.state.cpu()
+        out.copy_(self.state, non_blocking=True)
+        return out
 
     # ---- data out ----
     def get_state(self) -> BodyState:

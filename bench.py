@@ -15,7 +15,8 @@ replica (a single scene does not shard: replicas only) and the time is the max o
 Rank 0 prints one JSON line.
 
 `e2e` is the same metric through the public API with the body state in pinned host memory:
-every step uploads the state (set_body_state), steps, and downloads it again.
+every step uploads the state (set_state_packed), steps, and downloads it again
+(get_state_packed).
 
 `--impl reference` times the CPU restatement of the same algorithm (the oracle; the reference
 runs these engines through Warp, which is not installed) on the same workload, one replica per
@@ -850,13 +851,11 @@ def main():
     h_end = e.check_errors()
     launches_per_step = max(e.kernels_per_step.values()) if e.kernels_per_step else 0
 
-    # end to end through the public API with the state in pinned host memory
+    # end to end through the public API with the state in pinned host memory (one packed copy
+    # each way: positions, quaternions, velocities, angular velocities)
     N = e.N
-    hx = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
-    hq = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
-    hv = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
-    hw = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
-    hx.copy_(e.xc[:, :3]); hq.copy_(e.q); hv.copy_(e.v[:, :3]); hw.copy_(e.w[:, :3])
+    hstate = torch.empty((4, N, 4), dtype=torch.float32, pin_memory=True)
+    e.get_state_packed(hstate)
     torch.cuda.synchronize()
     e2e_ms = 0.0
     K2 = max(min(args.steps, 100) // 2, 3)
@@ -865,16 +864,15 @@ def main():
         flush.fill_(float(k))
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        e.set_body_state(hx, hq, hv, hw)
+        e.set_state_packed(hstate)
         e.step(dt, S)
-        hx.copy_(e.xc[:, :3], non_blocking=True); hq.copy_(e.q, non_blocking=True)
-        hv.copy_(e.v[:, :3], non_blocking=True); hw.copy_(e.w[:, :3], non_blocking=True)
+        e.get_state_packed(hstate)
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
         colors.append(e.header_dict()["n_colors"])
     e.check_errors()
-    bytes_io = N * (3 + 4 + 3 + 3) * 4
+    bytes_io = hstate.numel() * 4
 
     per_scene = None
     if wl["engine"] == "batched":

@@ -166,3 +166,27 @@ def test_colouring_beyond_register_pairs(me, oracle_mod):
     sg, so = g.get_state(), o.get_state()
     for name in ("xc", "Rm", "vc", "om"):
         np.testing.assert_array_equal(getattr(sg, name), getattr(so, name), err_msg=name)
+
+
+def test_packed_state_round_trip(me):
+    """get_state_packed / set_state_packed move the whole body state in one copy each way: a run
+    that downloads and re-uploads its state every step stays bytewise equal to one that does
+    not, and the packed planes are the positions, quaternions and velocities get_state reads."""
+    import torch
+    S = _pile(200, box=(5.0, 5.0, 4.0))
+    a = _fill(me.BoxContactEngine(mu=0.5, vit=16, pit=10), S)
+    b = _fill(me.BoxContactEngine(mu=0.5, vit=16, pit=10), S)
+    host = torch.empty((4, len(S["centers"]), 4), dtype=torch.float32, pin_memory=True)
+    for _ in range(60):
+        a.step(DT, 2)
+        b.get_state_packed(host)
+        b.set_state_packed(host)
+        b.step(DT, 2)
+    torch.cuda.synchronize()
+    for x, y in zip(_state(a), _state(b)):
+        np.testing.assert_array_equal(x, y)
+    p = b.get_state_packed().numpy()
+    st = b.get_state()
+    np.testing.assert_array_equal(p[0, :, :3], st.xc)
+    np.testing.assert_array_equal(p[2, :, :3], st.vc)
+    np.testing.assert_array_equal(p[3, :, :3], st.om)
