@@ -13,7 +13,8 @@ from .boxes import BatchedBoxEngine, BoxContactEngine, autotune, partition_scene
 from .colored import (AppliedWarmContactEngine, ColorCacheContactEngine, DeferredForceContactEngine,
                       FixedFrameContactEngine, GraphColoredContactEngine)
 from .engine import BodyState, ContactEngine, RelaxedJacobiContactEngine, quat_to_R, voxbox
+from .handle import HandleBoxEngine
 
 __all__ = ["BodyState", "ContactEngine", "RelaxedJacobiContactEngine", "GraphColoredContactEngine",
            "FixedFrameContactEngine", "AppliedWarmContactEngine", "DeferredForceContactEngine",
-           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "_lib"]
+           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "HandleBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "_lib"]

@@ -120,7 +120,25 @@ ERR_BITS = {1: "contact capacity overflow", 2: "a body pair carries more than 10
             16: "colouring did not finish in its round budget", 32: "a bead has more than 64 neighbours within 2R",
             64: "pair capacity overflow", 128: "a grid barrier of the persistent solve gave up waiting"}
 
+class Config(ctypes.Structure):
+    """b2c_config: an engine handle's configuration (b2c_config_init fills the defaults)."""
+    _fields_ = [("kind", c_int32), ("device", c_int32), ("vit", c_int32), ("pit", c_int32),
+                ("mu", ctypes.c_double), ("dims", ctypes.c_double * 3), ("margin", ctypes.c_double),
+                ("flags", c_int32), ("color_cap", c_int32), ("solve_blocks", c_int32), ("cand_per_body", c_int32),
+                ("barrier_timeout_ns", ctypes.c_int64), ("graph", c_int32)]
+
+
+class StepHeader(ctypes.Structure):
+    """b2c_step_header: the last substep's counters and the handle's diagnostics."""
+    _fields_ = [("last", c_int32 * 8), ("color_cache_hits", c_int32), ("color_cache_misses", c_int32),
+                ("graph_captures", c_int32), ("kernels_per_step", c_int32), ("bodies", c_int32),
+                ("built", c_int32)]
+
+
+ENGINE_BOX = 1
+
 _P = ctypes.POINTER
+_D = ctypes.c_double
 _SIGS = {
     "b2c_version": ([], c_int32),
     "b2c_graph_kernel_nodes": ([c_void_p], c_int32),
@@ -161,6 +179,24 @@ _SIGS = {
     "b2c_bncp_solve": ([_P(Bncp), c_int32, ctypes.c_double, c_int32, c_void_p], c_int32),
     "b2c_bncp_sensitivity": ([_P(Bncp), c_void_p, c_void_p, c_void_p], c_int32),
     "b2c_bncp_vjp": ([_P(Bncp), c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_config_init": ([_P(Config)], None),
+    "b2c_box_body_setup": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+                           c_int32),
+    "b2c_create": ([_P(Config), _P(c_void_p)], c_int32),
+    "b2c_add_bodies": ([c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_set_body_mu": ([c_void_p, c_int32, c_int32, c_void_p], c_int32),
+    "b2c_set_body_scene": ([c_void_p, c_int32, c_int32, c_void_p], c_int32),
+    "b2c_body_count": ([c_void_p], c_int32),
+    "b2c_set_kinematic": ([c_void_p, c_int32, c_void_p], c_int32),
+    "b2c_step": ([c_void_p, _D, c_int32, c_void_p], c_int32),
+    "b2c_sync_header": ([c_void_p, _P(StepHeader)], c_int32),
+    "b2c_get_state": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_get_state_packed": ([c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_set_state_packed": ([c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_contact_forces": ([c_void_p, c_void_p], c_int32),
+    "b2c_state_save": ([c_void_p, c_void_p, _P(ctypes.c_size_t)], c_int32),
+    "b2c_state_load": ([c_void_p, c_void_p, ctypes.c_size_t], c_int32),
+    "b2c_destroy": ([_P(c_void_p)], c_int32),
     "b2c_box_narrowphase_test": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
 }

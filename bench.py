@@ -140,6 +140,44 @@ def make_engine(me, wl, scene):
     return e
 
 
+def cabi_e2e(me, wl, scene, start, flush, stream, K):
+    """Milliseconds of K end-to-end steps through the C ABI's engine handle: the same boxes
+    from the packed state `start` (the Python engine's state where its own end-to-end loop
+    ended), 3 untimed steps (the build, the graph capture, a warm store), then per step
+    b2c_set_state_packed from pinned host memory, b2c_step and b2c_get_state_packed back, on
+    `stream`, L2 flushed in between."""
+    import ctypes
+
+    import torch
+    h = me.HandleBoxEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
+                           color_cap=wl["color_cap"])
+    h.add_boxes(scene["centers"], dims=scene["dims"], density=scene["density"], mu=scene["mu"])
+    dt, S = wl["dt"], wl["substeps"]
+    L, s, check = h.L, ctypes.c_void_p(stream.cuda_stream), me._lib.check
+    host = torch.empty((4, h.N, 4), dtype=torch.float32, pin_memory=True)
+    host.copy_(start)
+    hp = ctypes.c_void_p(host.data_ptr())
+    check(L.b2c_set_state_packed(h._h, hp, s), "b2c_set_state_packed")
+    for _ in range(3):
+        check(L.b2c_step(h._h, dt, S, s), "b2c_step")
+    check(L.b2c_get_state_packed(h._h, hp, s), "b2c_get_state_packed")
+    torch.cuda.synchronize()
+    ms = 0.0
+    for k in range(K):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        check(L.b2c_set_state_packed(h._h, hp, s), "b2c_set_state_packed")
+        check(L.b2c_step(h._h, dt, S, s), "b2c_step")
+        check(L.b2c_get_state_packed(h._h, hp, s), "b2c_get_state_packed")
+        b.record(stream)
+        b.synchronize()
+        ms += a.elapsed_time(b)
+    h.header()
+    h.close()
+    return ms
+
+
 def make_oracle(wl, scene):
     from oracle import oracle as O
     if wl["engine"] == "box":
@@ -873,6 +911,8 @@ def main():
         colors.append(e.header_dict()["n_colors"])
     e.check_errors()
     bytes_io = hstate.numel() * 4
+    # the same loop through the C ABI's engine handle (library-owned device memory)
+    cabi_ms = cabi_e2e(me, wl, scene, hstate, flush, stream, K2) if wl["engine"] == "box" else 0.0
 
     per_scene = None
     if wl["engine"] == "batched":
@@ -888,10 +928,10 @@ def main():
             solve_ms.append(st["solve"])
             solve_bytes.append(e.solve_bytes())
         e.check_errors()
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    t = torch.tensor([ms, e2e_ms, cabi_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms, cabi_ms = float(t[0]), float(t[1]), float(t[2])
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -951,6 +991,10 @@ def main():
             "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
             "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h_end,
             "colors_e2e_steps": {"max": max(colors), "mean": float(np.mean(colors))}}
+    if cabi_ms > 0:
+        line["e2e_cabi"] = {"value": n_job * K2 / (cabi_ms / 1e3), "unit": "body-steps/s",
+                            "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io, "steps": K2,
+                            "calls": "b2c_set_state_packed, b2c_step, b2c_get_state_packed on a b2c_create handle"}
     if "published" in wl:
         line["baseline"] = {"value": wl["published"][0], "unit": "body-steps/s", "source": wl["published"][1]}
     if per_scene is not None:

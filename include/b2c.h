@@ -470,6 +470,100 @@ B2C_API int32_t b2c_bncp_sensitivity(const b2c_bncp *p, double *dlam_dmu, double
  * backward of the batched adjoint, ncp_batch_gpu.py:1172-1186). */
 B2C_API int32_t b2c_bncp_vjp(const b2c_bncp *p, const double *glam, double *gb, double *gmu, b2c_stream s);
 
+/* ---------------------------------------------------------------------------------------------
+ * Engine handle: the ContactEngine protocol (src/motion_engine/contact_engine.py:48-55) as C
+ * calls, for callers without a tensor library.  A handle owns its device memory (one
+ * allocation, sized at the first step from the bodies added; adding bodies afterwards rebuilds
+ * from the added centres, as the reference's add_body does, contact_engine_gpu.py:205-207) and
+ * runs b2c_box_substep, the launch sequence the Python box engine runs, so a handle and the
+ * Python engine over the same bodies give the same bits.  Kind: the box engine (solid boxes,
+ * float64 SAT contacts, the ColorCache pair solve).
+ *
+ * Centres, sizes, densities and dt are float64 as in the reference's Python setup: the body
+ * arrays are computed in float64 and rounded once to float32 (Box.Ib, ncp_gpu.py:1105-1109).
+ * Calls without a stream argument run on the stream of the last b2c_step (the legacy default
+ * stream before the first) and return when their work is done.  A handle is used from one host
+ * thread at a time.
+ * ------------------------------------------------------------------------------------------- */
+#define B2C_ENGINE_BOX 1
+
+typedef struct b2c_config {
+    int32_t kind;               /* B2C_ENGINE_BOX */
+    int32_t device;             /* CUDA device ordinal */
+    int32_t vit, pit;           /* velocity / position sweeps per substep */
+    double mu;                  /* friction of bodies without their own (b2c_set_body_mu) */
+    double dims[3];             /* box edges of bodies added without their own */
+    double margin;              /* contact margin (the reference's 2e-3) */
+    int32_t flags;              /* B2C_COLOR_* */
+    int32_t color_cap;          /* colour cap, <= 512 */
+    int32_t solve_blocks;       /* launch form of the persistent solve (b2c_color_params) */
+    int32_t cand_per_body;      /* candidate pairs reserved per body */
+    int64_t barrier_timeout_ns; /* grid-barrier wait limit; <= 0: 1 s */
+    int32_t graph;              /* 1: each (dt, substeps) step is captured into a CUDA graph
+                                   after its first eager run and replayed afterwards */
+} b2c_config;
+
+/* Counters read back by b2c_sync_header (the Python engines' diagnostics attributes). */
+typedef struct b2c_step_header {
+    b2c_header last;            /* counters of the last substep */
+    int32_t color_cache_hits, color_cache_misses;
+    int32_t graph_captures;     /* CUDA graphs captured so far */
+    int32_t kernels_per_step;   /* kernel nodes of the last captured step graph (0: none yet) */
+    int32_t bodies;
+    int32_t built;              /* 1 once the device arrays exist */
+} b2c_step_header;
+
+/* The box engine's defaults: vit 16, pit 10, mu 0.5, dims 0.3 x 0.3 x 0.2, margin 2e-3, flags
+ * fixed frame | apply warm | cache | warm start | first fit | row form, colour cap 512, solve form
+ * picked from the body count, 16 candidates per body, 1 s barrier limit, graphs on, device 0. */
+B2C_API void b2c_config_init(b2c_config *c);
+/* Host-side body arrays of n solid boxes (Box.Ib, ncp_gpu.py:1105-1109): mass = density x the
+ * box volume and the diagonal body inertia in float64; xc4 (n,4) centre, invM (n) (0 when
+ * kinematic), IbInv12 (n,12) inverse inertia rows (the identity when kinematic), M (n) mass.
+ * Host pointers; no device work.  B2C_EARG for a non-positive mass or a non-finite inverse. */
+B2C_API int32_t b2c_box_body_setup(int32_t n, const double *center3, const double *dims3, const double *density,
+                                   const int32_t *kin, float *xc4, float *invM, float *IbInv12, double *M);
+/* Validates the configuration and returns a handle; no device work until the first step. */
+B2C_API int32_t b2c_create(const b2c_config *c, void **h);
+/* Appends n bodies (add_body / add_box): centres (n,3); densities (n) or NULL (1000); edges
+ * (n,3) or NULL (the configured dims); kinematic flags (n) or NULL (none).  Bodies get the
+ * configured friction and scene 0. */
+B2C_API int32_t b2c_add_bodies(void *h, int32_t n, const double *center3, const double *density, const double *dims3,
+                               const int32_t *kin);
+/* Per-body friction of bodies [first, first+n): a pair uses sqrt(mu_a mu_b), the ground mu_a. */
+B2C_API int32_t b2c_set_body_mu(void *h, int32_t first, int32_t n, const double *mu);
+/* Scene of bodies [first, first+n) for a batch of independent scenes (bodies of different
+ * scenes never touch; each colours as it would alone). */
+B2C_API int32_t b2c_set_body_scene(void *h, int32_t first, int32_t n, const int32_t *scene);
+B2C_API int32_t b2c_body_count(const void *h);
+/* Live kinematic update (contact_engine_gpu.py:241-249): the body moves to xc3 and gets
+ * invM = 0, v = w = 0. */
+B2C_API int32_t b2c_set_kinematic(void *h, int32_t i, const double *xc3);
+/* Advances dt in `substeps` substeps of dt / substeps, asynchronously on s.  Before launching it
+ * reads the previous step's device error bits: if any are set it clears them and returns
+ * B2C_ECAPACITY or B2C_ETIMEOUT without stepping (the Python engines raise RuntimeError). */
+B2C_API int32_t b2c_step(void *h, double dt, int32_t substeps, b2c_stream s);
+/* Waits for the last step and returns its counters. */
+B2C_API int32_t b2c_sync_header(void *h, b2c_step_header *out);
+/* get_state: xc (n,3), q (n,4) quaternion (x, y, z, w), v (n,3), w (n,3) float32, host or device
+ * pointers, any of them NULL to skip. */
+B2C_API int32_t b2c_get_state(void *h, float *xc, float *q, float *v, float *w);
+/* The whole body state as one (4, n, 4) float32 block (planes xc, q, v, w, rows padded to four
+ * floats): one copy on s, asynchronous for pinned host or device memory. */
+B2C_API int32_t b2c_get_state_packed(void *h, float *state, b2c_stream s);
+B2C_API int32_t b2c_set_state_packed(void *h, const float *state, b2c_stream s);
+/* contact_forces: f3 (n,3) float64 host = M (v_after - v_before) / dt of the last substep
+ * (deferred_force.py:66-74); kinematic rows 0. */
+B2C_API int32_t b2c_contact_forces(void *h, double *f3);
+/* Checkpoint: everything a later step reads (body state, masses and kinematic flags, the warm
+ * store, the colour cache, the counters), so that a handle over the same bodies and
+ * configuration that loads the blob continues bit for bit.  blob == NULL: *size receives the
+ * size needed. */
+B2C_API int32_t b2c_state_save(void *h, void *blob, size_t *size);
+B2C_API int32_t b2c_state_load(void *h, const void *blob, size_t size);
+/* Frees the handle and its device memory and sets *h = NULL. */
+B2C_API int32_t b2c_destroy(void **h);
+
 #ifdef __cplusplus
 }
 #endif
