@@ -6,19 +6,27 @@ namespace b2c {
 // k_grav + k_invIw, contact_engine_gpu.py:40-53.  v += (0, 0, -g) dt for dynamic bodies
 // (each component `v + g dt` is one fused multiply-add, as the reference build contracted it);
 // invIw = (R IbInv) R^T, zero for kinematic bodies.
+// With vgrav set it also keeps the velocity after gravity there (the deferred-force reference
+// point, deferred_force.py:33); with pv / po set it clears the position pass's pseudo-velocities
+// (deferred_force.py:37-38, 54-55): the copy and the clears a substep starts with, in the same
+// launch.
 __global__ void k_body_predict(int n, float *__restrict__ v, const float *__restrict__ invM, float dt,
                                const float *__restrict__ q, const float *__restrict__ IbInv,
-                               const int *__restrict__ kin, float *__restrict__ invIw)
+                               const int *__restrict__ kin, float *__restrict__ invIw, float *__restrict__ vgrav,
+                               float *__restrict__ pv, float *__restrict__ po)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    float4 a = ld4(v, i);
     if (invM[i] > 0.0f) {
-        float4 a = ld4(v, i);
         a.x = fmaf(0.0f, dt, a.x);
         a.y = fmaf(0.0f, dt, a.y);
         a.z = fmaf(-B2C_G, dt, a.z);
         st4(v, i, a);
     }
+    if (vgrav) st4(vgrav, i, a);
+    if (pv) st4(pv, i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    if (po) st4(po, i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
     m3 out;
     if (kin[i] == 1) {
         out = m3{f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 0.0f}};
@@ -51,7 +59,18 @@ __global__ void k_body_integrate(int n, float *__restrict__ xc, float *__restric
 int body_predict(const b2c_bodies *b, float dt, cudaStream_t s)
 {
     if (b->n <= 0) return B2C_OK;
-    k_body_predict<<<blocks_for(b->n), kThreads, 0, s>>>(b->n, b->v, b->invM, dt, b->q, b->IbInv, b->kin, b->invIw);
+    k_body_predict<<<blocks_for(b->n), kThreads, 0, s>>>(b->n, b->v, b->invM, dt, b->q, b->IbInv, b->kin, b->invIw,
+                                                         nullptr, nullptr, nullptr);
+    return check_launch("body_predict");
+}
+
+// the first launch of a substep: predict, vgrav = v after gravity, and (clear_pseudo) pv = po = 0
+int body_predict_substep(const b2c_bodies *b, float dt, float *vgrav, bool clear_pseudo, cudaStream_t s)
+{
+    if (b->n <= 0) return B2C_OK;
+    k_body_predict<<<blocks_for(b->n), kThreads, 0, s>>>(b->n, b->v, b->invM, dt, b->q, b->IbInv, b->kin, b->invIw,
+                                                         vgrav, clear_pseudo ? b->pv : nullptr,
+                                                         clear_pseudo ? b->po : nullptr);
     return check_launch("body_predict");
 }
 

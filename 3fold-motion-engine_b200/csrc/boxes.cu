@@ -13,7 +13,7 @@
 namespace b2c {
 
 int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, cudaStream_t s);
-int body_predict(const b2c_bodies *b, float dt, cudaStream_t s);
+int body_predict_substep(const b2c_bodies *b, float dt, float *vgrav, bool clear_pseudo, cudaStream_t s);
 int body_integrate(const b2c_bodies *b, float dt, cudaStream_t s);
 int color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p, cudaStream_t s);
 int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr, const b2c_color_params *p,
@@ -681,12 +681,7 @@ extern "C" int32_t b2c_box_substep(const b2c_bodies *b, b2c_boxes *bx, b2c_conta
     }
     cudaStream_t st = b2c::stream_of(s);
     int rc;
-    if ((rc = b2c::body_predict(b, dt, st))) return rc;
-    if (b->n > 0) {
-        cudaMemcpyAsync(vgrav, b->v, sizeof(float) * 4 * (size_t)b->n, cudaMemcpyDeviceToDevice, st);
-        cudaMemsetAsync(b->pv, 0, sizeof(float) * 4 * (size_t)b->n, st);
-        cudaMemsetAsync(b->po, 0, sizeof(float) * 4 * (size_t)b->n, st);
-    }
+    if ((rc = b2c::body_predict_substep(b, dt, vgrav, true, st))) return rc;
     if ((rc = b2c::box_candidates(b, bx, hdr, st))) return rc;
     if ((rc = b2c::box_contacts(b, bx, kept, kept_keys, pr, warm, hdr, p, st))) return rc;
     if ((rc = b2c::color_pairs(b, pr, hdr, p, st))) return rc;

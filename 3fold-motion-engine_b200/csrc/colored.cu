@@ -22,7 +22,7 @@
 namespace b2c {
 
 int exclusive_scan(const int *in, int *out, int n, const int *dn, int *scratch, cudaStream_t s);
-int body_predict(const b2c_bodies *b, float dt, cudaStream_t s);
+int body_predict_substep(const b2c_bodies *b, float dt, float *vgrav, bool clear_pseudo, cudaStream_t s);
 int body_integrate(const b2c_bodies *b, float dt, cudaStream_t s);
 int bead_world(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
 int grid_build(const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
@@ -1007,13 +1007,8 @@ extern "C" int32_t b2c_color_substep(const b2c_bodies *b, const b2c_beads *beads
     }
     cudaStream_t st = b2c::stream_of(s);
     int rc;
-    if ((rc = b2c::body_predict(b, dt, st))) return rc;
-    if (b->n > 0) {
-        cudaMemcpyAsync(vgrav, b->v, sizeof(float) * 4 * (size_t)b->n, cudaMemcpyDeviceToDevice, st);
-        // pv / po start every substep at zero (deferred_force.py:37-38, 54-55)
-        cudaMemsetAsync(b->pv, 0, sizeof(float) * 4 * (size_t)b->n, st);
-        cudaMemsetAsync(b->po, 0, sizeof(float) * 4 * (size_t)b->n, st);
-    }
+    // predict, vgrav, and pv / po cleared for the substep (deferred_force.py:37-38, 54-55)
+    if ((rc = b2c::body_predict_substep(b, dt, vgrav, true, st))) return rc;
     if ((rc = b2c::bead_world(b, beads, g, st))) return rc;
     if ((rc = b2c::grid_build(beads, g, st))) return rc;
     if ((rc = b2c::bead_contacts_sorted(beads, g, c, m, hdr, st))) return rc;

@@ -230,7 +230,7 @@ int jacobi_solve(const b2c_bodies *b, b2c_contacts *c, const b2c_header *hdr, in
     return check_launch("jacobi_solve");
 }
 
-int body_predict(const b2c_bodies *b, float dt, cudaStream_t s);
+int body_predict_substep(const b2c_bodies *b, float dt, float *vgrav, bool clear_pseudo, cudaStream_t s);
 int body_integrate(const b2c_bodies *b, float dt, cudaStream_t s);
 int bead_world(const b2c_bodies *b, const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
 int grid_build(const b2c_beads *beads, b2c_grid *g, cudaStream_t s);
@@ -258,8 +258,7 @@ extern "C" int32_t b2c_jacobi_substep(const b2c_bodies *b, const b2c_beads *bead
     }
     cudaStream_t st = b2c::stream_of(s);
     int rc;
-    if ((rc = b2c::body_predict(b, dt, st))) return rc;
-    if (b->n > 0) cudaMemcpyAsync(vgrav, b->v, sizeof(float) * 4 * (size_t)b->n, cudaMemcpyDeviceToDevice, st);
+    if ((rc = b2c::body_predict_substep(b, dt, vgrav, false, st))) return rc;
     if ((rc = b2c::bead_world(b, beads, g, st))) return rc;
     if ((rc = b2c::grid_build(beads, g, st))) return rc;
     if ((rc = b2c::bead_contacts(beads, g, c, hdr, st))) return rc;

@@ -119,3 +119,20 @@ def test_colour_cap_error_is_a_status(me):
     with pytest.raises(RuntimeError, match="colour cap"):
         h.step(DT, 1)
     assert h.header()["error"] == 0
+
+
+def test_handle_scenes_equal_batched_engine(me):
+    """Scenes on a handle (b2c_set_body_scene) give BatchedBoxEngine's bits."""
+    sc = importlib.import_module("motion_engine_b200.scenes")
+    scenes = sc.batched_scenes(n_scenes=12, nmin=6, nmax=200, seed_n=7)
+    g = me.BatchedBoxEngine(scenes, mu=0.55, vit=16, pit=10)
+    h = me.HandleBoxEngine(mu=0.55, vit=16, pit=10, cand_per_body=12)
+    for k, s in enumerate(scenes):
+        h.add_boxes(s["centers"], dims=s["dims"], density=s["density"], mu=s["mu"],
+                    kin=s.get("kin", np.zeros(len(s["centers"]), bool)), scene=k)
+    for _ in range(100):
+        g.step(DT, 2)
+        h.step(DT, 2)
+    assert g.get_state_packed().numpy().tobytes() == h.get_state_packed().tobytes()
+    hg, hh = g.check_errors(), h.header()
+    assert (hg["n_pairs"], hg["n_colors"]) == (hh["n_pairs"], hh["n_colors"])
