@@ -150,7 +150,7 @@ def cabi_e2e(me, wl, scene, start, flush, stream, K):
 
     import torch
     h = me.HandleBoxEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
-                           color_cap=wl["color_cap"])
+                           color_cap=wl["color_cap"], device=torch.cuda.current_device())
     h.add_boxes(scene["centers"], dims=scene["dims"], density=scene["density"], mu=scene["mu"])
     dt, S = wl["dt"], wl["substeps"]
     L, s, check = h.L, ctypes.c_void_p(stream.cuda_stream), me._lib.check
