@@ -752,20 +752,38 @@ __global__ void k_warm_gather_row(const b2c_header *__restrict__ hdr, int nbodie
         unsigned long long m = body_colors[b];
         if (!m) continue;
         f3 vv = ld3(v, b), ww = ld3(w, b);
-        while (m) {
-            const int c = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            const int e = body_slots[64 * b + c];
+        int e = body_slots[64 * b + (__ffsll((long long)m) - 1)];
+        m &= m - 1;
+        // The loads run ahead of the arithmetic: the next pair's slot while a pair is applied,
+        // a pair's first contact with its header, the next contact's words while a contact is
+        // applied.  The first contact's words are read before the count arrives: they lie inside
+        // the slot's record whatever its count (and every pair has at least one contact).  The
+        // arithmetic and its order are those of the colour phases.
+        for (;;) {
             const int s = e >> 1;
             const bool sideB = (e & 1) != 0;
+            const int rf = sideB ? kRRB : kRRA;
+            int e_next = -1;
+            if (m) {
+                e_next = body_slots[64 * b + (__ffsll((long long)m) - 1)];
+                m &= m - 1;
+            }
             const int4 h = R.hdr()[s];
             const float4 mm = R.body(6)[s];
             const m3 I = load_inertia(R, s, sideB ? 3 : 0);
             const float iM = sideB ? mm.y : mm.x;
+            float4 n_cn = R.contact(kRN, 0)[s], n_ct1 = R.contact(kRT1, 0)[s], n_im = R.contact(kRImp, 0)[s];
+            float4 n_r = R.contact(rf, 0)[s];
             for (int k = 0; k < h.z; ++k) {
-                const float4 cn = R.contact(kRN, k)[s], ct1 = R.contact(kRT1, k)[s], im = R.contact(kRImp, k)[s];
+                const float4 cn = n_cn, ct1 = n_ct1, im = n_im, rr = n_r;
+                if (k + 1 < h.z) {
+                    n_cn = R.contact(kRN, k + 1)[s];
+                    n_ct1 = R.contact(kRT1, k + 1)[s];
+                    n_im = R.contact(kRImp, k + 1)[s];
+                    n_r = R.contact(rf, k + 1)[s];
+                }
                 const f3 nrm = xyz(cn), t1 = xyz(ct1), t2 = cross3(nrm, t1);
-                const f3 r = xyz(sideB ? R.contact(kRRB, k)[s] : R.contact(kRRA, k)[s]);
+                const f3 r = xyz(rr);
                 const float jn = im.x, j1 = im.y, j2 = im.z;
                 const f3 J{fmaf(j2, t2.x, fmaf(jn, nrm.x, j1 * t1.x)), fmaf(j2, t2.y, fmaf(jn, nrm.y, j1 * t1.y)),
                            fmaf(j2, t2.z, fmaf(jn, nrm.z, j1 * t1.z))};
@@ -781,6 +799,8 @@ __global__ void k_warm_gather_row(const b2c_header *__restrict__ hdr, int nbodie
                     ww = sub3(ww, dw);
                 }
             }
+            if (e_next < 0) break;
+            e = e_next;
         }
         st4(v, b, f4(vv, 0.0f));
         st4(w, b, f4(ww, 0.0f));
