@@ -40,7 +40,12 @@ class Pairs(ctypes.Structure):
                 ("porder", c_void_p), ("cstart", c_void_p), ("ccount", c_void_p), ("claim", c_void_p),
                 ("cached_a", c_void_p), ("cached_b", c_void_p), ("cached_mass", c_void_p),
                 ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
-                ("body_colors", c_void_p), ("body_local", c_void_p), ("body_slots", c_void_p)]
+                ("body_colors", c_void_p), ("body_local", c_void_p), ("body_slots", c_void_p),
+                ("n_scenes", c_int32), ("scene_body_start", c_void_p), ("scene_order", c_void_p),
+                ("pair_slot", c_void_p), ("scene_slots", c_void_p)]
+
+
+SOLVE_SCENES = 0x100000  # b2c_color_params.solve_blocks: one CTA per scene (B2C_SOLVE_SCENES)
 
 
 class Warm(ctypes.Structure):

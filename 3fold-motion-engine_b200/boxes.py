@@ -170,6 +170,18 @@ class BoxContactEngine(_BeadEngineBase):
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
             "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots, _ptr(pb["body_colors"]),
             _ptr(self.local_t), _ptr(pb["body_slots"]))
+        # the scene schedule of the solve (one CTA per scene): possible when each scene's bodies
+        # are contiguous and the scenes in body order, as a batch adds them
+        self.scene_schedule = self.n_scenes > 1 and bool(np.all(np.diff(sc) >= 0))
+        if self.scene_schedule:
+            counts = np.bincount(sc, minlength=self.n_scenes)
+            self.s_bufs = dict(start=torch.from_numpy(np.r_[0, np.cumsum(counts)].astype(np.int32)).to(dev),
+                               order=torch.from_numpy(np.argsort(-counts, kind="stable").astype(np.int32)).to(dev),
+                               pair_slot=i32(pcap), scene_slots=i32(pcap))
+            sb = self.s_bufs
+            self.c_pairs.n_scenes = self.n_scenes
+            self.c_pairs.scene_body_start, self.c_pairs.scene_order = _ptr(sb["start"]), _ptr(sb["order"])
+            self.c_pairs.pair_slot, self.c_pairs.scene_slots = _ptr(sb["pair_slot"]), _ptr(sb["scene_slots"])
         self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
         self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
         self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
@@ -204,7 +216,10 @@ class BoxContactEngine(_BeadEngineBase):
 
     def set_solve_blocks(self, n: int):
         """Launch form of the persistent solve: 0 auto, 1 one CTA, n > 1 a cooperative grid of n
-        CTAs, -n a cluster of n CTAs.  Results do not depend on it.  Drops captured graphs."""
+        CTAs, -n a cluster of n CTAs, _lib.SOLVE_SCENES one CTA per scene (a batch in the row
+        form).  Results do not depend on it.  Drops captured graphs."""
+        if int(n) == _lib.SOLVE_SCENES and self._built and not (self.scene_schedule and self.row_form):
+            raise ValueError(f"{self.name}: the scene schedule needs several scenes in body order and the row form")
         self.solve_blocks = int(n)
         if self._built:
             self.c_params.solve_blocks = self.solve_blocks
@@ -313,10 +328,11 @@ _TUNED = {}
 
 
 def autotune(engine, dt, substeps=1, candidates=(-16, -8, 148, 74), steps=2):
-    """Pick the persistent solve's launch form (a cluster of 16 or 8 CTAs, or a cooperative grid
-    of 148 or 74 CTAs) by timing `steps` live steps of each.  The launch forms give bit-identical
-    results (the tests check it), so tuning on live steps does not change the trajectory.  The
-    choice is cached per (bodies, scenes, colours) and applied to the engine."""
+    """Pick the persistent solve's launch form (a cluster of 16 or 8 CTAs, a cooperative grid
+    of 148 or 74 CTAs, and for a batch also one CTA per scene) by timing `steps` live steps of
+    each.  The launch forms give bit-identical results (the tests check it), so tuning on live
+    steps does not change the trajectory.  The choice is cached per (bodies, scenes, colours)
+    and applied to the engine."""
     import torch
     h = engine.header_dict() if engine._built else {"n_colors": 0}
     key = (engine.N if engine._built else len(engine._centers), getattr(engine, "n_scenes", 1), h["n_colors"])
@@ -324,6 +340,9 @@ def autotune(engine, dt, substeps=1, candidates=(-16, -8, 148, 74), steps=2):
         engine.set_solve_blocks(_TUNED[key][0])
         return _TUNED[key]
     times = {}
+    candidates = list(candidates)
+    if getattr(engine, "scene_schedule", False) and engine.row_form and _lib.SOLVE_SCENES not in candidates:
+        candidates.append(_lib.SOLVE_SCENES)
     for cand in candidates:
         engine.set_solve_blocks(cand)
         engine.step(dt, substeps)  # capture / first run of this form

@@ -169,11 +169,13 @@ __global__ void k_pair_gather_row(const b2c_header *__restrict__ hdr, const int 
                                   const int *__restrict__ pbj, b2c_contacts kept, const float *__restrict__ xc,
                                   const float *__restrict__ invIw, const float *__restrict__ invM,
                                   const float *__restrict__ body_mu, float mu, float dt, Records R, b2c_header *hdr_w,
-                                  const int *__restrict__ col, int *__restrict__ body_slots)
+                                  const int *__restrict__ col, int *__restrict__ body_slots,
+                                  int *__restrict__ pair_slot)
 {
     const int P = (hdr->n_pairs > 0 && hdr->n_colors > 0) ? hdr->n_pairs : 0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P; s += gridDim.x * blockDim.x) {
         const int p = porder[s];
+        if (pair_slot) pair_slot[p] = s;  // the scene schedule's map from pair to record slot
         const int bi = pbi[p], bj = pbj[p];
         int n = pcount[p];
         if (n > R.K) {
@@ -1083,6 +1085,122 @@ __global__ void __launch_bounds__(kClusterThreadsRow) k_color_solve_cluster_row(
     solve_phases<kCluster, true, true>(a, B);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Scene schedule: one CTA per scene of a batch.  Scenes share no bodies, so each scene's colour
+// phases only have to wait for the scene's own pairs: the CTA barrier replaces the barrier over
+// all scenes, and a scene's phase lasts as long as its own heaviest pair.  The pair tasks, the
+// passes and the colour order inside a scene are those of solve_phases, so the bits are too.
+// ---------------------------------------------------------------------------------------------
+struct SceneSched {
+    const int *pbi, *col, *body_start, *order, *pair_slot;
+    int *slots;
+};
+
+// first index in [0, n) whose pbi is >= body (pbi is sorted)
+__device__ __forceinline__ int first_pair_of(const int *pbi, int n, int body)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pbi[mid] < body) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class BA>
+__device__ __forceinline__ void solve_phases_scene(const SolveArgs &a, const SceneSched &sc, const BA &B)
+{
+    const int P = a.hdr->n_pairs, ncg = a.hdr->n_colors;
+    if (P == 0 || ncg == 0) return;  // uniform over all CTAs
+    __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors], s_cur[kMaxSolveColors];
+    __shared__ int s_pa, s_pb, s_nc;
+    const int scene = sc.order ? sc.order[blockIdx.x] : (int)blockIdx.x;
+    if (threadIdx.x == 0) {
+        s_pa = first_pair_of(sc.pbi, P, sc.body_start[scene]);
+        s_pb = first_pair_of(sc.pbi, P, sc.body_start[scene + 1]);
+    }
+    for (int c = threadIdx.x; c < kMaxSolveColors; c += blockDim.x) s_ccount[c] = 0;
+    __syncthreads();
+    const int pa = s_pa, pb = s_pb;
+    // this scene's pairs by colour: counts, offsets, then its record slots in colour order
+    for (int p = pa + (int)threadIdx.x; p < pb; p += blockDim.x) atomicAdd(&s_ccount[sc.col[p]], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0, nc = 0;
+        for (int c = 0; c < ncg && c < kMaxSolveColors; ++c) {
+            s_cstart[c] = acc;
+            s_cur[c] = acc;
+            acc += s_ccount[c];
+            if (s_ccount[c]) nc = c + 1;
+        }
+        s_nc = nc;
+    }
+    __syncthreads();
+    for (int p = pa + (int)threadIdx.x; p < pb; p += blockDim.x)
+        sc.slots[pa + atomicAdd(&s_cur[sc.col[p]], 1)] = sc.pair_slot[p];
+    __syncthreads();
+    const int nc = s_nc;
+    if (nc == 0) return;  // uniform within the CTA
+    const int *slots = sc.slots + pa;
+    const int me = (int)threadIdx.x, nth = (int)blockDim.x;
+    const int vpasses = (a.apply_warm ? 1 : 0) + a.vit;
+    const int passes = vpasses > a.pit ? vpasses : a.pit;
+    auto task_slot = [&](int pass, int ci, int t, bool &pos) -> int {
+        const int cnt = s_ccount[ci], p0 = (cnt + 31) & ~31;
+        if (t < cnt) {
+            pos = false;
+            return pass < vpasses ? slots[s_cstart[ci] + t] : -1;
+        }
+        pos = true;
+        return (pass < a.pit && t >= p0 && t < p0 + cnt) ? slots[s_cstart[ci] + (t - p0)] : -1;
+    };
+    RowPre pre;
+    int pre_t = -1;
+    bool pos;
+    {
+        const int sl = task_slot(0, 0, me, pos);
+        if (sl >= 0) {
+            pre = row_pre(a.rec, sl, pos);
+            pre_t = me;
+        }
+    }
+    for (int pass = 0; pass < passes; ++pass) {
+        const bool warm = a.apply_warm && pass == 0;
+        for (int ci = 0; ci < nc; ++ci) {
+            const int cnt = s_ccount[ci], ntask = ((cnt + 31) & ~31) + cnt;
+            for (int t = me; t < ntask; t += nth) {
+                const int sl = task_slot(pass, ci, t, pos);
+                if (sl < 0) continue;
+                const RowPre q = (t == pre_t) ? pre : row_pre(a.rec, sl, pos);
+                if (!pos) {
+                    if (warm) pair_apply_warm_row(a, sl, B, q);
+                    else pair_velocity_row(a, sl, B, q);
+                } else {
+                    pair_position_row(a, sl, B, q);
+                }
+            }
+            pre_t = -1;
+            const int np = ci + 1 < nc ? pass : pass + 1, nci = ci + 1 < nc ? ci + 1 : 0;
+            if (nc > 1 && np < passes) {
+                const int sl = task_slot(np, nci, me, pos);
+                if (sl >= 0) {
+                    pre = row_pre(a.rec, sl, pos);
+                    pre_t = me;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+constexpr int kSceneThreads = 256;
+__global__ void __launch_bounds__(kSceneThreads, 2) k_color_solve_scenes(SolveArgs a, SceneSched sc)
+{
+    const GlobalBodies B{a.v, a.w, a.pv, a.po};
+    solve_phases_scene(a, sc, B);
+}
+
 // dynamic shared memory of a solve launch: the contact staging of its threads
 static size_t stage_bytes(int threads) { return (size_t)kStageBytesPerThread * threads; }
 
@@ -1097,6 +1215,8 @@ static void allow_stage_smem()
                          (int)stage_bytes(kClusterThreads));
     cudaFuncSetAttribute(k_color_solve_cluster_row, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)stage_bytes(kClusterThreadsRow));
+    cudaFuncSetAttribute(k_color_solve_scenes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)stage_bytes(kSceneThreads));
     done = true;
 }
 
@@ -1170,13 +1290,19 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
+    const bool scenes = p->solve_blocks == B2C_SOLVE_SCENES;
+    if (scenes && !(a.row && pr->n_scenes > 0 && pr->scene_body_start && pr->pair_slot && pr->scene_slots)) {
+        set_error("color_solve: the scene schedule needs the row form and b2c_pairs' scene arrays");
+        return B2C_EARG;
+    }
     // the warm start body by body (one launch) instead of a pass of colour phases
     const bool warm_bodies = a.row && a.apply_warm && (p->flags & B2C_COLOR_FIRST_FIT) && pr->body_slots &&
                              pr->body_colors;
     if (a.row)
         k_pair_gather_row<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi,
                                                      pr->pbj, *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, dt,
-                                                     a.rec, hdr, pr->col, warm_bodies ? pr->body_slots : nullptr);
+                                                     a.rec, hdr, pr->col, warm_bodies ? pr->body_slots : nullptr,
+                                                     scenes ? pr->pair_slot : nullptr);
     else
         k_pair_gather<<<pgrid, kThreads, 0, s>>>(hdr, pr->porder, pr->pstart, pr->kcount, pr->pidx, pr->pbi, pr->pbj,
                                                  *kept, b->xc, b->invIw, b->invM, p->body_mu, p->mu, a.rec, hdr);
@@ -1191,7 +1317,14 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     }
 
     int mode = p->solve_blocks;
-    if (mode == 0) {  // auto: one CTA for tiny scenes, else a cluster (colours wider than it loop)
+    if (scenes) {
+        allow_stage_smem();
+        const SceneSched sc{pr->pbi, pr->col, pr->scene_body_start, pr->scene_order, pr->pair_slot,
+                            pr->scene_slots};
+        k_color_solve_scenes<<<pr->n_scenes, kSceneThreads, stage_bytes(kSceneThreads), s>>>(a, sc);
+        if ((rc = check_launch("color_solve_scenes"))) return rc;
+        mode = 0;
+    } else if (mode == 0) {  // auto: one CTA for tiny scenes, else a cluster (colours wider than it loop)
         if (b->n <= 64) mode = 1;
         else mode = -kClusterMax;
     }

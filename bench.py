@@ -863,7 +863,8 @@ def main():
         # the solve's launch form, picked on live (untimed) steps after the warm-up, then one more
         # untimed step on the chosen form (its graph capture)
         best, times = me.autotune(e, dt, S, steps=4)
-        tuned = {"solve_blocks": best, "ms_per_step": {str(k): round(v, 4) for k, v in times.items()}}
+        form = lambda k: "scenes" if k == me._lib.SOLVE_SCENES else str(k)
+        tuned = {"solve_blocks": form(best), "ms_per_step": {form(k): round(v, 4) for k, v in times.items()}}
         e.step(dt, S)
     e.check_errors()
     torch.cuda.synchronize()

@@ -186,6 +186,16 @@ typedef struct b2c_pairs {
                                 [64 b + c]; the warm start is then applied body by body in
                                 colour order (the same bits as colour by colour) instead of in
                                 one pass of colour phases. */
+    /* Scene schedule of the solve (b2c_color_params.solve_blocks == B2C_SOLVE_SCENES, row form):
+     * one CTA per scene, each scene's colour phases separated by its own CTA barrier, not by
+     * a barrier over all scenes.  Scenes share no bodies, so the bits are those of the other
+     * forms.  The bodies of a scene are contiguous and the scenes in body order; a scene's pairs
+     * are then contiguous too (pairs are sorted by their first body).  Zero / NULL when unused. */
+    int32_t n_scenes;
+    const int32_t *scene_body_start; /* (n_scenes+1) first body of each scene */
+    const int32_t *scene_order;      /* (n_scenes) launch order of the scenes (largest first), or NULL */
+    int32_t *pair_slot;              /* (capacity) record slot of each pair, written by the gather */
+    int32_t *scene_slots;            /* (capacity) each scene's record slots grouped by colour */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -246,6 +256,8 @@ typedef struct b2c_boxes {
 #define B2C_COLOR_PER_CONTACT 16 /* no manifold reduction; every contact is its own chunk and is
                                     coloured on the contact graph (the plain coloured engine) */
 
+#define B2C_SOLVE_SCENES 0x100000 /* b2c_color_params.solve_blocks: the scene schedule */
+
 typedef struct b2c_color_params {
     int32_t vit, pit;        /* velocity / position sweeps */
     int32_t max_points;      /* manifold points kept per pair (<= 8) */
@@ -255,7 +267,8 @@ typedef struct b2c_color_params {
     int32_t color_cap;       /* error when the pair graph needs more colours (<= max_colors) */
     int32_t solve_blocks;    /* persistent solve shape: 0 = pick from the body count; n > 0 = n CTAs
                                 with a grid barrier (1 = one CTA, block barriers); -n = a thread-block
-                                cluster of n CTAs with the hardware cluster barrier */
+                                cluster of n CTAs with the hardware cluster barrier;
+                                B2C_SOLVE_SCENES = one CTA per scene (b2c_pairs' scene schedule) */
     int64_t barrier_timeout_ns; /* grid-barrier wait limit */
     const float *body_mu;    /* (bodies) per-body friction, or NULL for the scalar mu: a body pair's
                                 contacts use sqrt(mu_a mu_b), a ground pair mu_a */

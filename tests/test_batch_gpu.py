@@ -67,7 +67,7 @@ def test_autotune_keeps_results(me):
         a.step(DT, 2)
         b.step(DT, 2)
     best, times = me.autotune(a, DT, 2, steps=1)
-    assert best in times and len(times) == 4
+    assert best in times and len(times) == 5 and me._lib.SOLVE_SCENES in times
     for _ in range(sum(1 + 1 for _ in times)):  # the tuner advanced a by 2 steps per candidate
         b.step(DT, 2)
     for _ in range(10):
@@ -75,3 +75,24 @@ def test_autotune_keeps_results(me):
         b.step(DT, 2)
     for x, y in zip(_state(a), _state(b)):
         np.testing.assert_array_equal(x, y)
+
+
+def test_scene_schedule_same_bits(me):
+    """One CTA per scene (the scene schedule) gives the bits of the grid and cluster forms: the
+    scenes share no bodies and each keeps its colour order."""
+    scenes = _scenes(24, 400, seed=11)
+    runs = []
+    for form in (148, -16, me._lib.SOLVE_SCENES):
+        g = me.BatchedBoxEngine(scenes, mu=0.55, vit=16, pit=10)
+        g.set_solve_blocks(form)
+        for _ in range(120):
+            g.step(DT, 2)
+        g.check_errors()
+        runs.append(g.get_state_packed().numpy().tobytes())
+    assert runs[0] == runs[1] == runs[2]
+    alone = me.BoxContactEngine(mu=0.55, vit=16, pit=10, cand_per_body=12)
+    with pytest.raises(ValueError, match="scene schedule"):
+        for c, d, de, m in zip(scenes[0]["centers"], scenes[0]["dims"], scenes[0]["density"], scenes[0]["mu"]):
+            alone.add_box(c, dims=d, density=de, mu=m)
+        alone.step(DT, 2)
+        alone.set_solve_blocks(me._lib.SOLVE_SCENES)
