@@ -16,7 +16,8 @@ Rank 0 prints one JSON line.
 
 `e2e` is the same metric through the public API with the body state in pinned host memory:
 every step uploads the state (set_state_packed), steps, and downloads it again
-(get_state_packed).
+(get_state_packed).  For the box workloads `e2e_cabi` repeats that loop through the C engine
+handle (b2c_set_state_packed, b2c_step, b2c_get_state_packed), from the same state.
 
 `--impl reference` times the CPU restatement of the same algorithm (the oracle; the reference
 runs these engines through Warp, which is not installed) on the same workload, one replica per
