@@ -8,7 +8,7 @@ reference's engine classes.
 The directory name is not a Python identifier, so the package is imported under the alias
 ``motion_engine_b200`` (see ``__graft_entry__.load_package``).
 """
-from . import _lib, build
+from . import _lib, build, metrics
 from .boxes import BatchedBoxEngine, BoxContactEngine, autotune, partition_scenes
 from .colored import (AppliedWarmContactEngine, ColorCacheContactEngine, DeferredForceContactEngine,
                       FixedFrameContactEngine, GraphColoredContactEngine)
@@ -17,4 +17,4 @@ from .handle import HandleBoxEngine
 
 __all__ = ["BodyState", "ContactEngine", "RelaxedJacobiContactEngine", "GraphColoredContactEngine",
            "FixedFrameContactEngine", "AppliedWarmContactEngine", "DeferredForceContactEngine",
-           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "HandleBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "_lib"]
+           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "HandleBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "metrics", "_lib"]

@@ -40,6 +40,7 @@ struct Engine {
     bool built = false;
     int N = 0, nbk = 0, cand_cap = 0, kept_cap = 0, pcap = 0;
     std::vector<double> M;            // masses, for contact_forces (inf once made kinematic)
+    std::vector<double> M0;           // every body's mass from its box and density, kinematic or not
     std::vector<int32_t> kinarr;
     char *arena = nullptr;
     size_t arena_bytes = 0;
@@ -311,6 +312,7 @@ int build(Engine *e)
     p.t2d = 1.0f, p.color_cap = std::min(e->cfg.color_cap, kMaxColors), p.solve_blocks = e->cfg.solve_blocks;
     p.barrier_timeout_ns = e->cfg.barrier_timeout_ns > 0 ? e->cfg.barrier_timeout_ns : 1000000000LL;
     p.body_mu = per_body_mu ? e->body_mu : nullptr;
+    e->M0 = M;
     e->M = M;
     e->kinarr = e->kin;
     e->built = true;
@@ -815,8 +817,12 @@ extern "C" int32_t b2c_state_load(void *h, const void *blob, size_t size)
         return cuda_fail("b2c_state_load", ce);
     if ((ce = cudaMemcpy(e->hdr_host, e->header, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return cuda_fail("b2c_state_load", ce);
-    for (int i = 0; i < e->N; ++i)
-        if (kin[i] && !e->kinarr[i]) e->kinarr[i] = 1, e->kin[i] = 1, e->M[i] = INFINITY;
+    // the blob's flags hold in both directions: a body made kinematic after the save is dynamic
+    // again, with its mass from the build
+    for (int i = 0; i < e->N; ++i) {
+        e->kinarr[i] = e->kin[i] = kin[i] ? 1 : 0;
+        e->M[i] = kin[i] ? INFINITY : e->M0[i];
+    }
     e->has_force = hd.has_force != 0;
     e->force_dt = hd.force_dt;
     return B2C_OK;

@@ -116,12 +116,44 @@ constexpr int noalloc_scratch_ints(int n)
 constexpr int kNoAllocScratchInts = noalloc_scratch_ints(kNoAllocMaxN);
 static __device__ __align__(256) int g_noalloc_scan_scratch[kNoAllocScratchInts];
 
-// Device address of the scratch array for the current device, looked up once per device (with
-// that device current) and cached.
+// Identifier of the calling thread's current CUDA context, 0 when there is none or it cannot be
+// read.  The driver's cuCtxGetCurrent / cuCtxGetId are reached through the runtime's entry-point
+// query, so the library does not link the driver library itself.
+typedef int (*ctx_current_fn)(void **);
+typedef int (*ctx_id_fn)(void *, unsigned long long *);
+static unsigned long long current_context_id()
+{
+    static ctx_current_fn get_cur = nullptr;
+    static ctx_id_fn get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {  // the callers hold the scratch mutex
+        tried = true;
+        void *f = nullptr, *g = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &g, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_cur = reinterpret_cast<ctx_current_fn>(f);
+            get_id = reinterpret_cast<ctx_id_fn>(g);
+        }
+        cudaGetLastError();  // a failed query leaves no sticky error behind
+    }
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch array for the current device.  It is looked up with that
+// device current and cached per device together with the context it belongs to; a call from
+// another context of the device (after cudaDeviceReset the runtime makes a new one and loads the
+// library's module again) looks it up again instead of reusing an address of a context that is
+// gone.
 static int noalloc_scratch(int **out)
 {
     static std::mutex mu;
     static int *addr[64] = {};
+    static unsigned long long ctx_of[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
@@ -129,7 +161,8 @@ static int noalloc_scratch(int **out)
         return B2C_ECUDA;
     }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!addr[dev] || ctx == 0 || ctx != ctx_of[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
         if (e != cudaSuccess || !p) {
@@ -137,6 +170,7 @@ static int noalloc_scratch(int **out)
             return B2C_ECUDA;
         }
         addr[dev] = static_cast<int *>(p);
+        ctx_of[dev] = current_context_id();  // the lookup made the device's context current
     }
     *out = addr[dev];
     return B2C_OK;
@@ -148,7 +182,7 @@ extern "C" int32_t b2c_scan_noalloc_max_n(void) { return b2c::kNoAllocMaxN; }
 
 extern "C" int32_t b2c_exclusive_scan_noalloc(const int32_t *in, int32_t *out, int32_t n, b2c_stream s)
 {
-    if (!in || !out || n < 0) {
+    if (n < 0 || (n > 0 && (!in || !out))) {
         b2c::set_error("b2c_exclusive_scan_noalloc: bad argument");
         return B2C_EARG;
     }
@@ -159,8 +193,8 @@ extern "C" int32_t b2c_exclusive_scan_noalloc(const int32_t *in, int32_t *out, i
         return B2C_EARG;
     }
     int *scratch = nullptr;
-    const int rc = b2c::noalloc_scratch(&scratch);
-    if (rc) return rc;
+    const int rc = b2c::noalloc_scratch(&scratch);  // also the whole of a call with n = 0
+    if (rc || n == 0) return rc;
     return b2c::exclusive_scan(in, out, n, nullptr, scratch, b2c::stream_of(s));
 }
 

@@ -344,6 +344,43 @@ class _BeadEngineBase:
     def com(self, i):
         return self.xc[i, :3].cpu().numpy()
 
+    def kept_contacts(self) -> dict:
+        """The contacts the last substep solved, in feature order, as numpy arrays named like
+        the reference engine's attributes (contact_engine_gpu_colored.py:1095-1103): ckeys, sbi,
+        sbj, spA, spB, sn, spen (depth) and the impulses after the solve jn, jt1, jt2, jp.  For
+        the manifold engines and the box engine these are the kept contacts.  The relaxed-Jacobi
+        engine solves every generated contact in the order the atomic append left them, has no
+        feature keys (ckeys is -1) and keeps no impulses per contact (zeros)."""
+        if not self._built:
+            self._build()
+        h = self.header_dict()
+        if hasattr(self, "k_keys"):
+            C = h["n_kept"]
+            keys, bi, bj, pA, pB, nrm, imp = (self.k_keys, self.k_bi, self.k_bj, self.k_pA, self.k_pB, self.k_n,
+                                              self.k_imp)
+        else:
+            C = h["n_contacts"]
+            keys = torch.full((max(C, 1),), -1, dtype=torch.int64)
+            bi, bj, pA, pB, nrm, imp = self.cbi, self.cbj, self.cpA, self.cpB, self.cn, self.cimp
+        pA_ = pA[:C].cpu().numpy()
+        imp_ = imp[:C].cpu().numpy()
+        return dict(ckeys=keys[:C].cpu().numpy(), sbi=bi[:C].cpu().numpy(), sbj=bj[:C].cpu().numpy(),
+                    spA=np.ascontiguousarray(pA_[:, :3]), spB=pB[:C, :3].cpu().numpy(),
+                    sn=nrm[:C, :3].cpu().numpy(), spen=np.ascontiguousarray(pA_[:, 3]),
+                    jn=np.ascontiguousarray(imp_[:, 0]), jt1=np.ascontiguousarray(imp_[:, 1]),
+                    jt2=np.ascontiguousarray(imp_[:, 2]), jp=np.ascontiguousarray(imp_[:, 3]))
+
+    def max_depth_device(self) -> torch.Tensor:
+        """The deepest penetration among the last substep's solved contacts, as a 0-d float32
+        device tensor computed on the engine's stream without a host read (0 without
+        contacts).  The quality figure beside a timed step."""
+        if hasattr(self, "k_pA"):
+            depth, n = self.k_pA[:, 3], self.header[_lib.HEADER_FIELDS.index("n_kept")]
+        else:
+            depth, n = self.cpA[:, 3], self.header[_lib.HEADER_FIELDS.index("n_contacts")]
+        live = torch.arange(depth.shape[0], device=depth.device, dtype=torch.int32) < n
+        return torch.where(live, depth, torch.zeros((), dtype=depth.dtype, device=depth.device)).max()
+
 
 class RelaxedJacobiContactEngine(_BeadEngineBase):
     """Relaxed Jacobi with int64 fixed-point accumulation on bead bodies: the B200 build of the

@@ -32,6 +32,7 @@ and its adjoint at the reference's batched-adjoint shape).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -54,7 +55,7 @@ WORKLOADS = {
     # 2 substeps x (16 velocity + 16 position sweeps), broadphase rebuilt every substep, 200 steps
     "stress100k": dict(engine="box", scene="box_lattice", n=100000, edge=(0.25, 0.25), box=(50.0, 50.0, 10.0),
                        mu_range=(0.6, 0.6), density=1000.0, vit=16, pit=16, substeps=2, dt=1 / 240, color_cap=32,
-                       preroll=100, steps=100, warmup=3),
+                       preroll=100, steps=200, warmup=3, parity_steps=20),
     # 512 independent box scenes of 8..2000 bodies (log-uniform), ~180k bodies, 10 % of each scene
     # 100x denser, advanced together by one batched engine; scenes are sharded over GPUs
     "batched512": dict(engine="batched", scene="batched", n_scenes=512, nmin=8, nmax=2000, edge=(0.2, 0.6),
@@ -91,6 +92,13 @@ WORKLOADS = {
                               pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                               published=(1e4 / 5.599e-3, "reference relaxed Jacobi, 5.599 ms/step, RTX 5070 "
                                          "(docs/RUNNING.md:374-379)")),
+    # plain relaxed Jacobi on a vertical stack of 16 unit cubes (1 m edge, 1 kg: density 1, 1000
+    # beads each) with seeded 1 mm xy jitter, mu 0.5, 40 velocity / 20 position iterations, relax
+    # 0.2, 1 substep, dt 1/240, 240 steps; penetration target 1e-3 m (max over adjacent pairs of
+    # 1.0 - dz, and 0.5 - z of the lowest cube)
+    "jacobi_stack16": dict(engine="jacobi", scene="unit_cube_stack", n=16, dims=(1.0, 1.0, 1.0), density=1.0,
+                           mu=0.5, vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=240, warmup=3,
+                           stack_pitch=1.0, stack_ground=0.5, pen_target_m=1e-3),
 }
 DEFAULT_WORKLOAD = "boxes10k"
 
@@ -117,6 +125,8 @@ def scene_of(wl):
                               density=wl["density"])
     if wl["scene"] == "random_boxes":
         return sc.random_boxes(n=wl["n"], edge=wl["edge"], box=wl["box"], mu=wl["mu_range"], density=wl["density"])
+    if wl["scene"] == "unit_cube_stack":
+        return {"centers": sc.unit_cube_stack(wl["n"])}
     return {"centers": sc.lattice(wl["n"]) if wl["scene"] == "lattice" else sc.stack(wl["n"])}
 
 
@@ -137,7 +147,7 @@ def make_engine(me, wl, scene):
     else:
         raise ValueError(wl["engine"])
     for c in scene["centers"]:
-        e.add_body(c)
+        e.add_body(c, density=wl.get("density", 700.0))
     return e
 
 
@@ -191,8 +201,84 @@ def make_oracle(wl, scene):
     else:
         o = O.ColoredOracle(mode="color_cache", dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
     for c in scene["centers"]:
-        o.add_body(c)
+        o.add_body(c, density=wl.get("density", 700.0))
     return o
+
+
+def state_digest(xc, q, v, w) -> str:
+    """sha256 of a body state: positions (N,3), quaternions (N,4), velocities and angular
+    velocities (N,3), float32, concatenated in that order."""
+    h = hashlib.sha256()
+    for a in (xc, q, v, w):
+        h.update(np.ascontiguousarray(a, np.float32).tobytes())
+    return h.hexdigest()
+
+
+def combine_digests(digests) -> str:
+    """One digest over per-scene digests in scene order."""
+    return hashlib.sha256("".join(digests).encode()).hexdigest()
+
+
+def _oracle_state(o):
+    return o.body_state() if hasattr(o, "body_state") else (o.b.xc, o.b.q, o.b.v, o.b.w)
+
+
+def _parity_worker(workload, idx, steps):
+    """The oracle over the workload's first `steps` steps from its initial state: one state
+    digest, or for a batch one per scene of `idx` (scenes are independent, so each runs alone)."""
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ge.load_package()
+    wl = WORKLOADS[workload]
+    sc = scene_of(wl)
+    t0 = time.perf_counter()
+    out = []
+    if wl["engine"] == "batched":
+        for i in idx:
+            o = _box_oracle(wl, sc["scenes"][i])
+            for _ in range(steps):
+                o.step(wl["dt"], wl["substeps"])
+            out.append((i, state_digest(*o.body_state())))
+    else:
+        o = make_oracle(wl, sc)
+        for _ in range(steps):
+            o.step(wl["dt"], wl["substeps"])
+        out.append((0, state_digest(*_oracle_state(o))))
+    return out, time.perf_counter() - t0
+
+
+class ParityCheck:
+    """The oracle's state digest after the workload's first `steps` steps, computed in spawned
+    processes while the GPU runs (started before the first GPU call), to set beside the GPU
+    engine's digest at the same step.  A batch is split over processes by scene (LPT)."""
+
+    def __init__(self, args, wl, steps, scene_idx=None):
+        import multiprocessing as mp
+        self.steps = steps
+        self.batched = scene_idx is not None
+        if scene_idx is None:
+            parts = [[0]]
+        else:
+            counts = [len(sc["centers"]) for sc in scene_of(wl)["scenes"]]
+            nproc = max(1, min((os.cpu_count() or 2) - 1, 16, len(scene_idx)))
+            sub = [counts[i] for i in scene_idx]
+            parts = [[scene_idx[j] for j in p] for p in partition_scenes(sub, nproc) if p]
+        self.pool = mp.get_context("spawn").Pool(len(parts))
+        self.res = self.pool.starmap_async(_parity_worker, [(args.workload, p, steps) for p in parts])
+
+    def result(self, gpu_digest, timeout=900.0):
+        out = {"steps": self.steps, "gpu_sha256": gpu_digest, "oracle_sha256": None, "equal": None}
+        try:
+            res = self.res.get(timeout=timeout)
+            digests = dict(d for part, _ in res for d in part)
+            od = combine_digests([digests[k] for k in sorted(digests)]) if self.batched else digests[0]
+            out.update(oracle_sha256=od, equal=od == out["gpu_sha256"],
+                       oracle_s=round(max(t for _, t in res), 1))
+        except Exception as ex:  # the oracle did not finish: reported, not raised
+            out["note"] = f"oracle digest unavailable: {type(ex).__name__}"
+        finally:
+            self.pool.terminate()
+        return out
 
 
 class ClockSampler:
@@ -371,6 +457,8 @@ def run_reference(args, wl):
     pre_s = time.perf_counter() - t_pre
     fd, path = tempfile.mkstemp(suffix=".npz")
     os.close(fd)
+    parity = ({"steps": wl["preroll"], "oracle_sha256": state_digest(*_oracle_state(o))}
+              if wl["preroll"] > 0 else None)
     try:
         st = o.body_state() if hasattr(o, "body_state") else None
         np.savez(path, **{k: np.asarray(v) for k, v in scene.items()},
@@ -397,7 +485,7 @@ def run_reference(args, wl):
                                        f"after the workload's {wl['preroll']} set-up steps (oracle, {pre_s:.0f} s) and "
                                        f"{args.warmup} warm-up steps; the reference's Warp CPU path is not installed"},
             "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall}
+            "parity": parity, "wall_s": wall}
     print(json.dumps(line), flush=True)
 
 
@@ -790,6 +878,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the oracle digest at the parity step (it runs in spawned processes)")
     ap.add_argument("--save-state", default=None,
                     help="write the body state after the set-up steps to this .npz (profiling aid)")
     ap.add_argument("--load-state", default=None,
@@ -824,6 +914,12 @@ def main():
         n_job = sum(counts)
         mine = partition_scenes(counts, world)[rank]
         scene = {"scenes": [scene["scenes"][i] for i in mine]}
+    # the oracle's digest at the parity step, computed beside the GPU run (rank 0; spawned before
+    # the first GPU call)
+    parity_steps = wl.get("parity_steps") or (wl["preroll"] if wl["preroll"] > 0 else args.warmup)
+    parity = None
+    if rank == 0 and not args.load_state and not args.no_parity:
+        parity = ParityCheck(args, wl, parity_steps, mine if wl["engine"] == "batched" else None)
     cpu_base = None
     do_cpu = rank == 0 and not args.no_cpu_baseline
     if do_cpu and wl["engine"] not in ("box", "batched"):
@@ -847,18 +943,35 @@ def main():
 
     e = make_engine(me, wl, scene)
     dt, S = wl["dt"], wl["substeps"]
+    gpu_digest = None
+
+    def gpu_state_digest():
+        st = e.get_state_packed().numpy()
+        xc, q, v, w = st[0, :, :3], st[1], st[2, :, :3], st[3, :, :3]
+        if wl["engine"] != "batched":
+            return state_digest(xc, q, v, w)
+        return combine_digests([state_digest(xc[sl], q[sl], v[sl], w[sl])
+                                for sl in (e.scene_slice(k) for k in range(len(scene["scenes"])))])
+
+    n_done = 0
     if args.load_state:
         d = np.load(args.load_state)
         e.set_body_state(d["xc"], d["q"], d["v"], d["w"])
     else:
         for _ in range(wl["preroll"]):
             e.step(dt, S)
+            n_done += 1
+            if n_done == parity_steps and parity is not None:
+                gpu_digest = gpu_state_digest()
     if args.save_state:
         torch.cuda.synchronize()
         np.savez(args.save_state, xc=e.xc[:, :3].cpu().numpy(), q=e.q.cpu().numpy(), v=e.v[:, :3].cpu().numpy(),
                  w=e.w[:, :3].cpu().numpy())
     for _ in range(args.warmup):
         e.step(dt, S)
+        n_done += 1
+        if n_done == parity_steps and parity is not None:
+            gpu_digest = gpu_state_digest()
     tuned = None
     if wl["engine"] in ("batched", "color_cache"):
         # the solve's launch form, picked on live (untimed) steps after the warm-up, then one more
@@ -879,15 +992,21 @@ def main():
     counts = []
     barrier()
     torch.cuda.synchronize()
+    depth, hdrs = [], []  # per timed step, on the device, outside the events: deepest contact, counters
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
             evs[k][0].record(stream)
             e.step(dt, S)
             evs[k][1].record(stream)
+            depth.append(e.max_depth_device())
+            hdrs.append(e.header.clone())
         torch.cuda.synchronize()
         barrier()
     ms = sum(a.elapsed_time(b) for a, b in evs)
+    depth = torch.stack(depth).cpu().numpy().astype(np.float64)
+    hdrs = torch.stack(hdrs).cpu().numpy()
+    colours_timed = hdrs[:, me._lib.HEADER_FIELDS.index("n_colors")]
     h_end = e.check_errors()
     launches_per_step = max(e.kernels_per_step.values()) if e.kernels_per_step else 0
 
@@ -952,6 +1071,26 @@ def main():
                     "sample": f"{n} steps of the same workload from the GPU's body state at the start of the timed "
                               f"region, on one host core ({el:.1f} s; the oracle restatement, not the reference's "
                               f"Warp CPU path)"}
+    # quality beside the time: the reference's M5 gate over a per-step penetration series
+    metrics = me.metrics
+    if "stack_pitch" in wl:
+        # the reference's own M5 figure for a stack (adjacent spacing against the rest pitch, the
+        # lowest body against the ground) over the workload's steps from its initial state, on a
+        # fresh engine: the engine is bit-identical run to run, so this replays the same trajectory
+        q_e = make_engine(me, wl, scene_of(wl))
+        pens = []
+        for _ in range(wl["steps"]):
+            q_e.step(dt, S)
+            pens.append(metrics.stack_penetration(q_e.xc[:, 2].cpu().numpy(), wl["stack_pitch"],
+                                                  ground=wl.get("stack_ground")))
+        quality = dict(metrics.m5(pens), series="stack spacing against the rest pitch and the ground, per step "
+                                                "(engine_metrics.py M5) over the workload's steps from the start")
+        if "pen_target_m" in wl:
+            quality.update(target_m=wl["pen_target_m"], meets_target=bool(quality["max_pen_m"] <= wl["pen_target_m"]))
+    else:
+        quality = dict(metrics.m5(depth), series="deepest solved contact of each timed step (M5's rule, "
+                                                 "engine_metrics.py:265-293, over this series)")
+    parity_line = parity.result(gpu_digest) if parity is not None else None
     peaks, peak_kind = _peaks()
     value = n_job * args.steps / (ms / 1e3)
     roof = None
@@ -993,6 +1132,8 @@ def main():
                     "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io, "steps": K2},
             "gpu_launches": launches_per_step * args.steps, "launches_per_step": launches_per_step,
             "roofline": roof, "cpu_baseline": cpu_base, "stage_ms": stage_ms, "last_step": h_end,
+            "quality": quality, "parity": parity_line,
+            "colors_timed_steps": {"max": int(colours_timed.max()), "mean": float(colours_timed.mean())},
             "colors_e2e_steps": {"max": max(colors), "mean": float(np.mean(colors))}}
     if cabi_ms > 0:
         line["e2e_cabi"] = {"value": n_job * K2 / (cabi_ms / 1e3), "unit": "body-steps/s",

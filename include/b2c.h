@@ -293,8 +293,10 @@ B2C_API int32_t b2c_exclusive_scan(const int32_t *in, int32_t *out, int32_t n, i
  * one library-owned device array per device for at most b2c_scan_noalloc_max_n() = 2^24
  * elements; larger n returns B2C_EARG with a message.  Calls share that array: two calls that
  * overlap in time (concurrent streams or host threads) race, so order them on one stream.  The
- * first call on a device looks up the array's address; make it (n = 0 is enough) before any
- * stream capture begins on that device. */
+ * first call on a device looks up the array's address; make it before any stream capture begins
+ * on that device.  A call with n = 0 does only that, and accepts null in and out.  The address
+ * is cached per device and per CUDA context: after cudaDeviceReset the next call looks it up
+ * again, so make that call before a capture too. */
 B2C_API int32_t b2c_exclusive_scan_noalloc(const int32_t *in, int32_t *out, int32_t n, b2c_stream s);
 B2C_API int32_t b2c_scan_noalloc_max_n(void);
 

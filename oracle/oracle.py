@@ -208,6 +208,8 @@ def _col_sigs(L):
     L.or_col_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, P, P, P, P, ctypes.c_double,
                               ctypes.c_int, P]
     L.or_col_step.restype = ctypes.c_int
+    L.or_col_kept.argtypes = [P] * 12
+    L.or_col_kept.restype = ctypes.c_int
 
 
 class ColoredOracle:
@@ -289,6 +291,20 @@ class ColoredOracle:
     @property
     def n_contacts(self):
         return self.stats()["n_contacts"]
+
+    def kept_contacts(self) -> dict:
+        """The last substep's kept contacts in feature order, named as the reference's engine
+        attributes (ckeys, sbi, sbj, spA, spB, sn, spen, jn, jt1, jt2, jp; COL:1095-1103)."""
+        L = lib()
+        C = int(L.or_col_kept(self._h, *([None] * 11)))
+        out = dict(ckeys=np.zeros(C, np.int64), sbi=np.zeros(C, np.int32), sbj=np.zeros(C, np.int32),
+                   spA=np.zeros((C, 3), np.float32), spB=np.zeros((C, 3), np.float32), sn=np.zeros((C, 3), np.float32),
+                   spen=np.zeros(C, np.float32), jn=np.zeros(C, np.float32), jt1=np.zeros(C, np.float32),
+                   jt2=np.zeros(C, np.float32), jp=np.zeros(C, np.float32))
+        if C:
+            L.or_col_kept(self._h, *(_p(out[k]) for k in ("ckeys", "sbi", "sbj", "spA", "spB", "sn", "spen", "jn",
+                                                          "jt1", "jt2", "jp")))
+        return out
 
     def get_state(self) -> State:
         if self.b is None:

@@ -637,6 +637,9 @@ typedef struct {
     int ws_n;
     int64_t *ws_keys;
     float *ws_jn, *ws_jt1, *ws_jt2;
+    /* the rest of the last substep's kept contacts, for or_col_kept (COL:1095-1103 reads them back) */
+    int *ws_bi, *ws_bj;
+    float *ws_pA, *ws_pB, *ws_nrm, *ws_pen, *ws_jp;
     /* colour cache (contact_engine_gpu_color_cache.py:26-54) and the colour grouping it reuses */
     int cached_pairs, cached_colors, has_colors;
     int *cached_a, *cached_b;
@@ -654,6 +657,9 @@ OR_API void *or_col_create(int mode, int vit, int pit, int mx, float mu, float t
     e->mode = mode; e->vit = vit; e->pit = pit; e->mx = mx; e->mu = mu; e->t2d = t2d; e->cap = cap;
     e->ws_keys = malloc(sizeof(int64_t) * cap);
     e->ws_jn = malloc(sizeof(float) * cap); e->ws_jt1 = malloc(sizeof(float) * cap); e->ws_jt2 = malloc(sizeof(float) * cap);
+    e->ws_bi = malloc(sizeof(int) * cap); e->ws_bj = malloc(sizeof(int) * cap);
+    e->ws_pA = malloc(sizeof(float) * 3 * cap); e->ws_pB = malloc(sizeof(float) * 3 * cap);
+    e->ws_nrm = malloc(sizeof(float) * 3 * cap); e->ws_pen = malloc(sizeof(float) * cap); e->ws_jp = malloc(sizeof(float) * cap);
     e->cached_a = malloc(sizeof(int) * cap); e->cached_b = malloc(sizeof(int) * cap);
     e->cached_mass = malloc(sizeof(float) * (N > 0 ? N : 1)); e->cached_N = N;
     e->porder = malloc(sizeof(int) * cap); e->cstart = calloc(512, sizeof(int)); e->ccount = calloc(512, sizeof(int));
@@ -665,6 +671,7 @@ OR_API void or_col_destroy(void *h)
     col_engine_t *e = h;
     if (!e) return;
     free(e->ws_keys); free(e->ws_jn); free(e->ws_jt1); free(e->ws_jt2);
+    free(e->ws_bi); free(e->ws_bj); free(e->ws_pA); free(e->ws_pB); free(e->ws_nrm); free(e->ws_pen); free(e->ws_jp);
     free(e->cached_a); free(e->cached_b); free(e->cached_mass); free(e->porder); free(e->cstart); free(e->ccount);
     free(e);
 }
@@ -673,6 +680,23 @@ OR_API void or_col_stats(void *h, int *out)
     col_engine_t *e = h;
     out[0] = e->n_contacts; out[1] = e->n_kept; out[2] = e->n_pairs; out[3] = e->n_colors;
     out[4] = e->hits; out[5] = e->misses; out[6] = e->seg_overflow;
+}
+/* the kept contacts of the last substep in feature order: keys, bodies, points, normal, depth and
+ * the impulses after the solve (jn, jt1, jt2, jp); returns their count */
+OR_API int or_col_kept(void *h, int64_t *keys, int *bi, int *bj, float *pA, float *pB, float *n, float *pen,
+                       float *jn, float *jt1, float *jt2, float *jp)
+{
+    col_engine_t *e = h;
+    const int C = e->ws_n;
+    if (keys) {
+        memcpy(keys, e->ws_keys, sizeof(int64_t) * C); memcpy(bi, e->ws_bi, sizeof(int) * C);
+        memcpy(bj, e->ws_bj, sizeof(int) * C); memcpy(pA, e->ws_pA, sizeof(float) * 3 * C);
+        memcpy(pB, e->ws_pB, sizeof(float) * 3 * C); memcpy(n, e->ws_nrm, sizeof(float) * 3 * C);
+        memcpy(pen, e->ws_pen, sizeof(float) * C); memcpy(jn, e->ws_jn, sizeof(float) * C);
+        memcpy(jt1, e->ws_jt1, sizeof(float) * C); memcpy(jt2, e->ws_jt2, sizeof(float) * C);
+        memcpy(jp, e->ws_jp, sizeof(float) * C);
+    }
+    return C;
 }
 
 /* _planar, COL:585-590: float32 difference promoted to float64, contraction off */
@@ -1192,6 +1216,10 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
             memcpy(e->ws_keys, okeys, sizeof(int64_t) * Ck);
             memcpy(e->ws_jn, jn, sizeof(float) * Ck); memcpy(e->ws_jt1, jt1, sizeof(float) * Ck);
             memcpy(e->ws_jt2, jt2, sizeof(float) * Ck);
+            memcpy(e->ws_bi, sbi, sizeof(int) * Ck); memcpy(e->ws_bj, sbj, sizeof(int) * Ck);
+            memcpy(e->ws_pA, spA, sizeof(float) * 3 * Ck); memcpy(e->ws_pB, spB, sizeof(float) * 3 * Ck);
+            memcpy(e->ws_nrm, sn, sizeof(float) * 3 * Ck); memcpy(e->ws_pen, spen, sizeof(float) * Ck);
+            memcpy(e->ws_jp, jp, sizeof(float) * Ck);
             e->ws_n = Ck;
         } else {
             e->n_kept = 0; e->n_pairs = 0; e->n_colors = 0;

@@ -95,6 +95,34 @@ def test_checkpoint_resumes_bit_for_bit(me):
         c.state_load(blob)
 
 
+def test_load_undoes_a_later_kinematic_update(me):
+    """A blob saved while body i was dynamic, loaded after b2c_set_kinematic made it kinematic:
+    the body is dynamic again on the device and on the host, so the next steps and the contact
+    forces (its own row included, with its mass from the build) equal those of a handle that
+    never touched it.  Body i is the lowest box, which rests on the ground."""
+    S = _scene(200)
+    a = me.HandleBoxEngine(mu=0.5, vit=16, pit=10)
+    a.add_boxes(S["centers"], dims=S["dims"], density=S["density"], mu=S["mu"])
+    b = me.HandleBoxEngine(mu=0.5, vit=16, pit=10)
+    b.add_boxes(S["centers"], dims=S["dims"], density=S["density"], mu=S["mu"])
+    for _ in range(120):
+        a.step(DT, 2)
+        b.step(DT, 2)
+    i = int(np.argmin(a.get_state().xc[:, 2]))
+    blob = a.state_save()
+    a.set_kinematic(i, [0.0, 0.0, 3.0])
+    a.step(DT, 2)
+    assert np.all(a.contact_forces()[i] == 0)
+    a.state_load(blob)
+    for _ in range(20):
+        a.step(DT, 2)
+        b.step(DT, 2)
+    assert a.get_state_packed().tobytes() == b.get_state_packed().tobytes()
+    fa, fb = a.contact_forces(), b.contact_forces()
+    np.testing.assert_array_equal(fa, fb)
+    assert np.any(fb[i] != 0), "the lowest box rests on the ground and carries a contact force"
+
+
 def test_packed_state_round_trip_through_the_handle(me):
     S = _scene(150)
     a = me.HandleBoxEngine()

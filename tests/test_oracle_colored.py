@@ -43,3 +43,22 @@ def test_oracle_colored_against_reference(engine, scene, golden, oracle_mod):
         elif t in sel:
             g = golden[f"{engine}__{scene}__xc"][sel.index(t)]
             assert np.abs(st.xc.astype(np.float64) - g).max() < XC_TOL[engine], f"step {t}"
+
+
+def test_oracle_color_cache_lattice10k_against_receipt(oracle_mod):
+    """The reference's 10 000-body ColorCache receipt (reports/innovation_color_cache_profile_v2.npz):
+    40 steps of lattice(10000), vit 40, pit 20.  Positions, the selected contacts and the
+    position impulses are bitwise; the rest within the bounds of tests/cc10k.py.  The receipt
+    holds the last step only, so the first step where a velocity bit departs is not visible;
+    the contact geometry of step 40 being bitwise says that every position up to step 39 was."""
+    from cc10k import check_cc10k
+    from conftest import lattice
+    e = oracle_mod.ColoredOracle(mode="color_cache", dims=DIMS, mu=0.5, vit=40, pit=20)
+    for c in lattice(10000):
+        e.add_body(c)
+    for _ in range(40):
+        e.step(DT, 1)
+    st = e.stats()
+    assert (st["n_contacts"], st["n_kept"], st["n_pairs"], st["n_colors"], st["hits"], st["misses"]) == \
+        (87716, 40000, 10000, 2, 35, 2)  # the receipt's counts
+    check_cc10k(e.get_state(), e.contact_forces(), e.kept_contacts())

@@ -47,3 +47,15 @@ def test_noalloc_scan_rejects_too_large_n(me):
                                       nmax + 1, None)
     assert rc == 1
     assert b"exceeds the maximum" in L.b2c_last_error()
+
+
+def test_noalloc_setup_call_takes_null_arrays(me):
+    """n = 0 with null arrays is the set-up call (it only looks up the scratch address); a
+    negative n or null arrays with n > 0 are bad arguments."""
+    L = me._lib.load()
+    assert L.b2c_exclusive_scan_noalloc(None, None, 0, None) == 0
+    assert L.b2c_exclusive_scan_noalloc(None, None, -1, None) == 1
+    assert L.b2c_exclusive_scan_noalloc(None, None, 5, None) == 1
+    x = np.arange(100, dtype=np.int32)
+    ref, na = _scan_pair(me, x)
+    np.testing.assert_array_equal(na, ref)
