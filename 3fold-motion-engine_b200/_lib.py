@@ -150,6 +150,7 @@ _SIGS = {
     "b2c_pair_record_floats": ([c_int32, c_int32], ctypes.c_int64),
     "b2c_last_error": ([], ctypes.c_char_p),
     "b2c_scan_scratch_ints": ([c_int32], c_int32),
+    "b2c_barrier_words": ([], c_int32),
     "b2c_exclusive_scan": ([c_void_p, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
     "b2c_exclusive_scan_noalloc": ([c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "b2c_scan_noalloc_max_n": ([], c_int32),

@@ -162,7 +162,7 @@ class BoxContactEngine(_BeadEngineBase):
                            cached_a=i32(pcap), cached_b=i32(pcap),
                            cached_mass=torch.zeros(max(N, 1), dtype=torch.float32, device=dev), cache_state=i32(8),
                            body_colors=i64(N), body_slots=i32(64 * N),
-                           barrier=torch.zeros(2, dtype=torch.int32, device=dev),
+                           barrier=torch.zeros(int(self.L.b2c_barrier_words()), dtype=torch.int32, device=dev),
                            rec=torch.zeros(max(int(self.L.b2c_pair_record_floats(pcap, kslots)), 1),
                                            dtype=torch.float32, device=dev))
         pb = self.p_bufs

@@ -129,7 +129,7 @@ class GraphColoredContactEngine(_BeadEngineBase):
         self.p_bufs = dict(pbi=i32(pcap), pbj=i32(pcap), kcount=i32(pcap + 1), pstart=i32(pcap + 1), pidx=i32(cap),
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(2 * N),
                            cached_a=i32(pcap), cached_b=i32(pcap), cached_mass=f32(N), cache_state=i32(8),
-                           barrier=torch.zeros(2, dtype=torch.int32, device=dev),
+                           barrier=torch.zeros(int(self.L.b2c_barrier_words()), dtype=torch.int32, device=dev),
                            rec=f32(self.L.b2c_pair_record_floats(pcap, kslots)))
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (

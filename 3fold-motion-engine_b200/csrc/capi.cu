@@ -1,4 +1,5 @@
 // Library-wide C entry points: version and the per-thread error message.
+#include "b2c_barrier.cuh"
 #include "b2c_common.cuh"
 
 namespace b2c {
@@ -16,6 +17,11 @@ void set_error(const char *fmt, ...)
 }  // namespace b2c
 
 extern "C" int32_t b2c_version(void) { return 100; }
+extern "C" int32_t b2c_barrier_words(void)
+{
+    static_assert(b2c::kBarrierWords == B2C_BARRIER_WORDS, "the header's barrier size");
+    return b2c::kBarrierWords;
+}
 extern "C" const char *b2c_last_error(void) { return b2c::g_err; }
 
 static int count_kernel_nodes(cudaGraph_t g, int depth)

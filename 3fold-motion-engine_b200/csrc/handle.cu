@@ -16,6 +16,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "b2c_barrier.cuh"
 #include "b2c_common.cuh"
 
 namespace {
@@ -246,7 +247,7 @@ int build(Engine *e)
         take(pbi, pcap), take(pbj, pcap), take(kcount, pcap + 1), take(pstart, pcap + 1), take(pidx, kept_cap);
         take(col, pcap), take(porder, pcap), take(cstart, kMaxColors), take(ccount, kMaxColors);
         take(claim, 2 * (size_t)N), take(cached_a, pcap), take(cached_b, pcap), take(cached_mass, N);
-        take(cache_state, 8), take(body_colors, N), take(body_slots, 64 * (size_t)N), take(barrier, 2);
+        take(cache_state, 8), take(body_colors, N), take(body_slots, 64 * (size_t)N), take(barrier, b2c::kBarrierWords);
         take(rec, (size_t)rec_floats);
         take(wkeys, kept_cap), take(wimp, 4 * (size_t)kept_cap), take(wn, 1);
     };

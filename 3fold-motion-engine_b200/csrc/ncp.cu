@@ -24,6 +24,7 @@
 // with -fmad=false), so the oracle's C restatement reproduces the results bit for bit.
 #include <cooperative_groups.h>
 
+#include "b2c_barrier.cuh"
 #include "b2c_common.cuh"
 
 namespace cg = cooperative_groups;
@@ -277,18 +278,12 @@ struct SweepArgs {
 
 enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
-__device__ __forceinline__ unsigned long long ncp_global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident)
-// counts arrivals in a.bar[0] and releases through the generation in a.bar[1]; its wait is
-// bounded by a.timeout_ns, after which it sets kErrBarrier and every CTA leaves the sweep.
+// The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident) is
+// the per-CTA flag barrier of b2c_barrier.cuh over a.bar (its flags from word kBarrierFlagBase,
+// cleared by the host before the launch); `epoch` counts the grid barriers of this launch.  Its
+// wait is bounded by a.timeout_ns, after which it sets kErrBarrier and every CTA leaves the sweep.
 template <int kKind, typename T>
-__device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a)
+__device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a, unsigned int &epoch)
 {
     if (kKind == kBlock) {
         __syncthreads();
@@ -298,35 +293,9 @@ __device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a)
         cg::this_cluster().sync();
         return true;
     }
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned int *gen = a.bar + 1;
-        const unsigned int my_gen = *gen;
-        __threadfence();
-        const unsigned int prev = atomicAdd(a.bar, 1u);
-        if (prev == gridDim.x - 1) {
-            atomicExch(a.bar, 0u);
-            __threadfence();
-            atomicAdd(a.bar + 1, 1u);
-        } else {
-            const unsigned long long t0 = ncp_global_ns();
-            while (*gen == my_gen) {
-                if (ncp_global_ns() - t0 > (unsigned long long)a.timeout_ns) {
-                    atomicOr(a.stats + kError, kErrBarrier);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*(volatile int *)(a.stats + kError) & kErrBarrier) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+    ++epoch;
+    flag_arrive(a.bar + kBarrierFlagBase, epoch);
+    return flag_wait(a.bar + kBarrierFlagBase, epoch, a.timeout_ns, a.stats + kError, kErrBarrier);
 }
 
 template <typename T>
@@ -366,11 +335,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweeps(SweepArgs<T> a)
     // colour's float64 work to its first CTAs).  A contact keeps its thread in every sweep.
     const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
     const int tid = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);
+    unsigned int epoch = 0;
     for (int it = 0; it < a.iters; ++it)
         for (int ci = 0; ci < ncol; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
             for (int t = tid; t < cnt; t += nth) sweep_contact(a, a.order[s0 + t]);
-            if (!phase_barrier<kKind>(a)) return;
+            if (!phase_barrier<kKind>(a, epoch)) return;
         }
 }
 
@@ -605,7 +575,7 @@ int grid_blocks()
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweeps<T, kGrid>, kSweepThreads, 0);
-        cached = std::max(1, sms * per);
+        cached = std::min(kBarrierMaxCTAs, std::max(1, sms * per));
     }
     return cached;
 }
@@ -623,7 +593,8 @@ int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, 
     if (mode > 1) {  // a cooperative grid of at most the co-resident CTAs
         const int nblocks = std::min(mode, grid_blocks<T>());
         if (nblocks > 1) {
-            cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);  // arrival count (the generation keeps counting)
+            // the barrier's arrival flags start from zero in every launch
+            cudaMemsetAsync(st->barrier + kBarrierFlagBase, 0, sizeof(uint32_t) * (size_t)nblocks, s);
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(kSweepThreads);

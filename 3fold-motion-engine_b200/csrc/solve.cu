@@ -8,8 +8,8 @@
 //   * one CTA (tiny scenes): __syncthreads (~0.04 us measured on B200);
 //   * a thread-block cluster of up to 16 CTAs: the hardware cluster barrier
 //     (barrier.cluster arrive.release / wait.acquire; ~0.25 us measured);
-//   * a cooperative grid: an atomic grid barrier (~2.2 us measured) whose wait is bounded by a
-//     %globaltimer limit, after which it sets B2C_ERR_BARRIER_TIMEOUT and every CTA returns.
+//   * a cooperative grid: the per-CTA flag barrier of b2c_barrier.cuh, whose wait is bounded by
+//     a %globaltimer limit, after which it sets B2C_ERR_BARRIER_TIMEOUT and every CTA returns.
 //
 // Data layout.  The sweeps are bound by the latency of dependent loads, not by arithmetic or
 // bandwidth: following porder -> pair -> pidx -> contact -> body costs several L2 round trips
@@ -27,6 +27,7 @@
 // after a barrier, and L1 is not coherent across SMs.
 #include <cooperative_groups.h>
 
+#include "b2c_barrier.cuh"
 #include "b2c_common.cuh"
 
 namespace cg = cooperative_groups;
@@ -79,7 +80,7 @@ struct SolveArgs {
     float *v, *w, *pv, *po;
     float mu, t2d, dt;
     int vit, pit, fixed_frame, apply_warm, row;
-    unsigned int *bar_count, *bar_gen;
+    unsigned int *bar_flags;  // the grid barrier's per-CTA arrival flags
     long long timeout_ns;
 };
 
@@ -262,79 +263,22 @@ __global__ void k_imp_scatter(const b2c_header *__restrict__ hdr, const int *__r
 // ---------------------------------------------------------------------------------------------
 enum BarrierKind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-template <int kKind>
-__device__ __forceinline__ bool solve_barrier(const SolveArgs &a)
-{
-    if (kKind == kBlock) {
-        __syncthreads();
-        return true;
-    }
-    if (kKind == kCluster) {
-        cg::this_cluster().sync();
-        return true;
-    }
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned int *gen = a.bar_gen;
-        const unsigned int my_gen = *gen;
-        __threadfence();
-        const unsigned int prev = atomicAdd(a.bar_count, 1u);
-        if (prev == gridDim.x - 1) {
-            atomicExch(a.bar_count, 0u);
-            __threadfence();
-            atomicAdd(a.bar_gen, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            while (*gen == my_gen) {
-                if (global_ns() - t0 > (unsigned long long)a.timeout_ns) {
-                    atomicOr(a.err, B2C_ERR_BARRIER_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*(volatile int *)a.err & B2C_ERR_BARRIER_TIMEOUT) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-// The same barriers split into an arrive and a wait, so that a thread can issue loads that do
-// not depend on the other CTAs' work of the phase (its next task's fixed record words) in
-// between.  The grid form's arrive count and generation are the solve_barrier's.
+// The barrier between colour phases, split into an arrive and a wait, so that a thread can
+// issue loads that do not depend on the other CTAs' work of the phase (its next task's fixed
+// record words) in between.  The grid form counts its barriers in `epoch` (uniform over the
+// CTA) and arrives with that number in its flag (b2c_barrier.cuh).
 struct BarTok {
-    unsigned int gen;
+    unsigned int epoch;
 };
 template <int kKind>
-__device__ __forceinline__ BarTok bar_arrive(const SolveArgs &a)
+__device__ __forceinline__ BarTok bar_arrive(const SolveArgs &a, unsigned int &epoch)
 {
     BarTok tok{0u};
     if (kKind == kCluster) {
         asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
     } else if (kKind == kGrid) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            tok.gen = *(volatile unsigned int *)a.bar_gen;
-            __threadfence();
-            const unsigned int prev = atomicAdd(a.bar_count, 1u);
-            if (prev == gridDim.x - 1) {
-                atomicExch(a.bar_count, 0u);
-                __threadfence();
-                atomicAdd(a.bar_gen, 1u);
-            }
-        }
+        tok.epoch = ++epoch;
+        flag_arrive(a.bar_flags, tok.epoch);
     }
     return tok;
 }
@@ -349,24 +293,7 @@ __device__ __forceinline__ bool bar_wait(const SolveArgs &a, BarTok tok)
         asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
         return true;
     }
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned long long t0 = global_ns();
-        while (*(volatile unsigned int *)a.bar_gen == tok.gen) {
-            if (global_ns() - t0 > (unsigned long long)a.timeout_ns) {
-                atomicOr(a.err, B2C_ERR_BARRIER_TIMEOUT);
-                ok = 0;
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-        if (*(volatile int *)a.err & B2C_ERR_BARRIER_TIMEOUT) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+    return flag_wait(a.bar_flags, tok.epoch, a.timeout_ns, a.err, B2C_ERR_BARRIER_TIMEOUT);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1006,6 +933,7 @@ __device__ __forceinline__ void solve_phases(const SolveArgs &a, const BA &B)
     RowPre pre;
     int pre_t = -1;
     bool pos;
+    unsigned int epoch = 0;  // grid barriers passed in this launch
     {
         const int sl = task_slot(0, 0, me, pos);
         if (sl >= 0) {
@@ -1038,7 +966,7 @@ __device__ __forceinline__ void solve_phases(const SolveArgs &a, const BA &B)
                 }
             }
             pre_t = -1;
-            const BarTok tok = bar_arrive<kKind>(a);
+            const BarTok tok = bar_arrive<kKind>(a, epoch);
             const int np = ci + 1 < nc ? pass : pass + 1, nci = ci + 1 < nc ? ci + 1 : 0;
             if (nc > 1 && np < passes) {
                 const int sl = task_slot(np, nci, me, pos);
@@ -1158,6 +1086,7 @@ __device__ __forceinline__ void solve_phases_scene(const SolveArgs &a, const Sce
     RowPre pre;
     int pre_t = -1;
     bool pos;
+    unsigned int epoch = 0;  // grid barriers passed in this launch
     {
         const int sl = task_slot(0, 0, me, pos);
         if (sl >= 0) {
@@ -1229,7 +1158,7 @@ static int max_coresident_grid_blocks()
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         allow_stage_smem();
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_solve_grid, 256, stage_bytes(256));
-        cached = std::max(1, sms * std::max(per, 1));
+        cached = std::min(kBarrierMaxCTAs, std::max(1, sms * std::max(per, 1)));
     }
     return cached;
 }
@@ -1285,8 +1214,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
         set_error("color_solve: B2C_COLOR_ROW_FORM needs B2C_COLOR_FIXED_FRAME");
         return B2C_EARG;
     }
-    a.bar_count = pr->barrier;
-    a.bar_gen = pr->barrier + 1;
+    a.bar_flags = pr->barrier + kBarrierFlagBase;
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
@@ -1361,7 +1289,8 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             k_color_solve_block<<<1, 256, stage_bytes(256), s>>>(a);
             if ((rc = check_launch("color_solve_block"))) return rc;
         } else {
-            cudaMemsetAsync(pr->barrier, 0, sizeof(uint32_t), s);  // arrival count (generation keeps counting)
+            // the barrier's arrival flags start from zero in every launch
+            cudaMemsetAsync(a.bar_flags, 0, sizeof(uint32_t) * (size_t)nblocks, s);
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(256);

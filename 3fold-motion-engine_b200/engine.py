@@ -370,6 +370,17 @@ class _BeadEngineBase:
                     jn=np.ascontiguousarray(imp_[:, 0]), jt1=np.ascontiguousarray(imp_[:, 1]),
                     jt2=np.ascontiguousarray(imp_[:, 2]), jp=np.ascontiguousarray(imp_[:, 3]))
 
+    def warm_store(self) -> dict:
+        """The warm-start store the next substep looks its impulses up in (engines that keep
+        one): feature keys ascending, and jn, jt1, jt2 as stored."""
+        if not self._built:
+            self._build()
+        torch.cuda.synchronize(self.dev)
+        n = int(self.w_n[0].item())
+        imp = self.w_imp[:n].cpu().numpy()
+        return dict(keys=self.w_keys[:n].cpu().numpy(), jn=imp[:, 0].copy(), jt1=imp[:, 1].copy(),
+                    jt2=imp[:, 2].copy())
+
     def max_depth_device(self) -> torch.Tensor:
         """The deepest penetration among the last substep's solved contacts, as a 0-d float32
         device tensor computed on the engine's stream without a host read (0 without

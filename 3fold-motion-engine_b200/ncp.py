@@ -210,7 +210,7 @@ class NCPSolverB200:
         self.c_minv = z(NB, 4)
         self.stats = z(8, dtype=i32)
         self.res_max = z(1, dtype=torch.int64)
-        self.barrier = z(2, dtype=i32)
+        self.barrier = z(int(self.L.b2c_barrier_words()), dtype=i32)
         self.c_state = _lib.NcpState(MC, NB, NCOLMAX, *(_ptr(x) for x in (
             self.rho, self.lam, self.v, self.acc, self.res, self.u, self.col, self.order, self.cstart, self.ccount,
             self.claim, self.dyn, self.c_pa, self.c_pb, self.c_feat, self.c_minv, self.stats, self.res_max,

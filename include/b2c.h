@@ -128,6 +128,10 @@ typedef struct b2c_jacobi_params {
 
 #define B2C_ERR_BARRIER_TIMEOUT 128  /* a grid barrier of the persistent solve gave up waiting */
 
+/* uint32 words of a grid-barrier buffer (b2c_pairs.barrier, b2c_ncp_state.barrier): 32 words of
+ * padding, then one arrival flag for each of up to 512 CTAs; b2c_barrier_words() returns it */
+#define B2C_BARRIER_WORDS 544
+
 /* Scratch of the coloured chain's ordering and manifold stage (one slot per raw contact
  * unless noted).  Replaces the radix-sort buffers, segment flags and selection arrays of
  * _device_manifold (contact_engine_gpu_colored.py:1050-1087). */
@@ -166,7 +170,8 @@ typedef struct b2c_pairs {
     int32_t *cached_a, *cached_b; /* colour cache: pbi / pbj of the cached colouring */
     float *cached_mass;      /* (bodies) invM of the cached colouring */
     int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
-    uint32_t *barrier;       /* [count, generation] of the persistent solve's grid barrier */
+    uint32_t *barrier;       /* (B2C_BARRIER_WORDS) the persistent solve's grid barrier: one arrival
+                                flag per CTA of a cooperative launch, cleared before each launch */
     float *rec;              /* colour-major pair records of the solve, b2c_pair_record_floats()
                                 floats: per slot a header, both bodies' inverse inertia and mass,
                                 and per contact its normal|depth, the terms that stay fixed
@@ -282,6 +287,8 @@ B2C_API const char *b2c_last_error(void);
 B2C_API int32_t b2c_graph_kernel_nodes(void *graph);
 /* floats of b2c_pairs.rec for `pair_capacity` pairs of up to `kslots` contacts each */
 B2C_API int64_t b2c_pair_record_floats(int32_t pair_capacity, int32_t kslots);
+/* B2C_BARRIER_WORDS, the uint32 words a grid-barrier buffer needs */
+B2C_API int32_t b2c_barrier_words(void);
 /* ints of scratch that b2c_exclusive_scan needs for n elements */
 B2C_API int32_t b2c_scan_scratch_ints(int32_t n);
 /* exclusive prefix sum of n int32 (device pointers); out may alias nothing */
@@ -426,7 +433,7 @@ typedef struct b2c_ncp_state {
     int32_t *stats;            /* (8) n_colors, cache_valid, cached_C, cache_hit, hits, misses,
                                   rounds, error bits */
     uint64_t *res_max;         /* (1) bits of max_c residual_c (non-negative reals) */
-    uint32_t *barrier;         /* (2) grid barrier of the persistent sweep */
+    uint32_t *barrier;         /* (B2C_BARRIER_WORDS) grid barrier of the persistent sweep */
 } b2c_ncp_state;
 
 /* Per-call parameters: de Saxce correction, soft step (SoftStep.params: bias_rate, mass_scale,

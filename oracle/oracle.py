@@ -42,10 +42,13 @@ PINNED_VARIANTS.update(SITE_WUPD=0, SITE_BIAS=0)
 
 
 def build(force: bool = False) -> str:
-    """Compile liboracle.so beside this file (gcc, contraction off)."""
+    """Compile liboracle.so and its FP64 re-solve build liboracle64.so beside this file (gcc,
+    contraction off)."""
     so = os.path.join(_HERE, "liboracle.so")
-    src = os.path.join(_HERE, "oracle_contact.c")
-    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("oracle_contact.c", "oracle_ncp.c", "f64_prelude.h", "Makefile")]
+    newest = max(os.path.getmtime(f) for f in srcs)
+    outs = [so, os.path.join(_HERE, "liboracle64.so")]
+    if force or any(not os.path.exists(o) or os.path.getmtime(o) < newest for o in outs):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return so
 
@@ -66,6 +69,36 @@ def lib():
         _LIB = L
         set_variants(PINNED_VARIANTS)
     return _LIB
+
+
+_LIB64 = None
+
+
+def lib64():
+    """liboracle64.so: the coloured / ColorCache chain and the box engine compiled in float64
+    (f64_prelude.h), the FP64 re-solve the float32 tolerances are stated against."""
+    global _LIB64
+    if _LIB64 is None:
+        build()
+        L = ctypes.CDLL(os.path.join(_HERE, "liboracle64.so"))
+        L.or_set_variant.argtypes = [ctypes.c_int, ctypes.c_int]
+        for k, v in PINNED_VARIANTS.items():
+            L.or_set_variant(FV[k], int(v))
+        _col_sigs(L, ctypes.c_double)
+        _box_sigs(L, ctypes.c_double)
+        L._col_ready = True
+        _LIB64 = L
+    return _LIB64
+
+
+def _precision(precision):
+    """(numpy dtype, library) of an oracle precision, "float32" (the restatement of the
+    reference's arithmetic) or "float64" (the FP64 re-solve)."""
+    if precision == "float32":
+        return np.float32, lib()
+    if precision == "float64":
+        return np.float64, lib64()
+    raise ValueError(f"precision is 'float32' or 'float64', not {precision!r}")
 
 
 def set_variants(d: dict) -> None:
@@ -122,6 +155,15 @@ def build_bodies(centers, dens, kin, dims) -> BodySetup:
                      v=np.zeros((N, 3), np.float32), w=np.zeros((N, 3), np.float32),
                      invM=invM.astype(np.float32), IbInv=IbInv.astype(np.float32).reshape(N, 3, 3),
                      kin=kinarr.astype(np.int32), M=M.astype(np.float64))
+
+
+def _cast_bodies(b: BodySetup, F) -> BodySetup:
+    """The body arrays in the oracle's precision: the float32 setup values themselves, widened
+    for the FP64 re-solve (so both precisions start from the same inputs)."""
+    if F is np.float32:
+        return b
+    return BodySetup(rest=b.rest.astype(F), xc=b.xc.astype(F), q=b.q.astype(F), v=b.v.astype(F), w=b.w.astype(F),
+                     invM=b.invM.astype(F), IbInv=b.IbInv.astype(F), kin=b.kin, M=b.M)
 
 
 def quat_to_R(q: np.ndarray) -> np.ndarray:
@@ -198,10 +240,10 @@ class JacobiOracle:
         return self.force.copy()
 
 
-def _col_sigs(L):
+def _col_sigs(L, F=ctypes.c_float):
     P = ctypes.c_void_p
-    L.or_col_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
-                                ctypes.c_int, ctypes.c_int]
+    L.or_col_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int,
+                                ctypes.c_int]
     L.or_col_create.restype = P
     L.or_col_destroy.argtypes = [P]
     L.or_col_stats.argtypes = [P, P]
@@ -210,6 +252,14 @@ def _col_sigs(L):
     L.or_col_step.restype = ctypes.c_int
     L.or_col_kept.argtypes = [P] * 12
     L.or_col_kept.restype = ctypes.c_int
+    L.or_col_warm_get.argtypes = [P] * 5
+    L.or_col_warm_get.restype = ctypes.c_int
+    L.or_col_warm_set.argtypes = [P, ctypes.c_int, P, P, P, P]
+    L.or_col_warm_set.restype = ctypes.c_int
+    L.or_col_pre.argtypes = [P] * 4
+    L.or_col_pre.restype = ctypes.c_int
+    L.or_col_inject.argtypes = [P, ctypes.c_int, P, P, P, P]
+    L.or_col_inject.restype = ctypes.c_int
 
 
 class ColoredOracle:
@@ -225,9 +275,11 @@ class ColoredOracle:
     """
 
     def __init__(self, mode="color_cache", dims=(0.3, 0.3, 0.2), vit=40, pit=20, mu=0.5, max_points=4,
-                 t2_damp=1.0, cap=MAXC):
+                 t2_damp=1.0, cap=MAXC, precision="float32"):
         assert mode in ("pair_chunks", "color_cache", "plain")
         self.mode = mode
+        self.precision = precision
+        self.F, self.L = _precision(precision)
         self.name = f"{mode}_oracle"
         self.dims = dims; self.vit = vit; self.pit = pit; self.mu = mu; self.mx = max_points; self.t2d = t2_damp
         self.cap = cap
@@ -242,16 +294,16 @@ class ColoredOracle:
         return len(self._centers) - 1
 
     def _build(self):
-        L = lib()
+        L = self.L
         if not hasattr(L, "_col_ready"):
             _col_sigs(L); L._col_ready = True
-        self.b = build_bodies(self._centers, self._dens, self._kin, self.dims)
+        self.b = _cast_bodies(build_bodies(self._centers, self._dens, self._kin, self.dims), self.F)
         N = len(self._centers); P = len(self.b.rest)
         self.N = N; self.P = P
         self.rest_all = np.ascontiguousarray(np.tile(self.b.rest, (N, 1)))
         self.owner = np.repeat(np.arange(N, dtype=np.int32), P)
-        self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
-        self.vgrav = np.zeros((N, 3), np.float32)
+        self.pv = np.zeros((N, 3), self.F); self.po = np.zeros((N, 3), self.F)
+        self.vgrav = np.zeros((N, 3), self.F)
         if self._h:
             L.or_col_destroy(self._h)
         self._h = L.or_col_create({"pair_chunks": 0, "color_cache": 1, "plain": 2}[self.mode], self.vit, self.pit,
@@ -261,21 +313,21 @@ class ColoredOracle:
     def __del__(self):
         try:
             if self._h:
-                lib().or_col_destroy(self._h)
+                self.L.or_col_destroy(self._h)
         except Exception:
             pass
 
     def set_kinematic(self, i, xc):
         self._kin[i] = 1; self._centers[i] = list(xc)
         if self.b is not None:
-            self.b.xc[i] = np.array(xc, np.float32); self.b.invM[i] = 0.0
+            self.b.xc[i] = np.array(np.array(xc, np.float32), self.F); self.b.invM[i] = 0.0
             self.b.v[i] = 0.0; self.b.w[i] = 0.0; self.b.kin[i] = 1; self.b.M[i] = np.inf
 
     def step(self, dt, substeps=1):
         if self.b is None:
             self._build()
         b = self.b
-        rc = lib().or_col_step(self._h, self.N, self.N * self.P, _p(self.rest_all), _p(self.owner), _p(b.xc), _p(b.q),
+        rc = self.L.or_col_step(self._h, self.N, self.N * self.P, _p(self.rest_all), _p(self.owner), _p(b.xc), _p(b.q),
                                _p(b.v), _p(b.w), _p(self.pv), _p(self.po), _p(b.invM), _p(b.IbInv), _p(b.kin),
                                float(dt), int(substeps), _p(self.vgrav))
         if rc != 0:
@@ -284,7 +336,7 @@ class ColoredOracle:
 
     def stats(self):
         out = np.zeros(7, np.int32)
-        lib().or_col_stats(self._h, _p(out))
+        self.L.or_col_stats(self._h, _p(out))
         return dict(zip(("n_contacts", "n_kept", "n_pairs", "n_colors", "hits", "misses", "seg_overflow"),
                         out.tolist()))
 
@@ -295,16 +347,71 @@ class ColoredOracle:
     def kept_contacts(self) -> dict:
         """The last substep's kept contacts in feature order, named as the reference's engine
         attributes (ckeys, sbi, sbj, spA, spB, sn, spen, jn, jt1, jt2, jp; COL:1095-1103)."""
-        L = lib()
+        L, F = self.L, self.F
         C = int(L.or_col_kept(self._h, *([None] * 11)))
         out = dict(ckeys=np.zeros(C, np.int64), sbi=np.zeros(C, np.int32), sbj=np.zeros(C, np.int32),
-                   spA=np.zeros((C, 3), np.float32), spB=np.zeros((C, 3), np.float32), sn=np.zeros((C, 3), np.float32),
-                   spen=np.zeros(C, np.float32), jn=np.zeros(C, np.float32), jt1=np.zeros(C, np.float32),
-                   jt2=np.zeros(C, np.float32), jp=np.zeros(C, np.float32))
+                   spA=np.zeros((C, 3), F), spB=np.zeros((C, 3), F), sn=np.zeros((C, 3), F),
+                   spen=np.zeros(C, F), jn=np.zeros(C, F), jt1=np.zeros(C, F), jt2=np.zeros(C, F), jp=np.zeros(C, F))
         if C:
             L.or_col_kept(self._h, *(_p(out[k]) for k in ("ckeys", "sbi", "sbj", "spA", "spB", "sn", "spen", "jn",
                                                           "jt1", "jt2", "jp")))
         return out
+
+    def pre_solve_impulses(self) -> dict:
+        """jn, jt1, jt2 (float64 copies) of the last substep's kept contacts as its solve received
+        them: warm-started and, in the manifold engines, reduced onto the kept points."""
+        n = int(self.L.or_col_pre(self._h, None, None, None))
+        d = dict(jn=np.zeros(n), jt1=np.zeros(n), jt2=np.zeros(n))
+        self.L.or_col_pre(self._h, _p(d["jn"]), _p(d["jt1"]), _p(d["jt2"]))
+        return d
+
+    def inject(self, kept: dict, start: dict) -> None:
+        """Make the next substep solve `kept` (ckeys, sbi, sbj, spA, spB, sn, spen) from the
+        impulses `start` (jn, jt1, jt2) instead of the contacts it selects itself (one substep,
+        coloured engines): the FP64 re-solve of a float32 step on the float32 step's contacts."""
+        if self.b is None:
+            self._build()
+        n = len(kept["ckeys"])
+        f = np.zeros((n, 13))
+        f[:, 0:3], f[:, 3:6], f[:, 6:9] = kept["spA"], kept["spB"], kept["sn"]
+        f[:, 9] = kept["spen"]
+        f[:, 10], f[:, 11], f[:, 12] = start["jn"], start["jt1"], start["jt2"]
+        keys = np.ascontiguousarray(kept["ckeys"], np.int64)
+        bi, bj = (np.ascontiguousarray(kept[k], np.int32) for k in ("sbi", "sbj"))
+        if self.L.or_col_inject(self._h, n, _p(keys), _p(bi), _p(bj), _p(np.ascontiguousarray(f))) != 0:
+            raise ValueError("injected contacts exceed the oracle's capacity")
+
+    def warm_store(self) -> dict:
+        """The warm-start store the next substep looks its impulses up in: keys (int64) and
+        jn, jt1, jt2 (float64 copies of the stored values)."""
+        if self.b is None:
+            self._build()
+        n = int(self.L.or_col_warm_get(self._h, None, None, None, None))
+        d = dict(keys=np.zeros(n, np.int64), jn=np.zeros(n), jt1=np.zeros(n), jt2=np.zeros(n))
+        self.L.or_col_warm_get(self._h, _p(d["keys"]), _p(d["jn"]), _p(d["jt1"]), _p(d["jt2"]))
+        return d
+
+    def set_warm_store(self, d: dict) -> None:
+        """Replace the warm-start store (keys ascending; impulses rounded to this precision)."""
+        if self.b is None:
+            self._build()
+        k = np.ascontiguousarray(d["keys"], np.int64)
+        a = [np.ascontiguousarray(d[f], np.float64) for f in ("jn", "jt1", "jt2")]
+        if self.L.or_col_warm_set(self._h, len(k), _p(k), *(_p(x) for x in a)) != 0:
+            raise ValueError("warm store larger than the oracle's capacity")
+
+    def body_state(self):
+        """(xc, q, v, w) copies in the oracle's precision."""
+        if self.b is None:
+            self._build()
+        return self.b.xc.copy(), self.b.q.copy(), self.b.v.copy(), self.b.w.copy()
+
+    def set_body_state(self, xc, q, v, w):
+        """Overwrite positions, quaternions (x, y, z, w) and velocities (the warm store is kept)."""
+        if self.b is None:
+            self._build()
+        for dst, src in ((self.b.xc, xc), (self.b.q, q), (self.b.v, v), (self.b.w, w)):
+            dst[...] = np.asarray(src, self.F).reshape(dst.shape)
 
     def get_state(self) -> State:
         if self.b is None:
@@ -320,9 +427,9 @@ class ColoredOracle:
         return f
 
 
-def _box_sigs(L):
+def _box_sigs(L, F=ctypes.c_float):
     P = ctypes.c_void_p
-    L.or_box_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_float, P, P, P, P, P, P, P, P, P,
+    L.or_box_step.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, F, P, P, P, P, P, P, P, P, P,
                               ctypes.c_double, ctypes.c_int, ctypes.c_double, P, P, P]
     L.or_box_step.restype = ctypes.c_int
     L.or_box_box.argtypes = [P, P, P, P, P, P, ctypes.c_double, P, P, P, P]
@@ -367,7 +474,10 @@ class BoxOracle:
     2 applied warm, 4 colour cache, 8 warm start, 32 first-fit colours, 64 row form."""
     name = "box_color_cache_oracle"
 
-    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=111, margin=2e-3, cap=MAXC):
+    def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, flags=111, margin=2e-3, cap=MAXC,
+                 precision="float32"):
+        self.precision = precision
+        self.F, self.L = _precision(precision)
         self.dims = dims; self.mu = mu; self.vit = vit; self.pit = pit; self.flags = flags; self.margin = margin
         self.cap = cap
         self._centers, self._halves, self._dens, self._mus, self._kin = [], [], [], [], []
@@ -384,10 +494,11 @@ class BoxOracle:
         return len(self._centers) - 1
 
     def _build(self):
-        L = lib()
+        L = self.L
         if not hasattr(L, "_col_ready"):
             _col_sigs(L); L._col_ready = True
-        _box_sigs(L)
+        if L is lib():
+            _box_sigs(L)
         c = np.array(self._centers, float); h = np.array(self._halves, float); N = len(c)
         M = np.array(self._dens) * 8.0 * h[:, 0] * h[:, 1] * h[:, 2]
         e = 2.0 * h
@@ -401,11 +512,15 @@ class BoxOracle:
                            v=np.zeros((N, 3), np.float32), w=np.zeros((N, 3), np.float32),
                            invM=np.where(kin == 1, 0.0, 1.0 / M).astype(np.float32),
                            IbInv=IbInv.astype(np.float32), kin=kin.astype(np.int32), M=M)
+        self.b = _cast_bodies(self.b, self.F)
+        F = self.F
         self.half4 = np.zeros((N, 4), np.float32); self.half4[:, :3] = h
+        self.half4 = self.half4.astype(F)
         self.mus = np.array(self._mus, np.float32)
         self.per_body = bool(np.any(self.mus != np.float32(self.mu)))
-        self.pv = np.zeros((N, 3), np.float32); self.po = np.zeros((N, 3), np.float32)
-        self.vgrav = np.zeros((N, 3), np.float32)
+        self.mus = self.mus.astype(F)
+        self.pv = np.zeros((N, 3), F); self.po = np.zeros((N, 3), F)
+        self.vgrav = np.zeros((N, 3), F)
         sc = np.array(self._scenes, np.int32)
         self.scene = sc if len(sc) and sc.max() > 0 else None
         self.local = scene_local_index(sc)
@@ -415,8 +530,9 @@ class BoxOracle:
         if self.b is None:
             self._build()
         b = self.b
-        rc = lib().or_box_step(self._h, self.flags, self.N, _p(self.half4), _p(self.mus) if self.per_body else None,
-                               float(self.mu), _p(b.xc), _p(b.q), _p(b.v), _p(b.w), _p(self.pv), _p(self.po),
+        rc = self.L.or_box_step(self._h, self.flags, self.N, _p(self.half4), _p(self.mus) if self.per_body else None,
+                               float(self.F(np.float32(self.mu))), _p(b.xc), _p(b.q), _p(b.v), _p(b.w), _p(self.pv),
+                               _p(self.po),
                                _p(b.invM), _p(b.IbInv), _p(b.kin), float(dt), int(substeps),
                                float(np.float32(self.margin)), _p(self.vgrav),
                                None if self.scene is None else _p(self.scene), _p(self.local))
@@ -426,16 +542,27 @@ class BoxOracle:
 
     def stats(self):
         out = np.zeros(7, np.int32)
-        lib().or_col_stats(self._h, _p(out))
+        self.L.or_col_stats(self._h, _p(out))
         return dict(zip(("n_contacts", "n_kept", "n_pairs", "n_colors", "hits", "misses", "seg_overflow"),
                         out.tolist()))
+
+    def kept_contacts(self) -> dict:
+        """The last substep's kept contacts (see ColoredOracle.kept_contacts)."""
+        return ColoredOracle.kept_contacts(self)
+
+    def warm_store(self) -> dict:
+        """The warm-start store (see ColoredOracle.warm_store)."""
+        return ColoredOracle.warm_store(self)
+
+    def set_warm_store(self, d: dict) -> None:
+        ColoredOracle.set_warm_store(self, d)
 
     def set_body_state(self, xc, q, v, w):
         """Overwrite positions, quaternions (x, y, z, w) and velocities (the warm-start store is kept)."""
         if self.b is None:
             self._build()
         for dst, src in ((self.b.xc, xc), (self.b.q, q), (self.b.v, v), (self.b.w, w)):
-            dst[...] = np.asarray(src, np.float32).reshape(dst.shape)
+            dst[...] = np.asarray(src, self.F).reshape(dst.shape)
 
     def body_state(self):
         """(xc, q, v, w) float32 copies."""

@@ -640,6 +640,14 @@ typedef struct {
     /* the rest of the last substep's kept contacts, for or_col_kept (COL:1095-1103 reads them back) */
     int *ws_bi, *ws_bj;
     float *ws_pA, *ws_pB, *ws_nrm, *ws_pen, *ws_jp;
+    /* the last substep's kept impulses as the solve received them (warm-started, reduced) */
+    float *pre_jn, *pre_jt1, *pre_jt2;
+    /* the FP64 re-solve's input: when inj_n >= 0 the next substep solves these kept contacts
+     * (with these starting impulses) instead of the ones it selects itself */
+    int inj_n;
+    int64_t *inj_keys;
+    int *inj_bi, *inj_bj;
+    double *inj_f;       /* per contact: pA 3, pB 3, n 3, pen, jn, jt1, jt2 (13 doubles) */
     /* colour cache (contact_engine_gpu_color_cache.py:26-54) and the colour grouping it reuses */
     int cached_pairs, cached_colors, has_colors;
     int *cached_a, *cached_b;
@@ -660,6 +668,8 @@ OR_API void *or_col_create(int mode, int vit, int pit, int mx, float mu, float t
     e->ws_bi = malloc(sizeof(int) * cap); e->ws_bj = malloc(sizeof(int) * cap);
     e->ws_pA = malloc(sizeof(float) * 3 * cap); e->ws_pB = malloc(sizeof(float) * 3 * cap);
     e->ws_nrm = malloc(sizeof(float) * 3 * cap); e->ws_pen = malloc(sizeof(float) * cap); e->ws_jp = malloc(sizeof(float) * cap);
+    e->pre_jn = malloc(sizeof(float) * cap); e->pre_jt1 = malloc(sizeof(float) * cap); e->pre_jt2 = malloc(sizeof(float) * cap);
+    e->inj_n = -1; e->inj_keys = NULL; e->inj_bi = NULL; e->inj_bj = NULL; e->inj_f = NULL;
     e->cached_a = malloc(sizeof(int) * cap); e->cached_b = malloc(sizeof(int) * cap);
     e->cached_mass = malloc(sizeof(float) * (N > 0 ? N : 1)); e->cached_N = N;
     e->porder = malloc(sizeof(int) * cap); e->cstart = calloc(512, sizeof(int)); e->ccount = calloc(512, sizeof(int));
@@ -672,6 +682,8 @@ OR_API void or_col_destroy(void *h)
     if (!e) return;
     free(e->ws_keys); free(e->ws_jn); free(e->ws_jt1); free(e->ws_jt2);
     free(e->ws_bi); free(e->ws_bj); free(e->ws_pA); free(e->ws_pB); free(e->ws_nrm); free(e->ws_pen); free(e->ws_jp);
+    free(e->pre_jn); free(e->pre_jt1); free(e->pre_jt2);
+    free(e->inj_keys); free(e->inj_bi); free(e->inj_bj); free(e->inj_f);
     free(e->cached_a); free(e->cached_b); free(e->cached_mass); free(e->porder); free(e->cstart); free(e->ccount);
     free(e);
 }
@@ -680,6 +692,53 @@ OR_API void or_col_stats(void *h, int *out)
     col_engine_t *e = h;
     out[0] = e->n_contacts; out[1] = e->n_kept; out[2] = e->n_pairs; out[3] = e->n_colors;
     out[4] = e->hits; out[5] = e->misses; out[6] = e->seg_overflow;
+}
+/* the last substep's kept impulses before its solve, as float64 (the FP64 re-solve's input) */
+OR_API int or_col_pre(void *h, double *jn, double *jt1, double *jt2)
+{
+    col_engine_t *e = h;
+    for (int i = 0; jn && i < e->ws_n; ++i) { jn[i] = e->pre_jn[i]; jt1[i] = e->pre_jt1[i]; jt2[i] = e->pre_jt2[i]; }
+    return e->ws_n;
+}
+/* kept contacts for the next substep to solve in place of its own selection (n < 0: none).
+ * f holds 13 doubles per contact: pA, pB, n, depth, jn, jt1, jt2 (the starting impulses). */
+OR_API int or_col_inject(void *h, int n, const int64_t *keys, const int *bi, const int *bj, const double *f)
+{
+    col_engine_t *e = h;
+    free(e->inj_keys); free(e->inj_bi); free(e->inj_bj); free(e->inj_f);
+    e->inj_keys = NULL; e->inj_bi = NULL; e->inj_bj = NULL; e->inj_f = NULL;
+    e->inj_n = -1;
+    if (n < 0) return 0;
+    if (n > e->cap) return 1;
+    e->inj_keys = malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+    e->inj_bi = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    e->inj_bj = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    e->inj_f = malloc(sizeof(double) * 13 * (size_t)(n > 0 ? n : 1));
+    memcpy(e->inj_keys, keys, sizeof(int64_t) * n); memcpy(e->inj_bi, bi, sizeof(int) * n);
+    memcpy(e->inj_bj, bj, sizeof(int) * n); memcpy(e->inj_f, f, sizeof(double) * 13 * n);
+    e->inj_n = n;
+    return 0;
+}
+/* the warm-start store (the kept keys and impulses the next substep looks up), read and
+ * replaced in float64 so a store moves between the float32 oracle and its FP64 re-solve build */
+OR_API int or_col_warm_get(void *h, int64_t *keys, double *jn, double *jt1, double *jt2)
+{
+    col_engine_t *e = h;
+    for (int i = 0; keys && i < e->ws_n; ++i) {
+        keys[i] = e->ws_keys[i]; jn[i] = e->ws_jn[i]; jt1[i] = e->ws_jt1[i]; jt2[i] = e->ws_jt2[i];
+    }
+    return e->ws_n;
+}
+OR_API int or_col_warm_set(void *h, int n, const int64_t *keys, const double *jn, const double *jt1,
+                           const double *jt2)
+{
+    col_engine_t *e = h;
+    if (n < 0 || n > e->cap) return 1;
+    for (int i = 0; i < n; ++i) {
+        e->ws_keys[i] = keys[i]; e->ws_jn[i] = (float)jn[i]; e->ws_jt1[i] = (float)jt1[i]; e->ws_jt2[i] = (float)jt2[i];
+    }
+    e->ws_n = n;
+    return 0;
 }
 /* the kept contacts of the last substep in feature order: keys, bodies, points, normal, depth and
  * the impulses after the solve (jn, jt1, jt2, jp); returns their count */
@@ -1151,6 +1210,19 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
                 jn[Ck] = (float)jn_red[i]; jt1[Ck] = jt1_in[i]; jt2[Ck] = jt2_in[i]; jp[Ck] = 0.0f;
                 Ck++;
             }
+            if (e->inj_n >= 0) {  /* the FP64 re-solve: the given contacts replace the selection */
+                Ck = e->inj_n;
+                for (int i = 0; i < Ck; ++i) {
+                    const double *f = e->inj_f + 13 * (size_t)i;
+                    okeys[i] = e->inj_keys[i]; sbi[i] = e->inj_bi[i]; sbj[i] = e->inj_bj[i];
+                    st3(spA, i, V((float)f[0], (float)f[1], (float)f[2])); st3(spB, i, V((float)f[3], (float)f[4], (float)f[5]));
+                    st3(sn, i, V((float)f[6], (float)f[7], (float)f[8])); spen[i] = (float)f[9];
+                    jn[i] = (float)f[10]; jt1[i] = (float)f[11]; jt2[i] = (float)f[12]; jp[i] = 0.0f;
+                }
+                or_col_inject(e, -1, NULL, NULL, NULL, NULL);  /* one substep only */
+            }
+            memcpy(e->pre_jn, jn, sizeof(float) * Ck); memcpy(e->pre_jt1, jt1, sizeof(float) * Ck);
+            memcpy(e->pre_jt2, jt2, sizeof(float) * Ck);
             e->n_kept = Ck;
             memset(pv, 0, sizeof(float) * 3 * N); memset(po, 0, sizeof(float) * 3 * N);
             /* C7: pairs over the kept contacts (COL:1158-1176, 341-389); in the plain engine every

@@ -8,12 +8,17 @@ G_DT = 9.81 * DT  # the velocity one step of gravity gives, the scale of the vel
 R = 0.05
 
 
+def receipt():
+    """The receipt's arrays (float32 state and contacts, float64 forces)."""
+    return np.load(f"{ROOT}/tests/golden/cc10k_golden.npz")
+
+
 def _cc10k_bounds():
     """Per field: None = bitwise, else the largest admitted |got - receipt|.  The impulses are
     bounded at 1e-5 of the receipt's largest impulse of that row (the stated 1e-5 relative), the
     linear velocities at 1e-5 g dt, the angular ones at 1e-5 g dt / R and the forces at 1e-5 of
     the largest force."""
-    g = np.load(f"{ROOT}/tests/golden/cc10k_golden.npz")
+    g = receipt()
     tol = {k: None for k in ("xc", "ckeys", "sbi", "sbj", "spA", "spB", "sn", "spen", "jp")}
     tol.update(jn=1e-5 * float(np.abs(g["jn"]).max()), jt1=1e-5 * float(np.abs(g["jt1"]).max()),
                jt2=1e-5 * float(np.abs(g["jt2"]).max()), vc=1e-5 * G_DT, om=1e-5 * G_DT / R, Rm=1e-6,

@@ -51,14 +51,36 @@ def test_oracle_color_cache_lattice10k_against_receipt(oracle_mod):
     position impulses are bitwise; the rest within the bounds of tests/cc10k.py.  The receipt
     holds the last step only, so the first step where a velocity bit departs is not visible;
     the contact geometry of step 40 being bitwise says that every position up to step 39 was."""
-    from cc10k import check_cc10k
+    from cc10k import check_cc10k, receipt
     from conftest import lattice
+    from fp64 import compare, resolve_injected
     e = oracle_mod.ColoredOracle(mode="color_cache", dims=DIMS, mu=0.5, vit=40, pit=20)
     for c in lattice(10000):
         e.add_body(c)
-    for _ in range(40):
+    for _ in range(39):
         e.step(DT, 1)
+    before = e.body_state()
+    e.step(DT, 1)
     st = e.stats()
     assert (st["n_contacts"], st["n_kept"], st["n_pairs"], st["n_colors"], st["hits"], st["misses"]) == \
         (87716, 40000, 10000, 2, 35, 2)  # the receipt's counts
-    check_cc10k(e.get_state(), e.contact_forces(), e.kept_contacts())
+    kept = e.kept_contacts()
+    check_cc10k(e.get_state(), e.contact_forces(), kept)
+    # the last step's solve repeated in float64 on the same contacts: this float32 run and the
+    # reference's receipt both sit within float32 rounding of it
+    def make64():
+        o = oracle_mod.ColoredOracle(mode="color_cache", dims=DIMS, mu=0.5, vit=40, pit=20, precision="float64")
+        for c in lattice(10000):
+            o.add_body(c)
+        return o
+    o = resolve_injected(make64, before, kept, e.pre_solve_impulses(), DT)
+    ours = compare(kept, e.body_state(), o.kept_contacts(), o.body_state(), 9.81 * DT)
+    g = receipt()
+    ref_state = (g["xc"], None, g["vc"], g["om"])
+    theirs = compare({k: g[k] for k in kept}, ref_state, o.kept_contacts(), o.body_state(), 9.81 * DT)
+    print("10k lattice vs FP64 re-solve: this run", ours, "the reference's receipt", theirs)
+    for r in (ours, theirs):
+        assert r["matched"] == 1.0
+        for f in ("jn", "jt1", "jt2", "jp"):
+            assert r[f] <= 1e-5, (f, r[f])
+        assert r["v"] <= 1e-5

@@ -18,6 +18,7 @@ import pytest
 
 from cc10k import check_cc10k
 from conftest import DIMS, DT, cuda_ok, lattice
+from fp64 import compare, resolve_from_store
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_ok(), reason="needs a CUDA device")]
 
@@ -77,19 +78,38 @@ def _lockstep(e, o, steps, every, substeps=2):
 def test_boxes10k_matches_oracle(me, oracle_mod):
     """The bench's default workload: 10 000 random boxes (edges U[0.2, 0.6], per-body mu
     U[0.3, 0.8]) through the 300 set-up steps in which the pile forms and 20 steps of the timed
-    window, 2 substeps x (16 + 10) sweeps, bitwise against the oracle every 20 steps."""
+    window, 2 substeps x (16 + 10) sweeps, bitwise against the oracle every 20 steps.  Then the
+    GPU's next substep against its FP64 re-solve from the GPU's own state and warm store: the
+    impulses within 1e-5 of the largest FP64 impulse of their row, velocities within
+    1e-4 g dt (the bounds of tests/test_fp64_resolve.py)."""
     sc = importlib.import_module("motion_engine_b200.scenes").random_boxes(n=10000)
     e, o = _box_pair(me, oracle_mod, sc, 16, 10, 0.55)
     _lockstep(e, o, 320, 20)
     assert e.header_dict()["n_kept"] > 30000  # the pile has formed
+    st, wm = _gpu_state(e), e.warm_store()
+    e.step(DT / 2, 1)
+
+    def make64():
+        o64 = oracle_mod.BoxOracle(mu=0.55, vit=16, pit=10, precision="float64")
+        for c, d, m, de in zip(sc["centers"], sc["dims"], sc["mu"], sc["density"]):
+            o64.add_box(c, dims=d, density=de, mu=m)
+        return o64
+    o64 = resolve_from_store(make64, st, wm, DT / 2)
+    r = compare(e.kept_contacts(), _gpu_state(e), o64.kept_contacts(), o64.body_state(), 9.81 * DT / 2)
+    print("boxes10k GPU substep vs FP64 re-solve:", r)
+    assert r["matched"] == 1.0
+    for f in ("jn", "jt1", "jt2", "jp"):
+        assert r[f] <= 1e-5, (f, r[f])
+    assert r["v"] <= 1e-4
 
 
 def test_stress100k_first_steps_match_oracle(me, oracle_mod):
     """The 100 000-cube stress lattice (edge 0.25, mu 0.6, 2 substeps x (16 + 16) sweeps): its
-    first steps, with the lowest layer in contact, bitwise against the oracle."""
+    first 80 steps -- the lowest layer on the ground from the start, the upper layers landing on
+    it from about step 60 -- bitwise against the oracle every 20 steps."""
     sc = importlib.import_module("motion_engine_b200.scenes").box_lattice(n=100000)
     e, o = _box_pair(me, oracle_mod, sc, 16, 16, 0.6)
-    _lockstep(e, o, 4, 1)
+    _lockstep(e, o, 80, 20)
     assert e.header_dict()["n_kept"] > 10000
 
 
