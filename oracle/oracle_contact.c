@@ -642,6 +642,7 @@ typedef struct {
     float *ws_pA, *ws_pB, *ws_nrm, *ws_pen, *ws_jp;
     /* the last substep's kept impulses as the solve received them (warm-started, reduced) */
     float *pre_jn, *pre_jt1, *pre_jt2;
+    int kept_n;          /* kept contacts of the last substep (or_col_kept, or_col_pre) */
     /* the FP64 re-solve's input: when inj_n >= 0 the next substep solves these kept contacts
      * (with these starting impulses) instead of the ones it selects itself */
     int inj_n;
@@ -669,6 +670,7 @@ OR_API void *or_col_create(int mode, int vit, int pit, int mx, float mu, float t
     e->ws_pA = malloc(sizeof(float) * 3 * cap); e->ws_pB = malloc(sizeof(float) * 3 * cap);
     e->ws_nrm = malloc(sizeof(float) * 3 * cap); e->ws_pen = malloc(sizeof(float) * cap); e->ws_jp = malloc(sizeof(float) * cap);
     e->pre_jn = malloc(sizeof(float) * cap); e->pre_jt1 = malloc(sizeof(float) * cap); e->pre_jt2 = malloc(sizeof(float) * cap);
+    e->kept_n = 0;
     e->inj_n = -1; e->inj_keys = NULL; e->inj_bi = NULL; e->inj_bj = NULL; e->inj_f = NULL;
     e->cached_a = malloc(sizeof(int) * cap); e->cached_b = malloc(sizeof(int) * cap);
     e->cached_mass = malloc(sizeof(float) * (N > 0 ? N : 1)); e->cached_N = N;
@@ -697,8 +699,8 @@ OR_API void or_col_stats(void *h, int *out)
 OR_API int or_col_pre(void *h, double *jn, double *jt1, double *jt2)
 {
     col_engine_t *e = h;
-    for (int i = 0; jn && i < e->ws_n; ++i) { jn[i] = e->pre_jn[i]; jt1[i] = e->pre_jt1[i]; jt2[i] = e->pre_jt2[i]; }
-    return e->ws_n;
+    for (int i = 0; jn && i < e->kept_n; ++i) { jn[i] = e->pre_jn[i]; jt1[i] = e->pre_jt1[i]; jt2[i] = e->pre_jt2[i]; }
+    return e->kept_n;
 }
 /* kept contacts for the next substep to solve in place of its own selection (n < 0: none).
  * f holds 13 doubles per contact: pA, pB, n, depth, jn, jt1, jt2 (the starting impulses). */
@@ -746,7 +748,7 @@ OR_API int or_col_kept(void *h, int64_t *keys, int *bi, int *bj, float *pA, floa
                        float *jn, float *jt1, float *jt2, float *jp)
 {
     col_engine_t *e = h;
-    const int C = e->ws_n;
+    const int C = e->kept_n;
     if (keys) {
         memcpy(keys, e->ws_keys, sizeof(int64_t) * C); memcpy(bi, e->ws_bi, sizeof(int) * C);
         memcpy(bj, e->ws_bj, sizeof(int) * C); memcpy(pA, e->ws_pA, sizeof(float) * 3 * C);
@@ -1293,10 +1295,12 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
             memcpy(e->ws_nrm, sn, sizeof(float) * 3 * Ck); memcpy(e->ws_pen, spen, sizeof(float) * Ck);
             memcpy(e->ws_jp, jp, sizeof(float) * Ck);
             e->ws_n = Ck;
+            e->kept_n = Ck;
         } else {
             e->n_kept = 0; e->n_pairs = 0; e->n_colors = 0;
             memset(pv, 0, sizeof(float) * 3 * N); memset(po, 0, sizeof(float) * 3 * N);
             e->ws_n = 0;
+            e->kept_n = 0;
         }
         body_integrate(N, xc, q, v, w, pv, po, invM, sdt);
     }
@@ -1865,6 +1869,8 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             }
         }
         e->n_contacts = C; e->n_kept = C; e->n_pairs = P;
+        memcpy(e->pre_jn, jn, sizeof(float) * C); memcpy(e->pre_jt1, jt1, sizeof(float) * C);
+        memcpy(e->pre_jt2, jt2, sizeof(float) * C);
         if (P > 0) {
             int ncol, hit = 0;
             if ((flags & 4) && P == e->cached_pairs && e->has_colors) {
@@ -1926,14 +1932,16 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
         } else {
             e->n_colors = 0;
         }
-        if (flags & 8) {
-            memcpy(e->ws_keys, keys, sizeof(int64_t) * C);
-            memcpy(e->ws_jn, jn, sizeof(float) * C); memcpy(e->ws_jt1, jt1, sizeof(float) * C);
-            memcpy(e->ws_jt2, jt2, sizeof(float) * C);
-            e->ws_n = C;
-        } else {
-            e->ws_n = 0;
-        }
+        /* the kept contacts of this substep, for or_col_kept; with warm starting also the store */
+        memcpy(e->ws_keys, keys, sizeof(int64_t) * C);
+        memcpy(e->ws_jn, jn, sizeof(float) * C); memcpy(e->ws_jt1, jt1, sizeof(float) * C);
+        memcpy(e->ws_jt2, jt2, sizeof(float) * C);
+        memcpy(e->ws_bi, sbi, sizeof(int) * C); memcpy(e->ws_bj, sbj, sizeof(int) * C);
+        memcpy(e->ws_pA, spA, sizeof(float) * 3 * C); memcpy(e->ws_pB, spB, sizeof(float) * 3 * C);
+        memcpy(e->ws_nrm, sn, sizeof(float) * 3 * C); memcpy(e->ws_pen, spen, sizeof(float) * C);
+        memcpy(e->ws_jp, jp, sizeof(float) * C);
+        e->kept_n = C;
+        e->ws_n = (flags & 8) ? C : 0;
         body_integrate(N, xc, q, v, w, pv, po, invM, sdt);
     }
     free(invIw); free(keys); free(sbi); free(sbj); free(spA); free(spB); free(sn); free(spen);
