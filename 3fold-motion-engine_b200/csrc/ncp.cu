@@ -279,9 +279,9 @@ struct SweepArgs {
 enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
 // The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident) is
-// the per-CTA flag barrier of b2c_barrier.cuh over a.bar (its flags from word kBarrierFlagBase,
-// cleared by the host before the launch); `epoch` counts the grid barriers of this launch.  Its
-// wait is bounded by a.timeout_ns, after which it sets kErrBarrier and every CTA leaves the sweep.
+// the arrival-counter barrier of b2c_barrier.cuh over a.bar[0] (cleared by the host before the
+// launch); `epoch` counts the grid barriers of this launch.  Its wait is bounded by
+// a.timeout_ns, after which it sets kErrBarrier and every CTA leaves the sweep.
 template <int kKind, typename T>
 __device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a, unsigned int &epoch)
 {
@@ -294,8 +294,8 @@ __device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a, unsigned in
         return true;
     }
     ++epoch;
-    flag_arrive(a.bar + kBarrierFlagBase, epoch);
-    return flag_wait(a.bar + kBarrierFlagBase, epoch, a.timeout_ns, a.stats + kError, kErrBarrier);
+    grid_arrive(a.bar);
+    return grid_wait(a.bar, epoch, a.timeout_ns, a.stats + kError, kErrBarrier);
 }
 
 template <typename T>
@@ -593,8 +593,7 @@ int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, 
     if (mode > 1) {  // a cooperative grid of at most the co-resident CTAs
         const int nblocks = std::min(mode, grid_blocks<T>());
         if (nblocks > 1) {
-            // the barrier's arrival flags start from zero in every launch
-            cudaMemsetAsync(st->barrier + kBarrierFlagBase, 0, sizeof(uint32_t) * (size_t)nblocks, s);
+            cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);  // the arrival count restarts every launch
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(kSweepThreads);

@@ -8,8 +8,9 @@
 //   * one CTA (tiny scenes): __syncthreads (~0.04 us measured on B200);
 //   * a thread-block cluster of up to 16 CTAs: the hardware cluster barrier
 //     (barrier.cluster arrive.release / wait.acquire; ~0.25 us measured);
-//   * a cooperative grid: the per-CTA flag barrier of b2c_barrier.cuh, whose wait is bounded by
-//     a %globaltimer limit, after which it sets B2C_ERR_BARRIER_TIMEOUT and every CTA returns.
+//   * a cooperative grid: the arrival-counter barrier of b2c_barrier.cuh (~1.3 us measured),
+//     whose wait is bounded by a %globaltimer limit, after which it sets B2C_ERR_BARRIER_TIMEOUT
+//     and every CTA returns.
 //
 // Data layout.  The sweeps are bound by the latency of dependent loads, not by arithmetic or
 // bandwidth: following porder -> pair -> pidx -> contact -> body costs several L2 round trips
@@ -80,7 +81,7 @@ struct SolveArgs {
     float *v, *w, *pv, *po;
     float mu, t2d, dt;
     int vit, pit, fixed_frame, apply_warm, row;
-    unsigned int *bar_flags;  // the grid barrier's per-CTA arrival flags
+    unsigned int *bar_count;  // the grid barrier's arrival counter
     long long timeout_ns;
 };
 
@@ -266,7 +267,7 @@ enum BarrierKind { kBlock = 0, kCluster = 1, kGrid = 2 };
 // The barrier between colour phases, split into an arrive and a wait, so that a thread can
 // issue loads that do not depend on the other CTAs' work of the phase (its next task's fixed
 // record words) in between.  The grid form counts its barriers in `epoch` (uniform over the
-// CTA) and arrives with that number in its flag (b2c_barrier.cuh).
+// CTA): barrier k waits for k arrivals of every CTA (b2c_barrier.cuh).
 struct BarTok {
     unsigned int epoch;
 };
@@ -278,7 +279,7 @@ __device__ __forceinline__ BarTok bar_arrive(const SolveArgs &a, unsigned int &e
         asm volatile("barrier.cluster.arrive.release;\n" ::: "memory");
     } else if (kKind == kGrid) {
         tok.epoch = ++epoch;
-        flag_arrive(a.bar_flags, tok.epoch);
+        grid_arrive(a.bar_count);
     }
     return tok;
 }
@@ -293,7 +294,7 @@ __device__ __forceinline__ bool bar_wait(const SolveArgs &a, BarTok tok)
         asm volatile("barrier.cluster.wait.acquire;\n" ::: "memory");
         return true;
     }
-    return flag_wait(a.bar_flags, tok.epoch, a.timeout_ns, a.err, B2C_ERR_BARRIER_TIMEOUT);
+    return grid_wait(a.bar_count, tok.epoch, a.timeout_ns, a.err, B2C_ERR_BARRIER_TIMEOUT);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1086,7 +1087,6 @@ __device__ __forceinline__ void solve_phases_scene(const SolveArgs &a, const Sce
     RowPre pre;
     int pre_t = -1;
     bool pos;
-    unsigned int epoch = 0;  // grid barriers passed in this launch
     {
         const int sl = task_slot(0, 0, me, pos);
         if (sl >= 0) {
@@ -1214,7 +1214,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
         set_error("color_solve: B2C_COLOR_ROW_FORM needs B2C_COLOR_FIXED_FRAME");
         return B2C_EARG;
     }
-    a.bar_flags = pr->barrier + kBarrierFlagBase;
+    a.bar_count = pr->barrier;
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
@@ -1289,8 +1289,7 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
             k_color_solve_block<<<1, 256, stage_bytes(256), s>>>(a);
             if ((rc = check_launch("color_solve_block"))) return rc;
         } else {
-            // the barrier's arrival flags start from zero in every launch
-            cudaMemsetAsync(a.bar_flags, 0, sizeof(uint32_t) * (size_t)nblocks, s);
+            cudaMemsetAsync(a.bar_count, 0, sizeof(uint32_t), s);  // the arrival count restarts every launch
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
             cfg.blockDim = dim3(256);

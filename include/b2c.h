@@ -128,9 +128,9 @@ typedef struct b2c_jacobi_params {
 
 #define B2C_ERR_BARRIER_TIMEOUT 128  /* a grid barrier of the persistent solve gave up waiting */
 
-/* uint32 words of a grid-barrier buffer (b2c_pairs.barrier, b2c_ncp_state.barrier): 32 words of
- * padding, then one arrival flag for each of up to 512 CTAs; b2c_barrier_words() returns it */
-#define B2C_BARRIER_WORDS 544
+/* uint32 words of a grid-barrier buffer (b2c_pairs.barrier, b2c_ncp_state.barrier): the arrival
+ * counter, alone on its 128-byte line; b2c_barrier_words() returns it */
+#define B2C_BARRIER_WORDS 32
 
 /* Scratch of the coloured chain's ordering and manifold stage (one slot per raw contact
  * unless noted).  Replaces the radix-sort buffers, segment flags and selection arrays of
@@ -170,8 +170,8 @@ typedef struct b2c_pairs {
     int32_t *cached_a, *cached_b; /* colour cache: pbi / pbj of the cached colouring */
     float *cached_mass;      /* (bodies) invM of the cached colouring */
     int32_t *cache_state;    /* [cached pair count, cached colour count, valid, hits, misses] */
-    uint32_t *barrier;       /* (B2C_BARRIER_WORDS) the persistent solve's grid barrier: one arrival
-                                flag per CTA of a cooperative launch, cleared before each launch */
+    uint32_t *barrier;       /* (B2C_BARRIER_WORDS) the persistent solve's grid barrier: its arrival
+                                counter, cleared before each cooperative launch */
     float *rec;              /* colour-major pair records of the solve, b2c_pair_record_floats()
                                 floats: per slot a header, both bodies' inverse inertia and mass,
                                 and per contact its normal|depth, the terms that stay fixed

@@ -201,3 +201,30 @@ def test_barrier_wait_limit_reports_timeout(me):
             e.step(DT)
     x = torch.ones(4, device="cuda") * 2
     assert float(x.sum()) == 8.0
+
+
+def test_m5_stack16_against_reference_receipt(me, oracle_mod):
+    """The reference's own quality gate for the ColorCache engine (engine_metrics.py:265-293, its
+    receipt reports/innovation_stack_color_cache_l4.json): a 16-box stack at the rest pitch
+    0.205 m, vit 40, pit 10, 600 steps; penetration = max(0.205 - adjacent spacing).  The GPU
+    steps bitwise with the oracle throughout; its M5 passes (pen/R < 0.5, bounded drift) and lies
+    within 5 % of the receipt's 0.19564, the trajectories having parted by float32 ulps in a
+    stack that amplifies them over 600 steps (the stack8 golden arrays part at step 100)."""
+    from importlib import import_module
+    metrics = import_module("motion_engine_b200.metrics")
+    e = me.ColorCacheContactEngine(dims=DIMS, mu=0.5, vit=40, pit=10)
+    o = oracle_mod.ColoredOracle(mode="color_cache", dims=DIMS, mu=0.5, vit=40, pit=10)
+    for k in range(16):
+        e.add_body([0, 0, 0.101 + k * 0.205])
+        o.add_body([0, 0, 0.101 + k * 0.205])
+    pens = []
+    for t in range(600):
+        e.step(DT, 1)
+        o.step(DT, 1)
+        se = e.get_state()
+        assert se.xc.tobytes() == o.get_state().xc.tobytes(), f"step {t}"
+        z = np.sort(se.xc[:, 2])
+        pens.append(float(np.max(np.float32(0.205) - np.diff(z))))
+    q = metrics.m5(pens)
+    assert q["status"] == "PASS" and q["drift_class"] == "bounded"
+    assert abs(q["max_pen_over_R"] - 0.19563645124435425) < 0.05 * 0.19563645124435425, q

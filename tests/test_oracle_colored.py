@@ -84,3 +84,23 @@ def test_oracle_color_cache_lattice10k_against_receipt(oracle_mod):
         for f in ("jn", "jt1", "jt2", "jp"):
             assert r[f] <= 1e-5, (f, r[f])
         assert r["v"] <= 1e-5
+
+
+def test_oracle_m5_stack16_against_receipt(oracle_mod):
+    """The reference's M5 gate on the ColorCache engine (K = 16, vit 40, pit 10, 600 steps):
+    PASS, within 5 % of the receipt's max pen / R = 0.19564 (reports/innovation_stack_color_cache_l4.json)."""
+    import importlib
+    import __graft_entry__ as ge
+    ge.load_package()
+    metrics = importlib.import_module("motion_engine_b200.metrics")
+    e = oracle_mod.ColoredOracle(mode="color_cache", dims=DIMS, mu=0.5, vit=40, pit=10)
+    for k in range(16):
+        e.add_body([0, 0, 0.101 + k * 0.205])
+    pens = []
+    for _ in range(600):
+        e.step(DT, 1)
+        z = np.sort(e.get_state().xc[:, 2])
+        pens.append(float(np.max(np.float32(0.205) - np.diff(z))))
+    q = metrics.m5(pens)
+    assert q["status"] == "PASS"
+    assert abs(q["max_pen_over_R"] - 0.19563645124435425) < 0.05 * 0.19563645124435425, q
