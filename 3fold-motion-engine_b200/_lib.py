@@ -89,6 +89,17 @@ class NcpParams(ctypes.Structure):
                 ("barrier_timeout_ns", ctypes.c_int64)]
 
 
+class World(ctypes.Structure):
+    _fields_ = [("n", c_int32), ("max_contacts", c_int32), ("x", c_void_p), ("q", c_void_p), ("v", c_void_p),
+                ("w", c_void_p), ("half", c_void_p), ("mass", c_void_p), ("Ib", c_void_p), ("kin", c_void_p),
+                ("vkin", c_void_p), ("body_mu", c_void_p), ("mu", ctypes.c_double), ("xc32", c_void_p),
+                ("x4", c_void_p), ("half4", c_void_p), ("slot_p", c_void_p), ("slot_n", c_void_p),
+                ("slot_f", c_void_p), ("pa", c_void_p), ("pb", c_void_p), ("fid", c_void_p), ("key", c_void_p),
+                ("p", c_void_p), ("nrm", c_void_p), ("gap", c_void_p), ("attach", c_void_p), ("count", c_void_p),
+                ("warm_keys", c_void_p),
+                ("warm_lam", c_void_p), ("warm_n", c_void_p)]
+
+
 class Bncp(ctypes.Structure):
     _fields_ = [("n_env", c_int32), ("n_max", c_int32), ("nc", c_void_p), ("G", c_void_p), ("b", c_void_p),
                 ("mu", c_void_p), ("lam", c_void_p), ("res", c_void_p), ("iters", c_void_p), ("labels", c_void_p),
@@ -181,6 +192,25 @@ _SIGS = {
     "b2c_ncp_color": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
     "b2c_ncp_sweeps": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p], c_int32),
     "b2c_ncp_residual": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_void_p], c_int32),
+    "b2c_world_contacts": ([_P(World), _P(Boxes), c_void_p, c_void_p], c_int32),
+    "b2c_world_scene": ([_P(World), c_int32, _D, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                         c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_world_warm": ([_P(World), c_int32, c_void_p, c_void_p], c_int32),
+    "b2c_world_warm_adjoint": ([_P(World), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_world_store": ([_P(World), c_int32, c_void_p, c_void_p], c_int32),
+    "b2c_world_integrate": ([_P(World), c_void_p, _D, c_void_p], c_int32),
+    "b2c_ncp_adjoint": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                         c_void_p, c_void_p], c_int32),
+    "b2c_ncp_sweeps_record": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, ctypes.c_int64,
+                               c_void_p], c_int32),
+    "b2c_ncp_adjoint_unrolled": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, ctypes.c_int64,
+                                  c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_void_p], c_int32),
+    "b2c_world_adj_begin": ([_P(World), _P(NcpScene), c_void_p, _D, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "b2c_world_adj_end": ([_P(World), _P(NcpScene), c_void_p, c_void_p, c_void_p, _D, c_void_p, c_void_p, c_void_p,
+                           c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                           c_void_p], c_int32),
     "b2c_bncp_max_rows": ([], c_int32),
     "b2c_bncp_solve": ([_P(Bncp), c_int32, ctypes.c_double, c_int32, c_void_p], c_int32),
     "b2c_bncp_sensitivity": ([_P(Bncp), c_void_p, c_void_p, c_void_p], c_int32),

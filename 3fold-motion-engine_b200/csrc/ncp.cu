@@ -269,6 +269,7 @@ struct SweepArgs {
     const int *pa, *pb, *order, *cstart, *ccount, *dyn;
     T *lam, *v;
     long long *acc;
+    double *trace;  // null, or (iters, nc, kTraceWords): what each contact's update of each sweep started from
     int *stats;
     unsigned int *bar;
     long long timeout_ns;
@@ -277,6 +278,10 @@ struct SweepArgs {
 };
 
 enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
+
+// A recorded update: the contact's impulse before it (3) and the velocities of its bodies a, b
+// (6 + 6; zero where there is no body)
+constexpr int kTraceWords = 15;
 
 // The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident) is
 // the arrival-counter barrier of b2c_barrier.cuh over a.bar[0] (cleared by the host before the
@@ -299,12 +304,20 @@ __device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a, unsigned in
 }
 
 template <typename T>
-__device__ __forceinline__ void sweep_contact(const SweepArgs<T> &a, int c)
+__device__ __forceinline__ void sweep_contact(const SweepArgs<T> &a, int c, int it)
 {
     const int pa = a.pa[c], pb = a.pb[c];
     T u[3], z[3], zn[3];
     const T lo[3] = {a.lam[3 * (size_t)c], a.lam[3 * (size_t)c + 1], a.lam[3 * (size_t)c + 2]};
     contact_u(c, a.Ja, a.Jb, pa, pb, a.bias, a.v, u);
+    if (a.trace) {  // the bodies' rows of v are this thread's alone during the colour
+        double *t = a.trace + kTraceWords * ((size_t)it * a.nc + c);
+        for (int k = 0; k < 3; ++k) t[k] = (double)lo[k];
+        for (int k = 0; k < 6; ++k) {
+            t[3 + k] = pa >= 0 ? (double)__ldcg(a.v + 6 * (size_t)pa + k) : 0.0;
+            t[9 + k] = pb >= 0 ? (double)__ldcg(a.v + 6 * (size_t)pb + k) : 0.0;
+        }
+    }
     contact_z(u, lo, a.mu[c], a.rho[c], a.desaxce, a.soft, a.sep ? a.sep[c] : T(0), z);
     proj(z, a.mu[c], zn);
     a.lam[3 * (size_t)c] = zn[0];
@@ -339,7 +352,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweeps(SweepArgs<T> a)
     for (int it = 0; it < a.iters; ++it)
         for (int ci = 0; ci < ncol; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) sweep_contact(a, a.order[s0 + t]);
+            for (int t = tid; t < cnt; t += nth) sweep_contact(a, a.order[s0 + t], it);
             if (!phase_barrier<kKind>(a, epoch)) return;
         }
 }
@@ -505,6 +518,7 @@ SweepArgs<T> sweep_args(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_nc
     a.lam = (T *)st->lam;
     a.v = (T *)st->v;
     a.acc = reinterpret_cast<long long *>(st->acc);
+    a.trace = nullptr;
     a.stats = st->stats;
     a.bar = st->barrier;
     a.timeout_ns = (p && p->barrier_timeout_ns > 0) ? p->barrier_timeout_ns : 1000000000LL;  // default 1 s
@@ -581,10 +595,12 @@ int grid_blocks()
 }
 
 template <typename T>
-int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, int iters, cudaStream_t s)
+int sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, int iters, cudaStream_t s,
+           double *trace = nullptr)
 {
     if (iters <= 0 || sc->n_c == 0) return B2C_OK;
-    const SweepArgs<T> a = sweep_args<T>(sc, st, p, iters);
+    SweepArgs<T> a = sweep_args<T>(sc, st, p, iters);
+    a.trace = trace;
     int mode = p->solve_blocks;
     // auto: one CTA for small scenes; else every SM (the sweep's float64 work needs their issue
     // rate: on the 40 000-contact lattice a grid of 148 CTAs takes 4.6 ms for 40 sweeps, a
@@ -649,6 +665,471 @@ int residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p
     return check_launch("ncp_residual");
 }
 
+// ---------------------------------------------------------------------------------------------
+// The adjoint of the sweeps at a fixed point (float64): the implicit-function derivative of the
+// converged impulses, as the reverse of `iters` sweeps evaluated at the final iterate.
+//
+// A forward sweep maps lambda -> Phi(lambda; b, mu) with b = J v_free + bias; at its fixed point
+// lambda* the implicit function theorem gives d lambda* = (I - dPhi/dlambda)^-1 dPhi/d(b, mu).
+// Its transpose applied to an adjoint g is the limit of the reverse sweeps: starting from g,
+// each reverse sweep (colours in reverse order, each contact the transposed derivative of its
+// update at lambda*) pushes the adjoint back through one sweep and hands the free velocity, the
+// bias and the friction their share; `iters` reverse sweeps sum the first `iters` terms of that
+// Neumann series, the same truncation as `iters` forward sweeps from a warm start.
+//
+// One contact update (forward, in colour order, v the current body velocities):
+//   u = J v + bias,  z = lambda - rho (u + (mu |u_t|, 0, 0)),  lambda' = proj_K(z),
+//   v += Minv J^T (lambda' - lambda).
+// Its reverse, given the adjoints gl of lambda' and Vb of v after it:
+//   g  = gl + J Minv Vb;  (zb, mub) = the transposed derivative of proj_K at z applied to g;
+//   gl <- zb - J Minv Vb;  ub = -rho (zb + mu zb_n u_t / |u_t| on the tangential rows);
+//   Vb += J^T ub;  bias_b += ub;  mu_b += mub - rho |u_t| zb_n.
+// After the last (first) colour, the adjoint of v at the sweep's start goes to v_free (v =
+// v_free + Minv J^T lambda) and, through J Minv, back onto every gl; Vb restarts at zero.
+// Within a colour no two contacts share a dynamic body, so every write is the owner's; the
+// adjoint of kinematic and static bodies is not kept (their velocity is prescribed).
+// ---------------------------------------------------------------------------------------------
+struct AdjArgs {
+    int nc, nb, iters, desaxce;
+    const double *Ja, *Jb, *Minv, *mu, *rho, *lam, *u;
+    const double *trace;  // null: every reverse sweep at the final iterate (lam, u); else the recorded sweeps
+    const double *bias;
+    const int *pa, *pb, *order, *cstart, *ccount, *dyn;
+    double *gl, *vb, *vfree_b, *bias_b, *mu_b;
+    double *Ja_b, *Jb_b, *Minv_b, *rho_b;  // the recorded form's adjoints of the blocks and step sizes
+    int *stats;
+    unsigned int *bar;
+    long long timeout_ns;
+};
+
+// J_side (3x6) Minv_b (6x6) x, x = Vb of body b (6): out[3] += J (Minv x)
+__device__ __forceinline__ void add_j_minv(const double *J, const double *M, const double *x, double out[3])
+{
+    double t[6];
+    for (int k = 0; k < 6; ++k) {
+        double s = 0.0;
+        for (int j = 0; j < 6; ++j) s += M[k * 6 + j] * x[j];
+        t[k] = s;
+    }
+    for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < 6; ++k) s += J[r * 6 + k] * t[k];
+        out[r] += s;
+    }
+}
+
+// transposed derivative of proj_K (the branches of proj) at z, applied to g: zb, and mub
+__device__ __forceinline__ void proj_adjoint(const double z[3], double mu, const double g[3], double zb[3],
+                                             double &mub)
+{
+    const double zn = z[0], zt = sqrt(z[1] * z[1] + z[2] * z[2]);
+    if (zt <= mu * zn) {
+        zb[0] = g[0];
+        zb[1] = g[1];
+        zb[2] = g[2];
+        return;
+    }
+    if (mu * zt <= -zn) {
+        zb[0] = zb[1] = zb[2] = 0.0;
+        return;
+    }
+    // s = (zn + mu zt) / (1 + mu^2), f = mu s / zt, out = (s, f z1, f z2)
+    const double den = 1.0 + mu * mu;
+    const double sv = (zn + mu * zt) / den;
+    const double f = mu * sv / zt;
+    const double t1 = z[1] / zt, t2 = z[2] / zt;
+    const double ds_dzn = 1.0 / den;
+    const double ds_dt1 = mu * t1 / den, ds_dt2 = mu * t2 / den;
+    const double ds_dmu = (zt * den - 2.0 * mu * (zn + mu * zt)) / (den * den);
+    const double df_dzn = mu * ds_dzn / zt;
+    const double df_dt1 = mu * ds_dt1 / zt - mu * sv * t1 / (zt * zt);
+    const double df_dt2 = mu * ds_dt2 / zt - mu * sv * t2 / (zt * zt);
+    const double df_dmu = (sv + mu * ds_dmu) / zt;
+    const double gz = g[1] * z[1] + g[2] * z[2];
+    zb[0] = g[0] * ds_dzn + gz * df_dzn;
+    zb[1] = g[0] * ds_dt1 + f * g[1] + gz * df_dt1;
+    zb[2] = g[0] * ds_dt2 + f * g[2] + gz * df_dt2;
+    mub += g[0] * ds_dmu + gz * df_dmu;
+}
+
+__device__ void adj_contact(const AdjArgs &a, int c)
+{
+    const int A = a.pa[c], B = a.pb[c];
+    const bool dA = A >= 0 && a.dyn[A], dB = B >= 0 && a.dyn[B];
+    double vA[6], vBb[6];
+    double jm[3] = {0.0, 0.0, 0.0};
+    if (dA) {
+        for (int k = 0; k < 6; ++k) vA[k] = __ldcg(a.vb + 6 * (size_t)A + k);
+        add_j_minv(a.Ja + 18 * (size_t)c, a.Minv + 36 * (size_t)A, vA, jm);
+    }
+    if (dB) {
+        for (int k = 0; k < 6; ++k) vBb[k] = __ldcg(a.vb + 6 * (size_t)B + k);
+        add_j_minv(a.Jb + 18 * (size_t)c, a.Minv + 36 * (size_t)B, vBb, jm);
+    }
+    double g[3], z[3], u[3], lo[3];
+    const double mu = a.mu[c], rho = a.rho[c];
+    for (int k = 0; k < 3; ++k) {
+        g[k] = a.gl[3 * (size_t)c + k] + jm[k];
+        u[k] = a.u[3 * (size_t)c + k];
+        lo[k] = a.lam[3 * (size_t)c + k];
+    }
+    const double ut = sqrt(u[1] * u[1] + u[2] * u[2]);
+    const double s0 = a.desaxce ? u[0] + mu * ut : u[0];
+    z[0] = lo[0] - rho * s0;
+    z[1] = lo[1] - rho * u[1];
+    z[2] = lo[2] - rho * u[2];
+    double zb[3], mub = 0.0;
+    proj_adjoint(z, mu, g, zb, mub);
+    double ub[3];
+    ub[0] = -rho * zb[0];
+    ub[1] = -rho * zb[1];
+    ub[2] = -rho * zb[2];
+    if (a.desaxce) {
+        mub += -rho * ut * zb[0];
+        if (ut > 0.0) {
+            ub[1] += -rho * mu * (u[1] / ut) * zb[0];
+            ub[2] += -rho * mu * (u[2] / ut) * zb[0];
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        a.gl[3 * (size_t)c + k] = zb[k] - jm[k];
+        a.bias_b[3 * (size_t)c + k] += ub[k];
+    }
+    a.mu_b[c] += mub;
+    for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? dA : dB)) continue;
+        const int b = side == 0 ? A : B;
+        const double *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
+        const double *cur = side == 0 ? vA : vBb;
+        for (int k = 0; k < 6; ++k)
+            __stcg(a.vb + 6 * (size_t)b + k, cur[k] + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+    }
+}
+
+// The reverse of one recorded update of contact c in sweep `it` (sweep_contact):
+//   u = bias + Ja va + Jb vb,  z = lo - rho (u_n + mu |u_t| (de Saxce), u_t),  l = proj(z),
+//   v_a += Minv_a Ja^T (l - lo),  v_b likewise,
+// with va, vb and lo read back from the trace.  On entry gl[c] is the adjoint of l and vb the
+// adjoint of the velocities after the update; on exit gl[c] is the adjoint of lo and vb that of
+// the velocities before it.  The blocks' adjoints collect ub (x) v (from u) and dl (x) Minv vbar
+// (from the velocity change), the bodies' Minv adjoints vbar (x) J^T dl, rho_b[c] the adjoint of
+// rho.  Within a colour each dynamic body belongs to one contact, so the per-body sums need no
+// atomics.
+__device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
+{
+    const int A = a.pa[c], B = a.pb[c];
+    const bool dA = A >= 0 && a.dyn[A], dB = B >= 0 && a.dyn[B];
+    const double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
+    const double *JA = a.Ja + 18 * (size_t)c, *JB = a.Jb + 18 * (size_t)c;
+    double lo[3], va[6], vv[6];
+    for (int k = 0; k < 3; ++k) lo[k] = tr[k];
+    for (int k = 0; k < 6; ++k) {
+        va[k] = tr[3 + k];
+        vv[k] = tr[9 + k];
+    }
+    double u[3];
+    for (int i = 0; i < 3; ++i) {
+        double ui = a.bias[3 * (size_t)c + i];
+        if (A >= 0) {
+            double sacc = JA[6 * i] * va[0];
+            for (int j = 1; j < 6; ++j) sacc = sacc + JA[6 * i + j] * va[j];
+            ui = ui + sacc;
+        }
+        if (B >= 0) {
+            double sacc = JB[6 * i] * vv[0];
+            for (int j = 1; j < 6; ++j) sacc = sacc + JB[6 * i + j] * vv[j];
+            ui = ui + sacc;
+        }
+        u[i] = ui;
+    }
+    const double mu = a.mu[c], rho = a.rho[c];
+    const double ut = sqrt(u[1] * u[1] + u[2] * u[2]);
+    const double s0 = a.desaxce ? u[0] + mu * ut : u[0];
+    const double z[3] = {lo[0] - rho * s0, lo[1] - rho * u[1], lo[2] - rho * u[2]};
+    double l[3];
+    proj(z, mu, l);
+    const double dl[3] = {l[0] - lo[0], l[1] - lo[1], l[2] - lo[2]};
+    // the adjoints of the velocities after the update, and Minv times them
+    double wA[6] = {0, 0, 0, 0, 0, 0}, wB[6] = {0, 0, 0, 0, 0, 0}, mA[6] = {0, 0, 0, 0, 0, 0},
+           mB[6] = {0, 0, 0, 0, 0, 0};
+    double jm[3] = {0.0, 0.0, 0.0};
+    for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? dA : dB)) continue;
+        const int b = side == 0 ? A : B;
+        double *w = side == 0 ? wA : wB, *m = side == 0 ? mA : mB;
+        const double *M = a.Minv + 36 * (size_t)b, *J = side == 0 ? JA : JB;
+        for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
+        for (int k = 0; k < 6; ++k) {
+            double sacc = 0.0;
+            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
+            m[k] = sacc;
+        }
+        for (int r = 0; r < 3; ++r) {
+            double sacc = 0.0;
+            for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
+            jm[r] += sacc;
+        }
+    }
+    double g[3];
+    for (int k = 0; k < 3; ++k) g[k] = a.gl[3 * (size_t)c + k] + jm[k];
+    double zb[3], mub = 0.0;
+    proj_adjoint(z, mu, g, zb, mub);
+    double ub[3] = {-rho * zb[0], -rho * zb[1], -rho * zb[2]};
+    double rb = -(zb[0] * s0 + zb[1] * u[1] + zb[2] * u[2]);
+    if (a.desaxce) {
+        mub += -rho * ut * zb[0];
+        if (ut > 0.0) {
+            ub[1] += -rho * mu * (u[1] / ut) * zb[0];
+            ub[2] += -rho * mu * (u[2] / ut) * zb[0];
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        a.gl[3 * (size_t)c + k] = zb[k] - jm[k];
+        a.bias_b[3 * (size_t)c + k] += ub[k];
+    }
+    a.mu_b[c] += mub;
+    a.rho_b[c] += rb;
+    for (int side = 0; side < 2; ++side) {
+        const int b = side == 0 ? A : B;
+        if (b < 0) continue;
+        const bool d = side == 0 ? dA : dB;
+        const double *J = side == 0 ? JA : JB, *vf = side == 0 ? va : vv, *m = side == 0 ? mA : mB;
+        double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 6; ++k)
+                __stcg(Jbar + 6 * r + k, __ldcg(Jbar + 6 * r + k) + (ub[r] * vf[k] + (d ? dl[r] * m[k] : 0.0)));
+        if (!d) continue;
+        const double *w = side == 0 ? wA : wB;
+        double jt[6];  // J^T dl
+        for (int k = 0; k < 6; ++k) jt[k] = (J[k] * dl[0] + J[6 + k] * dl[1]) + J[12 + k] * dl[2];
+        double *Mb = a.Minv_b + 36 * (size_t)b;
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k) __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + w[i] * jt[k]);
+        for (int k = 0; k < 6; ++k)
+            __stcg(a.vb + 6 * (size_t)b + k, w[k] + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+    }
+}
+
+// unit eigenvector of the largest eigenvalue lm of a symmetric 3x3 W, from the largest cross
+// product of two rows of W - lm I; false when that eigenvalue is not simple (no derivative)
+__device__ bool eigvec_max3(const double W[3][3], double lm, double e[3])
+{
+    double R[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R[i][j] = W[i][j] - (i == j ? lm : 0.0);
+    double best = 0.0;
+    for (int p = 0; p < 3; ++p) {
+        const double *x = R[p], *y = R[(p + 1) % 3];
+        const double cr[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+        const double nn = cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2];
+        if (nn > best) {
+            best = nn;
+            for (int k = 0; k < 3; ++k) e[k] = cr[k];
+        }
+    }
+    if (!(best > 1e-20 * lm * lm * lm * lm)) return false;
+    const double inv = 1.0 / sqrt(best);
+    for (int k = 0; k < 3; ++k) e[k] *= inv;
+    return true;
+}
+
+// The start of the recorded sweeps, v = v_free + Minv sum_c J_c^T lo_c (setup, with lo the
+// warm start) and the step sizes rho_c = 1 / lambda_max(W_c), W_c = sum_sides J Minv J^T
+// (k_rho): gl[c] += J Minv vbar (the warm start's adjoint), the blocks' and Minv's adjoints,
+// and rho_b through d lambda_max = e^T dW e.  Run colour by colour like the sweeps.
+__device__ void adj_start_recorded(const AdjArgs &a, int c)
+{
+    const int A = a.pa[c], B = a.pb[c];
+    const double *tr = a.trace + kTraceWords * (size_t)c;  // sweep 0
+    const double lo[3] = {tr[0], tr[1], tr[2]};
+    const double rho = a.rho[c];
+    const double rb = a.rho_b[c];
+    double lmb = 0.0, e[3] = {0.0, 0.0, 0.0};
+    if (rb != 0.0 && rho > 0.0) {
+        double W[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (A >= 0) add_jmjt(W, a.Ja + 18 * (size_t)c, a.Minv + 36 * (size_t)A);
+        if (B >= 0) add_jmjt(W, a.Jb + 18 * (size_t)c, a.Minv + 36 * (size_t)B);
+        if (eigvec_max3(W, eigmax3(W), e)) lmb = -rho * rho * rb;  // rho = 1 / lambda_max
+    }
+    double jm[3] = {0.0, 0.0, 0.0};
+    for (int side = 0; side < 2; ++side) {
+        const int b = side == 0 ? A : B;
+        if (b < 0 || !a.dyn[b]) continue;
+        const double *M = a.Minv + 36 * (size_t)b, *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
+        double w[6], m[6], jt[6], je[6], jme[6];
+        for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
+        for (int k = 0; k < 6; ++k) {
+            double sacc = 0.0;
+            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
+            m[k] = sacc;
+            jt[k] = (J[k] * lo[0] + J[6 + k] * lo[1]) + J[12 + k] * lo[2];
+            je[k] = (J[k] * e[0] + J[6 + k] * e[1]) + J[12 + k] * e[2];
+        }
+        for (int k = 0; k < 6; ++k) {  // Minv J^T e
+            double sacc = 0.0;
+            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * je[j];
+            jme[k] = sacc;
+        }
+        for (int r = 0; r < 3; ++r) {
+            double sacc = 0.0;
+            for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
+            jm[r] += sacc;
+        }
+        double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 6; ++k)
+                __stcg(Jbar + 6 * r + k,
+                       __ldcg(Jbar + 6 * r + k) + (lo[r] * m[k] + 2.0 * lmb * e[r] * jme[k]));
+        double *Mb = a.Minv_b + 36 * (size_t)b;
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k)
+                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (w[i] * jt[k] + lmb * je[i] * je[k]));
+    }
+    for (int k = 0; k < 3; ++k) a.gl[3 * (size_t)c + k] += jm[k];
+}
+
+template <int kKind>
+__device__ __forceinline__ bool adj_barrier(const AdjArgs &a, unsigned int &epoch)
+{
+    if (kKind == kBlock) {
+        __syncthreads();
+        return true;
+    }
+    if (kKind == kCluster) {
+        cg::this_cluster().sync();
+        return true;
+    }
+    ++epoch;
+    grid_arrive(a.bar);
+    return grid_wait(a.bar, epoch, a.timeout_ns, a.stats + kError, kErrBarrier);
+}
+
+template <int kKind>
+__global__ void __launch_bounds__(kSweepThreads) k_adj_sweeps(AdjArgs a)
+{
+    const int ncol = a.stats[kNColors];
+    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
+    const int tid = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned int epoch = 0;
+    if (a.trace) {
+        // the recorded sweeps in reverse, then their start; vb carries through
+        for (int it = a.iters - 1; it >= 0; --it)
+            for (int ci = ncol - 1; ci >= 0; --ci) {
+                const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+                for (int t = tid; t < cnt; t += nth) adj_contact_recorded(a, a.order[s0 + t], it);
+                if (!adj_barrier<kKind>(a, epoch)) return;
+            }
+        for (int ci = 0; ci < ncol; ++ci) {
+            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            for (int t = tid; t < cnt; t += nth) adj_start_recorded(a, a.order[s0 + t]);
+            if (!adj_barrier<kKind>(a, epoch)) return;
+        }
+        for (int i = gid; i < 6 * a.nb; i += nth) {
+            a.vfree_b[i] += __ldcg(a.vb + i);
+            __stcg(a.vb + i, 0.0);
+        }
+        return;
+    }
+    for (int it = 0; it < a.iters; ++it) {
+        for (int ci = ncol - 1; ci >= 0; --ci) {
+            const int s0 = a.cstart[ci], cnt = a.ccount[ci];
+            for (int t = tid; t < cnt; t += nth) adj_contact(a, a.order[s0 + t]);
+            if (!adj_barrier<kKind>(a, epoch)) return;
+        }
+        // the sweep's start: v = v_free + Minv J^T lambda
+        for (int c = gid; c < a.nc; c += nth) {
+            const int A = a.pa[c], B = a.pb[c];
+            double jm[3] = {0.0, 0.0, 0.0}, x[6];
+            if (A >= 0 && a.dyn[A]) {
+                for (int k = 0; k < 6; ++k) x[k] = __ldcg(a.vb + 6 * (size_t)A + k);
+                add_j_minv(a.Ja + 18 * (size_t)c, a.Minv + 36 * (size_t)A, x, jm);
+            }
+            if (B >= 0 && a.dyn[B]) {
+                for (int k = 0; k < 6; ++k) x[k] = __ldcg(a.vb + 6 * (size_t)B + k);
+                add_j_minv(a.Jb + 18 * (size_t)c, a.Minv + 36 * (size_t)B, x, jm);
+            }
+            for (int k = 0; k < 3; ++k) a.gl[3 * (size_t)c + k] += jm[k];
+        }
+        if (!adj_barrier<kKind>(a, epoch)) return;
+        for (int i = gid; i < 6 * a.nb; i += nth) {
+            a.vfree_b[i] += __ldcg(a.vb + i);
+            __stcg(a.vb + i, 0.0);
+        }
+        if (!adj_barrier<kKind>(a, epoch)) return;
+    }
+}
+
+int adjoint_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, int iters,
+                   const double *trace, double *gl, double *vb, double *vfree_b, double *bias_b, double *mu_b,
+                   double *Ja_b, double *Jb_b, double *Minv_b, cudaStream_t s)
+{
+    if (iters <= 0 || sc->n_c == 0) return B2C_OK;
+    AdjArgs a;
+    a.nc = sc->n_c;
+    a.nb = sc->n_b;
+    a.iters = iters;
+    a.desaxce = p->desaxce;
+    a.Ja = (const double *)sc->Ja;
+    a.Jb = (const double *)sc->Jb;
+    a.Minv = (const double *)sc->Minv;
+    a.mu = (const double *)sc->mu;
+    a.rho = (const double *)st->rho;
+    a.lam = (const double *)st->lam;
+    a.u = (const double *)st->u;
+    a.trace = trace;
+    a.bias = (const double *)sc->bias;
+    a.Ja_b = Ja_b;
+    a.Jb_b = Jb_b;
+    a.Minv_b = Minv_b;
+    a.rho_b = (double *)st->res;
+    a.pa = sc->pa;
+    a.pb = sc->pb;
+    a.order = st->order;
+    a.cstart = st->cstart;
+    a.ccount = st->ccount;
+    a.dyn = st->dyn;
+    a.gl = gl;
+    a.vb = vb;
+    a.vfree_b = vfree_b;
+    a.bias_b = bias_b;
+    a.mu_b = mu_b;
+    a.stats = st->stats;
+    a.bar = st->barrier;
+    a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
+    cudaMemsetAsync(vb, 0, sizeof(double) * 6 * (size_t)sc->n_b, s);
+    if (trace) cudaMemsetAsync(st->res, 0, sizeof(double) * (size_t)sc->n_c, s);
+    int mode = p->solve_blocks;
+    if (mode == 0) mode = sc->n_c <= 16384 ? 1 : grid_blocks<double>();
+    if (mode > 1) {
+        int per = 0, dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_sweeps<kGrid>, kSweepThreads, 0);
+        const int nblocks = std::min(std::min(mode, kBarrierMaxCTAs), std::max(1, sms * per));
+        if (nblocks > 1) {
+            cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nblocks);
+            cfg.blockDim = dim3(kSweepThreads);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, k_adj_sweeps<kGrid>, a);
+            if (e != cudaSuccess) {
+                set_error("ncp_adjoint: cooperative launch of %d CTAs: %s", nblocks, cudaGetErrorString(e));
+                return B2C_ECUDA;
+            }
+            return check_launch("ncp_adjoint_grid");
+        }
+    }
+    k_adj_sweeps<kBlock><<<1, kSweepThreads, 0, s>>>(a);
+    return check_launch("ncp_adjoint");
+}
+
 }  // namespace ncp
 }  // namespace b2c
 
@@ -702,4 +1183,44 @@ extern "C" int32_t b2c_ncp_residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, 
     }
     return sc->dtype == 4 ? b2c::ncp::residual<float>(sc, st, p, b2c::stream_of(s))
                           : b2c::ncp::residual<double>(sc, st, p, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_ncp_adjoint(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                   int32_t iters, double *lam_bar, double *v_bar, double *vfree_bar, double *bias_bar,
+                                   double *mu_bar, b2c_stream s)
+{
+    if (!ncp_scene_ok(sc, st) || !p || sc->dtype != 8 || iters < 0 || !v_bar || !vfree_bar || p->soft ||
+        (sc->n_c > 0 && (!lam_bar || !bias_bar || !mu_bar))) {
+        b2c::set_error("b2c_ncp_adjoint: bad argument (float64 scenes only)");
+        return B2C_EARG;
+    }
+    return b2c::ncp::adjoint_sweeps(sc, st, p, iters, nullptr, lam_bar, v_bar, vfree_bar, bias_bar, mu_bar, nullptr,
+                                    nullptr, nullptr, b2c::stream_of(s));
+}
+
+extern "C" int32_t b2c_ncp_sweeps_record(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                         int32_t iters, double *trace, int64_t trace_len, b2c_stream s)
+{
+    if (!ncp_scene_ok(sc, st) || !p || sc->dtype != 8 || iters < 0 ||
+        (sc->n_c > 0 && iters > 0 && (!trace || trace_len < b2c::ncp::kTraceWords * (int64_t)iters * sc->n_c))) {
+        b2c::set_error("b2c_ncp_sweeps_record: bad argument (float64 scenes; trace of iters * n_c * 15 doubles)");
+        return B2C_EARG;
+    }
+    return b2c::ncp::sweeps<double>(sc, st, p, iters, b2c::stream_of(s), trace);
+}
+
+extern "C" int32_t b2c_ncp_adjoint_unrolled(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                            int32_t iters, const double *trace, int64_t trace_len, double *lam_bar,
+                                            double *v_bar, double *vfree_bar, double *bias_bar, double *mu_bar,
+                                            double *Ja_bar, double *Jb_bar, double *Minv_bar, b2c_stream s)
+{
+    if (!ncp_scene_ok(sc, st) || !p || sc->dtype != 8 || iters < 0 || !v_bar || !vfree_bar || p->soft ||
+        (sc->n_c > 0 && (!lam_bar || !bias_bar || !mu_bar || !Ja_bar || !Jb_bar || !Minv_bar)) ||
+        (sc->n_c > 0 && iters > 0 && (!trace || trace_len < b2c::ncp::kTraceWords * (int64_t)iters * sc->n_c))) {
+        b2c::set_error("b2c_ncp_adjoint_unrolled: bad argument (float64 hard-contact scenes; the trace of "
+                       "b2c_ncp_sweeps_record)");
+        return B2C_EARG;
+    }
+    return b2c::ncp::adjoint_sweeps(sc, st, p, iters, trace, lam_bar, v_bar, vfree_bar, bias_bar, mu_bar, Ja_bar,
+                                    Jb_bar, Minv_bar, b2c::stream_of(s));
 }

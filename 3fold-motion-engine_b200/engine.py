@@ -400,16 +400,19 @@ class RelaxedJacobiContactEngine(_BeadEngineBase):
     name = "relaxed_jacobi_b200"
 
     def __init__(self, dims=(0.3, 0.3, 0.2), relax=0.2, vit=40, pit=20, mu=0.5, device="cuda", graph=True,
-                 contact_capacity=MAXC):
+                 contact_capacity=MAXC, grid_dims=(128, 128, 32)):
         super().__init__(dims=dims, mu=mu, device=device, graph=graph)
         self.relax = float(relax)
         self.vit = int(vit)
         self.pit = int(pit)
         self.contact_capacity = int(contact_capacity)
+        # buckets of the bead hash grid (cell 2R, wrapping): a performance choice only -- the
+        # Jacobi sum is order free, so the contacts and the results do not depend on it
+        self.grid_dims = tuple(int(x) for x in grid_dims)
 
     def _build(self):
         self._setup_bodies()
-        self._setup_grid()
+        self._setup_grid(self.grid_dims)
         self._setup_contacts(self.contact_capacity)
         self.acc = torch.zeros((6, self.N), dtype=torch.int64, device=self.dev)
         self._struct_bodies()

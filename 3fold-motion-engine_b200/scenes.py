@@ -214,3 +214,44 @@ def ncp_lattice(n=10000, half=0.1, spacing=0.35, z0=0.0999, dz=0.1999, mass=1.0,
     bias[:, 0] = np.where(gap > 0, gap / dt, -0.2 * np.maximum(-gap - 1e-4, 0.0) / dt)
     return dict(Ja=Ja, Jb=Jb, Minv=Minv, v_free=vf, mu=np.full(nc, float(mu)),
                 body_pairs=np.stack([ca, cb], axis=1).astype(np.int32), dt=dt, bias=bias, feature=feat)
+
+
+def pushed_pyramids(n_scenes=256, edge=0.2, density=1000.0, mu=0.5, plate_speed=0.2, seed_jitter=7, seed_target=8,
+                    seed_v0=9, jitter=1e-3, target_sigma=0.05, v0_sigma=0.1):
+    """The differentiable workload: `n_scenes` copies of a 64-box stepped pyramid pushed along +x
+    by a kinematic plate.  A pyramid is four slices (along y, 3 mm apart) of layers 8-4-2-1-1
+    boxes wide (x, 1 mm apart), each layer centred on the one below; edge 0.2 m, density 1000.
+    Per scene: seeded uniform jitter of +-1 mm on every box position (seed 7), targets = the
+    nominal positions + N(0, 0.05) m (seed 8), initial velocities N(0, 0.1) m/s (seed 9).  The plate
+    (half extents 0.02 x 0.45 x 0.3, kinematic) starts 2 cm left of the base and moves at 0.2 m/s.
+    Returns dict(half (n,3), mass (n,), x (n,3), kin (n,), v_kin (n,6), scene (n,), mu (n,),
+    target (n,3), v0 (n,3)) over all scenes, the plate last in each scene (zero target and v0)."""
+    rj, rt, rv = (np.random.default_rng(s) for s in (seed_jitter, seed_target, seed_v0))
+    h = edge / 2
+    pos = []
+    widths = (8, 4, 2, 1, 1)
+    for sl in range(4):
+        y = (sl - 1.5) * (edge + 3e-3)
+        for k, wdt in enumerate(widths):
+            z = h + k * (edge + 1e-3)
+            for i in range(wdt):
+                pos.append([(i - (wdt - 1) / 2) * (edge + 1e-3), y, z])
+    pos = np.array(pos)
+    nb = len(pos)  # 64
+    plate_half = np.array([0.02, 0.45, 0.3])
+    plate_x = np.array([-(4 * (edge + 1e-3)) - 0.02 - plate_half[0], 0.0, plate_half[2] + 0.005])
+    out = {k: [] for k in ("half", "mass", "x", "kin", "v_kin", "scene", "mu", "target", "v0")}
+    for s in range(n_scenes):
+        x = pos + rj.uniform(-jitter, jitter, size=pos.shape)
+        out["x"].append(np.vstack([x, plate_x]))
+        out["half"].append(np.vstack([np.full((nb, 3), h), plate_half]))
+        out["mass"].append(np.r_[np.full(nb, density * edge ** 3), 1.0])
+        out["kin"].append(np.r_[np.zeros(nb, np.int32), 1])
+        vk = np.zeros((nb + 1, 6))
+        vk[nb, 0] = plate_speed
+        out["v_kin"].append(vk)
+        out["scene"].append(np.full(nb + 1, s, np.int32))
+        out["mu"].append(np.full(nb + 1, mu))
+        out["target"].append(np.vstack([pos + rt.normal(0.0, target_sigma, size=pos.shape), np.zeros(3)]))
+        out["v0"].append(np.vstack([rv.normal(0.0, v0_sigma, size=pos.shape), np.zeros(3)]))
+    return {k: np.concatenate(v) for k, v in out.items()}

@@ -92,6 +92,14 @@ WORKLOADS = {
                               pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                               published=(1e4 / 5.599e-3, "reference relaxed Jacobi, 5.599 ms/step, RTX 5070 "
                                          "(docs/RUNNING.md:374-379)")),
+    # the stress lattice under relaxed Jacobi: 100 000 bead boxes on the stress scene's seeded
+    # lattice in 50 x 50 x 10 m (5 % jitter), mu 0.6, 2 substeps x (16 velocity + 16 position
+    # iterations), the bead grid rebuilt every substep, 200 steps.  The bead engines need edges
+    # that are multiples of the 0.1 m bead pitch (a 0.25 m edge gives asymmetric bead offsets),
+    # so the edge is 0.3 m: 27 beads per box, 2.7 M beads
+    "stress100k_jacobi": dict(engine="jacobi", scene="box_lattice_beads", n=100000, dims=(0.3, 0.3, 0.3),
+                              density=1000.0, mu=0.6, vit=16, pit=16, substeps=2, dt=1 / 240, preroll=100, steps=200,
+                              warmup=3, parity_steps=8, contact_capacity=4_000_000, grid_dims=(512, 512, 128)),
     # plain relaxed Jacobi on a vertical stack of 16 unit cubes (1 m edge, 1 kg: density 1, 1000
     # beads each) with seeded 1 mm xy jitter, mu 0.5, 40 velocity / 20 position iterations, relax
     # 0.2, 1 substep, dt 1/240, 240 steps; penetration target 1e-3 m (max over adjacent pairs of
@@ -127,6 +135,8 @@ def scene_of(wl):
         return sc.random_boxes(n=wl["n"], edge=wl["edge"], box=wl["box"], mu=wl["mu_range"], density=wl["density"])
     if wl["scene"] == "unit_cube_stack":
         return {"centers": sc.unit_cube_stack(wl["n"])}
+    if wl["scene"] == "box_lattice_beads":
+        return {"centers": sc.box_lattice(n=wl["n"], edge=wl["dims"][0], extent=(50.0, 50.0, 10.0))["centers"]}
     return {"centers": sc.lattice(wl["n"]) if wl["scene"] == "lattice" else sc.stack(wl["n"])}
 
 
@@ -143,7 +153,8 @@ def make_engine(me, wl, scene):
     if wl["engine"] == "color_cache":
         e = me.ColorCacheContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
     elif wl["engine"] == "jacobi":
-        e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+        kw = {k: wl[k] for k in ("contact_capacity", "grid_dims") if k in wl}
+        e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"], **kw)
     else:
         raise ValueError(wl["engine"])
     for c in scene["centers"]:

@@ -460,6 +460,114 @@ B2C_API int32_t b2c_ncp_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const
 /* Natural-map residual per contact, its maximum and the contact velocity u (k_resid). */
 B2C_API int32_t b2c_ncp_residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
                                  b2c_stream s);
+/* The adjoint of the sweeps at their final iterate (float64 scenes): the implicit-function
+ * derivative of lambda* with respect to the free velocity, the bias and the friction, applied to
+ * lam_bar (n_c,3, consumed), as `iters` reverse sweeps at lambda* (the Neumann series of
+ * (I - dPhi/dlambda)^-T truncated at `iters` terms; dPhi the sweep, NG:485-568).  Needs the
+ * colouring of the last b2c_ncp_color and state->u of a b2c_ncp_residual at lambda*.  Adds to
+ * vfree_bar (n_b,6), bias_bar (n_c,3) and mu_bar (n_c); v_bar (n_b,6) is scratch.  No counterpart
+ * in the reference's NCPSolverGPU; its CPU sensitivity (ncp_ref.py:907-959) is the converged
+ * limit on a fixed branch.  The Jacobian blocks and Minv are held (no adjoint of them). */
+B2C_API int32_t b2c_ncp_adjoint(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                int32_t iters, double *lam_bar, double *v_bar, double *vfree_bar, double *bias_bar,
+                                double *mu_bar, b2c_stream s);
+/* b2c_ncp_sweeps (float64 scenes) that also records what every contact update of every sweep
+ * started from: trace[15 (it n_c + c) + 0..2] = the contact's impulse, [3..8] and [9..14] = the
+ * velocities (n_b,6 rows) of its bodies pa, pb (zero where there is none); trace_len >= 15 iters
+ * n_c doubles.  The impulses and velocities it leaves are bitwise those of b2c_ncp_sweeps. */
+B2C_API int32_t b2c_ncp_sweeps_record(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                      int32_t iters, double *trace, int64_t trace_len, b2c_stream s);
+/* The exact reverse of setup (warm or cold) and the `iters` sweeps recorded by
+ * b2c_ncp_sweeps_record (same scene, same colouring, hard contacts): lam_bar (n_c,3) holds the
+ * adjoint of the final impulses on entry and that of the starting impulses (the warm start) on
+ * return; adds to vfree_bar (n_b,6), bias_bar (n_c,3), mu_bar (n_c), and to the adjoints of the
+ * Jacobian blocks Ja_bar, Jb_bar (n_c,3,6) and of Minv_bar (n_b,6,6) -- through the contact
+ * velocities, the velocity changes and the step sizes rho_c = 1 / lambda_max(W_c) (where that
+ * eigenvalue is simple).  v_bar (n_b,6) is scratch; state->res is overwritten.  The derivative of
+ * what the sweeps computed, converged or not: where the converged impulses are not unique
+ * (redundant contacts) the one the sweeps reach depends on where they started, which the implicit
+ * form above cannot see.  No counterpart in the reference. */
+B2C_API int32_t b2c_ncp_adjoint_unrolled(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
+                                         int32_t iters, const double *trace, int64_t trace_len, double *lam_bar,
+                                         double *v_bar, double *vfree_bar, double *bias_bar, double *mu_bar,
+                                         double *Ja_bar, double *Jb_bar, double *Minv_bar, b2c_stream s);
+
+/* ---------------------------------------------------------------------------------------------
+ * The exact-cone box world: the reference's BoxWorld substep (src/motion_engine/ncp/ncp_gpu.py:
+ * 1237-1413) on the device, in float64, for one scene or many independent ones (the scene ids of
+ * b2c_boxes): SAT contacts -> build_scene -> the NCP above -> integration.  A substep is
+ *   b2c_world_contacts; (read *count); b2c_world_scene; [b2c_world_warm]; b2c_ncp_setup /
+ *   _color / _sweeps; [b2c_world_store]; b2c_world_integrate(state->v)
+ * with the NCP scene's pa / pb the world's contact arrays.  Kinematic bodies (kin = 1) have zero
+ * inverse mass and move with their prescribed velocity vkin.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct b2c_world {
+    int32_t n;                 /* bodies */
+    int32_t max_contacts;
+    double *x, *q, *v, *w;     /* (n,3), (n,4) (x, y, z, w), (n,3), (n,3): the state */
+    const double *half;        /* (n,3) half extents */
+    const double *mass;        /* (n) */
+    const double *Ib;          /* (n,3) principal moments m/12 (h_y^2 + h_z^2, ...) (Box.Ib, :1105-1109) */
+    const int32_t *kin;        /* (n) 1: kinematic */
+    const double *vkin;        /* (n,6) velocity of the kinematic bodies */
+    const double *body_mu;     /* (n) friction per body (pair: sqrt(mu_a mu_b), ground: mu_a), or NULL */
+    double mu;                 /* friction of every contact when body_mu is NULL */
+    float *xc32;               /* (n,4) float32 centres for the broadphase (b2c_boxes.half float32 too) */
+    double *x4, *half4;        /* (n,4) scratch: padded centres and half extents */
+    double *slot_p;            /* (candidate cap x 8, 4) contact point | gap */
+    double *slot_n;            /* (candidate cap, 4) normal of the candidate's contacts */
+    int32_t *slot_f;           /* (candidate cap x 8) feature id */
+    int32_t *pa, *pb, *fid;    /* (max_contacts) bodies (pb -1: ground), feature id (< 256) */
+    int64_t *key;              /* (max_contacts) (pa (n + 1) + pb + 1) 256 + fid, ascending */
+    double *p, *nrm, *gap;     /* (max_contacts,3), (max_contacts,3) from pb to pa, (max_contacts) */
+    int32_t *attach;           /* (max_contacts) what the contact moves with: bits 0-1 the point (0 pa,
+                                  1 pb, 2 between a corner of each), bits 2-3 the normal (0 fixed,
+                                  1 pa, 2 pb) -- read by the adjoint */
+    int32_t *count;            /* (1) contacts of the last b2c_world_contacts (may exceed max_contacts) */
+    int64_t *warm_keys;        /* (max_contacts) warm store: keys of the last stored substep ... */
+    double *warm_lam;          /* (max_contacts,3) ... their impulses */
+    int32_t *warm_n;           /* (1) */
+} b2c_world;
+
+/* box_plane_contacts / box_box_contacts (:1148-1227) over the broadphase candidates of bx
+ * (b2c_box_candidates on the float32 mirror), in float64; contacts compacted in candidate order. */
+B2C_API int32_t b2c_world_contacts(b2c_world *wd, b2c_boxes *bx, b2c_header *hdr, b2c_stream s);
+/* build_scene (:1291-1330) for the first n_contacts contacts: Ja, Jb (n_c,3,6), bias (n_c,3),
+ * mu, feature (n_c); Minv (n,6,6) and v_free (n,6) of every body (gravity on when gravity != 0). */
+B2C_API int32_t b2c_world_scene(const b2c_world *wd, int32_t n_contacts, double dt, int32_t gravity, double *Ja,
+                                double *Jb, double *Minv, double *vfree, double *bias, double *mu, int32_t *feature,
+                                b2c_stream s);
+/* lam (n_c,3) <- the warm store's impulse of the same key, else 0 (BoxWorld._warm, :1381-1384). */
+B2C_API int32_t b2c_world_warm(const b2c_world *wd, int32_t n_contacts, double *lam, b2c_stream s);
+/* The transpose of b2c_world_warm between two substeps: lam_bar (n_c,3) of this substep's contacts
+ * += tlam of the entry of the table (tkeys ascending, *tn entries, on the device) with the same
+ * key -- the table holding the next substep's contact keys and the adjoint of its warm start. */
+B2C_API int32_t b2c_world_warm_adjoint(const b2c_world *wd, int32_t n_contacts, const int64_t *tkeys,
+                                       const double *tlam, const int32_t *tn, double *lam_bar, b2c_stream s);
+/* warm store <- the contacts' keys and lam (:1393-1394). */
+B2C_API int32_t b2c_world_store(b2c_world *wd, int32_t n_contacts, const double *lam, b2c_stream s);
+/* v, w <- v6 (n,6); x += v dt; q <- normalize(q + 0.5 (w, 0) q dt) (:1399-1406). */
+B2C_API int32_t b2c_world_integrate(b2c_world *wd, const double *v6, double dt, b2c_stream s);
+/* The adjoint of one substep, in two halves around b2c_ncp_adjoint_unrolled.  The world holds the
+ * state before the substep, the NCP scene and state its recorded solve (V6 = the solved
+ * velocities).  begin: from the adjoints of the substep's result (xb_out (n,3), qb_out (n,4),
+ * vb_out, wb_out (n,3)) the integration's reverse into xb_in, qb_in (partial), Vb = vfree_bar
+ * (n,6) and lam_b (n_c,3) = J Minv Vb.  end (lam, V6: the solved impulses and velocities; Vb of
+ * begin; Ja_b, Jb_b (n_c,3,6) and Minv_b (n,6,6) of b2c_ncp_adjoint_unrolled): the bias through
+ * the gaps, the Jacobian blocks through the lever arms, the contact point and frame (the normal
+ * turning with its body, attach), the world inertias, and mu_c = sqrt(mu_a mu_b) onto the bodies
+ * -- summed in int64 fixed point (acc: n x 8 int64, zero on entry and on return) -- giving xb, qb
+ * (completed), vb, wb of the state before the substep, and mub_body (n, accumulated; may be
+ * NULL).  No counterpart in the reference. */
+B2C_API int32_t b2c_world_adj_begin(const b2c_world *wd, const b2c_ncp_scene *sc, const double *V6, double h,
+                                    const double *xb_out, const double *qb_out, const double *vb_out,
+                                    const double *wb_out, double *xb_in, double *qb_in, double *Vb, double *vfree_b,
+                                    double *lam_b, b2c_stream s);
+B2C_API int32_t b2c_world_adj_end(const b2c_world *wd, const b2c_ncp_scene *sc, const double *lam, const double *V6,
+                                  const double *Vb, double h, const double *bias_b, const double *mu_b,
+                                  const double *vfree_b, const double *Ja_b, const double *Jb_b, const double *Minv_b,
+                                  int64_t *acc, double *xb, double *qb, double *vb, double *wb, double *mub_body,
+                                  b2c_stream s);
 
 /* ---------------------------------------------------------------------------------------------
  * Batched exact-cone NCP in Delassus form and its implicit adjoint (the reference's batched
