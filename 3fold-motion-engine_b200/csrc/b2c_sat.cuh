@@ -69,10 +69,13 @@ __device__ inline void dface(d3 half, d3 x, const dR &R, int axis, double sgn, d
     poly[2] = dsub(dsub(c, u), v);
     poly[3] = dsub(dadd(c, u), v);
 }
-// _clip, ncp_gpu.py:1129-1145: Sutherland-Hodgman against |(p - c).ax| <= ha; poly holds 16
-__device__ inline int dclip(d3 *poly, int n, d3 c, d3 ax, double ha)
+// _clip, ncp_gpu.py:1129-1145: Sutherland-Hodgman against |(p - c).ax| <= ha; poly holds 16.
+// planes (optional): per vertex, the bit set of the three planes it lies on; a vertex made on
+// the side s of this axis lies on the two planes its edge's ends share and on plane code0 + si.
+__device__ inline int dclip(d3 *poly, int n, d3 c, d3 ax, double ha, int *planes = nullptr, int code0 = 0)
 {
     d3 out[16];
+    int pout[16];
     for (int si = 0; si < 2; ++si) {
         const double s = si == 0 ? 1.0 : -1.0;
         int m = 0;
@@ -80,10 +83,19 @@ __device__ inline int dclip(d3 *poly, int n, d3 c, d3 ax, double ha)
             const d3 p = poly[i], q = poly[(i + 1) % n];
             const double dp = s * ddot(dsub(p, c), ax) - ha;
             const double dq = s * ddot(dsub(q, c), ax) - ha;
-            if (dp <= 0 && m < 16) out[m++] = p;
-            if (dp * dq < 0 && m < 16) out[m++] = dadd(p, dscale(dsub(q, p), dp / (dp - dq)));
+            if (dp <= 0 && m < 16) {
+                if (planes) pout[m] = planes[i];
+                out[m++] = p;
+            }
+            if (dp * dq < 0 && m < 16) {
+                if (planes) pout[m] = (planes[i] & planes[(i + 1) % n]) | (1 << (code0 + si));
+                out[m++] = dadd(p, dscale(dsub(q, p), dp / (dp - dq)));
+            }
         }
-        for (int i = 0; i < m; ++i) poly[i] = out[i];
+        for (int i = 0; i < m; ++i) {
+            poly[i] = out[i];
+            if (planes) planes[i] = pout[i];
+        }
         n = m;
         if (n == 0) return 0;
     }
@@ -119,8 +131,12 @@ __device__ int box_plane(V4 hf, V4 xf, V4 qf, double margin, double4 *pts, int *
 }
 
 // box_box_contacts, ncp_gpu.py:1157-1227: normal from B to A, <= 4 points
-// attach (optional): what the contacts move with -- bits 0-1 the points (0: box A, 1: box B,
-// 2: halfway between a corner of each), bits 2-3 the normal (1: box A, 2: box B)
+// attach (optional, one per point): what the contacts move with -- bits 0-1 the points (0: box A,
+// 1: box B, 2: halfway between a corner of each), bits 2-3 the normal (1: box A, 2: box B); for a
+// face contact also the three planes the point lies on (bits 4-13, kAttachPlane*: the incident
+// box's faces 2 a + (sign < 0), the reference face's sides 6 + 2 (0: axis j, 1: axis k) +
+// (sign < 0)), the reference axis (bits 14-15) and bit 16 set when A is the reference box.
+constexpr int kAttachPlaneShift = 4, kAttachAxisShift = 14, kAttachRefA = 1 << 16;
 template <class V4>
 __device__ int box_box(V4 haf, V4 xaf, V4 qaf, V4 hbf, V4 xbf, V4 qbf, double margin, double4 *pts, d3 &nrm, int *fid,
                        int *attach = nullptr)
@@ -182,7 +198,7 @@ __device__ int box_box(V4 haf, V4 xaf, V4 qaf, V4 hbf, V4 xbf, V4 qbf, double ma
         pts[0] = make_double4(p.x, p.y, p.z, esp);
         nrm = dscale(eax, -1.0);
         fid[0] = 100 + eidx;
-        if (attach) *attach = 2;
+        if (attach) attach[0] = 2;
         return 1;
     }
     d3 rhalf, rx, ihalf, ix, nBA;
@@ -220,20 +236,27 @@ __device__ int box_box(V4 haf, V4 xaf, V4 qaf, V4 hbf, V4 xbf, V4 qbf, double ma
             }
         }
     d3 poly[16], in_n, in_c;
-    dface(ihalf, ix, iR, mmin / 2, (mmin % 2 == 0) ? 1.0 : -1.0, poly, in_n, in_c);
+    const int ia = mmin / 2, isg = mmin % 2;
+    dface(ihalf, ix, iR, ia, isg == 0 ? 1.0 : -1.0, poly, in_n, in_c);
+    // the incident face's corners c +-u +-v (dface) lie on the face and on two of its sides
+    const int ja = (ia + 1) % 3, ka = (ia + 2) % 3, fbit = 1 << (2 * ia + isg);
+    int planes[16] = {fbit | (1 << (2 * ja)) | (1 << (2 * ka)), fbit | (1 << (2 * ja + 1)) | (1 << (2 * ka)),
+                      fbit | (1 << (2 * ja + 1)) | (1 << (2 * ka + 1)), fbit | (1 << (2 * ja)) | (1 << (2 * ka + 1))};
     const int j = (raxis + 1) % 3, k = (raxis + 2) % 3;
-    int np_ = dclip(poly, 4, rc, rR.col[j], dget(rhalf, j));
+    int np_ = dclip(poly, 4, rc, rR.col[j], dget(rhalf, j), planes, 6);
     if (!np_) return 0;
-    np_ = dclip(poly, np_, rc, rR.col[k], dget(rhalf, k));
+    np_ = dclip(poly, np_, rc, rR.col[k], dget(rhalf, k), planes, 8);
     if (!np_) return 0;
     double gs[16];
     d3 ps[16];
+    int pl[16];
     int m = 0;
     for (int i = 0; i < np_; ++i) {
         const double g = ddot(dsub(poly[i], rc), rn);
         if (g < margin) {
             gs[m] = g;
             ps[m] = poly[i];
+            pl[m] = planes[i];
             ++m;
         }
     }
@@ -242,14 +265,17 @@ __device__ int box_box(V4 haf, V4 xaf, V4 qaf, V4 hbf, V4 xbf, V4 qbf, double ma
         for (int a = 1; a < m; ++a) {
             const double gv = gs[a];
             const d3 pv = ps[a];
+            const int lv = pl[a];
             int b = a - 1;
             while (b >= 0 && gs[b] > gv) {
                 gs[b + 1] = gs[b];
                 ps[b + 1] = ps[b];
+                pl[b + 1] = pl[b];
                 --b;
             }
             gs[b + 1] = gv;
             ps[b + 1] = pv;
+            pl[b + 1] = lv;
         }
         m = 4;
     }
@@ -257,9 +283,12 @@ __device__ int box_box(V4 haf, V4 xaf, V4 qaf, V4 hbf, V4 xbf, V4 qbf, double ma
     for (int i = 0; i < m; ++i) {
         pts[i] = make_double4(ps[i].x, ps[i].y, ps[i].z, gs[i]);
         fid[i] = base + i;
+        // points on the incident box, the normal on the reference box
+        if (attach)
+            attach[i] = (refA ? (1 | (1 << 2)) : (0 | (2 << 2))) | (pl[i] << kAttachPlaneShift) |
+                        (raxis << kAttachAxisShift) | (refA ? kAttachRefA : 0);
     }
     nrm = nBA;
-    if (attach) *attach = refA ? (1 | (1 << 2)) : (0 | (2 << 2));  // points on the incident box
     return m;
 }
 

@@ -550,11 +550,181 @@ int setup(const b2c_ncp_scene *sc, b2c_ncp_state *st, int warm, cudaStream_t s)
     return check_launch("ncp_setup");
 }
 
+// The same colouring over a cooperative grid: every Jones-Plassmann round is three grid phases
+// (reset the claims; claim; win) with the arrival-counter barrier between them, so a round costs
+// a few microseconds however many contacts there are (the one-CTA form walks all of them with
+// 1024 threads, once per round).  Jones-Plassmann is local -- a contact takes colour r when it
+// holds the smallest key at each of its dynamic bodies among the contacts still uncoloured -- so
+// the colours are those of k_color exactly; only the order of the contacts inside a colour
+// (which thread sweeps which contact) differs, and the sweeps do not depend on it.  Scratch words
+// of the barrier buffer: [8], [9] the uncoloured counts of alternate rounds, [10] the cache
+// mismatch flag (all zero at launch).
+constexpr int kColorGridThreads = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(kColorGridThreads)
+    k_color_grid(int nc, int nb, const int *__restrict__ pa, const int *__restrict__ pb, const int *__restrict__ feat,
+                 const T *__restrict__ Minv, const int *__restrict__ dyn, b2c_ncp_state st, int use_cache,
+                 int max_colors, long long timeout_ns)
+{
+    __shared__ int s_cnt;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const bool lead = gid == 0;
+    int *S = st.stats;
+    unsigned int *bar = st.barrier;
+    unsigned int epoch = 0;
+    T *cm = reinterpret_cast<T *>(st.cache_minv);
+    auto sync = [&]() -> bool {
+        ++epoch;
+        grid_arrive(bar);
+        return grid_wait(bar, epoch, timeout_ns, S + kError, kErrBarrier);
+    };
+    auto key_of = [&](int c) -> unsigned long long {
+        return mix64(((unsigned long long)(pa[c] + 1) * (unsigned long long)(nb + 1) + (unsigned long long)(pb[c] + 1)) *
+                         1048576ull +
+                     (unsigned long long)(unsigned)feat[c]);
+    };
+    if (use_cache && S[kCacheValid] == 1 && S[kCachedC] == nc) {
+        int mism = 0;
+        for (int c = gid; c < nc; c += nth)
+            mism |= (pa[c] != st.cache_pa[c]) | (pb[c] != st.cache_pb[c]) | (feat[c] != st.cache_feat[c]);
+        for (int i = gid; i < nb; i += nth)
+            mism |= (Minv[36 * (size_t)i] != cm[4 * (size_t)i]) | (Minv[36 * (size_t)i + 7] != cm[4 * (size_t)i + 1]) |
+                    (Minv[36 * (size_t)i + 14] != cm[4 * (size_t)i + 2]) | ((T)dyn[i] != cm[4 * (size_t)i + 3]);
+        if (mism) atomicOr(bar + 10, 1u);
+        if (!sync()) return;
+        if (__ldcg(bar + 10) == 0u) {
+            if (lead) {
+                S[kCacheHit] = 1;
+                S[kHits] += 1;
+            }
+            return;
+        }
+    }
+    for (int c = gid; c < nc; c += nth) st.col[c] = -1;
+    unsigned long long *claim = reinterpret_cast<unsigned long long *>(st.claim);
+    int r = 0;
+    bool done = nc == 0;
+    for (; !done && r <= nc && r < max_colors; ++r) {
+        for (int i = gid; i < nb; i += nth) claim[i] = ~0ull;
+        if (!sync()) return;
+        if (lead) bar[8 + ((r + 1) & 1)] = 0u;  // every CTA has read the previous round's count
+        for (int c = gid; c < nc; c += nth) {
+            if (st.col[c] >= 0) continue;
+            const unsigned long long k = key_of(c);
+            if (pa[c] >= 0 && dyn[pa[c]]) atomicMin(claim + pa[c], k);
+            if (pb[c] >= 0 && dyn[pb[c]]) atomicMin(claim + pb[c], k);
+        }
+        if (!sync()) return;
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        int left = 0;
+        for (int c = gid; c < nc; c += nth) {
+            if (st.col[c] >= 0) continue;
+            const unsigned long long k = key_of(c);
+            bool ok = true;
+            if (pa[c] >= 0 && dyn[pa[c]] && __ldcg(claim + pa[c]) != k) ok = false;
+            if (pb[c] >= 0 && dyn[pb[c]] && __ldcg(claim + pb[c]) != k) ok = false;
+            if (ok) st.col[c] = r;
+            else ++left;
+        }
+        if (left) atomicAdd(&s_cnt, left);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_cnt) atomicAdd(bar + 8 + (r & 1), (unsigned)s_cnt);
+        if (!sync()) return;
+        done = __ldcg(bar + 8 + (r & 1)) == 0u;
+    }
+    const int ncol = done ? (nc > 0 ? r : 0) : r;
+    if (!done || ncol > max_colors || ncol > kMaxColors) {
+        if (lead) {
+            S[kError] |= done ? kErrColorOverflow : kErrColorTimeout;
+            S[kNColors] = 0;
+            S[kCacheValid] = 0;
+            S[kRounds] = r;
+        }
+        return;
+    }
+    // counts per colour, then their exclusive scan (one thread), then the scatter with the
+    // counts as cursors (they end where they started)
+    for (int k = gid; k < ncol; k += nth) st.ccount[k] = 0;
+    if (!sync()) return;
+    for (int c = gid; c < nc; c += nth) atomicAdd(st.ccount + st.col[c], 1);
+    if (!sync()) return;
+    if (lead) {
+        int acc = 0;
+        for (int k = 0; k < ncol; ++k) {
+            st.cstart[k] = acc;
+            acc += __ldcg(st.ccount + k);
+            st.ccount[k] = 0;
+        }
+    }
+    if (!sync()) return;
+    for (int c = gid; c < nc; c += nth) {
+        const int k = st.col[c];
+        st.order[__ldcg(st.cstart + k) + atomicAdd(st.ccount + k, 1)] = c;
+    }
+    if (use_cache) {
+        for (int c = gid; c < nc; c += nth) {
+            st.cache_pa[c] = pa[c];
+            st.cache_pb[c] = pb[c];
+            st.cache_feat[c] = feat[c];
+        }
+        for (int i = gid; i < nb; i += nth) {
+            cm[4 * (size_t)i] = Minv[36 * (size_t)i];
+            cm[4 * (size_t)i + 1] = Minv[36 * (size_t)i + 7];
+            cm[4 * (size_t)i + 2] = Minv[36 * (size_t)i + 14];
+            cm[4 * (size_t)i + 3] = (T)dyn[i];
+        }
+    }
+    if (lead) {
+        S[kNColors] = ncol;
+        S[kRounds] = r;
+        S[kCacheHit] = 0;
+        S[kCacheValid] = use_cache ? 1 : 0;
+        S[kCachedC] = nc;
+        S[kMisses] += 1;
+    }
+}
+
 template <typename T>
 int color(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, cudaStream_t s)
 {
+    const int maxc = std::min(st->max_colors, kMaxColors);
+    int mode = p->solve_blocks;
+    if (mode == 0) mode = sc->n_c <= 16384 ? 1 : 2;
+    if (mode > 1) {  // a cooperative grid of one CTA per SM (fewer arrivals per barrier)
+        static int nblocks = -1;
+        if (nblocks < 0) {
+            int dev = 0, sms = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_color_grid<T>, kColorGridThreads, 0);
+            nblocks = per > 0 ? std::min(kBarrierMaxCTAs, sms) : 1;
+        }
+        if (nblocks > 1) {
+            cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t) * kBarrierWords, s);
+            const long long tmo = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nblocks);
+            cfg.blockDim = dim3(kColorGridThreads);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, k_color_grid<T>, sc->n_c, sc->n_b, sc->pa, sc->pb,
+                                                     sc->feature, (const T *)sc->Minv, st->dyn, *st, p->color_cache,
+                                                     maxc, tmo);
+            if (e != cudaSuccess) {
+                set_error("ncp_color: cooperative launch of %d CTAs: %s", nblocks, cudaGetErrorString(e));
+                return B2C_ECUDA;
+            }
+            return check_launch("ncp_color_grid");
+        }
+    }
     k_color<T><<<1, kColorThreads, 0, s>>>(sc->n_c, sc->n_b, sc->pa, sc->pb, sc->feature, (const T *)sc->Minv, st->dyn,
-                                           *st, p->color_cache, std::min(st->max_colors, kMaxColors));
+                                           *st, p->color_cache, maxc);
     return check_launch("ncp_color");
 }
 
@@ -718,6 +888,12 @@ __device__ __forceinline__ void add_j_minv(const double *J, const double *M, con
     }
 }
 
+// The de Saxce term mu |u_t| has a kink at u_t = 0, where a sticking contact sits: its slip
+// speed there is the rounding of the fixed-point velocity sums (1e-10 m/s), whose direction says
+// nothing.  Below this speed the adjoints take the term's derivative in u_t as zero (the stick
+// rows of the implicit-function system, ncp_ref.py:_active_system, carry no such term either).
+constexpr double kStickSpeed = 1e-8;
+
 // transposed derivative of proj_K (the branches of proj) at z, applied to g: zb, and mub
 __device__ __forceinline__ void proj_adjoint(const double z[3], double mu, const double g[3], double zb[3],
                                              double &mub)
@@ -786,7 +962,7 @@ __device__ void adj_contact(const AdjArgs &a, int c)
     ub[2] = -rho * zb[2];
     if (a.desaxce) {
         mub += -rho * ut * zb[0];
-        if (ut > 0.0) {
+        if (ut > kStickSpeed) {
             ub[1] += -rho * mu * (u[1] / ut) * zb[0];
             ub[2] += -rho * mu * (u[2] / ut) * zb[0];
         }
@@ -878,7 +1054,7 @@ __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
     double rb = -(zb[0] * s0 + zb[1] * u[1] + zb[2] * u[2]);
     if (a.desaxce) {
         mub += -rho * ut * zb[0];
-        if (ut > 0.0) {
+        if (ut > kStickSpeed) {
             ub[1] += -rho * mu * (u[1] / ut) * zb[0];
             ub[2] += -rho * mu * (u[2] / ut) * zb[0];
         }
@@ -933,10 +1109,59 @@ __device__ bool eigvec_max3(const double W[3][3], double lm, double e[3])
     return true;
 }
 
+// The derivative of rho_c = 1 / lambda_max(W_c) takes the projector P onto the eigenspace of
+// the largest eigenvalue lm, divided by its dimension k: d lm = tr(P dW) / k.  For a simple
+// eigenvalue (k = 1) that is the derivative; for a repeated one -- every corner contact of a
+// cube on the ground, whose inertia is isotropic, has lm twice -- lm is not differentiable and
+// tr(P dW) / k, the derivative of the mean of the k top eigenvalues, is what a central
+// difference measures.  Eigenvalues within 1e-6 lm of lm count as repeated.
+__device__ void top_projector(const double W[3][3], double lm, double P[3][3])
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) P[i][j] = 0.0;
+    const double c2 = W[0][0] + W[1][1] + W[2][2];
+    const double c1 = (W[0][0] * W[1][1] - W[0][1] * W[1][0]) + (W[0][0] * W[2][2] - W[0][2] * W[2][0]) +
+                      (W[1][1] * W[2][2] - W[1][2] * W[2][1]);
+    const double sm = c2 - lm, pr = c1 - lm * sm;  // the other two: sum and product
+    const double disc = sqrt(fmax(sm * sm - 4.0 * pr, 0.0));
+    const double l2 = 0.5 * (sm + disc), l3 = 0.5 * (sm - disc);
+    const double tol = 1e-6 * lm;
+    if (lm - l3 <= tol) {
+        for (int i = 0; i < 3; ++i) P[i][i] = 1.0 / 3.0;
+        return;
+    }
+    if (lm - l2 <= tol) {  // W - lm I ~ (l3 - lm) e3 e3^T: its largest row is along e3
+        int best = 0;
+        double bn = -1.0;
+        for (int r = 0; r < 3; ++r) {
+            double nn = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double x = W[r][k] - (r == k ? lm : 0.0);
+                nn += x * x;
+            }
+            if (nn > bn) {
+                bn = nn;
+                best = r;
+            }
+        }
+        double e3[3];
+        const double inv = 1.0 / sqrt(bn);
+        for (int k = 0; k < 3; ++k) e3[k] = (W[best][k] - (best == k ? lm : 0.0)) * inv;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) P[i][j] = 0.5 * ((i == j ? 1.0 : 0.0) - e3[i] * e3[j]);
+        return;
+    }
+    double e[3];
+    if (!eigvec_max3(W, lm, e)) return;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) P[i][j] = e[i] * e[j];
+}
+
 // The start of the recorded sweeps, v = v_free + Minv sum_c J_c^T lo_c (setup, with lo the
 // warm start) and the step sizes rho_c = 1 / lambda_max(W_c), W_c = sum_sides J Minv J^T
 // (k_rho): gl[c] += J Minv vbar (the warm start's adjoint), the blocks' and Minv's adjoints,
-// and rho_b through d lambda_max = e^T dW e.  Run colour by colour like the sweeps.
+// and rho_b through Wbar = -rho^2 rho_b P / k (top_projector).  Run colour by colour like the
+// sweeps.
 __device__ void adj_start_recorded(const AdjArgs &a, int c)
 {
     const int A = a.pa[c], B = a.pb[c];
@@ -944,46 +1169,55 @@ __device__ void adj_start_recorded(const AdjArgs &a, int c)
     const double lo[3] = {tr[0], tr[1], tr[2]};
     const double rho = a.rho[c];
     const double rb = a.rho_b[c];
-    double lmb = 0.0, e[3] = {0.0, 0.0, 0.0};
+    double Wb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (rb != 0.0 && rho > 0.0) {
         double W[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         if (A >= 0) add_jmjt(W, a.Ja + 18 * (size_t)c, a.Minv + 36 * (size_t)A);
         if (B >= 0) add_jmjt(W, a.Jb + 18 * (size_t)c, a.Minv + 36 * (size_t)B);
-        if (eigvec_max3(W, eigmax3(W), e)) lmb = -rho * rho * rb;  // rho = 1 / lambda_max
+        double P[3][3];
+        top_projector(W, eigmax3(W), P);
+        const double lmb = -rho * rho * rb;  // rho = 1 / lambda_max
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Wb[i][j] = lmb * P[i][j];
     }
     double jm[3] = {0.0, 0.0, 0.0};
     for (int side = 0; side < 2; ++side) {
         const int b = side == 0 ? A : B;
         if (b < 0 || !a.dyn[b]) continue;
         const double *M = a.Minv + 36 * (size_t)b, *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
-        double w[6], m[6], jt[6], je[6], jme[6];
+        double w[6], m[6], jt[6];
         for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
         for (int k = 0; k < 6; ++k) {
             double sacc = 0.0;
             for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
             m[k] = sacc;
             jt[k] = (J[k] * lo[0] + J[6 + k] * lo[1]) + J[12 + k] * lo[2];
-            je[k] = (J[k] * e[0] + J[6 + k] * e[1]) + J[12 + k] * e[2];
-        }
-        for (int k = 0; k < 6; ++k) {  // Minv J^T e
-            double sacc = 0.0;
-            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * je[j];
-            jme[k] = sacc;
         }
         for (int r = 0; r < 3; ++r) {
             double sacc = 0.0;
             for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
             jm[r] += sacc;
         }
+        // WJ = Wbar J (3x6), WJM = Wbar J Minv (3x6)
+        double WJ[3][6], WJM[3][6];
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 6; ++k) WJ[r][k] = (Wb[r][0] * J[k] + Wb[r][1] * J[6 + k]) + Wb[r][2] * J[12 + k];
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 6; ++k) {
+                double sacc = 0.0;
+                for (int j = 0; j < 6; ++j) sacc += WJ[r][j] * M[j * 6 + k];
+                WJM[r][k] = sacc;
+            }
         double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
         for (int r = 0; r < 3; ++r)
             for (int k = 0; k < 6; ++k)
-                __stcg(Jbar + 6 * r + k,
-                       __ldcg(Jbar + 6 * r + k) + (lo[r] * m[k] + 2.0 * lmb * e[r] * jme[k]));
+                __stcg(Jbar + 6 * r + k, __ldcg(Jbar + 6 * r + k) + (lo[r] * m[k] + 2.0 * WJM[r][k]));
         double *Mb = a.Minv_b + 36 * (size_t)b;
         for (int i = 0; i < 6; ++i)
-            for (int k = 0; k < 6; ++k)
-                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (w[i] * jt[k] + lmb * je[i] * je[k]));
+            for (int k = 0; k < 6; ++k) {
+                const double jwj = (J[i] * WJ[0][k] + J[6 + i] * WJ[1][k]) + J[12 + i] * WJ[2][k];
+                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (w[i] * jt[k] + jwj));
+            }
     }
     for (int k = 0; k < 3; ++k) a.gl[3 * (size_t)c + k] += jm[k];
 }

@@ -63,17 +63,17 @@ __global__ void k_narrow(const int *__restrict__ cand_offset, int n, int cap, co
     for (int c = tid; c < nc; c += gridDim.x * blockDim.x) {
         const int a = ca[c], b = cb[c];
         double4 pts[kSlots];
-        int fid[kSlots];
+        int fid[kSlots], att[kSlots] = {0, 0, 0, 0, 0, 0, 0, 0};  // ground: corners of box a, fixed normal
         d3 nrm = D3(0.0, 0.0, 1.0);
-        int m, att = 0;  // ground: the corners move with box a, the normal is fixed
+        int m;
         if (b < 0) m = box_plane(ld4d(half4, a), ld4d(x4, a), ld4d(q, a), margin, pts, fid);
         else m = box_box(ld4d(half4, a), ld4d(x4, a), ld4d(q, a), ld4d(half4, b), ld4d(x4, b), ld4d(q, b), margin, pts,
-                         nrm, fid, &att);
+                         nrm, fid, att);
         for (int k = 0; k < m; ++k) {
             reinterpret_cast<double4 *>(slot_p)[c * kSlots + k] = pts[k];
-            slot_f[c * kSlots + k] = fid[k];
+            slot_f[c * kSlots + k] = fid[k] | (att[k] << 8);  // fid < 256
         }
-        reinterpret_cast<double4 *>(slot_n)[c] = make_double4(nrm.x, nrm.y, nrm.z, (double)att);
+        reinterpret_cast<double4 *>(slot_n)[c] = make_double4(nrm.x, nrm.y, nrm.z, 0.0);
         cont_count[c] = m;
     }
 }
@@ -96,7 +96,7 @@ __global__ void k_emit(const int *__restrict__ cand_offset, int n, int cap, int 
             const int d = o + k;
             if (d >= max_contacts) break;
             const double4 ps = reinterpret_cast<const double4 *>(slot_p)[c * kSlots + k];
-            const int f = slot_f[c * kSlots + k];
+            const int f = slot_f[c * kSlots + k] & 255, at = slot_f[c * kSlots + k] >> 8;
             pa[d] = a;
             pb[d] = b;
             fid[d] = f;
@@ -104,7 +104,7 @@ __global__ void k_emit(const int *__restrict__ cand_offset, int n, int cap, int 
             st3d(p, d, D3(ps.x, ps.y, ps.z));
             st3d(nrm, d, D3(n4.x, n4.y, n4.z));
             gap[d] = ps.w;
-            attach[d] = (int)n4.w;
+            attach[d] = at;
         }
     }
 }
@@ -393,6 +393,19 @@ __global__ void k_adj_lambda(int nc, const int *__restrict__ pa, const int *__re
     for (int r = 0; r < 3; ++r) lb[3 * (size_t)c + r] = out[r];
 }
 
+// the three planes a face contact's point lies on (box_box's attach bits), or 0
+__device__ __forceinline__ int attach_planes(int att)
+{
+    const int m = (att >> kAttachPlaneShift) & 0x3FF;
+    return __popc(m) == 3 ? m : 0;
+}
+
+// d bias / d gap of build_scene's normal row
+__device__ __forceinline__ double dbias_dgap(double g, double h)
+{
+    return g > 0.0 ? 1.0 / h : (-g - kSlop > 0.0 ? kBeta / h : 0.0);
+}
+
 __device__ __forceinline__ void acc_add(long long *acc, double x)
 {
     atomicAdd(reinterpret_cast<unsigned long long *>(acc), (unsigned long long)llround(x * kAdjScale));
@@ -400,7 +413,7 @@ __device__ __forceinline__ void acc_add(long long *acc, double x)
 
 // acc per body: 10 int64 -- xb (3), thb (3), mub (1), pad
 __global__ void k_adj_contacts(int nc, const int *__restrict__ pa, const int *__restrict__ pb,
-                               const int *__restrict__ kin, const double *__restrict__ p,
+                               const int *__restrict__ kin, const int *__restrict__ attach, const double *__restrict__ p,
                                const double *__restrict__ nrm, const double *__restrict__ gap,
                                const double *__restrict__ x, const double *__restrict__ body_mu,
                                const double *__restrict__ mu_c, const double *__restrict__ bias_b,
@@ -408,9 +421,8 @@ __global__ void k_adj_contacts(int nc, const int *__restrict__ pa, const int *__
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
-    const double g = gap[c];
-    const double dbias = g > 0.0 ? 1.0 / h : (-g - kSlop > 0.0 ? kBeta / h : 0.0);
-    const double gb = bias_b[3 * (size_t)c] * dbias;
+    // a face contact's gap moves with its point: k_adj_geom takes it
+    const double gb = attach_planes(attach[c]) ? 0.0 : bias_b[3 * (size_t)c] * dbias_dgap(gap[c], h);
     const d3 n = ld3d(nrm, c), pc = ld3d(p, c);
     for (int side = 0; side < 2; ++side) {
         const int b = side == 0 ? pa[c] : pb[c];
@@ -464,7 +476,9 @@ __device__ __forceinline__ d3 basis_adjoint(d3 n, d3 h0, d3 h1, d3 h2)
 __global__ void k_adj_geom(int nc, const int *__restrict__ pa, const int *__restrict__ pb,
                            const int *__restrict__ kin, const int *__restrict__ attach,
                            const double *__restrict__ p, const double *__restrict__ nrm,
-                           const double *__restrict__ x, const double *__restrict__ Ja,
+                           const double *__restrict__ x, const double *__restrict__ q,
+                           const double *__restrict__ gap, const double *__restrict__ bias_b, double h,
+                           const double *__restrict__ Ja,
                            const double *__restrict__ Minv, const double *__restrict__ lam,
                            const double *__restrict__ Vb, const double *__restrict__ Ja_b,
                            const double *__restrict__ Jb_b, long long *__restrict__ acc)
@@ -504,12 +518,58 @@ __global__ void k_adj_geom(int nc, const int *__restrict__ pa, const int *__rest
         }
     }
     d3 xg[2] = {dscale(rb[0], -1.0), dscale(rb[1], -1.0)}, thg[2] = {D3(0, 0, 0), D3(0, 0, 0)};
-    const d3 pbar = dadd(rb[0], rb[1]);
-    for (int t = 0; t < 2; ++t) {
-        const double wgt = ppt == 2 ? 0.5 : ((ppt == t) ? 1.0 : 0.0);
-        if (wgt == 0.0 || body[t] < 0) continue;
-        thg[t] = dadd(thg[t], dscale(dcross(r[t], pbar), wgt));
-        xg[t] = dadd(xg[t], dscale(pbar, wgt));
+    d3 pbar = dadd(rb[0], rb[1]);
+    const int pm = attach_planes(att);
+    bool planes = false;
+    if (pm && body[1] >= 0) {
+        // A face contact: p lies on three planes, each fixed to the incident (I) or the reference
+        // (R) box, so n_k . dp = n_k . (dx_X + dth_X x r_X) for the plane's box X; with the
+        // reciprocal basis of the normals, dp's adjoint pbar splits into y_k n_k per plane.  The
+        // gap (p - c) . rn (c, rn: the reference face's centre and normal, rn = -n when A is the
+        // reference) moves with p and with the reference box.
+        const int sR = (att & kAttachRefA) ? 0 : 1, sI = 1 - sR;
+        const int raxis = (att >> kAttachAxisShift) & 3, j = (raxis + 1) % 3, k = (raxis + 2) % 3;
+        const d3 rn = sR == 0 ? dscale(n, -1.0) : n;
+        const double gb = bias_b[3 * (size_t)c] * dbias_dgap(gap[c], h);
+        pbar = dadd(pbar, dscale(rn, gb));
+        xg[sR] = dsub(xg[sR], dscale(rn, gb));
+        thg[sR] = dsub(thg[sR], dscale(dcross(r[sR], rn), gb));
+        const dR RI = dquat_R(ld4d(q, body[sI])), RR = dquat_R(ld4d(q, body[sR]));
+        d3 nk[3];
+        int own[3], m = 0;
+        for (int b = 0; b < 10 && m < 3; ++b) {
+            if (!((pm >> b) & 1)) continue;
+            nk[m] = b < 6 ? RI.col[b >> 1] : RR.col[b < 8 ? j : k];
+            own[m] = b < 6 ? sI : sR;
+            ++m;
+        }
+        const d3 c12 = dcross(nk[1], nk[2]), c20 = dcross(nk[2], nk[0]), c01 = dcross(nk[0], nk[1]);
+        const double det = ddot(nk[0], c12);
+        if (fabs(det) > 1e-9) {
+            planes = true;
+            const double y[3] = {ddot(pbar, c12) / det, ddot(pbar, c20) / det, ddot(pbar, c01) / det};
+            for (int t = 0; t < 3; ++t) {
+                const int X = own[t];
+                xg[X] = dadd(xg[X], dscale(nk[t], y[t]));
+                thg[X] = dadd(thg[X], dscale(dcross(r[X], nk[t]), y[t]));
+            }
+        }
+    }
+    if (!planes) {
+        if (pm) {  // degenerate planes: the point moves with the incident box, the gap as in k_adj_contacts
+            const double gb = bias_b[3 * (size_t)c] * dbias_dgap(gap[c], h);
+            for (int s = 0; s < 2; ++s) {
+                const double sg = s == 0 ? gb : -gb;
+                xg[s] = dadd(xg[s], dscale(n, sg));
+                thg[s] = dadd(thg[s], dscale(dcross(r[s], n), sg));
+            }
+        }
+        for (int t = 0; t < 2; ++t) {
+            const double wgt = ppt == 2 ? 0.5 : ((ppt == t) ? 1.0 : 0.0);
+            if (wgt == 0.0 || body[t] < 0) continue;
+            thg[t] = dadd(thg[t], dscale(dcross(r[t], pbar), wgt));
+            xg[t] = dadd(xg[t], dscale(pbar, wgt));
+        }
     }
     if (pn == 1 || pn == 2) {
         const d3 nb = basis_adjoint(n, Db[0], Db[1], Db[2]);
@@ -743,12 +803,14 @@ extern "C" int32_t b2c_world_adj_end(const b2c_world *wd, const b2c_ncp_scene *s
     cudaStream_t s = stream_of(stream);
     long long *A = reinterpret_cast<long long *>(acc);
     if (sc->n_c > 0)
-        k_adj_contacts<<<blocks_for(sc->n_c), kThreads, 0, s>>>(sc->n_c, sc->pa, sc->pb, wd->kin, wd->p, wd->nrm,
+        k_adj_contacts<<<blocks_for(sc->n_c), kThreads, 0, s>>>(sc->n_c, sc->pa, sc->pb, wd->kin, wd->attach, wd->p,
+                                                                 wd->nrm,
                                                                  wd->gap, wd->x, wd->body_mu,
                                                                  (const double *)sc->mu, bias_b, mu_b, h, A);
     if (sc->n_c > 0)
         k_adj_geom<<<blocks_for(sc->n_c), kThreads, 0, s>>>(sc->n_c, sc->pa, sc->pb, wd->kin, wd->attach, wd->p,
-                                                             wd->nrm, wd->x, (const double *)sc->Ja,
+                                                             wd->nrm, wd->x, wd->q, wd->gap, bias_b, h,
+                                                             (const double *)sc->Ja,
                                                              (const double *)sc->Minv, lam, Vb, Ja_b, Jb_b, A);
     if (wd->n > 0)
         k_adj_finish<<<blocks_for(wd->n), kThreads, 0, s>>>(wd->n, wd->q, wd->kin, vfree_b, A, xb, qb, vb, wb,

@@ -390,6 +390,77 @@ class NCPSolverB200:
     def contact_velocity(self):
         return self.u[:self.C].double().cpu().numpy().copy()
 
+    # ---- derivatives (float64 scenes) ----
+    def _adj_buffers(self):
+        C, NB, dev = self.C, self.NB, self.dev
+        z = lambda *shape: torch.zeros(*shape, dtype=torch.float64, device=dev)
+        return dict(vscr=z(max(NB, 1), 6), vfree=z(max(NB, 1), 6), bias=z(max(C, 1), 3), mu=z(max(C, 1)))
+
+    def vjp_implicit(self, lam_bar: np.ndarray, iters: int) -> dict:
+        """The implicit-function derivative at the impulses of the last solve (b2c_ncp_adjoint):
+        for lam_bar (n_c, 3), the adjoints of v_free (n_b, 6), bias (n_c, 3) and mu (n_c) --
+        lam_bar^T dlam*/d(.) -- as `iters` reverse sweeps at lam*.  The solve should have
+        converged; the Jacobian blocks and Minv are held."""
+        if self.dtype != "float64":
+            raise ValueError("vjp_implicit: float64 solvers only")
+        C = self.C
+        params = self._params(None, True)
+        s = self._stream()
+        _lib.check(self.L.b2c_ncp_residual(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                           ctypes.byref(params), s), "b2c_ncp_residual")
+        b = self._adj_buffers()
+        gl = torch.from_numpy(np.ascontiguousarray(lam_bar, np.float64).reshape(C, 3)).to(self.dev)
+        _lib.check(self.L.b2c_ncp_adjoint(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                          ctypes.byref(params), int(iters), ctypes.c_void_p(_ptr(gl)),
+                                          ctypes.c_void_p(_ptr(b["vscr"])), ctypes.c_void_p(_ptr(b["vfree"])),
+                                          ctypes.c_void_p(_ptr(b["bias"])), ctypes.c_void_p(_ptr(b["mu"])), s),
+                   "b2c_ncp_adjoint")
+        self._check_stats()
+        return dict(vfree=b["vfree"][:self.NB].cpu().numpy(), bias=b["bias"][:C].cpu().numpy(),
+                    mu=b["mu"][:C].cpu().numpy())
+
+    def vjp_recorded(self, bs: BlockScene, lam_bar: np.ndarray, iters: int, warm: Optional[np.ndarray] = None) -> dict:
+        """The exact derivative of `iters` sweeps from `warm` (or from zero): the solve runs again
+        recording every contact update (b2c_ncp_sweeps_record), then in reverse
+        (b2c_ncp_adjoint_unrolled).  For lam_bar (n_c, 3) the adjoints of v_free, bias, mu, the
+        blocks Ja, Jb (n_c, 3, 6), Minv (n_b, 6, 6) and the warm start (lam0, n_c x 3).  Also
+        returns the impulses of the solve (lam)."""
+        if self.dtype != "float64":
+            raise ValueError("vjp_recorded: float64 solvers only")
+        self.upload(bs)
+        C, NB, dev = self.C, self.NB, self.dev
+        params = self._params(None, True)
+        s = self._stream()
+        if warm is not None:
+            self.lam[:C].copy_(torch.from_numpy(np.asarray(warm, np.float64).reshape(C, 3)).to(dev))
+        _lib.check(self.L.b2c_ncp_setup(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                        1 if warm is not None else 0, s), "b2c_ncp_setup")
+        self.stats[3] = 0
+        _lib.check(self.L.b2c_ncp_color(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                        ctypes.byref(params), s), "b2c_ncp_color")
+        trace = torch.empty(15 * int(iters) * max(C, 1), dtype=torch.float64, device=dev)
+        _lib.check(self.L.b2c_ncp_sweeps_record(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                                ctypes.byref(params), int(iters), ctypes.c_void_p(_ptr(trace)),
+                                                trace.numel(), s), "b2c_ncp_sweeps_record")
+        lam = self.lam[:C].cpu().numpy().copy()
+        b = self._adj_buffers()
+        z = lambda *shape: torch.zeros(*shape, dtype=torch.float64, device=dev)
+        Jab, Jbb, Mb = z(max(C, 1), 18), z(max(C, 1), 18), z(max(NB, 1), 36)
+        gl = torch.from_numpy(np.ascontiguousarray(lam_bar, np.float64).reshape(C, 3)).to(dev)
+        _lib.check(self.L.b2c_ncp_adjoint_unrolled(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
+                                                   ctypes.byref(params), int(iters), ctypes.c_void_p(_ptr(trace)),
+                                                   trace.numel(), ctypes.c_void_p(_ptr(gl)),
+                                                   ctypes.c_void_p(_ptr(b["vscr"])),
+                                                   ctypes.c_void_p(_ptr(b["vfree"])), ctypes.c_void_p(_ptr(b["bias"])),
+                                                   ctypes.c_void_p(_ptr(b["mu"])), ctypes.c_void_p(_ptr(Jab)),
+                                                   ctypes.c_void_p(_ptr(Jbb)), ctypes.c_void_p(_ptr(Mb)), s),
+                   "b2c_ncp_adjoint_unrolled")
+        self._check_stats()
+        return dict(lam=lam, vfree=b["vfree"][:NB].cpu().numpy(), bias=b["bias"][:C].cpu().numpy(),
+                    mu=b["mu"][:C].cpu().numpy(), Ja=Jab[:C].reshape(C, 3, 6).cpu().numpy(),
+                    Jb=Jbb[:C].reshape(C, 3, 6).cpu().numpy(), Minv=Mb[:NB].reshape(NB, 6, 6).cpu().numpy(),
+                    lam0=gl[:C].cpu().numpy())
+
 
 def solve_scene_gpu(bs: BlockScene, iters: int = 200, dtype: str = "float32", **kw) -> SolveResult:
     s = NCPSolverB200(bs.n_b, max(bs.n_c, 1), dtype=dtype, **kw)

@@ -107,12 +107,15 @@ class BoxRollout:
         self.adj_lam = f64(MC, 3)
         self.adj_n = torch.zeros(1, dtype=torch.int32, device=dev)
         self.trace = f64(1)
+        self.max_c = 0
 
-    def _trace(self, C):
-        need = 15 * self.world.iters * C
+    def _size_trace(self):
+        """The sweep record of one substep: 15 doubles per contact and sweep, sized once per
+        backward by the most contacts a substep of the forward had."""
+        need = 15 * self.world.iters * max(self.max_c, 1)
         if self.trace.numel() < need:
+            self.trace = None
             self.trace = torch.empty(need, dtype=torch.float64, device=self.world.dev)
-        return self.trace[:need]
 
     def _reset(self, v0, mu):
         w, n = self.world, self.world.n
@@ -130,12 +133,14 @@ class BoxRollout:
         self._reset(v0, mu)
         h = w.dt / max(1, w.substeps)
         self.checkpoints = []
+        self.max_c = 0
         for _ in range(int(steps) * max(1, w.substeps)):
             if checkpoint:
                 cp = _Checkpoint(w)
                 cp.save(w, self._buf)
                 self.checkpoints.append(cp)
             w._substep(h)
+            self.max_c = max(self.max_c, w.n_contacts)
         self.h = h
         return w.x[:w.n].clone()
 
@@ -156,6 +161,7 @@ class BoxRollout:
         params = s._params(None, True)
         h = self.h
         p = lambda t: ctypes.c_void_p(_ptr(t))
+        self._size_trace()
         for cp in reversed(self.checkpoints):
             cp.restore(w)
             C = w.contacts_device()
@@ -163,7 +169,7 @@ class BoxRollout:
             warm = False
             if C:
                 warm = w.warm_start and w._have_warm
-                trace = self._trace(C)
+                trace = self.trace[:15 * w.iters * C]
                 w.solve_device(C, w.iters, warm, trace=trace)
                 V6 = s.v
             else:
