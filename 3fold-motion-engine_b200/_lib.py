@@ -201,6 +201,7 @@ _SIGS = {
     "b2c_world_integrate": ([_P(World), c_void_p, _D, c_void_p], c_int32),
     "b2c_ncp_adjoint": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                          c_void_p, c_void_p], c_int32),
+    "b2c_ncp_trace_words": ([], c_int32),
     "b2c_ncp_sweeps_record": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, ctypes.c_int64,
                                c_void_p], c_int32),
     "b2c_ncp_adjoint_unrolled": ([_P(NcpScene), _P(NcpState), _P(NcpParams), c_int32, c_void_p, ctypes.c_int64,

@@ -286,7 +286,8 @@ class BoxContactEngine(_BeadEngineBase):
         E = int(np.sum(invM[pbi] > 0) + np.sum((pbj >= 0) & (invM[np.maximum(pbj, 0)] > 0)))
         per_vel = 20 * P + 100 * E + 64 * Ck
         per_pos = 20 * P + 100 * E + 52 * Ck
-        warm = per_pos if self.apply_warm else 0
+        # the row form applies the warm start in k_warm_gather_row, outside the solve launch
+        warm = per_pos if (self.apply_warm and not self.row_form) else 0
         return dict(pairs=P, kept=Ck, endpoints=E, colors=h["n_colors"],
                     bytes=warm + self.vit * per_vel + self.pit * per_pos)
 

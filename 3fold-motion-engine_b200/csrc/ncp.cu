@@ -279,9 +279,11 @@ struct SweepArgs {
 
 enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
-// A recorded update: the contact's impulse before it (3) and the velocities of its bodies a, b
-// (6 + 6; zero where there is no body)
-constexpr int kTraceWords = 15;
+// A recorded update: the contact's impulse before it [0, 3) and the velocities of its bodies a, b
+// [3, 9), [9, 15) (zero where there is no body), written by the sweeps; the reverse sweep adds
+// the update's adjoints: ub [15, 18), the impulse change dl [18, 21) and the adjoints of both
+// bodies' velocities after the update [21, 27), [27, 33).
+constexpr int kTraceWords = 33;
 
 // The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident) is
 // the arrival-counter barrier of b2c_barrier.cuh over a.bar[0] (cleared by the host before the
@@ -862,7 +864,7 @@ int residual(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p
 struct AdjArgs {
     int nc, nb, iters, desaxce;
     const double *Ja, *Jb, *Minv, *mu, *rho, *lam, *u;
-    const double *trace;  // null: every reverse sweep at the final iterate (lam, u); else the recorded sweeps
+    double *trace;  // null: every reverse sweep at the final iterate (lam, u); else the recorded sweeps
     const double *bias;
     const int *pa, *pb, *order, *cstart, *ccount, *dyn;
     double *gl, *vb, *vfree_b, *bias_b, *mu_b;
@@ -987,16 +989,21 @@ __device__ void adj_contact(const AdjArgs &a, int c)
 //   v_a += Minv_a Ja^T (l - lo),  v_b likewise,
 // with va, vb and lo read back from the trace.  On entry gl[c] is the adjoint of l and vb the
 // adjoint of the velocities after the update; on exit gl[c] is the adjoint of lo and vb that of
-// the velocities before it.  The blocks' adjoints collect ub (x) v (from u) and dl (x) Minv vbar
-// (from the velocity change), the bodies' Minv adjoints vbar (x) J^T dl, rho_b[c] the adjoint of
-// rho.  Within a colour each dynamic body belongs to one contact, so the per-body sums need no
-// atomics.
+// the velocities before it, and bias_b, mu_b, rho_b hold the update's share.  Only vb and gl
+// are on the path to the next update; what the blocks' and Minv's adjoints need (ub, the impulse
+// change dl, the velocity adjoints) goes back into the trace for adj_start_recorded.
 __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
 {
     const int A = a.pa[c], B = a.pb[c];
     const bool dA = A >= 0 && a.dyn[A], dB = B >= 0 && a.dyn[B];
-    const double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
+    double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
     const double *JA = a.Ja + 18 * (size_t)c, *JB = a.Jb + 18 * (size_t)c;
+    // the velocity adjoints first: their loads wait on the previous colour, the rest does not
+    double wA[6] = {0, 0, 0, 0, 0, 0}, wB[6] = {0, 0, 0, 0, 0, 0};
+    if (dA)
+        for (int k = 0; k < 6; ++k) wA[k] = __ldcg(a.vb + 6 * (size_t)A + k);
+    if (dB)
+        for (int k = 0; k < 6; ++k) wB[k] = __ldcg(a.vb + 6 * (size_t)B + k);
     double lo[3], va[6], vv[6];
     for (int k = 0; k < 3; ++k) lo[k] = tr[k];
     for (int k = 0; k < 6; ++k) {
@@ -1024,26 +1031,15 @@ __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
     const double z[3] = {lo[0] - rho * s0, lo[1] - rho * u[1], lo[2] - rho * u[2]};
     double l[3];
     proj(z, mu, l);
-    const double dl[3] = {l[0] - lo[0], l[1] - lo[1], l[2] - lo[2]};
-    // the adjoints of the velocities after the update, and Minv times them
-    double wA[6] = {0, 0, 0, 0, 0, 0}, wB[6] = {0, 0, 0, 0, 0, 0}, mA[6] = {0, 0, 0, 0, 0, 0},
-           mB[6] = {0, 0, 0, 0, 0, 0};
-    double jm[3] = {0.0, 0.0, 0.0};
+    double jm[3] = {0.0, 0.0, 0.0};  // J Minv vbar
     for (int side = 0; side < 2; ++side) {
         if (!(side == 0 ? dA : dB)) continue;
-        const int b = side == 0 ? A : B;
-        double *w = side == 0 ? wA : wB, *m = side == 0 ? mA : mB;
-        const double *M = a.Minv + 36 * (size_t)b, *J = side == 0 ? JA : JB;
-        for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
+        const double *w = side == 0 ? wA : wB;
+        const double *M = a.Minv + 36 * (size_t)(side == 0 ? A : B), *J = side == 0 ? JA : JB;
         for (int k = 0; k < 6; ++k) {
             double sacc = 0.0;
             for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
-            m[k] = sacc;
-        }
-        for (int r = 0; r < 3; ++r) {
-            double sacc = 0.0;
-            for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
-            jm[r] += sacc;
+            for (int r = 0; r < 3; ++r) jm[r] += J[r * 6 + k] * sacc;
         }
     }
     double g[3];
@@ -1051,7 +1047,7 @@ __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
     double zb[3], mub = 0.0;
     proj_adjoint(z, mu, g, zb, mub);
     double ub[3] = {-rho * zb[0], -rho * zb[1], -rho * zb[2]};
-    double rb = -(zb[0] * s0 + zb[1] * u[1] + zb[2] * u[2]);
+    const double rb = -(zb[0] * s0 + zb[1] * u[1] + zb[2] * u[2]);
     if (a.desaxce) {
         mub += -rho * ut * zb[0];
         if (ut > kStickSpeed) {
@@ -1059,30 +1055,27 @@ __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
             ub[2] += -rho * mu * (u[2] / ut) * zb[0];
         }
     }
+    // on the path to the next update: the velocity adjoints and the impulse adjoint
+    for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? dA : dB)) continue;
+        const double *J = side == 0 ? JA : JB, *w = side == 0 ? wA : wB;
+        const int b = side == 0 ? A : B;
+        for (int k = 0; k < 6; ++k)
+            __stcg(a.vb + 6 * (size_t)b + k, w[k] + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+    }
     for (int k = 0; k < 3; ++k) {
         a.gl[3 * (size_t)c + k] = zb[k] - jm[k];
         a.bias_b[3 * (size_t)c + k] += ub[k];
     }
     a.mu_b[c] += mub;
     a.rho_b[c] += rb;
-    for (int side = 0; side < 2; ++side) {
-        const int b = side == 0 ? A : B;
-        if (b < 0) continue;
-        const bool d = side == 0 ? dA : dB;
-        const double *J = side == 0 ? JA : JB, *vf = side == 0 ? va : vv, *m = side == 0 ? mA : mB;
-        double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
-        for (int r = 0; r < 3; ++r)
-            for (int k = 0; k < 6; ++k)
-                __stcg(Jbar + 6 * r + k, __ldcg(Jbar + 6 * r + k) + (ub[r] * vf[k] + (d ? dl[r] * m[k] : 0.0)));
-        if (!d) continue;
-        const double *w = side == 0 ? wA : wB;
-        double jt[6];  // J^T dl
-        for (int k = 0; k < 6; ++k) jt[k] = (J[k] * dl[0] + J[6 + k] * dl[1]) + J[12 + k] * dl[2];
-        double *Mb = a.Minv_b + 36 * (size_t)b;
-        for (int i = 0; i < 6; ++i)
-            for (int k = 0; k < 6; ++k) __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + w[i] * jt[k]);
-        for (int k = 0; k < 6; ++k)
-            __stcg(a.vb + 6 * (size_t)b + k, w[k] + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+    for (int k = 0; k < 3; ++k) {
+        tr[15 + k] = ub[k];
+        tr[18 + k] = l[k] - lo[k];
+    }
+    for (int k = 0; k < 6; ++k) {
+        tr[21 + k] = wA[k];
+        tr[27 + k] = wB[k];
     }
 }
 
@@ -1157,16 +1150,18 @@ __device__ void top_projector(const double W[3][3], double lm, double P[3][3])
         for (int j = 0; j < 3; ++j) P[i][j] = e[i] * e[j];
 }
 
-// The start of the recorded sweeps, v = v_free + Minv sum_c J_c^T lo_c (setup, with lo the
-// warm start) and the step sizes rho_c = 1 / lambda_max(W_c), W_c = sum_sides J Minv J^T
-// (k_rho): gl[c] += J Minv vbar (the warm start's adjoint), the blocks' and Minv's adjoints,
-// and rho_b through Wbar = -rho^2 rho_b P / k (top_projector).  Run colour by colour like the
-// sweeps.
-__device__ void adj_start_recorded(const AdjArgs &a, int c)
+// After the reverse sweeps, per contact (colour by colour, so that each dynamic body belongs to
+// one contact at a time): the blocks' and Minv's adjoints summed over the recorded updates --
+// ub (x) v (through u) and dl (x) Minv vbar (through the velocity change) for the blocks,
+// vbar (x) J^T dl for Minv -- and the start of the sweeps, v = v_free + Minv sum_c J_c^T lo_c
+// (setup, lo the warm start) and rho_c = 1 / lambda_max(W_c), W_c = sum_sides J Minv J^T
+// (k_rho): gl[c] += J Minv vbar (the warm start's adjoint), lo (x) Minv vbar and vbar (x) J^T lo,
+// and rho_b through Wbar = -rho^2 rho_b P / k (top_projector).
+__device__ __noinline__ void adj_start_recorded(const AdjArgs &a, int c)
 {
     const int A = a.pa[c], B = a.pb[c];
-    const double *tr = a.trace + kTraceWords * (size_t)c;  // sweep 0
-    const double lo[3] = {tr[0], tr[1], tr[2]};
+    const double *tr0 = a.trace + kTraceWords * (size_t)c;  // sweep 0
+    const double lo[3] = {tr0[0], tr0[1], tr0[2]};
     const double rho = a.rho[c];
     const double rb = a.rho_b[c];
     double Wb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -1183,8 +1178,40 @@ __device__ void adj_start_recorded(const AdjArgs &a, int c)
     double jm[3] = {0.0, 0.0, 0.0};
     for (int side = 0; side < 2; ++side) {
         const int b = side == 0 ? A : B;
-        if (b < 0 || !a.dyn[b]) continue;
+        if (b < 0) continue;
+        const bool d = a.dyn[b] != 0;
         const double *M = a.Minv + 36 * (size_t)b, *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
+        const int vo = side == 0 ? 3 : 9, wo = side == 0 ? 21 : 27;
+        double Jacc[18], Macc[36];
+        for (int k = 0; k < 18; ++k) Jacc[k] = 0.0;
+        for (int k = 0; k < 36; ++k) Macc[k] = 0.0;
+        for (int it = 0; it < a.iters; ++it) {
+            const double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
+            const double ub[3] = {tr[15], tr[16], tr[17]};
+            for (int r = 0; r < 3; ++r)
+                for (int k = 0; k < 6; ++k) Jacc[6 * r + k] += ub[r] * tr[vo + k];
+            if (!d) continue;
+            const double dl[3] = {tr[18], tr[19], tr[20]};
+            double w[6], m[6];
+            for (int k = 0; k < 6; ++k) w[k] = tr[wo + k];
+            for (int k = 0; k < 6; ++k) {
+                double sacc = 0.0;
+                for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
+                m[k] = sacc;
+            }
+            for (int r = 0; r < 3; ++r)
+                for (int k = 0; k < 6; ++k) Jacc[6 * r + k] += dl[r] * m[k];
+            for (int k = 0; k < 6; ++k) {
+                const double jt = (J[k] * dl[0] + J[6 + k] * dl[1]) + J[12 + k] * dl[2];
+                for (int i = 0; i < 6; ++i) Macc[6 * i + k] += w[i] * jt;
+            }
+        }
+        double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
+        if (!d) {
+            for (int k = 0; k < 18; ++k) Jbar[k] += Jacc[k];
+            continue;
+        }
+        // the start: vbar of the sweeps' initial velocities
         double w[6], m[6], jt[6];
         for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
         for (int k = 0; k < 6; ++k) {
@@ -1198,25 +1225,21 @@ __device__ void adj_start_recorded(const AdjArgs &a, int c)
             for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
             jm[r] += sacc;
         }
-        // WJ = Wbar J (3x6), WJM = Wbar J Minv (3x6)
-        double WJ[3][6], WJM[3][6];
+        // WJ = Wbar J (3x6); Jbar += 2 Wbar J Minv, Minv_bar += J^T Wbar J
+        double WJ[3][6];
         for (int r = 0; r < 3; ++r)
             for (int k = 0; k < 6; ++k) WJ[r][k] = (Wb[r][0] * J[k] + Wb[r][1] * J[6 + k]) + Wb[r][2] * J[12 + k];
         for (int r = 0; r < 3; ++r)
             for (int k = 0; k < 6; ++k) {
                 double sacc = 0.0;
                 for (int j = 0; j < 6; ++j) sacc += WJ[r][j] * M[j * 6 + k];
-                WJM[r][k] = sacc;
+                Jbar[6 * r + k] += Jacc[6 * r + k] + lo[r] * m[k] + 2.0 * sacc;
             }
-        double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
-        for (int r = 0; r < 3; ++r)
-            for (int k = 0; k < 6; ++k)
-                __stcg(Jbar + 6 * r + k, __ldcg(Jbar + 6 * r + k) + (lo[r] * m[k] + 2.0 * WJM[r][k]));
         double *Mb = a.Minv_b + 36 * (size_t)b;
         for (int i = 0; i < 6; ++i)
             for (int k = 0; k < 6; ++k) {
                 const double jwj = (J[i] * WJ[0][k] + J[6 + i] * WJ[1][k]) + J[12 + i] * WJ[2][k];
-                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (w[i] * jt[k] + jwj));
+                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (Macc[6 * i + k] + w[i] * jt[k] + jwj));
             }
     }
     for (int k = 0; k < 3; ++k) a.gl[3 * (size_t)c + k] += jm[k];
@@ -1295,7 +1318,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_adj_sweeps(AdjArgs a)
 }
 
 int adjoint_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p, int iters,
-                   const double *trace, double *gl, double *vb, double *vfree_b, double *bias_b, double *mu_b,
+                   double *trace, double *gl, double *vb, double *vfree_b, double *bias_b, double *mu_b,
                    double *Ja_b, double *Jb_b, double *Minv_b, cudaStream_t s)
 {
     if (iters <= 0 || sc->n_c == 0) return B2C_OK;
@@ -1432,19 +1455,21 @@ extern "C" int32_t b2c_ncp_adjoint(const b2c_ncp_scene *sc, b2c_ncp_state *st, c
                                     nullptr, nullptr, b2c::stream_of(s));
 }
 
+extern "C" int32_t b2c_ncp_trace_words(void) { return b2c::ncp::kTraceWords; }
+
 extern "C" int32_t b2c_ncp_sweeps_record(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
                                          int32_t iters, double *trace, int64_t trace_len, b2c_stream s)
 {
     if (!ncp_scene_ok(sc, st) || !p || sc->dtype != 8 || iters < 0 ||
         (sc->n_c > 0 && iters > 0 && (!trace || trace_len < b2c::ncp::kTraceWords * (int64_t)iters * sc->n_c))) {
-        b2c::set_error("b2c_ncp_sweeps_record: bad argument (float64 scenes; trace of iters * n_c * 15 doubles)");
+        b2c::set_error("b2c_ncp_sweeps_record: bad argument (float64 scenes; trace of b2c_ncp_trace_words() * iters * n_c doubles)");
         return B2C_EARG;
     }
     return b2c::ncp::sweeps<double>(sc, st, p, iters, b2c::stream_of(s), trace);
 }
 
 extern "C" int32_t b2c_ncp_adjoint_unrolled(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
-                                            int32_t iters, const double *trace, int64_t trace_len, double *lam_bar,
+                                            int32_t iters, double *trace, int64_t trace_len, double *lam_bar,
                                             double *v_bar, double *vfree_bar, double *bias_bar, double *mu_bar,
                                             double *Ja_bar, double *Jb_bar, double *Minv_bar, b2c_stream s)
 {

@@ -299,11 +299,11 @@ __global__ void k_integrate(int n, const double *__restrict__ v6, double dt, dou
 //                  qb += 2 P(q) thb, where P(q) = d((w, 0) q)/dw maps a rotation vector to the
 //                  quaternion change.
 // Held at the substep's values: the contact set, the clipping of the manifold, the colouring.
-// Several contacts meet at one body, so the per-body sums run in int64 fixed point (round(2^40 x)
-// per term): they do not depend on the order of the atomics.  Kinematic bodies get no adjoint
-// (their motion is prescribed).
+// Several contacts meet at one body: the per-body sums are float64 atomics (an adjoint's range
+// -- 1e-9 to 1e7 in one rollout of colliding boxes -- overflows any fixed-point scale; the order
+// of the additions can move the last bits).  Kinematic bodies get no adjoint (their motion is
+// prescribed).
 // ---------------------------------------------------------------------------------------------
-constexpr double kAdjScale = 1099511627776.0;  // 2^40
 
 __device__ __forceinline__ void qmul_w_partials(double4 q, d3 w, double dq[4][4], double dw[4][3])
 {
@@ -406,9 +406,9 @@ __device__ __forceinline__ double dbias_dgap(double g, double h)
     return g > 0.0 ? 1.0 / h : (-g - kSlop > 0.0 ? kBeta / h : 0.0);
 }
 
-__device__ __forceinline__ void acc_add(long long *acc, double x)
+__device__ __forceinline__ void acc_add(double *acc, double x)
 {
-    atomicAdd(reinterpret_cast<unsigned long long *>(acc), (unsigned long long)llround(x * kAdjScale));
+    atomicAdd(acc, x);
 }
 
 // acc per body: 10 int64 -- xb (3), thb (3), mub (1), pad
@@ -417,7 +417,7 @@ __global__ void k_adj_contacts(int nc, const int *__restrict__ pa, const int *__
                                const double *__restrict__ nrm, const double *__restrict__ gap,
                                const double *__restrict__ x, const double *__restrict__ body_mu,
                                const double *__restrict__ mu_c, const double *__restrict__ bias_b,
-                               const double *__restrict__ mu_b, double h, long long *__restrict__ acc)
+                               const double *__restrict__ mu_b, double h, double *__restrict__ acc)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -430,7 +430,7 @@ __global__ void k_adj_contacts(int nc, const int *__restrict__ pa, const int *__
         const double sg = side == 0 ? 1.0 : -1.0;
         const d3 r = dsub(pc, ld3d(x, b));
         const d3 th = dcross(r, n);
-        long long *A = acc + 8 * (size_t)b;
+        double *A = acc + 8 * (size_t)b;
         if (gb != 0.0) {
             acc_add(A + 0, sg * gb * n.x);
             acc_add(A + 1, sg * gb * n.y);
@@ -481,7 +481,7 @@ __global__ void k_adj_geom(int nc, const int *__restrict__ pa, const int *__rest
                            const double *__restrict__ Ja,
                            const double *__restrict__ Minv, const double *__restrict__ lam,
                            const double *__restrict__ Vb, const double *__restrict__ Ja_b,
-                           const double *__restrict__ Jb_b, long long *__restrict__ acc)
+                           const double *__restrict__ Jb_b, double *__restrict__ acc)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -578,7 +578,7 @@ __global__ void k_adj_geom(int nc, const int *__restrict__ pa, const int *__rest
     }
     for (int s = 0; s < 2; ++s) {
         if (!dyn[s]) continue;
-        long long *Acc = acc + 8 * (size_t)body[s];
+        double *Acc = acc + 8 * (size_t)body[s];
         acc_add(Acc + 0, xg[s].x);
         acc_add(Acc + 1, xg[s].y);
         acc_add(Acc + 2, xg[s].z);
@@ -594,7 +594,7 @@ __global__ void k_adj_geom(int nc, const int *__restrict__ pa, const int *__rest
 // With dK = [dth]x K - K [dth]x: thb += ax(K Kb^T) - ax(Kb^T K), ax(X) = (X_yz - X_zy,
 // X_zx - X_xz, X_xy - X_yx).  Then qb += 2 P(q) thb, P = d((w, 0) q)/dw.
 __global__ void k_adj_finish(int n, const double *__restrict__ q, const int *__restrict__ kin,
-                             const double *__restrict__ vfree_b, long long *__restrict__ acc,
+                             const double *__restrict__ vfree_b, double *__restrict__ acc,
                              double *__restrict__ xb, double *__restrict__ qb, double *__restrict__ vb,
                              double *__restrict__ wb, double *__restrict__ mub_body, const double *__restrict__ V6,
                              const double *__restrict__ vfree, const double *__restrict__ Ib,
@@ -603,20 +603,20 @@ __global__ void k_adj_finish(int n, const double *__restrict__ q, const int *__r
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    long long *A = acc + 8 * (size_t)i;
+    double *A = acc + 8 * (size_t)i;
     if (kin[i]) {
         for (int k = 0; k < 3; ++k) vb[3 * (size_t)i + k] = wb[3 * (size_t)i + k] = 0.0;
-        for (int k = 0; k < 8; ++k) A[k] = 0;
+        for (int k = 0; k < 8; ++k) A[k] = 0.0;
         return;
     }
     double th[3];
     for (int k = 0; k < 3; ++k) {
-        xb[3 * (size_t)i + k] += (double)A[k] / kAdjScale;
-        th[k] = (double)A[3 + k] / kAdjScale;
+        xb[3 * (size_t)i + k] += A[k];
+        th[k] = A[3 + k];
         vb[3 * (size_t)i + k] = vfree_b[6 * (size_t)i + k];
         wb[3 * (size_t)i + k] = vfree_b[6 * (size_t)i + 3 + k];
     }
-    if (mub_body) mub_body[i] += (double)A[6] / kAdjScale;
+    if (mub_body) mub_body[i] += A[6];
     const double4 q0 = ld4d(q, i);
     if (V6 && Minv_b) {
         const double *M = Minv + 36 * (size_t)i, *Mb = Minv_b + 36 * (size_t)i;
@@ -653,7 +653,7 @@ __global__ void k_adj_finish(int n, const double *__restrict__ q, const int *__r
     double dq[4][4], dw[4][3];
     qmul_w_partials(q0, D3(0.0, 0.0, 0.0), dq, dw);
     for (int r = 0; r < 4; ++r) qb[4 * (size_t)i + r] += 2.0 * ((dw[r][0] * th[0] + dw[r][1] * th[1]) + dw[r][2] * th[2]);
-    for (int k = 0; k < 8; ++k) A[k] = 0;
+    for (int k = 0; k < 8; ++k) A[k] = 0.0;
 }
 
 }  // namespace world
@@ -792,7 +792,7 @@ extern "C" int32_t b2c_world_adj_begin(const b2c_world *wd, const b2c_ncp_scene 
 extern "C" int32_t b2c_world_adj_end(const b2c_world *wd, const b2c_ncp_scene *sc, const double *lam,
                                      const double *V6, const double *Vb, double h, const double *bias_b,
                                      const double *mu_b, const double *vfree_b, const double *Ja_b, const double *Jb_b,
-                                     const double *Minv_b, int64_t *acc, double *xb, double *qb, double *vb,
+                                     const double *Minv_b, double *acc, double *xb, double *qb, double *vb,
                                      double *wb, double *mub_body, b2c_stream stream)
 {
     if (!wd || !sc || sc->dtype != 8 || sc->n_b != wd->n || !(h > 0.0) || !V6 || !Vb || !vfree_b || !acc || !xb ||
@@ -801,7 +801,7 @@ extern "C" int32_t b2c_world_adj_end(const b2c_world *wd, const b2c_ncp_scene *s
         return B2C_EARG;
     }
     cudaStream_t s = stream_of(stream);
-    long long *A = reinterpret_cast<long long *>(acc);
+    double *A = acc;
     if (sc->n_c > 0)
         k_adj_contacts<<<blocks_for(sc->n_c), kThreads, 0, s>>>(sc->n_c, sc->pa, sc->pb, wd->kin, wd->attach, wd->p,
                                                                  wd->nrm,

@@ -431,6 +431,36 @@ class RelaxedJacobiContactEngine(_BeadEngineBase):
                                       ctypes.c_void_p(_ptr(self.vgrav)), ctypes.c_void_p(s))
             _lib.check(rc, "b2c_jacobi_substep")
 
+    def solve_sample(self, sdt: float):
+        """One b2c_jacobi_solve on the current contacts between CUDA events (it moves the state on:
+        call it last).  Returns (milliseconds, algorithmic bytes, counts).  Bytes per launch
+        sequence, each array element read or written once per launch: a velocity iteration
+        (k_jacobi_velocity + k_jacobi_apply) moves 68 C + (76 + 16 x 12) E + 144 N, a position
+        iteration 56 C + (76 + 16 x 6) E + 144 N -- C contacts, E their dynamic endpoints (a
+        body's xc, invM, invIw, v, w and its 6 int64 accumulators, 12 atomics per endpoint in the
+        velocity pass), N bodies (apply: 6 int64 read and cleared, v, w read and written)."""
+        h = self.header_dict()
+        C = min(int(h["n_contacts"]), self.contact_capacity)
+        bi = self.cbi[:C].long()
+        bj = self.cbj[:C].long()
+        dyn = self.invM > 0
+        E = int(dyn[bi].sum()) + int(((bj >= 0) & dyn[bj.clamp(min=0)]).sum())
+        N = self.N
+        vel = 68 * C + (76 + 16 * 12) * E + 144 * N
+        pos = 56 * C + (76 + 16 * 6) * E + 144 * N
+        s = torch.cuda.current_stream(self.dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(self.dev)
+        a.record(s)
+        _lib.check(self.L.b2c_jacobi_solve(ctypes.byref(self.c_bodies), ctypes.byref(self.c_contacts),
+                                           ctypes.c_void_p(_ptr(self.header)), ctypes.c_void_p(_ptr(self.acc)),
+                                           ctypes.byref(self.c_params), ctypes.c_float(sdt),
+                                           ctypes.c_void_p(s.cuda_stream)), "b2c_jacobi_solve")
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b), self.vit * vel + self.pit * pos, dict(contacts=C, endpoints=E, bodies=N,
+                                                                         vit=self.vit, pit=self.pit)
+
     def step(self, dt, substeps=1):
         if not self._built:
             self._build()

@@ -438,7 +438,8 @@ class NCPSolverB200:
         self.stats[3] = 0
         _lib.check(self.L.b2c_ncp_color(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
                                         ctypes.byref(params), s), "b2c_ncp_color")
-        trace = torch.empty(15 * int(iters) * max(C, 1), dtype=torch.float64, device=dev)
+        trace = torch.empty(int(self.L.b2c_ncp_trace_words()) * int(iters) * max(C, 1), dtype=torch.float64,
+                            device=dev)
         _lib.check(self.L.b2c_ncp_sweeps_record(ctypes.byref(self.c_scene), ctypes.byref(self.c_state),
                                                 ctypes.byref(params), int(iters), ctypes.c_void_p(_ptr(trace)),
                                                 trace.numel(), s), "b2c_ncp_sweeps_record")

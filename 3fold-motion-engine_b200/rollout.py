@@ -101,18 +101,19 @@ class BoxRollout:
         self.lam_b, self.bias_b, self.mu_b = f64(MC, 3), f64(MC, 3), f64(MC)
         self.Ja_b, self.Jb_b, self.Minv_b = f64(MC, 18), f64(MC, 18), f64(n, 36)
         self.mub_body = f64(n)
-        self.acc = torch.zeros((max(n, 1), 8), dtype=torch.int64, device=dev)
+        self.acc = torch.zeros((max(n, 1), 8), dtype=torch.float64, device=dev)
         # the warm-start adjoint handed from a substep to the one before it, by contact key
         self.adj_keys = torch.zeros(MC, dtype=torch.int64, device=dev)
         self.adj_lam = f64(MC, 3)
         self.adj_n = torch.zeros(1, dtype=torch.int32, device=dev)
         self.trace = f64(1)
+        self.words = int(world.L.b2c_ncp_trace_words())
         self.max_c = 0
 
     def _size_trace(self):
-        """The sweep record of one substep: 15 doubles per contact and sweep, sized once per
-        backward by the most contacts a substep of the forward had."""
-        need = 15 * self.world.iters * max(self.max_c, 1)
+        """The sweep record of one substep (b2c_ncp_trace_words() doubles per contact and sweep),
+        sized once per backward by the most contacts a substep of the forward had."""
+        need = self.words * self.world.iters * max(self.max_c, 1)
         if self.trace.numel() < need:
             self.trace = None
             self.trace = torch.empty(need, dtype=torch.float64, device=self.world.dev)
@@ -169,7 +170,7 @@ class BoxRollout:
             warm = False
             if C:
                 warm = w.warm_start and w._have_warm
-                trace = self.trace[:15 * w.iters * C]
+                trace = self.trace[:self.words * w.iters * C]
                 w.solve_device(C, w.iters, warm, trace=trace)
                 V6 = s.v
             else:

@@ -168,7 +168,7 @@ class BoxWorldB200:
     def solve_device(self, C: int, iters: int, warm: bool, trace=None):
         """The NCP solve of the scene just built: setup (from the warm store when `warm`), the
         colouring, `iters` sweeps.  The impulses stay in solver.lam, velocities in solver.v.
-        With `trace` (a float64 device tensor of at least 15 iters C elements) the sweeps also
+        With `trace` (a float64 device tensor of at least b2c_ncp_trace_words() iters C elements) the sweeps also
         record where every contact update started from (b2c_ncp_sweeps_record), bitwise the
         same solve, for the adjoint."""
         s, L, st = self.solver, self.L, self._stream()

@@ -1285,6 +1285,21 @@ def main():
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "k_color_solve (persistent chunk solve, one launch per substep)",
                 "launch_ms": avg_ms, "algorithmic_bytes_per_launch": avg_b, "counts": solve_bytes[-1]}
+    elif wl["engine"] == "jacobi":  # the iteration launches of one substep, timed after the timed region
+        j_ms, j_b, j_counts = e.solve_sample(dt / S)
+        achieved = j_b / (j_ms / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get(args.workload)
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "b2c_jacobi_solve: vit x (k_jacobi_velocity + k_jacobi_apply) + pit x (k_jacobi_position + "
+                          "k_jacobi_apply), one substep's iterations on the final state",
+                "launch_ms": j_ms, "algorithmic_bytes_per_launch": j_b, "counts": j_counts}
     cfg = {"workload": args.workload, "bodies": n_job if wl["engine"] == "batched" else wl["n"], "substeps": S,
            "vit": wl["vit"], "pit": wl["pit"], "dt": dt, "setup_steps": wl["preroll"],
            "l2": "flushed between timed steps (256 MiB write)",

@@ -472,9 +472,11 @@ B2C_API int32_t b2c_ncp_adjoint(const b2c_ncp_scene *sc, b2c_ncp_state *st, cons
                                 int32_t iters, double *lam_bar, double *v_bar, double *vfree_bar, double *bias_bar,
                                 double *mu_bar, b2c_stream s);
 /* b2c_ncp_sweeps (float64 scenes) that also records what every contact update of every sweep
- * started from: trace[15 (it n_c + c) + 0..2] = the contact's impulse, [3..8] and [9..14] = the
- * velocities (n_b,6 rows) of its bodies pa, pb (zero where there is none); trace_len >= 15 iters
- * n_c doubles.  The impulses and velocities it leaves are bitwise those of b2c_ncp_sweeps. */
+ * started from, b2c_ncp_trace_words() doubles per update: trace[W (it n_c + c) + 0..2] = the
+ * contact's impulse, [3..8] and [9..14] = the velocities (n_b,6 rows) of its bodies pa, pb (zero
+ * where there is none); the rest of each record is b2c_ncp_adjoint_unrolled's.  trace_len >= W
+ * iters n_c.  The impulses and velocities it leaves are bitwise those of b2c_ncp_sweeps. */
+B2C_API int32_t b2c_ncp_trace_words(void);
 B2C_API int32_t b2c_ncp_sweeps_record(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
                                       int32_t iters, double *trace, int64_t trace_len, b2c_stream s);
 /* The exact reverse of setup (warm or cold) and the `iters` sweeps recorded by
@@ -488,7 +490,7 @@ B2C_API int32_t b2c_ncp_sweeps_record(const b2c_ncp_scene *sc, b2c_ncp_state *st
  * (redundant contacts) the one the sweeps reach depends on where they started, which the implicit
  * form above cannot see.  No counterpart in the reference. */
 B2C_API int32_t b2c_ncp_adjoint_unrolled(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_params *p,
-                                         int32_t iters, const double *trace, int64_t trace_len, double *lam_bar,
+                                         int32_t iters, double *trace, int64_t trace_len, double *lam_bar,
                                          double *v_bar, double *vfree_bar, double *bias_bar, double *mu_bar,
                                          double *Ja_bar, double *Jb_bar, double *Minv_bar, b2c_stream s);
 
@@ -556,7 +558,8 @@ B2C_API int32_t b2c_world_integrate(b2c_world *wd, const double *v6, double dt, 
  * begin; Ja_b, Jb_b (n_c,3,6) and Minv_b (n,6,6) of b2c_ncp_adjoint_unrolled): the bias through
  * the gaps, the Jacobian blocks through the lever arms, the contact point and frame (the normal
  * turning with its body, attach), the world inertias, and mu_c = sqrt(mu_a mu_b) onto the bodies
- * -- summed in int64 fixed point (acc: n x 8 int64, zero on entry and on return) -- giving xb, qb
+ * -- summed per body with float64 atomics (acc: n x 8 doubles, zero on entry and on return; the
+ * order of the additions can move the last bits) -- giving xb, qb
  * (completed), vb, wb of the state before the substep, and mub_body (n, accumulated; may be
  * NULL).  No counterpart in the reference. */
 B2C_API int32_t b2c_world_adj_begin(const b2c_world *wd, const b2c_ncp_scene *sc, const double *V6, double h,
@@ -566,7 +569,7 @@ B2C_API int32_t b2c_world_adj_begin(const b2c_world *wd, const b2c_ncp_scene *sc
 B2C_API int32_t b2c_world_adj_end(const b2c_world *wd, const b2c_ncp_scene *sc, const double *lam, const double *V6,
                                   const double *Vb, double h, const double *bias_b, const double *mu_b,
                                   const double *vfree_b, const double *Ja_b, const double *Jb_b, const double *Minv_b,
-                                  int64_t *acc, double *xb, double *qb, double *vb, double *wb, double *mub_body,
+                                  double *acc, double *xb, double *qb, double *vb, double *wb, double *mub_body,
                                   b2c_stream s);
 
 /* ---------------------------------------------------------------------------------------------
