@@ -34,7 +34,8 @@ namespace ncp {
 
 constexpr double kScale = 1.0e10;
 constexpr int kColorThreads = 1024;
-constexpr int kSweepThreads = 512;
+constexpr int kSweepThreads = 1024;  // 64 groups of 16 lanes: one contact each
+constexpr int kAdjThreads = 512;     // the reverse sweeps: one thread per contact
 constexpr int kClusterMax = 16;
 constexpr int kMaxColors = 1024;  // the reference's _NCOLMAX
 
@@ -279,11 +280,12 @@ struct SweepArgs {
 
 enum Kind { kBlock = 0, kCluster = 1, kGrid = 2 };
 
-// A recorded update: the contact's impulse before it [0, 3) and the velocities of its bodies a, b
-// [3, 9), [9, 15) (zero where there is no body), written by the sweeps; the reverse sweep adds
-// the update's adjoints: ub [15, 18), the impulse change dl [18, 21) and the adjoints of both
-// bodies' velocities after the update [21, 27), [27, 33).
-constexpr int kTraceWords = 33;
+// A recorded update, written by the sweeps: the contact's impulse before it [0, 3), the
+// velocities of its bodies a, b [3, 9), [9, 15) (zero where there is no body), the impulse
+// change dl [18, 21), the projection's argument z [33, 36) and the contact velocity u [36, 39);
+// the reverse sweep adds the update's adjoints: ub [15, 18) and the adjoints of both bodies'
+// velocities after the update [21, 27), [27, 33).
+constexpr int kTraceWords = 39;
 
 // The barrier between colours.  The grid form (a cooperative launch, every CTA co-resident) is
 // the arrival-counter barrier of b2c_barrier.cuh over a.bar[0] (cleared by the host before the
@@ -305,38 +307,94 @@ __device__ __forceinline__ bool phase_barrier(const SweepArgs<T> &a, unsigned in
     return grid_wait(a.bar, epoch, a.timeout_ns, a.stats + kError, kErrBarrier);
 }
 
+// One contact update of k_sweep (:485-568): u = bias + Ja v_a + Jb v_b (contact_u's sums), the
+// projection of contact_z's argument, then for each dynamic body the swap of the contact's
+// rounded contribution Minv J^T lambda in the int64 accumulator (f_swap, :425-438) and the
+// body's velocity rebuilt from it (k_apply_c, :583-599).  It runs on a group of kGroup = 16
+// lanes, so that one contact's dependent chain is short: lanes 0..5 form the six 6-term sums of
+// u (row i = lane % 3 of side lane / 3); every lane then has u, z and the projection (the same
+// bits in each); lanes 0..11 each own one velocity component k of one side: row k of the
+// Minv J^T products, the accumulator swap and the velocity rebuild (one division each, in
+// parallel).  Every sum runs in the same order as a one-thread update would.
+constexpr int kGroup = 16;
+
 template <typename T>
-__device__ __forceinline__ void sweep_contact(const SweepArgs<T> &a, int c, int it)
+__device__ __forceinline__ T group_get(T x, int src, unsigned mask)
+{
+    return __shfl_sync(mask, x, src, kGroup);
+}
+
+template <typename T>
+__device__ __forceinline__ void sweep_contact_group(const SweepArgs<T> &a, int c, int it, int l, unsigned mask)
 {
     const int pa = a.pa[c], pb = a.pb[c];
-    T u[3], z[3], zn[3];
     const T lo[3] = {a.lam[3 * (size_t)c], a.lam[3 * (size_t)c + 1], a.lam[3 * (size_t)c + 2]};
-    contact_u(c, a.Ja, a.Jb, pa, pb, a.bias, a.v, u);
-    if (a.trace) {  // the bodies' rows of v are this thread's alone during the colour
-        double *t = a.trace + kTraceWords * ((size_t)it * a.nc + c);
-        for (int k = 0; k < 3; ++k) t[k] = (double)lo[k];
-        for (int k = 0; k < 6; ++k) {
-            t[3 + k] = pa >= 0 ? (double)__ldcg(a.v + 6 * (size_t)pa + k) : 0.0;
-            t[9 + k] = pb >= 0 ? (double)__ldcg(a.v + 6 * (size_t)pb + k) : 0.0;
+    // the six partial sums of u
+    T part = T(0), vs[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    if (l < 6) {
+        const int i = l % 3, side = l / 3, b = side == 0 ? pa : pb;
+        if (b >= 0) {
+            for (int j = 0; j < 6; ++j) vs[j] = __ldcg(a.v + 6 * (size_t)b + j);
+            const T *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c + 6 * i;
+            T sacc = J[0] * vs[0];
+            for (int j = 1; j < 6; ++j) sacc = sacc + J[j] * vs[j];
+            part = sacc;
         }
     }
+    T u[3];
+    for (int i = 0; i < 3; ++i) {
+        const T sa = group_get(part, i, mask), sb = group_get(part, 3 + i, mask);
+        T ui = a.bias[3 * (size_t)c + i];
+        if (pa >= 0) ui = ui + sa;
+        if (pb >= 0) ui = ui + sb;
+        u[i] = ui;
+    }
+    T z[3], zn[3];
     contact_z(u, lo, a.mu[c], a.rho[c], a.desaxce, a.soft, a.sep ? a.sep[c] : T(0), z);
     proj(z, a.mu[c], zn);
-    a.lam[3 * (size_t)c] = zn[0];
-    a.lam[3 * (size_t)c + 1] = zn[1];
-    a.lam[3 * (size_t)c + 2] = zn[2];
-    for (int side = 0; side < 2; ++side) {
-        const int b = side == 0 ? pa : pb;
-        if (b < 0 || !a.dyn[b]) continue;  // a static body's Minv is zero: nothing to add
-        const T *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
-        T dn[6], dold[6];
-        minv_jt(J, a.Minv + 36 * (size_t)b, zn, dn);
-        minv_jt(J, a.Minv + 36 * (size_t)b, lo, dold);
-        for (int k = 0; k < 6; ++k) {
+    if (a.trace) {
+        double *t = a.trace + kTraceWords * ((size_t)it * a.nc + c);
+        if (l == 0)
+            for (int k = 0; k < 3; ++k) {
+                t[k] = (double)lo[k];
+                t[18 + k] = (double)zn[k] - (double)lo[k];
+                t[33 + k] = (double)z[k];
+                t[36 + k] = (double)u[k];
+            }
+        if (l == 0 || l == 3)
+            for (int k = 0; k < 6; ++k) t[(l == 0 ? 3 : 9) + k] = (double)vs[k];
+    }
+    if (l == 0) {
+        a.lam[3 * (size_t)c] = zn[0];
+        a.lam[3 * (size_t)c + 1] = zn[1];
+        a.lam[3 * (size_t)c + 2] = zn[2];
+    }
+    if (l < 12) {
+        const int side = l / 6, k = l % 6, b = side == 0 ? pa : pb;
+        if (b >= 0 && a.dyn[b]) {
+            const T *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
+            const T *M = a.Minv + 36 * (size_t)b + 6 * k;
+            // row k of Minv (J^T l), minv_jt's order, for the new and the old impulse
+            T dn = T(0), dold = T(0);
+            for (int j = 0; j < 6; ++j) {
+                T tn = J[j] * zn[0];
+                tn = tn + J[6 + j] * zn[1];
+                tn = tn + J[12 + j] * zn[2];
+                T to = J[j] * lo[0];
+                to = to + J[6 + j] * lo[1];
+                to = to + J[12 + j] * lo[2];
+                if (j == 0) {
+                    dn = M[0] * tn;
+                    dold = M[0] * to;
+                } else {
+                    dn = dn + M[j] * tn;
+                    dold = dold + M[j] * to;
+                }
+            }
             long long *p = a.acc + 6 * (size_t)b + k;
-            const long long s = __ldcg(p) + (quant(dn[k]) - quant(dold[k]));
-            __stcg(p, s);
-            __stcg(a.v + 6 * (size_t)b + k, a.vfree[6 * (size_t)b + k] + (T)((double)s / kScale));
+            const long long sacc = __ldcg(p) + (quant(dn) - quant(dold));
+            __stcg(p, sacc);
+            __stcg(a.v + 6 * (size_t)b + k, a.vfree[6 * (size_t)b + k] + (T)((double)sacc / kScale));
         }
     }
 }
@@ -345,16 +403,17 @@ template <typename T, int kKind>
 __global__ void __launch_bounds__(kSweepThreads) k_sweeps(SweepArgs<T> a)
 {
     const int ncol = a.stats[kNColors];
-    // Task slot: chunk k = t / 32 of a colour runs on CTA k mod gridDim, so a colour narrower
-    // than the launch is spread over every SM of it (contiguous slots would give all of a
-    // colour's float64 work to its first CTAs).  A contact keeps its thread in every sweep.
-    const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
-    const int tid = ((((int)threadIdx.x >> 5) * nb + (int)blockIdx.x) << 5) | ((int)threadIdx.x & 31);
+    // Task slot: one group of kGroup lanes per contact; group g = (group in CTA) x CTAs + CTA,
+    // so consecutive contacts of a colour land on different CTAs and a colour narrower than
+    // the launch is spread over every SM of it.  A contact keeps its group in every sweep.
+    const int nb = gridDim.x, groups = nb * (blockDim.x / kGroup);
+    const int g = ((int)threadIdx.x / kGroup) * nb + (int)blockIdx.x, l = (int)threadIdx.x % kGroup;
+    const unsigned mask = 0xFFFFu << (((int)threadIdx.x & 31) & ~(kGroup - 1));
     unsigned int epoch = 0;
     for (int it = 0; it < a.iters; ++it)
         for (int ci = 0; ci < ncol; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) sweep_contact(a, a.order[s0 + t], it);
+            for (int t = g; t < cnt; t += groups) sweep_contact_group(a, a.order[s0 + t], it, l, mask);
             if (!phase_barrier<kKind>(a, epoch)) return;
         }
 }
@@ -912,17 +971,17 @@ __device__ __forceinline__ void proj_adjoint(const double z[3], double mu, const
         return;
     }
     // s = (zn + mu zt) / (1 + mu^2), f = mu s / zt, out = (s, f z1, f z2)
-    const double den = 1.0 + mu * mu;
-    const double sv = (zn + mu * zt) / den;
-    const double f = mu * sv / zt;
-    const double t1 = z[1] / zt, t2 = z[2] / zt;
-    const double ds_dzn = 1.0 / den;
-    const double ds_dt1 = mu * t1 / den, ds_dt2 = mu * t2 / den;
-    const double ds_dmu = (zt * den - 2.0 * mu * (zn + mu * zt)) / (den * den);
-    const double df_dzn = mu * ds_dzn / zt;
-    const double df_dt1 = mu * ds_dt1 / zt - mu * sv * t1 / (zt * zt);
-    const double df_dt2 = mu * ds_dt2 / zt - mu * sv * t2 / (zt * zt);
-    const double df_dmu = (sv + mu * ds_dmu) / zt;
+    const double den = 1.0 + mu * mu, iden = 1.0 / den, izt = 1.0 / zt;
+    const double sv = (zn + mu * zt) * iden;
+    const double f = mu * sv * izt;
+    const double t1 = z[1] * izt, t2 = z[2] * izt;
+    const double ds_dzn = iden;
+    const double ds_dt1 = mu * t1 * iden, ds_dt2 = mu * t2 * iden;
+    const double ds_dmu = (zt * den - 2.0 * mu * (zn + mu * zt)) * iden * iden;
+    const double df_dzn = mu * ds_dzn * izt;
+    const double df_dt1 = (mu * ds_dt1 - mu * sv * t1 * izt) * izt;
+    const double df_dt2 = (mu * ds_dt2 - mu * sv * t2 * izt) * izt;
+    const double df_dmu = (sv + mu * ds_dmu) * izt;
     const double gz = g[1] * z[1] + g[2] * z[2];
     zb[0] = g[0] * ds_dzn + gz * df_dzn;
     zb[1] = g[0] * ds_dt1 + f * g[1] + gz * df_dt1;
@@ -984,66 +1043,53 @@ __device__ void adj_contact(const AdjArgs &a, int c)
     }
 }
 
-// The reverse of one recorded update of contact c in sweep `it` (sweep_contact):
+// The reverse of one recorded update of contact c in sweep `it` (sweep_contact_group):
 //   u = bias + Ja va + Jb vb,  z = lo - rho (u_n + mu |u_t| (de Saxce), u_t),  l = proj(z),
 //   v_a += Minv_a Ja^T (l - lo),  v_b likewise,
-// with va, vb and lo read back from the trace.  On entry gl[c] is the adjoint of l and vb the
+// with z and u read back from the record.  On entry gl[c] is the adjoint of l and vb the
 // adjoint of the velocities after the update; on exit gl[c] is the adjoint of lo and vb that of
 // the velocities before it, and bias_b, mu_b, rho_b hold the update's share.  Only vb and gl
 // are on the path to the next update; what the blocks' and Minv's adjoints need (ub, the impulse
-// change dl, the velocity adjoints) goes back into the trace for adj_start_recorded.
-__device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
+// change dl, the velocity adjoints) goes back into the trace for adj_start_group.
+// It runs on a group of kGroup lanes (the forward's layout): lanes 0..5 the six sums of u,
+// lanes 0..11 one velocity component k of one side each (its vbar, row k of Minv vbar, its
+// share of J Minv vbar -- summed over the lanes by a fixed butterfly -- and its vbar update),
+// every lane the projection and its adjoint.
+__device__ void adj_contact_group(const AdjArgs &a, int c, int it, int l, unsigned mask)
 {
     const int A = a.pa[c], B = a.pb[c];
     const bool dA = A >= 0 && a.dyn[A], dB = B >= 0 && a.dyn[B];
     double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
     const double *JA = a.Ja + 18 * (size_t)c, *JB = a.Jb + 18 * (size_t)c;
-    // the velocity adjoints first: their loads wait on the previous colour, the rest does not
-    double wA[6] = {0, 0, 0, 0, 0, 0}, wB[6] = {0, 0, 0, 0, 0, 0};
-    if (dA)
-        for (int k = 0; k < 6; ++k) wA[k] = __ldcg(a.vb + 6 * (size_t)A + k);
-    if (dB)
-        for (int k = 0; k < 6; ++k) wB[k] = __ldcg(a.vb + 6 * (size_t)B + k);
-    double lo[3], va[6], vv[6];
-    for (int k = 0; k < 3; ++k) lo[k] = tr[k];
-    for (int k = 0; k < 6; ++k) {
-        va[k] = tr[3 + k];
-        vv[k] = tr[9 + k];
-    }
-    double u[3];
-    for (int i = 0; i < 3; ++i) {
-        double ui = a.bias[3 * (size_t)c + i];
-        if (A >= 0) {
-            double sacc = JA[6 * i] * va[0];
-            for (int j = 1; j < 6; ++j) sacc = sacc + JA[6 * i + j] * va[j];
-            ui = ui + sacc;
-        }
-        if (B >= 0) {
-            double sacc = JB[6 * i] * vv[0];
-            for (int j = 1; j < 6; ++j) sacc = sacc + JB[6 * i + j] * vv[j];
-            ui = ui + sacc;
-        }
-        u[i] = ui;
-    }
+    const int side = l / 6, k = l % 6, b = side == 0 ? A : B;
+    const bool mine = l < 12 && (side == 0 ? dA : dB);
+    const double *J = side == 0 ? JA : JB;
+    // only vbar waits on the previous colour; the record and the per-contact sums do not
+    const double w = mine ? __ldcg(a.vb + 6 * (size_t)b + k) : 0.0;
+    const double z[3] = {tr[33], tr[34], tr[35]}, u[3] = {tr[36], tr[37], tr[38]};
+    const double gl0[3] = {a.gl[3 * (size_t)c], a.gl[3 * (size_t)c + 1], a.gl[3 * (size_t)c + 2]};
     const double mu = a.mu[c], rho = a.rho[c];
     const double ut = sqrt(u[1] * u[1] + u[2] * u[2]);
     const double s0 = a.desaxce ? u[0] + mu * ut : u[0];
-    const double z[3] = {lo[0] - rho * s0, lo[1] - rho * u[1], lo[2] - rho * u[2]};
-    double l[3];
-    proj(z, mu, l);
-    double jm[3] = {0.0, 0.0, 0.0};  // J Minv vbar
-    for (int side = 0; side < 2; ++side) {
-        if (!(side == 0 ? dA : dB)) continue;
-        const double *w = side == 0 ? wA : wB;
-        const double *M = a.Minv + 36 * (size_t)(side == 0 ? A : B), *J = side == 0 ? JA : JB;
-        for (int k = 0; k < 6; ++k) {
-            double sacc = 0.0;
-            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
-            for (int r = 0; r < 3; ++r) jm[r] += J[r * 6 + k] * sacc;
+    // row k of Minv vbar for this lane's side, then J Minv vbar summed over the lanes
+    double mk = 0.0;
+    {
+        const int base = side * 6;
+        double wj[6];
+        for (int j = 0; j < 6; ++j) wj[j] = group_get(w, (base + j) & (kGroup - 1), mask);
+        if (mine) {
+            const double *M = a.Minv + 36 * (size_t)b + 6 * k;
+            for (int j = 0; j < 6; ++j) mk += M[j] * wj[j];
         }
     }
+    double jm[3];
+    for (int r = 0; r < 3; ++r) {
+        double x = mine ? J[6 * r + k] * mk : 0.0;
+        for (int off = kGroup / 2; off > 0; off >>= 1) x += __shfl_xor_sync(mask, x, off, kGroup);
+        jm[r] = x;
+    }
     double g[3];
-    for (int k = 0; k < 3; ++k) g[k] = a.gl[3 * (size_t)c + k] + jm[k];
+    for (int r = 0; r < 3; ++r) g[r] = gl0[r] + jm[r];
     double zb[3], mub = 0.0;
     proj_adjoint(z, mu, g, zb, mub);
     double ub[3] = {-rho * zb[0], -rho * zb[1], -rho * zb[2]};
@@ -1051,31 +1097,25 @@ __device__ void adj_contact_recorded(const AdjArgs &a, int c, int it)
     if (a.desaxce) {
         mub += -rho * ut * zb[0];
         if (ut > kStickSpeed) {
-            ub[1] += -rho * mu * (u[1] / ut) * zb[0];
-            ub[2] += -rho * mu * (u[2] / ut) * zb[0];
+            const double q = -rho * mu / ut;
+            ub[1] += q * u[1] * zb[0];
+            ub[2] += q * u[2] * zb[0];
         }
     }
-    // on the path to the next update: the velocity adjoints and the impulse adjoint
-    for (int side = 0; side < 2; ++side) {
-        if (!(side == 0 ? dA : dB)) continue;
-        const double *J = side == 0 ? JA : JB, *w = side == 0 ? wA : wB;
-        const int b = side == 0 ? A : B;
-        for (int k = 0; k < 6; ++k)
-            __stcg(a.vb + 6 * (size_t)b + k, w[k] + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+    if (mine) {
+        __stcg(a.vb + 6 * (size_t)b + k, w + ((J[k] * ub[0] + J[6 + k] * ub[1]) + J[12 + k] * ub[2]));
+        tr[21 + 6 * side + k] = w;
+    } else if (l < 12) {
+        tr[21 + 6 * side + k] = 0.0;
     }
-    for (int k = 0; k < 3; ++k) {
-        a.gl[3 * (size_t)c + k] = zb[k] - jm[k];
-        a.bias_b[3 * (size_t)c + k] += ub[k];
-    }
-    a.mu_b[c] += mub;
-    a.rho_b[c] += rb;
-    for (int k = 0; k < 3; ++k) {
-        tr[15 + k] = ub[k];
-        tr[18 + k] = l[k] - lo[k];
-    }
-    for (int k = 0; k < 6; ++k) {
-        tr[21 + k] = wA[k];
-        tr[27 + k] = wB[k];
+    if (l == 0) {
+        for (int r = 0; r < 3; ++r) {
+            a.gl[3 * (size_t)c + r] = zb[r] - jm[r];
+            a.bias_b[3 * (size_t)c + r] += ub[r];
+            tr[15 + r] = ub[r];
+        }
+        a.mu_b[c] += mub;
+        a.rho_b[c] += rb;
     }
 }
 
@@ -1156,8 +1196,10 @@ __device__ void top_projector(const double W[3][3], double lm, double P[3][3])
 // vbar (x) J^T dl for Minv -- and the start of the sweeps, v = v_free + Minv sum_c J_c^T lo_c
 // (setup, lo the warm start) and rho_c = 1 / lambda_max(W_c), W_c = sum_sides J Minv J^T
 // (k_rho): gl[c] += J Minv vbar (the warm start's adjoint), lo (x) Minv vbar and vbar (x) J^T lo,
-// and rho_b through Wbar = -rho^2 rho_b P / k (top_projector).
-__device__ __noinline__ void adj_start_recorded(const AdjArgs &a, int c)
+// and rho_b through Wbar = -rho^2 rho_b P / k (top_projector).  A group of kGroup lanes per
+// contact: lane (side, k), k < 6, owns column k of its side's block adjoint (3 entries) and of
+// its body's Minv adjoint (6 entries) and walks the sweeps for them.
+__device__ void adj_start_group(const AdjArgs &a, int c, int l, unsigned mask)
 {
     const int A = a.pa[c], B = a.pb[c];
     const double *tr0 = a.trace + kTraceWords * (size_t)c;  // sweep 0
@@ -1175,74 +1217,61 @@ __device__ __noinline__ void adj_start_recorded(const AdjArgs &a, int c)
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) Wb[i][j] = lmb * P[i][j];
     }
+    const int side = l / 6, k = l % 6, b = side == 0 ? A : B;
+    const bool on = l < 12 && b >= 0, d = on && a.dyn[b] != 0;
     double jm[3] = {0.0, 0.0, 0.0};
-    for (int side = 0; side < 2; ++side) {
-        const int b = side == 0 ? A : B;
-        if (b < 0) continue;
-        const bool d = a.dyn[b] != 0;
+    if (on) {
         const double *M = a.Minv + 36 * (size_t)b, *J = (side == 0 ? a.Ja : a.Jb) + 18 * (size_t)c;
         const int vo = side == 0 ? 3 : 9, wo = side == 0 ? 21 : 27;
-        double Jacc[18], Macc[36];
-        for (int k = 0; k < 18; ++k) Jacc[k] = 0.0;
-        for (int k = 0; k < 36; ++k) Macc[k] = 0.0;
+        double Jc[3] = {0.0, 0.0, 0.0}, Mc[6] = {0, 0, 0, 0, 0, 0};
         for (int it = 0; it < a.iters; ++it) {
             const double *tr = a.trace + kTraceWords * ((size_t)it * a.nc + c);
-            const double ub[3] = {tr[15], tr[16], tr[17]};
-            for (int r = 0; r < 3; ++r)
-                for (int k = 0; k < 6; ++k) Jacc[6 * r + k] += ub[r] * tr[vo + k];
+            const double ub[3] = {tr[15], tr[16], tr[17]}, vk = tr[vo + k];
+            for (int r = 0; r < 3; ++r) Jc[r] += ub[r] * vk;
             if (!d) continue;
             const double dl[3] = {tr[18], tr[19], tr[20]};
-            double w[6], m[6];
-            for (int k = 0; k < 6; ++k) w[k] = tr[wo + k];
-            for (int k = 0; k < 6; ++k) {
-                double sacc = 0.0;
-                for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
-                m[k] = sacc;
+            double w[6], mk = 0.0;
+            for (int j = 0; j < 6; ++j) {
+                w[j] = tr[wo + j];
+                mk += M[6 * k + j] * w[j];
             }
-            for (int r = 0; r < 3; ++r)
-                for (int k = 0; k < 6; ++k) Jacc[6 * r + k] += dl[r] * m[k];
-            for (int k = 0; k < 6; ++k) {
-                const double jt = (J[k] * dl[0] + J[6 + k] * dl[1]) + J[12 + k] * dl[2];
-                for (int i = 0; i < 6; ++i) Macc[6 * i + k] += w[i] * jt;
-            }
+            for (int r = 0; r < 3; ++r) Jc[r] += dl[r] * mk;
+            const double jt = (J[k] * dl[0] + J[6 + k] * dl[1]) + J[12 + k] * dl[2];
+            for (int i = 0; i < 6; ++i) Mc[i] += w[i] * jt;
         }
         double *Jbar = (side == 0 ? a.Ja_b : a.Jb_b) + 18 * (size_t)c;
-        if (!d) {
-            for (int k = 0; k < 18; ++k) Jbar[k] += Jacc[k];
-            continue;
-        }
-        // the start: vbar of the sweeps' initial velocities
-        double w[6], m[6], jt[6];
-        for (int k = 0; k < 6; ++k) w[k] = __ldcg(a.vb + 6 * (size_t)b + k);
-        for (int k = 0; k < 6; ++k) {
-            double sacc = 0.0;
-            for (int j = 0; j < 6; ++j) sacc += M[k * 6 + j] * w[j];
-            m[k] = sacc;
-            jt[k] = (J[k] * lo[0] + J[6 + k] * lo[1]) + J[12 + k] * lo[2];
-        }
-        for (int r = 0; r < 3; ++r) {
-            double sacc = 0.0;
-            for (int k = 0; k < 6; ++k) sacc += J[r * 6 + k] * m[k];
-            jm[r] += sacc;
-        }
-        // WJ = Wbar J (3x6); Jbar += 2 Wbar J Minv, Minv_bar += J^T Wbar J
-        double WJ[3][6];
-        for (int r = 0; r < 3; ++r)
-            for (int k = 0; k < 6; ++k) WJ[r][k] = (Wb[r][0] * J[k] + Wb[r][1] * J[6 + k]) + Wb[r][2] * J[12 + k];
-        for (int r = 0; r < 3; ++r)
-            for (int k = 0; k < 6; ++k) {
+        if (d) {
+            // the start: vbar of the sweeps' initial velocities
+            double w0[6], m0 = 0.0;
+            for (int j = 0; j < 6; ++j) {
+                w0[j] = __ldcg(a.vb + 6 * (size_t)b + j);
+                m0 += M[6 * k + j] * w0[j];
+            }
+            const double jt0 = (J[k] * lo[0] + J[6 + k] * lo[1]) + J[12 + k] * lo[2];
+            for (int r = 0; r < 3; ++r) jm[r] = J[6 * r + k] * m0;
+            // WJ = Wbar J (3x6); Jbar += 2 Wbar J Minv, Minv_bar += J^T Wbar J (column k)
+            double WJ[3][6];
+            for (int r = 0; r < 3; ++r)
+                for (int j = 0; j < 6; ++j) WJ[r][j] = (Wb[r][0] * J[j] + Wb[r][1] * J[6 + j]) + Wb[r][2] * J[12 + j];
+            for (int r = 0; r < 3; ++r) {
                 double sacc = 0.0;
                 for (int j = 0; j < 6; ++j) sacc += WJ[r][j] * M[j * 6 + k];
-                Jbar[6 * r + k] += Jacc[6 * r + k] + lo[r] * m[k] + 2.0 * sacc;
+                Jbar[6 * r + k] += Jc[r] + lo[r] * m0 + 2.0 * sacc;
             }
-        double *Mb = a.Minv_b + 36 * (size_t)b;
-        for (int i = 0; i < 6; ++i)
-            for (int k = 0; k < 6; ++k) {
+            double *Mb = a.Minv_b + 36 * (size_t)b;
+            for (int i = 0; i < 6; ++i) {
                 const double jwj = (J[i] * WJ[0][k] + J[6 + i] * WJ[1][k]) + J[12 + i] * WJ[2][k];
-                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (Macc[6 * i + k] + w[i] * jt[k] + jwj));
+                __stcg(Mb + 6 * i + k, __ldcg(Mb + 6 * i + k) + (Mc[i] + w0[i] * jt0 + jwj));
             }
+        } else {
+            for (int r = 0; r < 3; ++r) Jbar[6 * r + k] += Jc[r];
+        }
     }
-    for (int k = 0; k < 3; ++k) a.gl[3 * (size_t)c + k] += jm[k];
+    for (int r = 0; r < 3; ++r) {
+        double x = jm[r];
+        for (int off = kGroup / 2; off > 0; off >>= 1) x += __shfl_xor_sync(mask, x, off, kGroup);
+        if (l == 0) a.gl[3 * (size_t)c + r] += x;
+    }
 }
 
 template <int kKind>
@@ -1262,7 +1291,7 @@ __device__ __forceinline__ bool adj_barrier(const AdjArgs &a, unsigned int &epoc
 }
 
 template <int kKind>
-__global__ void __launch_bounds__(kSweepThreads) k_adj_sweeps(AdjArgs a)
+__global__ void __launch_bounds__(kAdjThreads) k_adj_sweeps(AdjArgs a)
 {
     const int ncol = a.stats[kNColors];
     const int nb = gridDim.x, nth = gridDim.x * blockDim.x;
@@ -1270,16 +1299,20 @@ __global__ void __launch_bounds__(kSweepThreads) k_adj_sweeps(AdjArgs a)
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned int epoch = 0;
     if (a.trace) {
-        // the recorded sweeps in reverse, then their start; vb carries through
+        // the recorded sweeps in reverse (a group of kGroup lanes per contact, the forward's
+        // task layout), then their start; vb carries through
+        const int groups = nb * (blockDim.x / kGroup);
+        const int g = ((int)threadIdx.x / kGroup) * nb + (int)blockIdx.x, l = (int)threadIdx.x % kGroup;
+        const unsigned mask = 0xFFFFu << (((int)threadIdx.x & 31) & ~(kGroup - 1));
         for (int it = a.iters - 1; it >= 0; --it)
             for (int ci = ncol - 1; ci >= 0; --ci) {
                 const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-                for (int t = tid; t < cnt; t += nth) adj_contact_recorded(a, a.order[s0 + t], it);
+                for (int t = g; t < cnt; t += groups) adj_contact_group(a, a.order[s0 + t], it, l, mask);
                 if (!adj_barrier<kKind>(a, epoch)) return;
             }
         for (int ci = 0; ci < ncol; ++ci) {
             const int s0 = a.cstart[ci], cnt = a.ccount[ci];
-            for (int t = tid; t < cnt; t += nth) adj_start_recorded(a, a.order[s0 + t]);
+            for (int t = g; t < cnt; t += groups) adj_start_group(a, a.order[s0 + t], l, mask);
             if (!adj_barrier<kKind>(a, epoch)) return;
         }
         for (int i = gid; i < 6 * a.nb; i += nth) {
@@ -1362,13 +1395,13 @@ int adjoint_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_par
         int per = 0, dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_sweeps<kGrid>, kSweepThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_sweeps<kGrid>, kAdjThreads, 0);
         const int nblocks = std::min(std::min(mode, kBarrierMaxCTAs), std::max(1, sms * per));
         if (nblocks > 1) {
             cudaMemsetAsync(st->barrier, 0, sizeof(uint32_t), s);
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(nblocks);
-            cfg.blockDim = dim3(kSweepThreads);
+            cfg.blockDim = dim3(kAdjThreads);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeCooperative;
@@ -1383,7 +1416,7 @@ int adjoint_sweeps(const b2c_ncp_scene *sc, b2c_ncp_state *st, const b2c_ncp_par
             return check_launch("ncp_adjoint_grid");
         }
     }
-    k_adj_sweeps<kBlock><<<1, kSweepThreads, 0, s>>>(a);
+    k_adj_sweeps<kBlock><<<1, kAdjThreads, 0, s>>>(a);
     return check_launch("ncp_adjoint");
 }
 

@@ -113,6 +113,9 @@ WORKLOADS = {
     # per-body mu; central differences with eps 1e-3 on the same float64 forward
     "pyramids256_rollout": dict(engine="rollout", n_scenes=256, rollout_steps=120, substeps=2, iters=16,
                                 dt=1 / 240, fd_eps=1e-3, steps=1, warmup=3),
+    # a short case of the same rollout (32 scenes, 10 steps): the profiling case of its kernels
+    "pyramids32_rollout10": dict(engine="rollout", n_scenes=32, rollout_steps=10, substeps=2, iters=16,
+                                 dt=1 / 240, fd_eps=1e-3, steps=1, warmup=3),
 }
 DEFAULT_WORKLOAD = "boxes10k"
 
