@@ -113,3 +113,34 @@ def test_large_batch_converges(bn):
     for e in (0, 1, 2, 4095):
         ref, _ = OB.pgs(G[e].cpu().numpy(), b[e].cpu().numpy(), mu[e].cpu().numpy(), 20000, 1e-14)
         assert np.max(np.abs(lam[e].cpu().numpy() - ref)) < 1e-9
+
+
+def test_stance_batch_matches_oracle(bn, oracle_mod):
+    """The shape of the batched-adjoint workload (legged stance: a floating base and 4 legs of 3
+    joints, nv = 18, 4 contacts, sliding, mu 0.5), 64 problems: the solve and a vector-Jacobian
+    product against the oracle's PGS and fixed-branch VJP, problem by problem."""
+    import torch
+    from importlib import import_module
+    from oracle import oracle_bncp as OB
+    S = import_module("motion_engine_b200.scenes")
+    J, Minv, vf, mu = S.stance_batch(B=64, nv=18, nc=4, mu=0.5)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    G, b = bn.delassus(t(J), t(Minv), t(vf))
+    w = t(np.random.default_rng(2).normal(size=tuple(b.shape)))
+    bb, mm = b.clone().requires_grad_(True), t(mu).requires_grad_(True)
+    lam = bn.ncp_solve(G, bb, mm, 20000, 1e-14)
+    (lam * w).sum().backward()
+    lam, gb, gm = lam.detach().cpu().numpy(), bb.grad.cpu().numpy(), mm.grad.cpu().numpy()
+    Gh, bh = G.cpu().numpy(), b.cpu().numpy()
+    checked = 0
+    for e in range(64):
+        ref, _ = OB.pgs(Gh[e], bh[e], mu[e], 20000, 1e-14)
+        assert np.max(np.abs(lam[e] - ref)) < 1e-9, e
+        dmu, db, _, status = OB.sensitivity(ref, Gh[e], bh[e], mu[e])
+        if status:  # a singular or boundary branch: no derivative (NaN in both)
+            continue
+        we = w[e].cpu().numpy()
+        ob, om = db.T @ we, dmu.T @ we
+        assert _rel(gb[e], ob) < 1e-7 and _rel(gm[e], om) < 1e-7, e
+        checked += 1
+    assert checked >= 48
