@@ -42,7 +42,7 @@ class Pairs(ctypes.Structure):
                 ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
                 ("body_colors", c_void_p), ("body_local", c_void_p), ("body_slots", c_void_p),
                 ("n_scenes", c_int32), ("scene_body_start", c_void_p), ("scene_order", c_void_p),
-                ("pair_slot", c_void_p), ("scene_slots", c_void_p)]
+                ("pair_slot", c_void_p), ("scene_slots", c_void_p), ("prio_hi", c_void_p)]
 
 
 SOLVE_SCENES = 0x100000  # b2c_color_params.solve_blocks: one CTA per scene (B2C_SOLVE_SCENES)
@@ -113,6 +113,7 @@ COLOR_WARM_START = 8
 COLOR_PER_CONTACT = 16
 COLOR_FIRST_FIT = 32
 COLOR_ROW_FORM = 64
+COLOR_REDUCED_CONTACTS = 128
 
 
 class Grid(ctypes.Structure):

@@ -2,9 +2,11 @@
 
 Mirrors of the reference's coloured engine family behind the ContactEngine protocol:
 
-* GraphColoredContactEngine  -- contact_engine_gpu_colored.py:793-1410.  Supported solve paths:
-  the plain per-contact colouring (manifold_reduce=False) and the pair-chunk path
-  (manifold_reduce=True, pair_chunks=True).  chunk_mode 'registers' and 'global' give the same
+* GraphColoredContactEngine  -- contact_engine_gpu_colored.py:793-1410.  Solve paths: the plain
+  per-contact colouring (manifold_reduce=False), the reduced set coloured contact by contact
+  (manifold_reduce=True, pair_chunks=False: the device manifold's priority, COL:776-787, 1105-1113)
+  and the pair-chunk path (manifold_reduce=True, pair_chunks=True).  chunk_mode 'registers' and
+  'global' give the same
   states in the reference and are one kernel here; manifold_on_host selects the same points as
   the device path, so it runs the device path.
 * FixedFrameContactEngine    -- contact_engine_gpu_fixed_frame.py:82-88 (normal-derived frame).
@@ -52,9 +54,6 @@ class GraphColoredContactEngine(_BeadEngineBase):
                 raise ValueError("contact_engine_gpu_colored: pair_chunks=True needs the device manifold "
                                  "reduction (manifold_reduce=True, manifold_on_host=False): a chunk is the "
                                  "<= manifold_max_points contacts of one body pair")
-        if manifold_reduce and not pair_chunks:
-            raise NotImplementedError("manifold_reduce without pair_chunks (per-contact colouring of the reduced "
-                                      "set) is not built; use pair_chunks=True or manifold_reduce=False")
         if not 1 <= int(manifold_max_points) <= 8:
             raise ValueError("manifold_max_points must be in 1..8")
         super().__init__(dims=dims, mu=mu, device=device, graph=True)
@@ -90,6 +89,8 @@ class GraphColoredContactEngine(_BeadEngineBase):
             f |= _lib.COLOR_WARM_START
         if not self.manifold_reduce:
             f |= _lib.COLOR_PER_CONTACT
+        elif not self.pair_chunks:
+            f |= _lib.COLOR_REDUCED_CONTACTS
         return f
 
     def _build(self):
@@ -105,8 +106,9 @@ class GraphColoredContactEngine(_BeadEngineBase):
         i64 = lambda n: torch.zeros(max(int(n), 1), dtype=torch.int64, device=dev)
         # body pairs: with the manifold reduction a pair keeps <= max_points contacts and the pair
         # graph of boxes is sparse (a few partners per body); the plain engine colours contacts
-        pcap = min(cap, 8 * N + 4096) if self.manifold_reduce else cap
-        kslots = self.manifold_max_points if self.manifold_reduce else 1
+        chunks = self.manifold_reduce and self.pair_chunks
+        pcap = min(cap, 8 * N + 4096) if chunks else cap
+        kslots = self.manifold_max_points if chunks else 1
         # kept contacts (feature order) and their keys
         self.k_bi, self.k_bj, self.k_fa, self.k_fb = i32(cap), i32(cap), i32(cap), i32(cap)
         self.k_pA, self.k_pB, self.k_n, self.k_imp = (torch.zeros((cap, 4), dtype=torch.float32, device=dev)
@@ -130,11 +132,13 @@ class GraphColoredContactEngine(_BeadEngineBase):
                            col=i32(pcap), porder=i32(pcap), cstart=i32(NCOLMAX), ccount=i32(NCOLMAX), claim=i64(2 * N),
                            cached_a=i32(pcap), cached_b=i32(pcap), cached_mass=f32(N), cache_state=i32(8),
                            barrier=torch.zeros(int(self.L.b2c_barrier_words()), dtype=torch.int32, device=dev),
-                           rec=f32(self.L.b2c_pair_record_floats(pcap, kslots)))
+                           rec=f32(self.L.b2c_pair_record_floats(pcap, kslots)), prio_hi=i32(pcap))
         pb = self.p_bufs
         self.c_pairs = _lib.Pairs(pcap, NCOLMAX, *(_ptr(pb[k]) for k in (
             "pbi", "pbj", "kcount", "pstart", "pidx", "col", "porder", "cstart", "ccount", "claim", "cached_a",
             "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots)
+        if self.manifold_reduce and not self.pair_chunks:
+            self.c_pairs.prio_hi = _ptr(pb["prio_hi"])
         # warm store
         self.w_keys, self.w_imp, self.w_n = i64(cap), torch.zeros((cap, 4), dtype=torch.float32, device=dev), i32(1)
         self.c_warm = _lib.Warm(cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))

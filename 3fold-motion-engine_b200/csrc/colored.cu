@@ -338,6 +338,56 @@ __global__ void k_select(const b2c_header *__restrict__ hdr, int mx, const int *
 
 __global__ void k_set_kept(b2c_header *hdr, const int *__restrict__ kidx) { hdr->n_kept = kidx[hdr->n_contacts]; }
 
+// The reduced set coloured contact by contact (COL:1105-1113 with the device manifold's priority,
+// k_prio_manifold, COL:776-787): every kept contact is a chunk of one, and runs of consecutive
+// kept contacts (feature order) of the same body pair are flagged for the priority.
+__global__ void k_kept_chunks(b2c_header *hdr, int cap, int pcap, b2c_contacts kept, int *__restrict__ pbi,
+                              int *__restrict__ pbj, int *__restrict__ kcount, int *__restrict__ pstart,
+                              int *__restrict__ pidx, int *__restrict__ runflag)
+{
+    const int Ck = hdr->n_kept;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        hdr->n_pairs = Ck < pcap ? Ck : pcap;
+        if (Ck > pcap) atomicOr(&hdr->error, B2C_ERR_PAIR_OVERFLOW);
+    }
+    for (int i = tid; i <= cap; i += gridDim.x * blockDim.x) {
+        if (i >= Ck || i >= pcap) {
+            runflag[i] = 0;
+            continue;
+        }
+        const int a = kept.bi[i], b = kept.bj[i];
+        pbi[i] = a;
+        pbj[i] = b;
+        kcount[i] = 1;
+        pstart[i] = i;
+        pidx[i] = i;
+        runflag[i] = (i == 0 || a != kept.bi[i - 1] || b != kept.bj[i - 1]) ? 1 : 0;
+    }
+}
+
+// first kept contact of each run (runs counted by the exclusive scan of the flags)
+__global__ void k_kept_runstart(const b2c_header *__restrict__ hdr, int pcap, const int *__restrict__ runflag,
+                                const int *__restrict__ runscan, int *__restrict__ runstart)
+{
+    const int Ck = min(hdr->n_kept, pcap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Ck; i += gridDim.x * blockDim.x)
+        if (runflag[i]) runstart[runscan[i]] = i;
+}
+
+// priority high part: the slot inside the run (at most 255), then the run's parity; the pair
+// index (= the kept rank) follows in claim_key, so the order is k_prio_manifold's
+__global__ void k_kept_prio(const b2c_header *__restrict__ hdr, int pcap, const int *__restrict__ runflag,
+                            const int *__restrict__ runscan, const int *__restrict__ runstart, int *__restrict__ prio_hi)
+{
+    const int Ck = min(hdr->n_kept, pcap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Ck; i += gridDim.x * blockDim.x) {
+        const int g = runscan[i] + runflag[i] - 1;
+        const int slot = min(i - runstart[g], 255);
+        prio_hi[i] = (slot << 19) | ((g & 1) << 18);
+    }
+}
+
 // plain coloured engine (COL:903-936, 1105-1137): every contact kept, one contact per chunk,
 // warm impulses uploaded as float32 (COL:931-936)
 __global__ void k_per_contact(b2c_header *hdr, long long stride, b2c_contacts c, const double *__restrict__ jn_in,
@@ -447,8 +497,10 @@ __device__ __forceinline__ unsigned long long claim_key(int p, int r, unsigned l
 // index.  With body_local (the box engine): a hash of the pair's two scene-local body indices,
 // so the colouring of a scene does not depend on where its pairs sit in a batch of scenes (ties
 // fall back to the pair index, whose order inside a scene is the same either way).
-__device__ __forceinline__ unsigned long long pair_hash(int p, int a, int b, const int *__restrict__ body_local)
+__device__ __forceinline__ unsigned long long pair_hash(int p, int a, int b, const int *__restrict__ body_local,
+                                                        const int *__restrict__ prio_hi)
 {
+    if (prio_hi) return (unsigned long long)(unsigned)prio_hi[p];  // B2C_COLOR_REDUCED_CONTACTS
     if (body_local) {
         const unsigned long long key = ((unsigned long long)(unsigned)(body_local[a] + 1) << 32) |
                                        (unsigned long long)(unsigned)(b >= 0 ? body_local[b] + 1 : 0);
@@ -476,7 +528,7 @@ struct JPPair {
 __device__ __forceinline__ JPPair jp_pair(int p, const b2c_pairs &pr, const float *__restrict__ invM)
 {
     const int a = pr.pbi[p], b = pr.pbj[p];
-    const unsigned long long h = pair_hash(p, a, b, pr.body_local);
+    const unsigned long long h = pair_hash(p, a, b, pr.body_local, pr.prio_hi);
     JPPair q;
     q.bi = invM[a] > 0.0f ? a : -1;
     q.bj = (b >= 0 && invM[b] > 0.0f) ? b : -1;
@@ -876,6 +928,21 @@ int manifold_reduce(const b2c_bodies *b, const b2c_beads *beads, const b2c_conta
     k_compact<<<cgrid, kThreads, 0, s>>>(hdr, stride, *c, m->keep, m->kidx, m->jn_red,
                                          reinterpret_cast<const float2 *>(m->jt_in), *kept,
                                          reinterpret_cast<long long *>(kept_keys));
+    if (p->flags & B2C_COLOR_REDUCED_CONTACTS) {
+        // every kept contact its own chunk; keep / kidx / gorder are free after the compaction
+        if (!pr->prio_hi || pcap < cap) {
+            set_error("manifold_reduce: B2C_COLOR_REDUCED_CONTACTS needs pairs->prio_hi and a pair capacity of "
+                      "one per contact");
+            return B2C_EARG;
+        }
+        k_kept_chunks<<<cgrid, kThreads, 0, s>>>(hdr, cap, pcap, *kept, pr->pbi, pr->pbj, pr->kcount, pr->pstart,
+                                                 pr->pidx, m->keep);
+        if ((rc = check_launch("kept_chunks"))) return rc;
+        if ((rc = exclusive_scan(m->keep, m->kidx, cap + 1, nullptr, m->scan_tmp, s))) return rc;
+        k_kept_runstart<<<cgrid, kThreads, 0, s>>>(hdr, pcap, m->keep, m->kidx, m->gorder);
+        k_kept_prio<<<cgrid, kThreads, 0, s>>>(hdr, pcap, m->keep, m->kidx, m->gorder, pr->prio_hi);
+        return check_launch("manifold_reduce");
+    }
     if ((rc = exclusive_scan(pr->kcount, pr->pstart, pcap + 1, &hdr->n_pairs, m->scan_tmp, s))) return rc;
     k_pair_kept<<<pgrid, kThreads, 0, s>>>(hdr, m->praw_start, m->praw_count, m->gorder, m->keep, m->kidx,
                                            pr->pstart, pr->pidx, pr->kcount, hdr);

@@ -201,6 +201,9 @@ typedef struct b2c_pairs {
     const int32_t *scene_order;      /* (n_scenes) launch order of the scenes (largest first), or NULL */
     int32_t *pair_slot;              /* (capacity) record slot of each pair, written by the gather */
     int32_t *scene_slots;            /* (capacity) each scene's record slots grouped by colour */
+    int32_t *prio_hi;                /* (capacity) or NULL: with B2C_COLOR_REDUCED_CONTACTS the
+                                        high part of each chunk's colouring priority (slot << 19 |
+                                        run parity << 18), written by b2c_manifold_reduce */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -260,6 +263,13 @@ typedef struct b2c_boxes {
                                      needs B2C_COLOR_FIXED_FRAME.  The box engine's default. */
 #define B2C_COLOR_PER_CONTACT 16 /* no manifold reduction; every contact is its own chunk and is
                                     coloured on the contact graph (the plain coloured engine) */
+#define B2C_COLOR_REDUCED_CONTACTS 128 /* the manifold reduction, then every kept contact is its own
+                                    chunk, coloured with the reduced set's priority (COL:776-787:
+                                    its slot inside its run of one body pair, then the parity of
+                                    that run, then its rank; the smaller first) -- the reference's
+                                    GraphColoredContactEngine(manifold_reduce=True,
+                                    pair_chunks=False).  Needs b2c_pairs.prio_hi and a pair
+                                    capacity of one per contact. */
 
 #define B2C_SOLVE_SCENES 0x100000 /* b2c_color_params.solve_blocks: the scene schedule */
 

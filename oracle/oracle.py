@@ -269,6 +269,9 @@ class ColoredOracle:
         pair_chunks=True) -- contact_engine_gpu_colored.py:793-1410, slip-basis chunk sweep.
     mode="plain": GraphColoredContactEngine() -- per-contact colouring, no manifold reduction
         (contact_engine_gpu_colored.py:903-936, 1105-1137, 188-320).
+    mode="reduced": GraphColoredContactEngine(manifold_reduce=True) -- the device manifold
+        reduction, then the kept contacts coloured one by one with k_prio_manifold's priority
+        (contact_engine_gpu_colored.py:776-787, 1105-1113).
     mode="color_cache": ColorCacheContactEngine -- contact_engine_gpu_color_cache.py:21-54 on top of
         DeferredForce / AppliedWarm / FixedFrame (fixed tangent frame, warm impulses applied once per
         colour before the sweeps, colouring reused while the pair graph and masses are unchanged).
@@ -276,7 +279,7 @@ class ColoredOracle:
 
     def __init__(self, mode="color_cache", dims=(0.3, 0.3, 0.2), vit=40, pit=20, mu=0.5, max_points=4,
                  t2_damp=1.0, cap=MAXC, precision="float32"):
-        assert mode in ("pair_chunks", "color_cache", "plain")
+        assert mode in ("pair_chunks", "color_cache", "plain", "reduced")
         self.mode = mode
         self.precision = precision
         self.F, self.L = _precision(precision)
@@ -306,7 +309,8 @@ class ColoredOracle:
         self.vgrav = np.zeros((N, 3), self.F)
         if self._h:
             L.or_col_destroy(self._h)
-        self._h = L.or_col_create({"pair_chunks": 0, "color_cache": 1, "plain": 2}[self.mode], self.vit, self.pit,
+        self._h = L.or_col_create({"pair_chunks": 0, "color_cache": 1, "plain": 2, "reduced": 3}[self.mode], self.vit,
+                                  self.pit,
                                   self.mx, self.mu,
                                   self.t2d, self.cap, N)
 

@@ -868,14 +868,17 @@ static int64_t local_priority(int p, int a, int b, const int *local)
 }
 
 static int color_pairs(col_engine_t *e, int P, int N, const int *pbi, const int *pbj, const float *invM,
-                       int first_fit, const int *local)
+                       int first_fit, const int *local, const int64_t *given)
 {
     int *col = malloc(sizeof(int) * (P > 0 ? P : 1));
     uint64_t *used = calloc((size_t)(N > 0 ? N : 1), sizeof(uint64_t));
     int ncol_ff = 0;
     int64_t *key = malloc(sizeof(int64_t) * (P > 0 ? P : 1));
     int64_t *claim = malloc(sizeof(int64_t) * (N > 0 ? N : 1));
-    for (int p = 0; p < P; ++p) { col[p] = -1; key[p] = local ? local_priority(p, pbi[p], pbj[p], local) : jp_priority(p); }
+    for (int p = 0; p < P; ++p) {
+        col[p] = -1;
+        key[p] = given ? given[p] : local ? local_priority(p, pbi[p], pbj[p], local) : jp_priority(p);
+    }
     int cur = 0;
     for (;;) {
         for (int i = 0; i < N; ++i) claim[i] = INT64_MAX;
@@ -1228,16 +1231,17 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
             e->n_kept = Ck;
             memset(pv, 0, sizeof(float) * 3 * N); memset(po, 0, sizeof(float) * 3 * N);
             /* C7: pairs over the kept contacts (COL:1158-1176, 341-389); in the plain engine every
-             * contact is coloured on its own (COL:1105-1137), i.e. a one-contact chunk */
+             * contact is coloured on its own (COL:1105-1137), i.e. a one-contact chunk, and so is
+             * every kept contact of the reduced set without pair chunks (mode 3) */
             int P = 0;
-            if (e->mode == 2) {
+            if (e->mode == 2 || e->mode == 3) {
                 for (int i = 0; i < Ck; ++i) { pidx[i] = i; pstart[i] = i; pcount[i] = 1; pbi[i] = sbi[i]; pbj[i] = sbj[i]; }
                 P = Ck;
             } else {
                 for (int i = 0; i < Ck; ++i) keys[i] = (int64_t)sbi[i] * (int64_t)(N + 1) + (int64_t)sbj[i] + 1;
                 argsort_stable(keys, Ck, pidx);
             }
-            for (int i = 0; i < Ck && e->mode != 2;) {
+            for (int i = 0; i < Ck && e->mode != 2 && e->mode != 3;) {
                 int L = 1;
                 while (i + L < Ck && keys[pidx[i + L]] == keys[pidx[i]]) L++;
                 if (L > 8) { rc = 2; L = 8; }
@@ -1260,7 +1264,22 @@ OR_API int or_col_step(void *h, int N, int nbead, const float *rest, const int *
                 ncol = e->cached_colors;
                 e->hits++;
             } else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM, 0, NULL);
+                /* mode 3 (the reduced set, contact by contact): k_prio_manifold's priority,
+                 * COL:776-787 -- the slot inside the run of one body pair (kept contacts in
+                 * feature order), then the run's parity, then the rank */
+                int64_t *given = NULL;
+                if (e->mode == 3) {
+                    given = malloc(sizeof(int64_t) * (P > 0 ? P : 1));
+                    int g = -1, start = 0;
+                    for (int i = 0; i < P; ++i) {
+                        if (i == 0 || sbi[i] != sbi[i - 1] || sbj[i] != sbj[i - 1]) { g++; start = i; }
+                        int64_t slot = i - start < 255 ? i - start : 255;
+                        int64_t rank = (int64_t)i < 1099511627775LL ? (int64_t)i : 1099511627775LL;
+                        given[i] = (slot << 48) | ((int64_t)(g % 2) << 40) | rank;
+                    }
+                }
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, 0, NULL, given);
+                free(given);
                 e->has_colors = 1;
                 if (e->mode == 1) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);
@@ -1880,7 +1899,7 @@ OR_API int or_box_step(void *h, int flags, int N, const float *half, const float
             }
             if (hit) { ncol = e->cached_colors; e->hits++; }
             else {
-                ncol = color_pairs(e, P, N, pbi, pbj, invM, (flags & 32) ? 1 : 0, local);
+                ncol = color_pairs(e, P, N, pbi, pbj, invM, (flags & 32) ? 1 : 0, local, NULL);
                 e->has_colors = 1;
                 if (flags & 4) {
                     memcpy(e->cached_a, pbi, sizeof(int) * P); memcpy(e->cached_b, pbj, sizeof(int) * P);

@@ -28,6 +28,8 @@ def _make(me, engine, **kw):
         return me.ColorCacheContactEngine(**kw)
     if engine == "pair_chunks":
         return me.GraphColoredContactEngine(manifold_reduce=True, graph_capture=True, pair_chunks=True, **kw)
+    if engine == "reduced":
+        return me.GraphColoredContactEngine(manifold_reduce=True, **kw)
     return me.GraphColoredContactEngine(**kw)
 
 
@@ -68,7 +70,7 @@ def _random_scene(seed, n_cols=3):
     return centers, dens
 
 
-@pytest.mark.parametrize("engine", ["color_cache", "pair_chunks", "plain"])
+@pytest.mark.parametrize("engine", ["color_cache", "pair_chunks", "plain", "reduced"])
 def test_colored_matches_oracle(engine, me, oracle_mod):
     """Jittered columns with mixed densities and two substeps: bit-exact against the oracle."""
     centers, dens = _random_scene(3)
@@ -142,7 +144,7 @@ def test_set_solve_blocks_mid_run_keeps_bits(me):
 
 def test_contract_checks(me):
     """contact_engine_gpu_colored.py:1414-1515 on the engines built here."""
-    for engine in ("plain", "pair_chunks", "color_cache"):
+    for engine in ("plain", "pair_chunks", "color_cache", "reduced"):
         e = _make(me, engine)
         assert isinstance(e, me.ContactEngine)
         for c in stack(8):
@@ -154,7 +156,7 @@ def test_contract_checks(me):
         zs = sorted(st.xc[:, 2])
         seps = [zs[i + 1] - zs[i] for i in range(7)]
         assert ke < 0.5 and all(0.15 < s < 0.25 for s in seps), engine
-        if engine != "plain":
+        if engine in ("pair_chunks", "color_cache"):
             assert e.n_colors < 8
         e2 = _make(me, engine)
         e2.add_body([0, 0, 0.101])

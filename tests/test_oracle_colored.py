@@ -104,3 +104,24 @@ def test_oracle_m5_stack16_against_receipt(oracle_mod):
     q = metrics.m5(pens)
     assert q["status"] == "PASS"
     assert abs(q["max_pen_over_R"] - 0.19563645124435425) < 0.05 * 0.19563645124435425, q
+
+
+def test_oracle_reduced_set_keeps_m5_on_the_k8_stack(oracle_mod):
+    """GraphColoredContactEngine(manifold_reduce=True) without pair chunks: the reduced set coloured
+    contact by contact.  The reference picks vit = 40 for this path as "the lowest of the sweep at
+    which the reduced K=8 stack keeps M5" (contact_engine_gpu_colored.py:801-802); the restated
+    path keeps M5 there too."""
+    import importlib
+    import __graft_entry__ as ge
+    ge.load_package()
+    metrics = importlib.import_module("motion_engine_b200.metrics")
+    e = oracle_mod.ColoredOracle(mode="reduced", dims=DIMS, mu=0.5, vit=40, pit=20)
+    for k in range(8):
+        e.add_body([0, 0, 0.101 + k * 0.205])
+    pens = []
+    for _ in range(600):
+        e.step(DT, 1)
+        z = np.sort(e.get_state().xc[:, 2])
+        pens.append(float(np.max(np.float32(0.205) - np.diff(z))))
+    q = metrics.m5(pens)
+    assert q["status"] == "PASS", q
