@@ -11,10 +11,11 @@ The directory name is not a Python identifier, so the package is imported under 
 from . import _lib, build, metrics
 from .boxes import BatchedBoxEngine, BoxContactEngine, autotune, partition_scenes
 from .colored import (AppliedWarmContactEngine, ColorCacheContactEngine, DeferredForceContactEngine,
-                      FixedFrameContactEngine, GraphColoredContactEngine)
+                      FixedFrameContactEngine, GraphColoredContactEngine, IslandSolveContactEngine)
 from .engine import BodyState, ContactEngine, RelaxedJacobiContactEngine, quat_to_R, voxbox
 from .handle import HandleBoxEngine
+from .islands import partition_pairs
 
 __all__ = ["BodyState", "ContactEngine", "RelaxedJacobiContactEngine", "GraphColoredContactEngine",
            "FixedFrameContactEngine", "AppliedWarmContactEngine", "DeferredForceContactEngine",
-           "ColorCacheContactEngine", "BoxContactEngine", "BatchedBoxEngine", "HandleBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "metrics", "_lib"]
+           "ColorCacheContactEngine", "IslandSolveContactEngine", "partition_pairs", "BoxContactEngine", "BatchedBoxEngine", "HandleBoxEngine", "autotune", "partition_scenes", "quat_to_R", "voxbox", "build", "metrics", "_lib"]

@@ -42,7 +42,7 @@ class Pairs(ctypes.Structure):
                 ("cache_state", c_void_p), ("barrier", c_void_p), ("rec", c_void_p), ("kslots", c_int32),
                 ("body_colors", c_void_p), ("body_local", c_void_p), ("body_slots", c_void_p),
                 ("n_scenes", c_int32), ("scene_body_start", c_void_p), ("scene_order", c_void_p),
-                ("pair_slot", c_void_p), ("scene_slots", c_void_p), ("prio_hi", c_void_p)]
+                ("pair_slot", c_void_p), ("scene_slots", c_void_p), ("prio_hi", c_void_p), ("isl_work", c_void_p)]
 
 
 SOLVE_SCENES = 0x100000  # b2c_color_params.solve_blocks: one CTA per scene (B2C_SOLVE_SCENES)
@@ -114,6 +114,8 @@ COLOR_PER_CONTACT = 16
 COLOR_FIRST_FIT = 32
 COLOR_ROW_FORM = 64
 COLOR_REDUCED_CONTACTS = 128
+COLOR_ISLANDS = 256
+ISLAND_MAX_PAIRS = 64  # B2C_ISLAND_MAX_PAIRS
 
 
 class Grid(ctypes.Structure):
@@ -182,6 +184,9 @@ _SIGS = {
     "b2c_color_solve": ([_P(Bodies), _P(Contacts), _P(Pairs), c_void_p, _P(ColorParams), c_float, c_void_p],
                         c_int32),
     "b2c_warm_store": ([_P(Contacts), c_void_p, _P(Warm), c_void_p, c_void_p], c_int32),
+    "b2c_island_work_ints": ([c_int32, c_int32], ctypes.c_int64),
+    "b2c_island_partition": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p], c_int32),
     "b2c_color_substep": ([_P(Bodies), _P(Beads), _P(Grid), _P(Contacts), _P(Manifold), _P(Contacts), c_void_p,
                            _P(Pairs), _P(Warm), c_void_p, _P(ColorParams), c_float, c_void_p, c_void_p], c_int32),
     "b2c_box_candidates": ([_P(Bodies), _P(Boxes), c_void_p, c_void_p], c_int32),

@@ -15,6 +15,9 @@ Mirrors of the reference's coloured engine family behind the ContactEngine proto
 * DeferredForceContactEngine -- contact_engine_gpu_deferred_force.py:7-74.
 * ColorCacheContactEngine    -- contact_engine_gpu_color_cache.py:21-54 (colouring reused while
   the pair graph and the masses are unchanged).
+* IslandSolveContactEngine   -- contact_engine_gpu_island_solve.py:253-287 (the pair graph split
+  into islands of dynamic bodies; one thread per island runs its sweeps when no island has more
+  than 64 pairs).
 
 A whole step (every substep: prediction, bead grid, contacts in feature order, manifold
 reduction, pairs, colouring, the persistent chunk solve, warm store, integration) is one fixed
@@ -39,6 +42,7 @@ class GraphColoredContactEngine(_BeadEngineBase):
     _fixed_frame = False
     _apply_warm = False
     _color_cache = False
+    _islands = False
 
     def __init__(self, dims=(0.3, 0.3, 0.2), vit=None, pit=20, mu=0.5, warm_start=True, t2_damp=1.0,
                  manifold_reduce=False, manifold_max_points=4, manifold_on_host=False, profile=False,
@@ -85,6 +89,8 @@ class GraphColoredContactEngine(_BeadEngineBase):
             f |= _lib.COLOR_APPLY_WARM
         if self._color_cache:
             f |= _lib.COLOR_CACHE
+        if self._islands:
+            f |= _lib.COLOR_ISLANDS
         if self.warm_start:
             f |= _lib.COLOR_WARM_START
         if not self.manifold_reduce:
@@ -139,6 +145,9 @@ class GraphColoredContactEngine(_BeadEngineBase):
             "cached_b", "cached_mass", "cache_state", "barrier", "rec")), kslots)
         if self.manifold_reduce and not self.pair_chunks:
             self.c_pairs.prio_hi = _ptr(pb["prio_hi"])
+        if self._islands:
+            pb["isl_work"] = i32(self.L.b2c_island_work_ints(N, pcap))
+            self.c_pairs.isl_work = _ptr(pb["isl_work"])
         # warm store
         self.w_keys, self.w_imp, self.w_n = i64(cap), torch.zeros((cap, 4), dtype=torch.float32, device=dev), i32(1)
         self.c_warm = _lib.Warm(cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
@@ -297,3 +306,42 @@ class ColorCacheContactEngine(DeferredForceContactEngine):
     device (contact_engine_gpu_color_cache.py:21-54)."""
     name = "color_cache_b200"
     _color_cache = True
+
+
+class IslandSolveContactEngine(ColorCacheContactEngine):
+    """The ColorCache engine with the island solve (contact_engine_gpu_island_solve.py:253-287).
+
+    The reference partitions the pairs on the host after each colour-cache miss
+    (``partition_pairs``) and runs one thread per island when the largest island has at most 64
+    pairs, else the coloured chunk launch.  Here the partition runs on the device inside the
+    captured step (skipped on a colour-cache hit), and the choice between the island solve and
+    the persistent colour-phase solve is made on the device.  Both give the ColorCache engine's
+    bits."""
+    name = "island_solve_b200"
+    _islands = True
+
+    def _island_info(self):
+        if not self._built:
+            return (0, 0)
+        info = self.p_bufs["isl_work"][:2].cpu().numpy()
+        return int(info[0]), int(info[1])
+
+    @property
+    def island_count(self):
+        """Islands of the last partition."""
+        return self._island_info()[0]
+
+    @property
+    def max_island_pairs(self):
+        """Pairs of the largest island of the last partition."""
+        return self._island_info()[1]
+
+    @property
+    def island_rebuilds(self):
+        """Partitions computed: one per colour-cache miss, as in the reference."""
+        return self.color_cache_misses
+
+    @property
+    def island_solve_active(self):
+        """True when the last substep ran the island solve (no island above 64 pairs)."""
+        return self._built and self.max_island_pairs <= _lib.ISLAND_MAX_PAIRS

@@ -83,7 +83,16 @@ struct SolveArgs {
     int vit, pit, fixed_frame, apply_warm, row;
     unsigned int *bar_count;  // the grid barrier's arrival counter
     long long timeout_ns;
+    const int *island_info;   // the island partition's statistics (B2C_COLOR_ISLANDS) or NULL
 };
+
+// The island solve ran this substep (its partition has no island above B2C_ISLAND_MAX_PAIRS
+// pairs): the persistent forms have nothing to do.  Every thread of every CTA reads the same
+// word, written by an earlier launch, so the early return is uniform.
+__device__ __forceinline__ bool islands_took_solve(const SolveArgs &a)
+{
+    return a.island_info && a.island_info[1] <= B2C_ISLAND_MAX_PAIRS;
+}
 
 // ---------------------------------------------------------------------------------------------
 // gather (once per substep) and scatter
@@ -353,10 +362,14 @@ __device__ __forceinline__ float4 *stage_word(int f, int j)
 {
     return s_stage + ((f * kRowBatch + j) * (int)blockDim.x + (int)threadIdx.x);
 }
+// kL1: the copy allocates in L1 (cp.async.ca), for a kernel whose thread re-reads the same
+// records many times and is the only one that writes them (the island solve); otherwise L2 only.
+template <bool kL1 = false>
 __device__ __forceinline__ void cp_async16(float4 *dst, const float4 *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+    if (kL1) asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all()
 {
@@ -366,16 +379,17 @@ __device__ __forceinline__ void cp_async_wait_all()
 // issue the copies of contacts k0 .. k0 + kRowBatch - 1 of slot s (those below the slot count
 // K; a slot beyond the pair's count holds stale words that are never read); the position chunk
 // skips t1
+template <bool kL1 = false>
 __device__ __forceinline__ void stage_rows(const Records &R, int s, int k0, bool pos)
 {
 #pragma unroll
     for (int j = 0; j < kRowBatch; ++j) {
         if (k0 + j < R.K) {
-            cp_async16(stage_word(kRN, j), &R.contact(kRN, k0 + j)[s]);
-            cp_async16(stage_word(kRRA, j), &R.contact(kRRA, k0 + j)[s]);
-            cp_async16(stage_word(kRRB, j), &R.contact(kRRB, k0 + j)[s]);
-            if (!pos) cp_async16(stage_word(kRT1, j), &R.contact(kRT1, k0 + j)[s]);
-            cp_async16(stage_word(kRImp, j), &R.contact(kRImp, k0 + j)[s]);
+            cp_async16<kL1>(stage_word(kRN, j), &R.contact(kRN, k0 + j)[s]);
+            cp_async16<kL1>(stage_word(kRRA, j), &R.contact(kRRA, k0 + j)[s]);
+            cp_async16<kL1>(stage_word(kRRB, j), &R.contact(kRRB, k0 + j)[s]);
+            if (!pos) cp_async16<kL1>(stage_word(kRT1, j), &R.contact(kRT1, k0 + j)[s]);
+            cp_async16<kL1>(stage_word(kRImp, j), &R.contact(kRImp, k0 + j)[s]);
         }
     }
 }
@@ -397,9 +411,10 @@ struct RowPre {
     float4 mm;
     m3 IA, IB;
 };
+template <bool kL1 = false>
 __device__ __forceinline__ RowPre row_pre(const Records &R, int s, bool pos)
 {
-    stage_rows(R, s, 0, pos);
+    stage_rows<kL1>(R, s, 0, pos);
     RowPre q;
     q.h = R.hdr()[s];
     q.mm = R.body(6)[s];
@@ -910,7 +925,7 @@ template <int kKind, bool kRow, bool kFixed, class BA>
 __device__ __forceinline__ void solve_phases(const SolveArgs &a, const BA &B)
 {
     const int nc = a.hdr->n_colors;
-    if (a.hdr->n_pairs == 0 || nc == 0) return;  // uniform over all CTAs
+    if (a.hdr->n_pairs == 0 || nc == 0 || islands_took_solve(a)) return;  // uniform over all CTAs
     __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors];
     for (int c = threadIdx.x; c < nc && c < kMaxSolveColors; c += blockDim.x) {
         s_cstart[c] = a.cstart[c];
@@ -1041,7 +1056,7 @@ template <class BA>
 __device__ __forceinline__ void solve_phases_scene(const SolveArgs &a, const SceneSched &sc, const BA &B)
 {
     const int P = a.hdr->n_pairs, ncg = a.hdr->n_colors;
-    if (P == 0 || ncg == 0) return;  // uniform over all CTAs
+    if (P == 0 || ncg == 0 || islands_took_solve(a)) return;  // uniform over all CTAs
     __shared__ int s_cstart[kMaxSolveColors], s_ccount[kMaxSolveColors], s_cur[kMaxSolveColors];
     __shared__ int s_pa, s_pb, s_nc;
     const int scene = sc.order ? sc.order[blockIdx.x] : (int)blockIdx.x;
@@ -1130,6 +1145,91 @@ __global__ void __launch_bounds__(kSceneThreads, 2) k_color_solve_scenes(SolveAr
     solve_phases_scene(a, sc, B);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Island solve (IslandSolveContactEngine's solve kernel, contact_engine_gpu_island_solve.py:230-249):
+// one thread runs the warm start and the velocity sweeps of one island, pair after pair in
+// colour order, and another thread its position sweeps.  An island's pairs share no dynamic
+// body with any other island's, so no other thread reads or writes its bodies' velocities, and
+// every pair sees the values it sees in the colour phases: the same bits, with no barrier.
+// The bodies are read and written with ordinary (L1-cached) accesses: each body's v, w (or pv,
+// po) belong to one thread for the whole launch, and static bodies are only read.  Task t of
+// the velocity range [0, P) is the island that starts at position t of the island-ordered slot
+// list (isl_at[t] > 0); the position range follows at P rounded up to a warp.
+// ---------------------------------------------------------------------------------------------
+struct IslandBodies {
+    float *v, *w, *pv, *po;
+    __device__ __forceinline__ f3 get(int b, int k) const
+    {
+        const float *p = k == 0 ? v : k == 1 ? w : k == 2 ? pv : po;
+        return xyz(reinterpret_cast<const float4 *>(p)[b]);
+    }
+    __device__ __forceinline__ void set(int b, int k, f3 x) const
+    {
+        float *p = k == 0 ? v : k == 1 ? w : k == 2 ? pv : po;
+        reinterpret_cast<float4 *>(p)[b] = f4(x, 0.0f);
+    }
+};
+
+template <bool kRow, bool kFixed>
+__device__ __forceinline__ void island_tasks(const SolveArgs &a, const int *__restrict__ slots,
+                                             const int *__restrict__ isl_at)
+{
+    const int P = a.hdr->n_pairs;
+    if (P == 0 || a.hdr->n_colors == 0 || !(a.island_info[1] <= B2C_ISLAND_MAX_PAIRS)) return;
+    const IslandBodies B{a.v, a.w, a.pv, a.po};
+    const int p32 = (P + 31) & ~31;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p32 + P; t += gridDim.x * blockDim.x) {
+        const bool pos = t >= p32;
+        const int at = pos ? t - p32 : t;
+        if (at >= P) continue;
+        const int cnt = isl_at[at];
+        if (cnt == 0) continue;
+        const int *sl = slots + at;
+        // A pair's impulses, stored by this thread in one sweep, are read back by the staging
+        // copies of the next: the fence orders the stores before the copies.
+        if (!pos) {
+            if (a.apply_warm) {
+                for (int j = 0; j < cnt; ++j) {
+                    const int s = sl[j];
+                    const RowPre q = row_pre<true>(a.rec, s, false);
+                    if (kRow) pair_apply_warm_row(a, s, B, q);
+                    else pair_apply_warm(a, s, B, q);
+                }
+            }
+            for (int it = 0; it < a.vit; ++it) {
+                for (int j = 0; j < cnt; ++j) {
+                    const int s = sl[j];
+                    __threadfence_block();
+                    const RowPre q = row_pre<true>(a.rec, s, false);
+                    if (kRow) pair_velocity_row(a, s, B, q);
+                    else pair_velocity<IslandBodies, kFixed>(a, s, B, q);
+                }
+            }
+        } else {
+            for (int it = 0; it < a.pit; ++it) {
+                for (int j = 0; j < cnt; ++j) {
+                    const int s = sl[j];
+                    __threadfence_block();
+                    const RowPre q = row_pre<true>(a.rec, s, true);
+                    if (kRow) pair_position_row(a, s, B, q);
+                    else pair_position(a, s, B, q);
+                }
+            }
+        }
+    }
+}
+
+constexpr int kIslandThreads = 128;
+__global__ void __launch_bounds__(kIslandThreads) k_island_solve(SolveArgs a, const int *slots, const int *isl_at)
+{
+    if (a.row) island_tasks<true, true>(a, slots, isl_at);
+    else if (a.fixed_frame) island_tasks<false, true>(a, slots, isl_at);
+    else island_tasks<false, false>(a, slots, isl_at);
+}
+
+int island_partition_engine(const b2c_bodies *b, b2c_pairs *pr, b2c_header *hdr, const int **info,
+                            const int **slots, const int **isl_at, cudaStream_t s);
+
 // dynamic shared memory of a solve launch: the contact staging of its threads
 static size_t stage_bytes(int threads) { return (size_t)kStageBytesPerThread * threads; }
 
@@ -1146,6 +1246,8 @@ static void allow_stage_smem()
                          (int)stage_bytes(kClusterThreadsRow));
     cudaFuncSetAttribute(k_color_solve_scenes, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)stage_bytes(kSceneThreads));
+    cudaFuncSetAttribute(k_island_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)stage_bytes(kIslandThreads));
     done = true;
 }
 
@@ -1216,6 +1318,12 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
     }
     a.bar_count = pr->barrier;
     a.timeout_ns = p->barrier_timeout_ns > 0 ? p->barrier_timeout_ns : 1000000000LL;
+    a.island_info = nullptr;
+    const bool islands = (p->flags & B2C_COLOR_ISLANDS) != 0;
+    if (islands && !pr->isl_work) {
+        set_error("color_solve: B2C_COLOR_ISLANDS needs b2c_pairs.isl_work");
+        return B2C_EARG;
+    }
 
     const int pgrid = std::min(blocks_for(pr->capacity), kSMs * 8);
     const bool scenes = p->solve_blocks == B2C_SOLVE_SCENES;
@@ -1244,6 +1352,14 @@ int color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_head
         a.apply_warm = 0;
     }
 
+    if (islands) {
+        const int *isl_slots = nullptr, *isl_at = nullptr;
+        if ((rc = island_partition_engine(b, pr, hdr, &a.island_info, &isl_slots, &isl_at, s))) return rc;
+        allow_stage_smem();
+        k_island_solve<<<std::min(blocks_for(2LL * pr->capacity + 32, kIslandThreads), kSMs * 4), kIslandThreads,
+                         stage_bytes(kIslandThreads), s>>>(a, isl_slots, isl_at);
+        if ((rc = check_launch("island_solve"))) return rc;
+    }
     int mode = p->solve_blocks;
     if (scenes) {
         allow_stage_smem();

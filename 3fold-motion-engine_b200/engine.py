@@ -177,7 +177,26 @@ class _BeadEngineBase:
         self.header = torch.zeros(8, dtype=torch.int32, device=dev)
         self._hdr_host = torch.zeros(8, dtype=torch.int32, pin_memory=True)
 
-    def _setup_grid(self, dims=(128, 128, 32)):
+    def _auto_grid_dims(self, budget=1 << 22):
+        """Hash-grid dims for the scene as added: enough cells of 2R per axis to cover the bodies'
+        initial extent plus a margin without wrapping (a power of two, at least 8), within
+        `budget` buckets (the widest axis halved until it fits).  Buckets that alias only cost
+        time: the contact set, and its order after the per-bead sort, do not depend on the dims."""
+        c = np.asarray(self._centers, np.float64).reshape(-1, 3)
+        half = 0.5 * max(self.dims) + 2.0 * R
+        ext = (c.max(axis=0) - c.min(axis=0)) + 2.0 * half if len(c) else np.zeros(3)
+        cells = np.ceil(ext / (2.0 * R)).astype(np.int64) + 4
+        dims = [max(8, 1 << int(np.ceil(np.log2(max(int(n), 1))))) for n in cells]
+        dims = [min(d, cap) for d, cap in zip(dims, (1024, 1024, 256))]
+        while dims[0] * dims[1] * dims[2] > budget:
+            k = int(np.argmax(dims))
+            dims[k] //= 2
+        return tuple(int(d) for d in dims)
+
+    def _setup_grid(self, dims=None):
+        if dims is None:
+            dims = self._auto_grid_dims()
+        self.grid_dims_used = tuple(int(x) for x in dims)
         dev = self.dev
         nbk = dims[0] * dims[1] * dims[2]
         i32 = lambda n: torch.zeros(n, dtype=torch.int32, device=dev)
@@ -400,7 +419,7 @@ class RelaxedJacobiContactEngine(_BeadEngineBase):
     name = "relaxed_jacobi_b200"
 
     def __init__(self, dims=(0.3, 0.3, 0.2), relax=0.2, vit=40, pit=20, mu=0.5, device="cuda", graph=True,
-                 contact_capacity=MAXC, grid_dims=(128, 128, 32)):
+                 contact_capacity=MAXC, grid_dims=None):
         super().__init__(dims=dims, mu=mu, device=device, graph=graph)
         self.relax = float(relax)
         self.vit = int(vit)
@@ -408,7 +427,7 @@ class RelaxedJacobiContactEngine(_BeadEngineBase):
         self.contact_capacity = int(contact_capacity)
         # buckets of the bead hash grid (cell 2R, wrapping): a performance choice only -- the
         # Jacobi sum is order free, so the contacts and the results do not depend on it
-        self.grid_dims = tuple(int(x) for x in grid_dims)
+        self.grid_dims = None if grid_dims is None else tuple(int(x) for x in grid_dims)
 
     def _build(self):
         self._setup_bodies()

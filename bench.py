@@ -24,8 +24,9 @@ runs these engines through Warp, which is not installed) on the same workload, o
 host core, rank 0 only.
 
 Other workloads (--workload): stress100k (100 000-cube lattice), batched512 (512 uneven
-scenes in one engine), colorcache_lattice10k and jacobi_lattice10k (the reference's 10k bead
-lattice, with vs_baseline against its published timings), ncp_lattice10k (the exact-cone NCP
+scenes in one engine), colorcache_lattice10k, island_lattice10k and jacobi_lattice10k (the
+reference's 10k bead lattice under its ColorCache, island-solve and relaxed-Jacobi engines, with
+vs_baseline against their published timings), ncp_lattice10k (the exact-cone NCP
 solve of the reference's LatticeWorld fixture) and adjoint4096 (the batched NCP forward solve
 and its adjoint at the reference's batched-adjoint shape).
 """
@@ -69,6 +70,14 @@ WORKLOADS = {
                                   vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                                   published=(1e4 / 3.684e-3, "reference ColorCache, 3.684 ms/step, NVIDIA L4 "
                                              "(reports/innovation_stack_color_cache_l4.json)")),
+    # the same fixture under the island solve (IslandSolveContactEngine: 5 000 islands of two pairs,
+    # one thread per island, no colour barriers; the ColorCache engine's bits); published: 2.817 and
+    # 2.887 ms per step on an NVIDIA L4, the faster taken (reports/innovation_island_solve.json,
+    # legs[*].island.timing)
+    "island_lattice10k": dict(engine="island", scene="lattice", n=10000, dims=(0.3, 0.3, 0.2), mu=0.5,
+                              vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
+                              published=(1e4 / 2.817e-3, "reference IslandSolveContactEngine, 2.817 ms/step, "
+                                         "NVIDIA L4 (reports/innovation_island_solve.json)")),
     # the same lattice under relaxed Jacobi; published: 5.599 ms per step at N = 10 000 on an RTX 5070
     # (docs/RUNNING.md:374-379)
     # the batched exact-cone NCP and its adjoint at the shape of the reference's batched-adjoint
@@ -161,6 +170,8 @@ def make_engine(me, wl, scene):
         return e
     if wl["engine"] == "color_cache":
         e = me.ColorCacheContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
+    elif wl["engine"] == "island":
+        e = me.IslandSolveContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"])
     elif wl["engine"] == "jacobi":
         kw = {k: wl[k] for k in ("contact_capacity", "grid_dims") if k in wl}
         e = me.RelaxedJacobiContactEngine(dims=wl["dims"], mu=wl["mu"], vit=wl["vit"], pit=wl["pit"], **kw)

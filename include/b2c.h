@@ -204,6 +204,9 @@ typedef struct b2c_pairs {
     int32_t *prio_hi;                /* (capacity) or NULL: with B2C_COLOR_REDUCED_CONTACTS the
                                         high part of each chunk's colouring priority (slot << 19 |
                                         run parity << 18), written by b2c_manifold_reduce */
+    int32_t *isl_work;               /* b2c_island_work_ints(bodies, capacity) ints, zero-filled
+                                        before the first substep, or NULL: the island partition of
+                                        the solve with B2C_COLOR_ISLANDS */
 } b2c_pairs;
 
 /* Warm-start store: kept feature keys (sorted) and their impulses, from the previous substep. */
@@ -270,6 +273,17 @@ typedef struct b2c_boxes {
                                     GraphColoredContactEngine(manifold_reduce=True,
                                     pair_chunks=False).  Needs b2c_pairs.prio_hi and a pair
                                     capacity of one per contact. */
+
+#define B2C_COLOR_ISLANDS 256    /* the island solve (IslandSolveContactEngine,
+                                    contact_engine_gpu_island_solve.py:253-291): the pair graph is
+                                    partitioned into islands of dynamic bodies on the device
+                                    (recomputed on every colour-cache miss); when no island has more
+                                    than B2C_ISLAND_MAX_PAIRS pairs, one thread per island runs its
+                                    warm start, velocity sweeps and (on another thread) position
+                                    sweeps over its pairs in colour order, with no barrier between
+                                    colours -- the same bits as the persistent solve, which runs
+                                    instead when an island is larger.  Needs b2c_pairs.isl_work. */
+#define B2C_ISLAND_MAX_PAIRS 64  /* largest island the island solve takes (the reference's 64) */
 
 #define B2C_SOLVE_SCENES 0x100000 /* b2c_color_params.solve_blocks: the scene schedule */
 
@@ -371,6 +385,24 @@ B2C_API int32_t b2c_color_pairs(const b2c_bodies *b, b2c_pairs *pr, b2c_header *
  * between colours. */
 B2C_API int32_t b2c_color_solve(const b2c_bodies *b, b2c_contacts *kept, b2c_pairs *pr, b2c_header *hdr,
                                 const b2c_color_params *p, float dt, b2c_stream s);
+/* ints of the island workspace (b2c_pairs.isl_work, b2c_island_partition's work) */
+B2C_API int64_t b2c_island_work_ints(int32_t n_bodies, int32_t pair_capacity);
+/* partition_pairs (contact_engine_gpu_island_solve.py:7-34) on the device: the pairs
+ * (pbi[p], pbj[p]) of bodies with inverse masses inv_mass, taken in the order `order` (a
+ * permutation of the n_pairs pairs, or NULL for 0..n_pairs-1), grouped into islands.  Two dynamic
+ * bodies (inverse mass > 0) of one pair are in one island; static bodies and the ground (pbj < 0)
+ * join nothing.  Writes, in the reference's output order (islands by their smallest body, a pair
+ * without a dynamic body keyed bodies + p; each island's pairs in `order`):
+ *   packed (n_pairs) the pair indices island by island, starts / counts (n_pairs room) each
+ *   island's offset into packed and its pair count, info[0] the number of islands, info[1] the
+ *   most pairs of one island (info: 4 device ints).
+ * work: b2c_island_work_ints(n_bodies, n_pairs) device ints.  The arguments are not validated
+ * on the device (the reference raises ValueError for bad shapes, negative or non-finite masses,
+ * endpoints out of range and a non-permutation order; the Python wrapper checks them). */
+B2C_API int32_t b2c_island_partition(const int32_t *pbi, const int32_t *pbj, const float *inv_mass,
+                                     const int32_t *order, int32_t n_pairs, int32_t n_bodies, int32_t *work,
+                                     int32_t *packed, int32_t *starts, int32_t *counts, int32_t *info,
+                                     b2c_stream s);
 /* _store_warm_device (COL:1089-1093). */
 B2C_API int32_t b2c_warm_store(const b2c_contacts *kept, const int64_t *kept_keys, b2c_warm *warm,
                                const b2c_header *hdr, b2c_stream s);
