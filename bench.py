@@ -1297,7 +1297,9 @@ def main():
                 traffic = None
         roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_color_solve (persistent chunk solve, one launch per substep)",
+                "kernel": ("k_island_solve (one thread per island; b2c_color_solve with its record gather and "
+                           "impulse scatter)" if wl["engine"] == "island" else
+                           "k_color_solve (persistent chunk solve, one launch per substep)"),
                 "launch_ms": avg_ms, "algorithmic_bytes_per_launch": avg_b, "counts": solve_bytes[-1]}
     elif wl["engine"] == "jacobi":  # the iteration launches of one substep, timed after the timed region
         j_ms, j_b, j_counts = e.solve_sample(dt / S)
