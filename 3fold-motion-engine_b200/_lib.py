@@ -106,6 +106,25 @@ class Bncp(ctypes.Structure):
                 ("status", c_void_p)]
 
 
+class Admm(ctypes.Structure):
+    """b2c_admm"""
+    _fields_ = [("n_env", c_int32), ("nc", c_int32), ("nv", c_int32)] + [(k, c_void_p) for k in (
+        "J", "Minv", "v_free", "mu", "lam", "u", "v_plus", "res", "mask", "rho", "nslip", "labels", "dlam_tau",
+        "dv_tau", "dlam_mu", "dbv_in")]
+
+
+class AdmmParams(ctypes.Structure):
+    """b2c_admm_params"""
+    _fields_ = [("flags", c_int32), ("n_iter", c_int32), ("cg_iters", c_int32), ("refresh_every", c_int32),
+                ("tol", ctypes.c_double), ("chunk", c_int32), ("desax", c_int32), ("rho_mode", c_int32),
+                ("jacobi_sweeps", c_int32), ("alpha_eta", ctypes.c_double), ("dt", ctypes.c_double),
+                ("jdir", c_int32), ("n_calls", c_int32), ("grad_cg", c_int32), ("do_mu", c_int32)]
+
+
+ADMM_FORWARD, ADMM_GRADIENT, ADMM_GRAD_GIVEN = 1, 2, 4
+ADMM_RHO = {"sqrt": 0, "lmin": 1, "lmax": 2, "regime": 3, "given": 4}
+ADMM_MAX_CONTACTS, ADMM_MAX_DOFS = 8, 32
+
 COLOR_FIXED_FRAME = 1
 COLOR_APPLY_WARM = 2
 COLOR_CACHE = 4
@@ -218,6 +237,8 @@ _SIGS = {
     "b2c_world_adj_end": ([_P(World), _P(NcpScene), c_void_p, c_void_p, c_void_p, _D, c_void_p, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                            c_void_p], c_int32),
+    "b2c_admm_smem_bytes": ([c_int32, c_int32], ctypes.c_int64),
+    "b2c_admm_solve": ([_P(Admm), _P(AdmmParams), c_void_p], c_int32),
     "b2c_bncp_max_rows": ([], c_int32),
     "b2c_bncp_solve": ([_P(Bncp), c_int32, ctypes.c_double, c_int32, c_void_p], c_int32),
     "b2c_bncp_sensitivity": ([_P(Bncp), c_void_p, c_void_p, c_void_p], c_int32),

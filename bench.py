@@ -90,6 +90,18 @@ WORKLOADS = {
                         published=(4096 / 428.49e-3, "reference batched ADMM forward, 428.49 ms at B = 4096, "
                                    "RTX 5070 (reproducibility/p2/data/reference/batch_throughput_slip.txt)"),
                         published_grad_ms=119.61, published_fwd_ms=428.49),
+    # the reference's batched ADMM itself at its benchmark's configuration (B = 4096 sliding-stance
+    # problems, nv 18, 4 contacts, mu 0.5, rho from the regime, 200 ADMM iterations of 8 CG steps,
+    # refresh every 4, then the two gradient directions with 60 CG steps per sigma-map application):
+    # one step is one launch of the forward and the gradient; published: forward 428.49 ms
+    # (9 559 env-steps/s), forward + gradient 530.10 ms on an RTX 5070
+    # (reproducibility/p2/data/reference/batch_throughput_slip.txt)
+    "admm4096": dict(engine="admm", B=4096, nv=18, nc=4, mu=0.5, n_iter=200, cg=8, refresh=4, tol=1e-8, grad_cg=60,
+                     steps=20, warmup=3,
+                     published=(4096 / 530.10e-3, "reference BatchProxADMMGPU forward + gradient (2 directions), "
+                                "530.10 ms at B = 4096, RTX 5070 (reproducibility/p2/data/reference/"
+                                "batch_throughput_slip.txt)"),
+                     published_fwd_ms=428.49, published_grad_ms=119.61, published_both_ms=530.10),
     # the reference's exact-cone NCP timing fixture (LatticeWorld, N = 10 000, n_c = 40 000, float64,
     # 40 PGS sweeps: residual 7.778e-05, 8 colours); one step solves the resident scene again
     # (setup, colouring through the cache, 40 sweeps); published: 11.21 ms per step = 280.2 us per
@@ -625,6 +637,166 @@ def run_reference_adjoint(args, wl):
     print(json.dumps(line), flush=True)
 
 
+def _admm_cpu_worker(args_):
+    """The ADMM oracle (forward and both gradient directions) on problems [lo, hi) of the stance
+    batch, in blocks of 8 until the budget is spent; returns (problems done, seconds)."""
+    workload, lo, hi, budget = args_
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ge.load_package()
+    from oracle import oracle_badmm as OA
+    wl = WORKLOADS[workload]
+    J, Minv, v, mu = _stance(wl)
+    done, t0 = 0, time.perf_counter()
+    for a in range(lo, hi, 8):
+        b = min(hi, a + 8)
+        o = OA.BatchADMMOracle(J[a:b], Minv[a:b], v[a:b], mu[a:b], 1.0 / 240.0).set_rho("regime")
+        o.forward(wl["n_iter"], wl["cg"], wl["refresh"], wl["tol"])
+        o.gradient(n_calls=wl["nc"] + 2, grad_cg=wl["grad_cg"])
+        done += b - a
+        if time.perf_counter() - t0 > budget:
+            break
+    return done, time.perf_counter() - t0
+
+
+def run_reference_admm(args, wl):
+    """--impl reference for the ADMM workload: the ADMM oracle (numpy) on every host core."""
+    import multiprocessing as mp
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    B = wl["B"]
+    cuts = [B * k // procs for k in range(procs + 1)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_admm_cpu_worker, [(args.workload, cuts[k], cuts[k + 1], 30.0) for k in range(procs)])
+    value = sum(r[0] for r in res) / max(r[1] for r in res)
+    line = {"impl": "reference", "metric": "env-steps/s", "value": value, "unit": "env-steps/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload, **{k: v for k, v in wl.items() if k not in ("warmup", "steps")}},
+            "dtype": "f64", "data": "synthetic",
+            "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": procs, "kind": "port",
+                             "sample": f"{sum(r[0] for r in res)} of the {B} problems, forward and both gradient "
+                                       f"directions, {procs} processes capped at ~30 s (the ADMM oracle in numpy; "
+                                       f"the reference's Warp path is not installed)"},
+            "e2e": {"value": value, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_admm(args, wl):
+    """The reference's batched ADMM and its adjoint, one launch per step (forward from zero and
+    both gradient directions), the forward alone timed beside it.  With N ranks every rank solves
+    its own batch (weak scaling)."""
+    import torch
+    import __graft_entry__ as ge
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ge.load_package()
+    cpu_base = None
+    if rank == 0 and not args.no_cpu_baseline:  # before the first GPU call
+        n, el = _admm_cpu_worker((args.workload, 0, wl["B"], 15.0))
+        cpu_base = {"value": n / el, "unit": "env-steps/s", "cores": 1, "kind": "port",
+                    "sample": f"{n} problems of the batch, forward and both gradient directions, on one host core "
+                              f"({el:.1f} s; the ADMM oracle in numpy)"}
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from motion_engine_b200 import badmm
+    J, Minv, v, mu = _stance(wl)
+    B, C, NV = wl["B"], wl["nc"], wl["nv"]
+    s = badmm.BatchProxADMM(B, NV, C, device=dev).upload(J, Minv, v, mu, 1.0 / 240.0).set_rho("regime")
+    kw = dict(cg_iters=wl["cg"], refresh_every=wl["refresh"], tol=wl["tol"], n_calls=C + 2, grad_cg=wl["grad_cg"])
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        s.step_and_grad(wl["n_iter"], **kw)
+        s.launch(1, wl["n_iter"], wl["cg"], wl["refresh"], wl["tol"])
+    torch.cuda.synchronize()
+    both, fwd = [], []
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            s.step_and_grad(wl["n_iter"], **kw)
+            e1.record()
+            s.launch(1, wl["n_iter"], wl["cg"], wl["refresh"], wl["tol"])
+            e2.record()
+            e2.synchronize()
+            both.append(e0.elapsed_time(e1))
+            fwd.append(e1.elapsed_time(e2))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    t = torch.tensor([float(np.mean(both)), float(np.mean(fwd))], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    both_ms, fwd_ms = float(t[0]), float(t[1])
+    grad_ms = both_ms - fwd_ms
+    value = B * world / (both_ms / 1e3)
+    s.step_and_grad(wl["n_iter"], **kw)
+    torch.cuda.synchronize()
+    res = s.res.cpu().numpy()
+    labels = np.bincount(s.labels.cpu().numpy().ravel(), minlength=3).tolist()
+    # end to end through the public API: the problems from pinned host memory, the solution and
+    # both gradients back, every step
+    hJ, hM, hv, hmu = (torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in (J, Minv, v, mu))
+    outs = [torch.empty(tuple(t_.shape), dtype=torch.float64).pin_memory()
+            for t_ in (s.lam, s.v_plus, s.dlam_tau, s.dv_tau, s.dlam_mu)]
+    K2 = max(3, min(args.steps, 10))
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(K2):
+        s.upload(hJ.to(dev, non_blocking=True), hM.to(dev, non_blocking=True), hv.to(dev, non_blocking=True),
+                 hmu.to(dev, non_blocking=True), 1.0 / 240.0)
+        s.step_and_grad(wl["n_iter"], **kw)
+        for o_, t_ in zip(outs, (s.lam, s.v_plus, s.dlam_tau, s.dv_tau, s.dlam_mu)):
+            o_.copy_(t_, non_blocking=True)
+    z.record()
+    z.synchronize()
+    e2e_ms = a.elapsed_time(z) / K2
+    peaks, peak_kind = _peaks()
+    alg = B * (3 * C * NV + NV * NV + NV + C) * 8 + B * (2 * 3 * C * 3 + NV + 2 * NV) * 8  # inputs once, outputs
+    roof = {"bound": "hbm", "achieved": alg / (both_ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": alg / (both_ms / 1e3) / 1e9 / peaks["hbm_gbs"], "traffic": None, "peak_kind": peak_kind,
+            "kernel": "k_admm (one warp per problem: set-up, ADMM, active set, grad_affine in shared memory)",
+            "launch_ms": both_ms, "algorithmic_bytes_per_launch": alg,
+            "note": "latency-bound: each warp iterates its problem in shared memory; the inputs are read once"}
+    if rank == 0:
+        line = {"metric": "env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": both_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": value / wl["published"][0], "dtype": "f64",
+                "data": "synthetic (seeded legged-stance batch, the reference's shapes)",
+                "config": {"workload": args.workload, "B": B, "nv": NV, "contacts": C, "mu": wl["mu"],
+                           "rho": "regime", "admm_iters": wl["n_iter"], "cg": wl["cg"], "refresh": wl["refresh"],
+                           "tol": wl["tol"], "grad_cg": wl["grad_cg"], "n_calls": C + 2,
+                           "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"batches x{world}"},
+                "baseline": {"value": wl["published"][0], "unit": "env-steps/s", "source": wl["published"][1]},
+                "adjoint": {"fwd_ms": fwd_ms, "grad_ms_2dir": grad_ms, "fwd_plus_grad_ms": both_ms,
+                            "grad_over_fwd": grad_ms / fwd_ms,
+                            "reference": {"fwd_ms": wl["published_fwd_ms"], "grad_ms_2dir": wl["published_grad_ms"],
+                                          "fwd_plus_grad_ms": wl["published_both_ms"],
+                                          "grad_over_fwd": wl["published_grad_ms"] / wl["published_fwd_ms"]}},
+                "residual": {"max": float(np.nanmax(res)), "median": float(np.nanmedian(res)),
+                             "below_1e-8": float(np.mean(res < 1e-8)),
+                             "note": "the reference's run reports frac<1e-8 0.0000 and a median 1.49e-04"},
+                "contacts_by_label": dict(zip(("open", "stick", "slip"), labels)),
+                "clocks": clk.summary(),
+                "e2e": {"value": B / (e2e_ms / 1e3), "unit": "env-steps/s",
+                        "h2d_bytes_per_step": int(sum(x.numel() * 8 for x in (hJ, hM, hv, hmu))),
+                        "d2h_bytes_per_step": int(sum(o_.numel() * 8 for o_ in outs)), "steps": K2},
+                "gpu_launches": args.steps * 2, "launches_per_step": 1,
+                "roofline": roof, "cpu_baseline": cpu_base}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_adjoint(args, wl):
     """The batched NCP forward solve and its adjoint.  A step solves the whole batch (from zero)
     to the workload's residual; the gradient is two vector-Jacobian products (two seeds), as the
@@ -1084,6 +1256,8 @@ def main():
         args.warmup = wl["warmup"]
     args.warmup = max(args.warmup, 3)
     import __graft_entry__ as ge
+    if wl["engine"] == "admm":
+        return run_reference_admm(args, wl) if args.impl == "reference" else run_admm(args, wl)
     if wl["engine"] == "bncp":
         ge.load_package()
         return run_reference_adjoint(args, wl) if args.impl == "reference" else run_adjoint(args, wl)

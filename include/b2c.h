@@ -646,6 +646,69 @@ B2C_API int32_t b2c_bncp_sensitivity(const b2c_bncp *p, double *dlam_dmu, double
 B2C_API int32_t b2c_bncp_vjp(const b2c_bncp *p, const double *glam, double *gb, double *gmu, b2c_stream s);
 
 /* ---------------------------------------------------------------------------------------------
+ * Batched proximal ADMM with its adjoint: the reference's BatchProxADMMGPU
+ * (src/motion_engine/ncp/ncp_batch_gpu.py:918-1313).  n_env independent problems of nc point
+ * contacts on nv generalised velocities each (J: 3 nc x nv rows n, t1, t2 per contact), solved
+ * matrix-free (G x = J (M^-1 J^T x), with M^-1 J^T x summed in int64 at a per-problem
+ * power-of-two scale, NB:326-388) by ADMM with a block-Jacobi preconditioned CG x-step, the
+ * exact cone projection and a per-problem convergence mask; then the fixed-branch adjoint by
+ * grad_affine (NB:1172-1186).  One warp per problem runs the whole solve in one launch.
+ * ------------------------------------------------------------------------------------------- */
+#define B2C_ADMM_MAX_CONTACTS 8
+#define B2C_ADMM_MAX_DOFS 32
+#define B2C_ADMM_FORWARD 1      /* set-up and n_iter ADMM iterations from zero (NB:1190-1195) */
+#define B2C_ADMM_GRADIENT 2     /* then d/dtau_jdir and d/dmu at the first slip contact (NB:1197-1206) */
+#define B2C_ADMM_GRAD_GIVEN 4   /* instead of the forward: grad_affine at the given lam and u for the
+                                   b-direction dbv_in (the reference's own adjoint test,
+                                   tests/test_ncp_batch_adjoint.py:55-76) */
+#define B2C_ADMM_RHO_SQRT 0     /* rho = sqrt(lambda_min+ lambda_max) of G (k_rho NB:261-288) */
+#define B2C_ADMM_RHO_LMIN 1
+#define B2C_ADMM_RHO_LMAX 2
+#define B2C_ADMM_RHO_REGIME 3   /* lambda_max when the bilateral solution leaves a cone, else lambda_min+ */
+#define B2C_ADMM_RHO_GIVEN 4    /* b2c_admm.rho as given */
+
+typedef struct b2c_admm {
+    int32_t n_env, nc, nv;
+    const double *J;        /* (n_env, 3 nc, nv) row-major */
+    const double *Minv;     /* (n_env, nv, nv) */
+    const double *v_free;   /* (n_env, nv); b = J v_free */
+    const double *mu;       /* (n_env, nc) */
+    double *lam;            /* (n_env, nc, 3) out (FORWARD) or in (GRAD_GIVEN) */
+    double *u;              /* (n_env, nc, 3) contact velocity of the last refresh; out or in likewise */
+    double *v_plus;         /* (n_env, nv) v_free + M^-1 J^T lam (FORWARD) */
+    double *res;            /* (n_env) natural residual of the last refresh, NaN when none ran, or NULL */
+    int32_t *mask;          /* (n_env) 1 = still iterating (not below tol), or NULL */
+    double *rho;            /* (n_env) the ADMM penalty used (out), or in with B2C_ADMM_RHO_GIVEN; or NULL */
+    int32_t *nslip;         /* (n_env) slip contacts of the active set (GRADIENT / GRAD_GIVEN) */
+    int32_t *labels;        /* (n_env, nc) 0 open, 1 stick, 2 slip */
+    double *dlam_tau;       /* (n_env, nc, 3) dlam for db = dt J M^-1 e_jdir (or for dbv_in) */
+    double *dv_tau;         /* (n_env, nv) dv+ for the same direction */
+    double *dlam_mu;        /* (n_env, nc, 3) dlam / dmu at each problem's first slip contact */
+    const double *dbv_in;   /* (n_env, nc, 3) the b-direction of B2C_ADMM_GRAD_GIVEN, else NULL */
+} b2c_admm;
+
+typedef struct b2c_admm_params {
+    int32_t flags;          /* B2C_ADMM_FORWARD [| B2C_ADMM_GRADIENT] or B2C_ADMM_GRAD_GIVEN */
+    int32_t n_iter, cg_iters, refresh_every;
+    double tol;             /* a problem freezes once its residual at a refresh is below tol */
+    int32_t chunk;          /* > 0: the refresh count restarts every `chunk` iterations (the reference's
+                               chunked forward, NB:1112-1143); 0: one block (its step-and-gradient graph) */
+    int32_t desax;          /* natural residual with the de Saxce term */
+    int32_t rho_mode;       /* B2C_ADMM_RHO_* */
+    int32_t jacobi_sweeps;  /* cyclic Jacobi sweeps of G's spectrum (the reference's 10) */
+    double alpha_eta;       /* eta = alpha |G_cc| (the reference's default 0) */
+    double dt;              /* db = dt J M^-1 e_jdir */
+    int32_t jdir;           /* generalised coordinate of the tau direction */
+    int32_t n_calls;        /* applications of the sigma map (n_slip max + 2; <= 0: nc + 2) */
+    int32_t grad_cg;        /* CG iterations of each application */
+    int32_t do_mu;          /* also the mu direction */
+} b2c_admm_params;
+
+/* dynamic shared memory of one problem (-1 when nc or nv is out of range) */
+B2C_API int64_t b2c_admm_smem_bytes(int32_t nc, int32_t nv);
+B2C_API int32_t b2c_admm_solve(const b2c_admm *a, const b2c_admm_params *p, b2c_stream s);
+
+/* ---------------------------------------------------------------------------------------------
  * Engine handle: the ContactEngine protocol (src/motion_engine/contact_engine.py:48-55) as C
  * calls, for callers without a tensor library.  A handle owns its device memory (one
  * allocation, sized at the first step from the bodies added; adding bodies afterwards rebuilds

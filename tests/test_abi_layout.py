@@ -13,7 +13,7 @@ from conftest import ROOT
 PAIRS = {"Bodies": "b2c_bodies", "Beads": "b2c_beads", "Grid": "b2c_grid", "Contacts": "b2c_contacts",
          "JacobiParams": "b2c_jacobi_params", "Manifold": "b2c_manifold", "Pairs": "b2c_pairs", "Warm": "b2c_warm",
          "Boxes": "b2c_boxes", "ColorParams": "b2c_color_params", "NcpScene": "b2c_ncp_scene",
-         "NcpState": "b2c_ncp_state", "NcpParams": "b2c_ncp_params", "Bncp": "b2c_bncp", "Config": "b2c_config",
+         "NcpState": "b2c_ncp_state", "NcpParams": "b2c_ncp_params", "Bncp": "b2c_bncp", "Admm": "b2c_admm", "AdmmParams": "b2c_admm_params", "Config": "b2c_config",
          "StepHeader": "b2c_step_header", "World": "b2c_world"}
 
 
