@@ -64,8 +64,12 @@ class BoxContactEngine(_BeadEngineBase):
 
     def __init__(self, dims=(0.3, 0.3, 0.2), mu=0.5, vit=16, pit=10, fixed_frame=True, apply_warm=True,
                  color_cache=True, warm_start=True, margin=MARGIN, device="cuda", color_cap=NCOLMAX,
-                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16, first_fit=True, row_form=True):
+                 solve_blocks=0, barrier_timeout_s=1.0, cand_per_body=16, first_fit=True, row_form=True,
+                 islands=False):
         super().__init__(dims=dims, mu=mu, device=device, graph=True)
+        # the island solve (B2C_COLOR_ISLANDS): one thread per island when no island has more than
+        # 64 pairs, else the colour phases; the same bits either way
+        self.islands = bool(islands)
         self.vit, self.pit = int(vit), int(pit)
         self.fixed_frame, self.apply_warm = bool(fixed_frame), bool(apply_warm)
         self.color_cache, self.warm_start = bool(color_cache), bool(warm_start)
@@ -182,13 +186,17 @@ class BoxContactEngine(_BeadEngineBase):
             self.c_pairs.n_scenes = self.n_scenes
             self.c_pairs.scene_body_start, self.c_pairs.scene_order = _ptr(sb["start"]), _ptr(sb["order"])
             self.c_pairs.pair_slot, self.c_pairs.scene_slots = _ptr(sb["pair_slot"]), _ptr(sb["scene_slots"])
+        if self.islands:
+            pb["isl_work"] = i32(self.L.b2c_island_work_ints(N, pcap))
+            self.c_pairs.isl_work = _ptr(pb["isl_work"])
         self.w_keys, self.w_imp, self.w_n = i64(kept_cap), f4(kept_cap), i32(1)
         self.c_warm = _lib.Warm(kept_cap, _ptr(self.w_keys), _ptr(self.w_imp), _ptr(self.w_n))
         self.c_bodies = _lib.Bodies(N, _ptr(self.xc), _ptr(self.q), _ptr(self.v), _ptr(self.w), _ptr(self.pv),
                                     _ptr(self.po), _ptr(self.invM), _ptr(self.IbInv), _ptr(self.kin), _ptr(self.invIw))
         flags = ((_lib.COLOR_FIXED_FRAME if self.fixed_frame else 0) | (_lib.COLOR_APPLY_WARM if self.apply_warm else 0)
                  | (_lib.COLOR_CACHE if self.color_cache else 0) | (_lib.COLOR_WARM_START if self.warm_start else 0)
-                 | (_lib.COLOR_FIRST_FIT if self.first_fit else 0) | (_lib.COLOR_ROW_FORM if self.row_form else 0))
+                 | (_lib.COLOR_FIRST_FIT if self.first_fit else 0) | (_lib.COLOR_ROW_FORM if self.row_form else 0)
+                 | (_lib.COLOR_ISLANDS if self.islands else 0))
         self.c_params = _lib.ColorParams(self.vit, self.pit, 8, flags, self.mu, 1.0, min(self.color_cap, NCOLMAX),
                                          self.solve_blocks, self.barrier_timeout_ns,
                                          _ptr(self.body_mu) if self.per_body_mu else None)
@@ -227,6 +235,20 @@ class BoxContactEngine(_BeadEngineBase):
 
     def set_kinematic(self, i, xc):
         super().set_kinematic(i, xc)
+
+    @property
+    def island_count(self):
+        """Islands of the last partition (islands=True)."""
+        return int(self.p_bufs["isl_work"][0].item()) if self._built and self.islands else 0
+
+    @property
+    def max_island_pairs(self):
+        """Pairs of the largest island of the last partition (islands=True)."""
+        return int(self.p_bufs["isl_work"][1].item()) if self._built and self.islands else 0
+
+    @property
+    def island_solve_active(self):
+        return self.islands and self._built and self.max_island_pairs <= _lib.ISLAND_MAX_PAIRS
 
     @property
     def color_cache_hits(self):

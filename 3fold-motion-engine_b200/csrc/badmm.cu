@@ -14,8 +14,7 @@
 //    Cholesky solve (k_bilat), rho (k_rho), the block-Jacobi preconditioner (k_pjac);
 //  * the matrix-free product G x + (eta + rho) x (NB:326-388): y = J^T x per contact, then
 //    M^-1 y per contact rounded at a power-of-two scale 2^floor(log2(2^52 / (kappa |x|inf)))
-//    and summed in int64 (shared-memory 64-bit atomics: the sum does not depend on the order),
-//    w = acc / scale, then J w;
+//    and summed in int64 (exact: the sum does not depend on the order), w = acc / scale, then J w;
 //  * ADMM (NB:466-543, 1075-1099): x-step by block-Jacobi preconditioned CG warm-started from
 //    the last x, z = proj_K(x + gamma / rho), gamma += rho (x - z), and every `refresh_every`
 //    iterations u = G z + b, the slip speeds, the natural residual and the convergence mask (a
@@ -43,7 +42,6 @@ struct Env {
     double *mu, *s, *eta, *rhoc, *slipf, *sig, *sigo, *siga, *res, *gnorm;
     double *Gd, *Pj, *Zm, *Ps;  // 9 per contact, row-major
     double *Bm, *Aw, *rw;
-    unsigned long long *acc;
     int *sidx;
     int C, NV, M;
     double kap, rho;
@@ -58,7 +56,7 @@ __host__ __device__ inline size_t env_doubles(int C, int NV)
 }
 __host__ __device__ inline size_t env_bytes(int C, int NV)
 {
-    return env_doubles(C, NV) * 8 + (size_t)NV * 8 + (size_t)C * 4 + 16;
+    return env_doubles(C, NV) * 8 + (size_t)C * 4 + 16;
 }
 
 __device__ inline Env carve(double *base, int C, int NV)
@@ -95,8 +93,6 @@ __device__ inline Env carve(double *base, int C, int NV)
     E.Bm = take((size_t)C * C);
     E.Aw = take((size_t)C * C);
     E.rw = take(C);
-    E.acc = reinterpret_cast<unsigned long long *>(p);
-    p += NV;
     E.sidx = reinterpret_cast<int *>(p);
     E.kap = 0.0;
     E.rho = 0.0;
@@ -164,52 +160,67 @@ __device__ inline double eigmax3(const double A[9])
     return out;
 }
 
-// the matrix-free product (k_scale, k_jt, k_mscat, k_acc2w, k_gath): xout = G xin + (eta + rho') xin
+// the matrix-free product (k_scale, k_jt, k_mscat, k_acc2w, k_gath): xout = G xin + (eta + rho') xin.
+// Lane k (< nv) owns row k of M^-1: it forms every contact's M^-1 (J^T x)_c entry k with the
+// contacts' sums interleaved (independent chains), rounds each at the scale and adds them in its
+// own int64 register -- exact, so no atomics and no order dependence.  The scale is a power of
+// two, so acc / scale is the exact product acc * 2^-e.
 __device__ void matvec(Env &E, const double *xin, double *xout, bool use_rho)
 {
     const int ln = lane_id(), C = E.C, NV = E.NV, M = E.M;
-    double m = 0.0;
-    for (int i = ln; i < M; i += 32) m = fmax(m, fabs(xin[i]));
+    double m = ln < M ? fabs(xin[ln]) : 0.0;
     m = warp_max(m);
     const double t = E.kap * m;
-    double scal = 1.0;
+    double scal = 1.0, inv = 1.0;
     if (t > 0.0) {
         int e = ilogb(kScaleBound / t);  // floor(log2(2^52 / t)), exactly
         e = e < -1000 ? -1000 : (e > 1000 ? 1000 : e);
         scal = ldexp(1.0, e);
+        inv = ldexp(1.0, -e);
     }
-    for (int q = ln; q < C * NV; q += 32) {
-        const int c = q / NV, l = q - c * NV;
-        E.yt[q] = E.J[(3 * c) * NV + l] * xin[3 * c] + E.J[(3 * c + 1) * NV + l] * xin[3 * c + 1] +
-                  E.J[(3 * c + 2) * NV + l] * xin[3 * c + 2];
-    }
-    for (int k = ln; k < NV; k += 32) E.acc[k] = 0ull;
-    __syncwarp();
-    for (int q = ln; q < C * NV; q += 32) {
-        const int c = q / NV, k = q - c * NV;
-        double s = 0.0;
-        const double *mrow = E.Mi + (size_t)k * NV, *y = E.yt + (size_t)c * NV;
-        for (int l = 0; l < NV; ++l) s = s + mrow[l] * y[l];
-        atomicAdd(&E.acc[k], (unsigned long long)llround(s * scal));
+    if (ln < NV) {
+        for (int c = 0; c < C; ++c) {
+            const double *jr = E.J + (size_t)(3 * c) * NV + ln;
+            E.yt[c * NV + ln] = jr[0] * xin[3 * c] + jr[NV] * xin[3 * c + 1] + jr[2 * NV] * xin[3 * c + 2];
+        }
     }
     __syncwarp();
-    for (int k = ln; k < NV; k += 32) E.wv[k] = (double)(long long)E.acc[k] / scal;
+    if (ln < NV) {
+        double sc[B2C_ADMM_MAX_CONTACTS];
+#pragma unroll
+        for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c) sc[c] = 0.0;
+        const double *mrow = E.Mi + (size_t)ln * NV;
+        for (int l = 0; l < NV; ++l) {
+            const double ml = mrow[l];
+#pragma unroll
+            for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c)
+                if (c < C) sc[c] = sc[c] + ml * E.yt[c * NV + l];
+        }
+        long long acc = 0;
+#pragma unroll
+        for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c)
+            if (c < C) acc += llround(sc[c] * scal);
+        E.wv[ln] = (double)acc * inv;
+    }
     __syncwarp();
     const double rr = use_rho ? E.rho : 0.0;
-    for (int i = ln; i < M; i += 32) {
+    if (ln < M) {
         double u = 0.0;
-        const double *jrow = E.J + (size_t)i * NV;
+        const double *jrow = E.J + (size_t)ln * NV;
         for (int k = 0; k < NV; ++k) u = u + jrow[k] * E.wv[k];
-        xout[i] = u + (E.eta[i / 3] + rr) * xin[i];
+        xout[ln] = u + (E.eta[ln / 3] + rr) * xin[ln];
     }
     __syncwarp();
 }
 
-// k_dot (NB:408-416), evaluated by every lane (the same value everywhere)
+// k_dot (NB:408-416): the products lane by lane, summed by a butterfly; IEEE addition is
+// commutative, so every lane ends with the same bits
 __device__ __forceinline__ double dot(const Env &E, const double *a, const double *b)
 {
-    double s = 0.0;
-    for (int c = 0; c < E.C; ++c) s = s + a[3 * c] * b[3 * c] + a[3 * c + 1] * b[3 * c + 1] + a[3 * c + 2] * b[3 * c + 2];
+    const int ln = lane_id();
+    double s = ln < E.M ? a[ln] * b[ln] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
     return s;
 }
 

@@ -176,7 +176,7 @@ def make_engine(me, wl, scene):
                                    color_cap=wl["color_cap"])
     if wl["engine"] == "box":
         e = me.BoxContactEngine(mu=float(np.mean(wl["mu_range"])), vit=wl["vit"], pit=wl["pit"],
-                                color_cap=wl["color_cap"])
+                                color_cap=wl["color_cap"], islands=bool(wl.get("islands", False)))
         for c, d, m, de in zip(scene["centers"], scene["dims"], scene["mu"], scene["density"]):
             e.add_box(c, dims=d, density=de, mu=m)
         return e
@@ -1241,6 +1241,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--islands", choices=("on", "off"), default=None,
+                    help="box workloads: the island solve on or off (default: the workload's setting)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the oracle digest at the parity step (it runs in spawned processes)")
     ap.add_argument("--save-state", default=None,
@@ -1249,7 +1251,9 @@ def main():
                     help="start from a state written by --save-state instead of running the set-up steps "
                          "(profiling aid: short runs with few launches before the captured ones)")
     args = ap.parse_args()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.islands is not None:
+        wl["islands"] = args.islands == "on"
     if args.steps is None:
         args.steps = wl["steps"]
     if args.warmup is None:
@@ -1502,7 +1506,11 @@ def main():
         cfg.update(autotuned=tuned)
     if wl["engine"] == "box":
         cfg.update(edge=wl["edge"], volume=wl["box"], mu=wl["mu_range"], density=wl["density"],
-                   color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3")
+                   color_cap=wl["color_cap"], contacts="SAT box/plane + box/box, margin 2e-3",
+                   island_solve=bool(wl.get("islands", False)))
+        if wl.get("islands"):
+            cfg.update(islands={"count": e.island_count, "max_pairs": e.max_island_pairs,
+                                "island_kernel_ran": bool(e.island_solve_active)})
     line = {"metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong" if wl["engine"] == "batched" else "weak",

@@ -162,3 +162,37 @@ def test_island_engine_runs_repeat_bit_identical(me):
         runs.append(e.get_state())
     for n in ("xc", "Rm", "vc", "om"):
         assert getattr(runs[0], n).tobytes() == getattr(runs[1], n).tobytes(), n
+
+
+def _box_pair(me, sc, islands_kw, **kw):
+    engines = []
+    for isl in (True, False):
+        e = me.BoxContactEngine(mu=0.6, vit=16, pit=10, islands=isl, **kw)
+        for c, d, m, de in zip(sc["centers"], sc["dims"], sc["mu"], sc["density"]):
+            e.add_box(c, dims=d, density=de, mu=m)
+        engines.append(e)
+    return engines
+
+
+@pytest.mark.parametrize("scene,active", [("stress_lattice", True), ("pile", False)])
+def test_box_engine_island_solve_equals_colour_phases(scene, active, me):
+    """The box engine's row form with the island solve: a stress-style cube lattice that falls
+    into separate columns (islands of a few pairs: the island kernel runs) and a random pile (one
+    island above 64 pairs: the colour phases run) give the bits of the engine without it."""
+    from importlib import import_module
+    scenes = import_module("motion_engine_b200.scenes")
+    if scene == "stress_lattice":
+        sc = scenes.box_lattice(n=600, edge=0.25, extent=(10.0, 10.0, 2.0))
+        steps = 90
+    else:
+        sc = scenes.jittered_boxes(300, height=3.0, rng=np.random.default_rng(5))
+        steps = 240
+    isl, ref = _box_pair(me, sc, True)
+    for t in range(steps):
+        isl.step(1 / 240, 2)
+        ref.step(1 / 240, 2)
+        a, b = isl.get_state_packed().numpy(), ref.get_state_packed().numpy()
+        assert a.tobytes() == b.tobytes(), f"{scene} step {t}"
+    assert isl.contact_forces().tobytes() == ref.contact_forces().tobytes()
+    assert isl.island_solve_active == active
+    assert isl.island_count > (50 if active else 0)
