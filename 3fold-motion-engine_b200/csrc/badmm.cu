@@ -165,6 +165,7 @@ __device__ inline double eigmax3(const double A[9])
 // contacts' sums interleaved (independent chains), rounds each at the scale and adds them in its
 // own int64 register -- exact, so no atomics and no order dependence.  The scale is a power of
 // two, so acc / scale is the exact product acc * 2^-e.
+template <int kC>
 __device__ void matvec(Env &E, const double *xin, double *xout, bool use_rho)
 {
     const int ln = lane_id(), C = E.C, NV = E.NV, M = E.M;
@@ -179,27 +180,26 @@ __device__ void matvec(Env &E, const double *xin, double *xout, bool use_rho)
         inv = ldexp(1.0, -e);
     }
     if (ln < NV) {
-        for (int c = 0; c < C; ++c) {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
             const double *jr = E.J + (size_t)(3 * c) * NV + ln;
             E.yt[c * NV + ln] = jr[0] * xin[3 * c] + jr[NV] * xin[3 * c + 1] + jr[2 * NV] * xin[3 * c + 2];
         }
     }
     __syncwarp();
     if (ln < NV) {
-        double sc[B2C_ADMM_MAX_CONTACTS];
+        double sc[kC];
 #pragma unroll
-        for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c) sc[c] = 0.0;
+        for (int c = 0; c < kC; ++c) sc[c] = 0.0;
         const double *mrow = E.Mi + (size_t)ln * NV;
         for (int l = 0; l < NV; ++l) {
             const double ml = mrow[l];
 #pragma unroll
-            for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c)
-                if (c < C) sc[c] = sc[c] + ml * E.yt[c * NV + l];
+            for (int c = 0; c < kC; ++c) sc[c] = sc[c] + ml * E.yt[c * NV + l];
         }
         long long acc = 0;
 #pragma unroll
-        for (int c = 0; c < B2C_ADMM_MAX_CONTACTS; ++c)
-            if (c < C) acc += llround(sc[c] * scal);
+        for (int c = 0; c < kC; ++c) acc += llround(sc[c] * scal);
         E.wv[ln] = (double)acc * inv;
     }
     __syncwarp();
@@ -236,6 +236,7 @@ __device__ __forceinline__ void papply(const Env &E, const double *P, const doub
 }
 
 // the Schur operator of the fixed-branch system (NB:1040-1043): yout = Z^T G Z y + D y
+template <int kC>
 __device__ void sopv(Env &E, const double *y, double *yout)
 {
     const int ln = lane_id();
@@ -245,7 +246,7 @@ __device__ void sopv(Env &E, const double *y, double *yout)
         E.tmp[i] = z[0] * y[3 * c] + z[1] * y[3 * c + 1] + z[2] * y[3 * c + 2];
     }
     __syncwarp();
-    matvec(E, E.tmp, E.tmp2, false);
+    matvec<kC>(E, E.tmp, E.tmp2, false);
     for (int i = ln; i < E.M; i += 32) {
         const int c = i / 3, col = i - 3 * c;
         const double *z = E.Zm + 9 * c;
@@ -258,13 +259,14 @@ __device__ void sopv(Env &E, const double *y, double *yout)
 enum Op { kOpAdmm = 0, kOpSchur = 1 };
 
 // _pcg (NB:1048-1073); the x update skips a frozen problem when use_mask
+template <int kC>
 __device__ void pcg(Env &E, const double *rhs, double *x, int n_it, Op op, const double *P, bool warm_zero,
                     bool use_mask)
 {
     const int ln = lane_id(), M = E.M;
     auto apply = [&](const double *v, double *o) {
-        if (op == kOpAdmm) matvec(E, v, o, true);
-        else sopv(E, v, o);
+        if (op == kOpAdmm) matvec<kC>(E, v, o, true);
+        else sopv<kC>(E, v, o);
     };
     if (warm_zero) {
         for (int i = ln; i < M; i += 32) {
@@ -301,6 +303,7 @@ __device__ void pcg(Env &E, const double *rhs, double *x, int n_it, Op op, const
 }
 
 // one ADMM iteration (NB:1075-1082)
+template <int kC>
 __device__ void admm_iter(Env &E, int cg_iters)
 {
     const int ln = lane_id(), M = E.M;
@@ -310,7 +313,7 @@ __device__ void admm_iter(Env &E, int cg_iters)
         E.rhs[i] = -((g + E.gam[i]) - E.rho * E.zv[i]);
     }
     __syncwarp();
-    pcg(E, E.rhs, E.x, cg_iters, kOpAdmm, E.Pj, false, true);
+    pcg<kC>(E, E.rhs, E.x, cg_iters, kOpAdmm, E.Pj, false, true);
     if (E.mask != 0) {
         for (int c = ln; c < E.C; c += 32) {
             double v[3], z[3];
@@ -325,10 +328,11 @@ __device__ void admm_iter(Env &E, int cg_iters)
 }
 
 // the Cadoux refresh, the natural residual and the mask (NB:1084-1092, 498-543)
+template <int kC>
 __device__ double refresh(Env &E, double tol, bool desax)
 {
     const int ln = lane_id();
-    matvec(E, E.zv, E.tmp2, false);
+    matvec<kC>(E, E.zv, E.tmp2, false);
     for (int i = ln; i < E.M; i += 32) E.u[i] = E.tmp2[i] + E.bb[i];
     __syncwarp();
     for (int c = ln; c < E.C; c += 32) {
@@ -580,6 +584,7 @@ __device__ void build_active(Env &E, double tol_lam, double tol_rel)
 }
 
 // one application of the affine sigma map (NB:1162-1170)
+template <int kC>
 __device__ void grad_once(Env &E, int cg)
 {
     const int ln = lane_id(), M = E.M;
@@ -590,14 +595,14 @@ __device__ void grad_once(Env &E, int cg)
         E.rhs[i] = v;
     }
     __syncwarp();
-    pcg(E, E.rhs, E.yv, cg, kOpSchur, E.Ps, true, false);
+    pcg<kC>(E, E.rhs, E.yv, cg, kOpSchur, E.Ps, true, false);
     for (int i = ln; i < M; i += 32) {
         const int c = i / 3, row = i - 3 * c;
         const double *z = E.Zm + 9 * c + 3 * row;
         E.dlam[i] = (z[0] * E.yv[3 * c] + z[1] * E.yv[3 * c + 1] + z[2] * E.yv[3 * c + 2]) + E.pinh[i];
     }
     __syncwarp();
-    matvec(E, E.dlam, E.tmp2, false);
+    matvec<kC>(E, E.dlam, E.tmp2, false);
     for (int c = ln; c < E.C; c += 32)
         E.sigo[c] = E.slipf[c] > 0.5 ? E.what[3 * c + 1] * (E.tmp2[3 * c + 1] + E.dbv[3 * c + 1]) +
                                             E.what[3 * c + 2] * (E.tmp2[3 * c + 2] + E.dbv[3 * c + 2])
@@ -606,11 +611,12 @@ __device__ void grad_once(Env &E, int cg)
 }
 
 // grad_affine (NB:1172-1186): dlam for the current (pinh, dbv)
+template <int kC>
 __device__ void grad_affine(Env &E, int n_calls, int cg)
 {
     const int ln = lane_id(), C = E.C, M = E.M;
     const int K = n_calls - 2;
-    matvec(E, E.pinh, E.tmp, false);
+    matvec<kC>(E, E.pinh, E.tmp, false);
     for (int i = ln; i < M; i += 32) E.tmp2[i] = E.tmp[i] + E.dbv[i];
     __syncwarp();
     for (int i = ln; i < M; i += 32) {
@@ -620,7 +626,7 @@ __device__ void grad_affine(Env &E, int n_calls, int cg)
     }
     for (int c = ln; c < C; c += 32) E.sig[c] = 0.0;
     __syncwarp();
-    grad_once(E, cg);
+    grad_once<kC>(E, cg);
     for (int c = ln; c < C; c += 32) E.siga[c] = E.sigo[c];
     __syncwarp();
     for (int j = 0; j < K; ++j) {
@@ -628,7 +634,7 @@ __device__ void grad_affine(Env &E, int n_calls, int cg)
         __syncwarp();
         if (ln == 0 && j >= 0 && j < E.nslip) E.sig[E.sidx[j]] = 1.0;
         __syncwarp();
-        grad_once(E, cg);
+        grad_once<kC>(E, cg);
         if (j < E.nslip)
             for (int i = ln; i < E.nslip; i += 32) {
                 const int c = E.sidx[i];
@@ -683,9 +689,10 @@ __device__ void grad_affine(Env &E, int n_calls, int cg)
         }
     }
     __syncwarp();
-    grad_once(E, cg);
+    grad_once<kC>(E, cg);
 }
 
+template <int kC>
 __global__ void __launch_bounds__(32, 16) k_admm(b2c_admm P, b2c_admm_params prm)
 {
     extern __shared__ double s_env[];
@@ -697,9 +704,9 @@ __global__ void __launch_bounds__(32, 16) k_admm(b2c_admm P, b2c_admm_params prm
     double resm = CUDART_NAN;
     if (prm.flags & B2C_ADMM_FORWARD) {
         for (int i = 0; i < prm.n_iter; ++i) {
-            admm_iter(E, prm.cg_iters);
+            admm_iter<kC>(E, prm.cg_iters);
             const int k = prm.chunk > 0 ? i % prm.chunk : i;
-            if (prm.refresh_every > 0 && (k + 1) % prm.refresh_every == 0) resm = refresh(E, prm.tol, prm.desax != 0);
+            if (prm.refresh_every > 0 && (k + 1) % prm.refresh_every == 0) resm = refresh<kC>(E, prm.tol, prm.desax != 0);
         }
     } else {
         // the impulses and velocities are given (the gradient of an outside solve)
@@ -710,7 +717,7 @@ __global__ void __launch_bounds__(32, 16) k_admm(b2c_admm P, b2c_admm_params prm
         __syncwarp();
     }
     // v+ = v_free + M^-1 J^T lam (NB:1057-1062)
-    matvec(E, E.zv, E.tmp, false);
+    matvec<kC>(E, E.zv, E.tmp, false);
     if (prm.flags & B2C_ADMM_FORWARD) {
         for (int i = ln; i < M; i += 32) {
             P.lam[(size_t)e * M + i] = E.zv[i];
@@ -732,10 +739,10 @@ __global__ void __launch_bounds__(32, 16) k_admm(b2c_admm P, b2c_admm_params prm
             E.dbv[i] = (prm.flags & B2C_ADMM_GRAD_GIVEN) ? P.dbv_in[(size_t)e * M + i] : prm.dt * E.MJ[i * NV + j];
         }
         __syncwarp();
-        grad_affine(E, n_calls, prm.grad_cg);
+        grad_affine<kC>(E, n_calls, prm.grad_cg);
         for (int i = ln; i < M; i += 32) P.dlam_tau[(size_t)e * M + i] = E.dlam[i];
         if (!(prm.flags & B2C_ADMM_GRAD_GIVEN)) {
-            matvec(E, E.dlam, E.tmp, false);
+            matvec<kC>(E, E.dlam, E.tmp, false);
             for (int k = ln; k < NV; k += 32) P.dv_tau[(size_t)e * NV + k] = prm.dt * E.Mi[k * NV + j] + E.wv[k];
             // mu at the first slip contact (k_pmu): pinh = -lam_n w_hat there, db = 0
             for (int i = ln; i < M; i += 32) {
@@ -749,7 +756,7 @@ __global__ void __launch_bounds__(32, 16) k_admm(b2c_admm P, b2c_admm_params prm
                 E.pinh[3 * cc + 2] = -E.zv[3 * cc] * E.what[3 * cc + 2];
             }
             __syncwarp();
-            if (prm.do_mu) grad_affine(E, n_calls, prm.grad_cg);
+            if (prm.do_mu) grad_affine<kC>(E, n_calls, prm.grad_cg);
             for (int i = ln; i < M; i += 32) P.dlam_mu[(size_t)e * M + i] = prm.do_mu ? E.dlam[i] : 0.0;
         }
         for (int c = ln; c < C; c += 32)
@@ -796,11 +803,25 @@ extern "C" int32_t b2c_admm_solve(const b2c_admm *a, const b2c_admm_params *p, b
     }
     if (a->n_env == 0) return B2C_OK;
     const size_t smem = badmm::env_bytes(a->nc, a->nv);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(badmm::k_admm, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        attr = true;
+    static bool attr_set[B2C_ADMM_MAX_CONTACTS + 1] = {};
+    switch (a->nc) {
+#define B2C_ADMM_CASE(n)                                                                                  \
+    case n:                                                                                               \
+        if (!attr_set[n]) {                                                                               \
+            cudaFuncSetAttribute(badmm::k_admm<n>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024); \
+            attr_set[n] = true;                                                                           \
+        }                                                                                                 \
+        badmm::k_admm<n><<<a->n_env, 32, smem, stream_of(st)>>>(*a, *p);                                 \
+        break;
+        B2C_ADMM_CASE(1)
+        B2C_ADMM_CASE(2)
+        B2C_ADMM_CASE(3)
+        B2C_ADMM_CASE(4)
+        B2C_ADMM_CASE(5)
+        B2C_ADMM_CASE(6)
+        B2C_ADMM_CASE(7)
+        B2C_ADMM_CASE(8)
+#undef B2C_ADMM_CASE
     }
-    badmm::k_admm<<<a->n_env, 32, smem, stream_of(st)>>>(*a, *p);
     return check_launch("admm");
 }

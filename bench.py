@@ -70,7 +70,7 @@ WORKLOADS = {
                                   vit=40, pit=20, substeps=1, dt=1 / 240, preroll=0, steps=300, warmup=20,
                                   published=(1e4 / 3.684e-3, "reference ColorCache, 3.684 ms/step, NVIDIA L4 "
                                              "(reports/innovation_stack_color_cache_l4.json)")),
-    # the same fixture under the island solve (IslandSolveContactEngine: 5 000 islands of two pairs,
+    # the same fixture under the island solve (IslandSolveContactEngine: 5 041 islands of at most two pairs,
     # one thread per island, no colour barriers; the ColorCache engine's bits); published: 2.817 and
     # 2.887 ms per step on an NVIDIA L4, the faster taken (reports/innovation_island_solve.json,
     # legs[*].island.timing)

@@ -43,6 +43,29 @@ def test_color_cache_lattice10k_against_reference_receipt(me, oracle_mod):
     check_cc10k(se, e.contact_forces(), ke)
 
 
+def test_island_solve_lattice10k_against_reference_receipt(me):
+    """The island engine on the same receipt run: the island kernel takes the solve (5 041
+    columns of one or two boxes: islands of at most two pairs), the result is the ColorCache engine's bit for bit and within the
+    receipt's bounds (the reference's island engine gives its ColorCache bits, its probe's
+    exact_reference gate)."""
+    isl = me.IslandSolveContactEngine(dims=DIMS, mu=0.5, vit=40, pit=20)
+    cc = me.ColorCacheContactEngine(dims=DIMS, mu=0.5, vit=40, pit=20)
+    for c in lattice(10000):
+        isl.add_body(c)
+        cc.add_body(c)
+    for _ in range(40):
+        isl.step(DT, 1)
+        cc.step(DT, 1)
+    assert isl.island_solve_active and isl.island_count == 5041 and isl.max_island_pairs == 2  # 71 x 71 columns
+    si, sc = isl.get_state(), cc.get_state()
+    for name in ("xc", "Rm", "vc", "om"):
+        assert getattr(si, name).tobytes() == getattr(sc, name).tobytes(), name
+    ki, kc = isl.kept_contacts(), cc.kept_contacts()
+    for k in kc:
+        assert ki[k].tobytes() == kc[k].tobytes(), k
+    check_cc10k(si, isl.contact_forces(), ki)
+
+
 def _digest(*arrays):
     h = hashlib.sha256()
     for a in arrays:
