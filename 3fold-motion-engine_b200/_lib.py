@@ -110,7 +110,7 @@ class Admm(ctypes.Structure):
     """b2c_admm"""
     _fields_ = [("n_env", c_int32), ("nc", c_int32), ("nv", c_int32)] + [(k, c_void_p) for k in (
         "J", "Minv", "v_free", "mu", "lam", "u", "v_plus", "res", "mask", "rho", "nslip", "labels", "dlam_tau",
-        "dv_tau", "dlam_mu", "dbv_in")]
+        "dv_tau", "dlam_mu", "dbv_in", "b_in")]
 
 
 class AdmmParams(ctypes.Structure):

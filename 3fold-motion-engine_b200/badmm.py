@@ -57,14 +57,17 @@ class BatchProxADMM:
         self.dt = 1.0
         self.alpha_eta, self.jacobi_sweeps = 0.0, 10
         self._in = None
+        self._b = None
 
     def _t(self, a, shape):
         t = torch.as_tensor(a, dtype=torch.float64)
         return t.reshape(shape).to(self.dev).contiguous()
 
-    def upload(self, J, Minv, v_free, mu, dt, alpha_eta=0.0, jacobi_sweeps=10):
-        """NB:974-1000.  Arrays may be numpy or torch (host or device)."""
+    def upload(self, J, Minv, v_free, mu, dt, alpha_eta=0.0, jacobi_sweeps=10, b=None):
+        """NB:974-1000.  Arrays may be numpy or torch (host or device).  `b` (B, nc, 3), when
+        given, is the free contact velocity itself (a stored problem's q) instead of J v_free."""
         B_, C, NV = self.B, self.C, self.NV
+        self._b = None if b is None else self._t(b, (B_, C, 3))
         mu_t = torch.as_tensor(mu, dtype=torch.float64).reshape(-1)
         mu_t = mu_t.expand(B_ * C) if mu_t.numel() == 1 else mu_t
         self._in = (self._t(J, (B_, 3 * C, NV)), self._t(Minv, (B_, NV, NV)), self._t(v_free, (B_, NV)),
@@ -92,7 +95,8 @@ class BatchProxADMM:
         J, Mi, vf, mu = self._in
         return _lib.Admm(self.B, self.C, self.NV, p(J), p(Mi), p(vf), p(mu), p(self.lam), p(self.u), p(self.v_plus),
                          p(self.res), p(self.mask), p(self.rho), p(self.nslip), p(self.labels), p(self.dlam_tau),
-                         p(self.dv_tau), p(self.dlam_mu), p(dbv) if dbv is not None else None)
+                         p(self.dv_tau), p(self.dlam_mu), p(dbv) if dbv is not None else None,
+                         p(self._b) if self._b is not None else None)
 
     def launch(self, flags, n_iter=0, cg_iters=8, refresh_every=4, tol=1e-8, chunk=0, desax=True, jdir=0,
                n_calls=None, grad_cg=60, do_mu=True, dbv=None, stream=None):

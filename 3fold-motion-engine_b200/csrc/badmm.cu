@@ -372,7 +372,7 @@ __device__ void setup(Env &E, const b2c_admm &P, const b2c_admm_params &prm, int
     for (int i = ln; i < M; i += 32) {
         double s = 0.0;
         for (int k = 0; k < NV; ++k) s = s + E.J[i * NV + k] * E.vf[k];
-        E.bb[i] = s;
+        E.bb[i] = P.b_in ? P.b_in[(size_t)e * M + i] : s;
     }
     // kappa = C max_i sum_l |M^-1_il| max_(c,k) sum_r |J_(3c+r)k| + 1e-300
     double m1 = 0.0, m2 = 0.0;

@@ -685,6 +685,7 @@ typedef struct b2c_admm {
     double *dv_tau;         /* (n_env, nv) dv+ for the same direction */
     double *dlam_mu;        /* (n_env, nc, 3) dlam / dmu at each problem's first slip contact */
     const double *dbv_in;   /* (n_env, nc, 3) the b-direction of B2C_ADMM_GRAD_GIVEN, else NULL */
+    const double *b_in;     /* (n_env, nc, 3) the free contact velocity b itself, or NULL for J v_free */
 } b2c_admm;
 
 typedef struct b2c_admm_params {

@@ -147,7 +147,7 @@ def round_away(x):
 class BatchADMMOracle:
     """NB's BatchProxADMMGPU restated: upload / set_rho / forward / gradient, per problem."""
 
-    def __init__(self, J, Minv, v_free, mu, dt, alpha_eta=0.0, jacobi_sweeps=10):
+    def __init__(self, J, Minv, v_free, mu, dt, alpha_eta=0.0, jacobi_sweeps=10, b=None):
         J = np.ascontiguousarray(J, np.float64)
         self.B, self.M, self.NV = J.shape
         self.C = self.M // 3
@@ -157,7 +157,8 @@ class BatchADMMOracle:
         self.vfree = np.ascontiguousarray(v_free, np.float64).reshape(B, NV)
         self.mu = np.broadcast_to(np.asarray(mu, np.float64).reshape(-1), (B * C,)).reshape(B, C).copy()
         self.dt = float(dt)
-        self.bb = np.einsum("bik,bk->bi", J, self.vfree)
+        self.bb = (np.einsum("bik,bk->bi", J, self.vfree) if b is None
+                   else np.asarray(b, np.float64).reshape(B, M).copy())
         self.kap = (C * np.abs(self.Mi).sum(axis=2).max(axis=1)
                     * np.abs(J.reshape(B, C, 3, NV)).sum(axis=2).max(axis=(1, 2)) + 1e-300)
         self.MJ = np.einsum("bkl,bil->bik", self.Mi, J)
