@@ -5,7 +5,7 @@ src/motion_engine/ncp/ncp_ref.py's solve_ncp_pgs (2000 sweeps, tol 1e-15, as tha
 classified, and differentiated by its fixed-branch implicit sensitivity (ncp_ref.sensitivity,
 :907-959).  numpy only.
 
-Run:  python tests/golden/make_admm_golden.py [/path/to/reference]
+Run:  python tests/golden/make_admm_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -32,7 +32,15 @@ def all_slip_scene(n_c):
     return G, b, mu
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp import ncp_ref as R
     out, names = {}, []
@@ -52,4 +60,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

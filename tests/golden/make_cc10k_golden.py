@@ -11,7 +11,7 @@ jn, jt1, jt2, jp).  The probe ran four workers (two plain, two profiled); its re
 
 Written here: cc10k_golden.npz with the arrays of the first plain worker.
 
-Run:  python tests/golden/make_cc10k_golden.py [/path/to/reference]
+Run:  python tests/golden/make_cc10k_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -21,6 +21,14 @@ import numpy as np
 FIELDS = ("xc", "Rm", "vc", "om", "force", "ckeys", "sbi", "sbj", "spA", "spB", "sn", "spen", "jn", "jt1", "jt2",
           "jp")
 LEGS = ("plain_0", "plain_1", "profiled_0", "profiled_1")
+
+
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
 
 
 def main(ref):
@@ -36,4 +44,4 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_root())

@@ -15,7 +15,7 @@ Written here: golden_l4.npz with, per engine and scene,
 plus `initial__<engine>__<scene>__<name>` sha256 of the built body arrays (xc, q, v, w, invM,
 IbInv, rest).
 
-Run:  python tests/golden/make_golden.py [/path/to/reference]
+Run:  python tests/golden/make_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import hashlib
 import json
@@ -29,7 +29,15 @@ ENGINES = ("jacobi", "pair_chunks", "color_cache")
 SCENES = {"stack8": None, "lattice1000": (3, 9, 39)}
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     src = np.load(os.path.join(ref, "reports/cross_hardware_l4.npz"))
     meta = json.load(open(os.path.join(ref, "reports/cross_hardware_l4.json")))
     out = {}
@@ -60,4 +68,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

@@ -6,7 +6,7 @@ float64 CPU solver (src/motion_engine/ncp/ncp_ref.py: solve_ncp_pgs with de Saxc
 convergence, and natural_residual).  Soft-step parameters from SoftStep.params.  Everything
 imported here is numpy-only (Warp is not needed).
 
-Run:  python tests/golden/make_ncp_golden.py [/path/to/reference]
+Run:  python tests/golden/make_ncp_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -14,7 +14,15 @@ import sys
 import numpy as np
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp import ncp_gpu as G
     from motion_engine.ncp import ncp_ref as R
@@ -63,4 +71,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

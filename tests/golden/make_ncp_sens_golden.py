@@ -6,7 +6,7 @@ fixed-branch implicit-function derivatives (src/motion_engine/ncp/ncp_ref.py: cl
 sensitivity -> dlam/dmu (3 n_c, n_c) and dlam/db (3 n_c, 3 n_c), b = J v_free + bias) and its
 diagnostics (singular, boundary).  numpy only.
 
-Run:  python tests/golden/make_ncp_sens_golden.py [/path/to/reference]
+Run:  python tests/golden/make_ncp_sens_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -17,7 +17,15 @@ SCENES = ("wellposed_8_8_1", "wellposed_16_8_2", "wellposed_6_6_3", "wellposed_1
 LABELS = {"open": 0, "stick": 1, "slip": 2}
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp import ncp_ref as R
     here = os.path.dirname(os.path.abspath(__file__))
@@ -39,4 +47,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

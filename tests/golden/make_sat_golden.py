@@ -9,7 +9,7 @@ Cases: face-face resting stacks with small tilts and offsets, random orientation
 separations (touching, overlapping and apart), edge-on-edge crossings, and boxes near the
 ground plane.
 
-Run:  python tests/golden/make_sat_golden.py [/path/to/reference]
+Run:  python tests/golden/make_sat_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -31,7 +31,15 @@ def _rand_quat(rng, scale=None):
     return q.astype(np.float32)
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp.ncp_gpu import Box, box_box_contacts, box_plane_contacts
     rng = np.random.default_rng(20261203)
@@ -98,4 +106,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

@@ -8,7 +8,7 @@ bounds of G (scenes/table.json: lambda_min_pos, lambda_max).  The scene files th
 (all but the two largest, 11 and 12, 4 MB of the package's 5.3 MB) are copied into
 scenes_v1.json.gz so that the reader's tests run without the reference.
 
-Run:  python tests/golden/make_scenes_v1_golden.py [/path/to/reference]
+Run:  python tests/golden/make_scenes_v1_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import gzip
 import importlib.util
@@ -20,7 +20,15 @@ import types
 import numpy as np
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.modules.setdefault("h5py", types.ModuleType("h5py"))
     spec = importlib.util.spec_from_file_location("ref_loader", os.path.join(ref, "data", "ncp", "loader.py"))
     L = importlib.util.module_from_spec(spec)
@@ -51,4 +59,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

@@ -3,7 +3,7 @@ reference's own CPU code (src/motion_engine/ncp/ncp_ref.py: scene_random, scene_
 solve_ncp_pgs, classify, sensitivity (the fixed-branch implicit-function response, :907-959)
 and sensitivity_fd (central finite differences, :962-987)).  numpy only.
 
-Run:  python tests/golden/make_sens_golden.py [/path/to/reference]
+Run:  python tests/golden/make_sens_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -11,7 +11,15 @@ import sys
 import numpy as np
 
 
-def main(ref="/root/reference"):
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
+def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp import ncp_ref as R
     out = {}
@@ -44,4 +52,4 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(reference_root())

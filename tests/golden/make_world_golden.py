@@ -13,7 +13,7 @@ points at one depth, and "keep the 4 deepest" then depends on the last bits of t
 Written here: world_golden.npz with the scene (half, mass, x0, q0, v0) and per step x, q, v, w and
 the contact count.
 
-Run:  python tests/golden/make_world_golden.py [/path/to/reference]
+Run:  python tests/golden/make_world_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import os
 import sys
@@ -54,6 +54,14 @@ class _ConvergedCpuSolver:
                                   iters=0, n_colors=0, cache_hit=False)
 
 
+def reference_root():
+    """The reference checkout: the first argument, else $B2C_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("B2C_REFERENCE")
+    if not ref:
+        raise SystemExit(f"usage: python {os.path.basename(__file__)} /path/to/reference  (or set B2C_REFERENCE)")
+    return ref
+
+
 def main(ref):
     sys.path.insert(0, os.path.join(ref, "src"))
     from motion_engine.ncp import ncp_gpu as G
@@ -80,4 +88,4 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_root())
