@@ -78,3 +78,16 @@ def test_product_partition_checks_arguments_on_the_host(me):
         me.partition_pairs(a, b, np.array([1.0, -1.0]), order)
     e = np.zeros(0, np.int32)
     assert all(len(x) == 0 for x in me.partition_pairs(e, e, np.ones(2), e))
+
+
+def test_oracle_equals_the_reference_partition():
+    """The reference's own partition_pairs, run on seeded random graphs
+    (tests/golden/make_islands_golden.py): the oracle returns the same arrays."""
+    import os
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "islands_golden.npz"))
+    for k in range(int(g["n_cases"])):
+        args = [g[f"c{k}/{x}"] for x in ("a", "b", "mass", "order")]
+        got = oracle_partition(*args)
+        for arr, name in zip(got, ("packed", "starts", "counts")):
+            assert np.array_equal(arr, g[f"c{k}/{name}"]), (k, name)

@@ -196,3 +196,16 @@ def test_box_engine_island_solve_equals_colour_phases(scene, active, me):
     assert isl.contact_forces().tobytes() == ref.contact_forces().tobytes()
     assert isl.island_solve_active == active
     assert isl.island_count > (50 if active else 0)
+
+
+def test_device_partition_equals_the_reference_partition(me):
+    """The device partition against the reference's own partition_pairs outputs
+    (tests/golden/islands_golden.npz), array for array."""
+    import os
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "islands_golden.npz"))
+    for k in range(int(g["n_cases"])):
+        args = [g[f"c{k}/{x}"] for x in ("a", "b", "mass", "order")]
+        got = me.partition_pairs(*args)
+        for arr, name in zip(got, ("packed", "starts", "counts")):
+            assert np.array_equal(arr, g[f"c{k}/{name}"]), (k, name)
