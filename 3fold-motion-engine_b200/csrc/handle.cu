@@ -456,6 +456,11 @@ extern "C" int32_t b2c_create(const b2c_config *c, void **h)
                        c->kind, B2C_ENGINE_BOX);
         return B2C_EARG;
     }
+    if (c->flags & B2C_COLOR_ISLANDS) {
+        b2c::set_error("b2c_create: B2C_COLOR_ISLANDS is not available on the handle interface (the stage calls "
+                       "take it with b2c_pairs.isl_work)");
+        return B2C_EARG;
+    }
     const bool dims_ok = c->dims[0] > 0.0 && c->dims[1] > 0.0 && c->dims[2] > 0.0 && finite3(c->dims);
     const bool frame_ok = !(c->flags & B2C_COLOR_ROW_FORM) || (c->flags & B2C_COLOR_FIXED_FRAME);
     if (c->vit < 0 || c->pit < 0 || !(c->mu >= 0.0) || !std::isfinite(c->mu) || !dims_ok || !(c->margin >= 0.0) ||

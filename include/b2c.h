@@ -733,7 +733,7 @@ typedef struct b2c_config {
     double mu;                  /* friction of bodies without their own (b2c_set_body_mu) */
     double dims[3];             /* box edges of bodies added without their own */
     double margin;              /* contact margin (the reference's 2e-3) */
-    int32_t flags;              /* B2C_COLOR_* */
+    int32_t flags;              /* B2C_COLOR_* (not B2C_COLOR_PER_CONTACT or B2C_COLOR_ISLANDS) */
     int32_t color_cap;          /* colour cap, <= 512 */
     int32_t solve_blocks;       /* launch form of the persistent solve (b2c_color_params) */
     int32_t cand_per_body;      /* candidate pairs reserved per body */

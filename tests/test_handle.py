@@ -59,6 +59,11 @@ def test_config_defaults_and_bad_configs(me):
         assert not h.value
         if field == "kind":
             assert b"kind" in L.b2c_last_error()
+    b = me._lib.Config()
+    L.b2c_config_init(ctypes.byref(b))
+    b.flags |= me._lib.COLOR_ISLANDS
+    assert L.b2c_create(ctypes.byref(b), ctypes.byref(h)) == 1 and not h.value
+    assert b"ISLANDS" in L.b2c_last_error()
     assert L.b2c_create(ctypes.byref(c), None) == 1
 
 
