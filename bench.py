@@ -26,7 +26,8 @@ host core, rank 0 only.
 Other workloads (--workload): stress100k (100 000-cube lattice), batched512 (512 uneven
 scenes in one engine), colorcache_lattice10k, island_lattice10k and jacobi_lattice10k (the
 reference's 10k bead lattice under its ColorCache, island-solve and relaxed-Jacobi engines, with
-vs_baseline against their published timings), ncp_lattice10k (the exact-cone NCP
+vs_baseline against their published timings), admm4096 (the reference's batched ADMM and its
+adjoint at its own benchmark configuration), ncp_lattice10k (the exact-cone NCP
 solve of the reference's LatticeWorld fixture) and adjoint4096 (the batched NCP forward solve
 and its adjoint at the reference's batched-adjoint shape).
 """
