@@ -6,8 +6,10 @@ A scene describes one contact problem  u = W lambda + q  with  W = J M^-1 J^T + 
 bodies and contacts (`model = "body_contacts"`: per contact a frame (normal, t1, t2), its two
 bodies a, b (-1 = the static world) and lever arms; per body its inverse mass and inertia, or a
 full inverse-mass block) or through the operator itself (`model = "operator"`: J and M^-1,
-base64 little-endian float64 or lists).  The HDF5 copy of each scene (FCLIB layout) is not read:
-h5py is not installed in this image, and the JSON alone defines the problem.
+base64 little-endian float64 or lists).  The HDF5 copy of each scene (the compact FCLIB
+local-problem layout: W's lower triangle in CSC under /fclib_local/W with symmetric_packed = 1,
+q and mu under /fclib_local/vectors) is read by ``read_hdf5_problem`` through ``hdf5_lite`` (h5py
+is not installed in this image); ``verify`` compares the two as the package's loader does.
 
 Device solves:
 * body-contact scenes without compliance (eta = 0) become a ``ncp.BlockScene`` (3-DOF point
@@ -176,3 +178,38 @@ def admm_problem(scenes):
     nv = J.shape[2]
     return J, Minv, np.zeros((len(scenes), nv)), np.stack([s.mu for s in scenes]), np.stack(
         [s.b.reshape(-1, 3) for s in scenes])
+
+
+def read_hdf5_problem(path):
+    """(W, q, mu) of a scene's HDF5 copy (the package loader's read_hdf5_problem)."""
+    from .hdf5_lite import H5File
+    f = H5File(path)
+    n = int(f["fclib_local/W/n"].ravel()[0])
+    m = int(f["fclib_local/W/m"].ravel()[0])
+    nz = int(f["fclib_local/W/nz"].ravel()[0])
+    if nz != -1:
+        raise ValueError(f"{path}: compressed-column storage expected (nz = -1), got nz = {nz}")
+    x = f["fclib_local/W/x"].astype(np.float64)
+    rows = f["fclib_local/W/i"].astype(np.int64)
+    colp = f["fclib_local/W/p"].astype(np.int64)
+    L = np.zeros((n, m))
+    cols = np.repeat(np.arange(len(colp) - 1), np.diff(colp))
+    L[rows[:len(cols)], cols] = x[:len(cols)]
+    if int(f.attrs("fclib_local/W").get("symmetric_packed") or 0):
+        W = L + L.T - np.diag(np.diag(L))
+    else:
+        W = L
+    return W, f["fclib_local/vectors/q"].astype(np.float64), f["fclib_local/vectors/mu"].astype(np.float64)
+
+
+def verify(sc: ContactSceneV1, hdf5_path) -> dict:
+    """The JSON reconstruction against the HDF5 copy: W's relative Frobenius and max-element
+    differences, and the largest differences of q and mu (the package's acceptance: W to 1e-15
+    relative, q to 1e-15, mu exactly)."""
+    W, q, mu = read_hdf5_problem(hdf5_path)
+    Wj = sc.delassus()
+    scale = float(np.abs(W).max()) or 1.0
+    nrm = float(np.linalg.norm(W)) or 1.0
+    return dict(W_rel_fro=float(np.linalg.norm(Wj - W) / nrm), W_rel_max=float(np.abs(Wj - W).max() / scale),
+                q_abs=float(np.abs(sc.b - q).max()) if q.shape == sc.b.shape else float("nan"),
+                mu_abs=float(np.abs(sc.mu - mu).max()) if mu.shape == sc.mu.shape else float("nan"))

@@ -6,16 +6,20 @@ never touches it.  For every scene: b, mu, eta, the Frobenius norm and trace of 
 a seeded vector r; the full G for scenes of at most 256 rows; the package's published spectral
 bounds of G (scenes/table.json: lambda_min_pos, lambda_max).  The scene files themselves
 (all but the two largest, 11 and 12, 4 MB of the package's 5.3 MB) are copied into
-scenes_v1.json.gz so that the reader's tests run without the reference.
+scenes_v1.json.gz so that the reader's tests run without the reference, and the HDF5 copies of
+the fifteen small ones (about 20 kB each; every one holds contiguous and deflate-chunked
+datasets) into scenes_v1_hdf5.zip.
 
 Run:  python tests/golden/make_scenes_v1_golden.py /path/to/reference   (or with B2C_REFERENCE set)
 """
 import gzip
+import io
 import importlib.util
 import json
 import os
 import sys
 import types
+import zipfile
 
 import numpy as np
 
@@ -54,8 +58,13 @@ def main(ref):
     out["table/lambda_max"] = np.array([float(r["lambda_max"]) for r in table])
     here = os.path.dirname(os.path.abspath(__file__))
     np.savez_compressed(os.path.join(here, "scenes_v1_golden.npz"), **out)
-    with gzip.open(os.path.join(here, "scenes_v1.json.gz"), "wt") as f:
+    with gzip.GzipFile(os.path.join(here, "scenes_v1.json.gz"), "wb", mtime=0) as gz, \
+            io.TextIOWrapper(gz, encoding="utf-8") as f:
         json.dump(files, f)
+    small = [i for i in range(L.N_SCENES) if i not in range(7, 13)]
+    with zipfile.ZipFile(os.path.join(here, "scenes_v1_hdf5.zip"), "w", zipfile.ZIP_STORED) as z:
+        for i in small:
+            z.write(os.path.join(ref, "data", "ncp", "scenes", f"{i:02d}.hdf5"), f"{i:02d}.hdf5")
 
 
 if __name__ == "__main__":

@@ -78,3 +78,33 @@ def test_reader_rejects_other_schemas(sv1, package):
     raw = dict(package[0], schema="contact-scene-v0")
     with pytest.raises(ValueError):
         sv1.read_scene(raw)
+
+
+def test_hdf5_copies_equal_the_json_reconstruction(sv1, package, tmp_path):
+    """The package's own acceptance (data/ncp/loader.py verify): each scene's HDF5 copy, read by
+    hdf5_lite, equals its JSON reconstruction -- W to 1e-15 relative (Frobenius), q to 1e-15, mu
+    exactly -- on the fifteen small scenes carried in tests/golden/scenes_v1_hdf5.zip."""
+    import zipfile
+    with zipfile.ZipFile(os.path.join(ROOT, "tests", "golden", "scenes_v1_hdf5.zip")) as z:
+        z.extractall(tmp_path)
+        names = sorted(z.namelist())
+    assert len(names) == 15
+    for name in names:
+        i = int(name[:2])
+        r = sv1.verify(sv1.read_scene(package[i]), os.path.join(tmp_path, name))
+        assert r["W_rel_fro"] <= 1e-15 and r["q_abs"] <= 1e-15 and r["mu_abs"] == 0.0, (i, r)
+
+
+def test_hdf5_reader_structure(me, tmp_path):
+    import zipfile
+    hl = importlib.import_module("motion_engine_b200.hdf5_lite")
+    with zipfile.ZipFile(os.path.join(ROOT, "tests", "golden", "scenes_v1_hdf5.zip")) as z:
+        z.extract("00.hdf5", tmp_path)
+    f = hl.H5File(os.path.join(tmp_path, "00.hdf5"))
+    assert f.keys("/") == ["fclib_local"]
+    assert f.keys("fclib_local/W") == ["i", "m", "n", "nz", "nzmax", "p", "x"]
+    assert f.attrs("fclib_local/W")["symmetric_packed"] == 1
+    n, nzmax = int(f["fclib_local/W/n"][0]), int(f["fclib_local/W/nzmax"][0])
+    assert n == 12 and nzmax == n * (n + 1) // 2 == len(f["fclib_local/W/x"])
+    with pytest.raises(ValueError):
+        hl.H5File(os.path.join(ROOT, "tests", "golden", "scenes_v1.json.gz"))
